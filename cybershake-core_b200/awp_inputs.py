@@ -1,0 +1,362 @@
+"""Seeded synthetic inputs in the reference formats, and their file writers.
+
+No public dataset is involved: the benchmark configurations use media, source
+time functions and SGT point sets generated here from fixed seeds.
+
+  media      float32 [z][y][x][nvar], z = 0 at the free surface
+             (record layout read by AWP-ODC-SGT/src/structure.f:142-173)
+  source     text: "x y z" then NST lines "axx, ayy, azz, axz, ayz, axy"
+             (AWP-ODC-SGT/src/source.f:170-198, AWP-*-SGT/utils/build_src.py)
+  cordfile   count, then "x y z" lines sorted by (y, x, z)
+             (AWP-ODC-SGT/src/io.f:424-434, SgtHead/gen_awp_cordfile.py:35-39)
+  IN3D       "value NAME" lines in the order of AWP-ODC-SGT/src/io.f:327-417
+
+Random numbers come from splitmix64 so that any other language can reproduce
+the point sets bit for bit.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """splitmix64 (Steele, Lea, Flood 2014), the published 64-bit mixer."""
+
+    def __init__(self, seed: int):
+        self.state = seed & MASK64
+
+    def next_u64(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+    def below(self, n: int) -> int:
+        """Uniform integer in [0, n) by rejection (no modulo bias)."""
+        limit = (1 << 64) - ((1 << 64) % n)
+        while True:
+            v = self.next_u64()
+            if v < limit:
+                return v % n
+
+
+def sgt_points(nx: int, ny: int, zmax: int, npts: int, seed: int = 0) -> np.ndarray:
+    """npts distinct cordfile points, x in [1,nx], y in [1,ny], z in [1,zmax]
+    (z = 1 at the surface), sorted by (y, x, z) like gen_awp_cordfile.py."""
+    if npts > nx * ny * zmax:
+        raise ValueError("more points than cells")
+    rng = SplitMix64(seed)
+    seen = set()
+    pts: List[Tuple[int, int, int]] = []
+    while len(pts) < npts:
+        x = 1 + rng.below(nx)
+        y = 1 + rng.below(ny)
+        z = 1 + rng.below(zmax)
+        if (x, y, z) in seen:
+            continue
+        seen.add((x, y, z))
+        pts.append((x, y, z))
+    pts.sort(key=lambda p: (p[1], p[0], p[2]))
+    return np.asarray(pts, dtype=np.int32)
+
+
+def gaussian_derivative_stf(nst: int, dt: float, f0: float = 0.5, amp: float = 1.0e15,
+                            column: int = 0) -> np.ndarray:
+    """[nst][6] source table; column `column` holds
+    amp * (t - t0) * exp(-(pi f0 (t - t0))^2), t = n*dt, t0 = 1.5/f0 (FP64)."""
+    t = np.arange(nst, dtype=np.float64) * dt
+    t0 = 1.5 / f0
+    s = amp * (t - t0) * np.exp(-(math.pi * f0 * (t - t0)) ** 2)
+    out = np.zeros((nst, 6), dtype=np.float32)
+    out[:, column] = s.astype(np.float32)
+    return out
+
+
+def homogeneous_media(nx: int, ny: int, nz: int, vp: float = 6000.0, vs: float = 3464.0,
+                      rho: float = 2700.0) -> np.ndarray:
+    m = np.empty((nz, ny, nx, 3), dtype=np.float32)
+    m[..., 0] = vp
+    m[..., 1] = vs
+    m[..., 2] = rho
+    return m
+
+
+def correlated_field(shape: Tuple[int, int, int], corr_cells: float, seed: int) -> np.ndarray:
+    """Zero-mean, unit-std Gaussian random field with Gaussian autocorrelation
+    exp(-r^2/a^2), a = corr_cells (white noise filtered by a Gaussian of
+    sigma a/2).  Built on a grid coarsened so the filter spans about 4 coarse
+    cells, then trilinearly interpolated; shape is (nz, ny, nx)."""
+    sigma = corr_cells / 2.0
+    cf = max(1, int(sigma // 2))
+    cshape = tuple(int(math.ceil(n / cf)) + 2 for n in shape)
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(cshape).astype(np.float32)
+    s = sigma / cf
+    spec = np.fft.rfftn(w)
+    kz = np.fft.fftfreq(cshape[0])[:, None, None]
+    ky = np.fft.fftfreq(cshape[1])[None, :, None]
+    kx = np.fft.rfftfreq(cshape[2])[None, None, :]
+    g = np.exp(-2.0 * (math.pi * s) ** 2 * (kx * kx + ky * ky + kz * kz))
+    f = np.fft.irfftn(spec * g, s=cshape, axes=(0, 1, 2)).astype(np.float32)
+    f -= f.mean()
+    f /= max(float(f.std()), 1e-30)
+    if cf == 1:
+        return np.ascontiguousarray(f[1:1 + shape[0], 1:1 + shape[1], 1:1 + shape[2]])
+    out = f
+    for ax, n in enumerate(shape):
+        pos = np.arange(n, dtype=np.float64) / cf + 0.5
+        i0 = np.floor(pos).astype(np.int64)
+        wgt = (pos - i0).astype(np.float32)
+        a = np.take(out, i0, axis=ax)
+        b = np.take(out, i0 + 1, axis=ax)
+        bshape = [1, 1, 1]
+        bshape[ax] = n
+        wgt = wgt.reshape(bshape)
+        out = a * (1 - wgt) + b * wgt
+    out -= out.mean()
+    out /= max(float(out.std()), 1e-30)
+    return np.ascontiguousarray(out.astype(np.float32))
+
+
+def layered_media(nx: int, ny: int, nz: int, dh: float, seed: int, nlayers: int = 8,
+                  vs_top: float = 500.0, vs_bot: float = 4000.0, pert_std: float = 0.05,
+                  corr_len: float = 2000.0,
+                  basin: Optional[dict] = None) -> np.ndarray:
+    """1-D layered model (nlayers of equal thickness, Vs geometric from vs_top to
+    vs_bot), Vp = 1.73 Vs, rho = 310 Vp^0.25 (Gardner, SI units), times
+    (1 + pert_std * correlated field) on Vp and Vs.  Optional basin: ellipsoid
+    {cx, cy, rx, ry, depth} (metres) where Vs ramps from 400 m/s at the surface
+    to 1000 m/s at its floor."""
+    depth = (np.arange(nz, dtype=np.float64) + 0.5) * dh
+    thick = nz * dh / nlayers
+    layer = np.minimum((depth // thick).astype(np.int64), nlayers - 1)
+    vs_l = vs_top * (vs_bot / vs_top) ** (np.arange(nlayers) / max(nlayers - 1, 1))
+    vs1 = vs_l[layer].astype(np.float32)
+    vs = np.broadcast_to(vs1[:, None, None], (nz, ny, nx)).astype(np.float32)
+    if basin is not None:
+        x = (np.arange(nx) + 0.5) * dh
+        y = (np.arange(ny) + 0.5) * dh
+        r2 = ((x[None, :] - basin["cx"]) / basin["rx"]) ** 2 + ((y[:, None] - basin["cy"]) / basin["ry"]) ** 2
+        floor = basin["depth"] * np.sqrt(np.clip(1.0 - r2, 0.0, None))        # (ny, nx)
+        for k in range(nz):
+            inside = depth[k] < floor
+            if not inside.any():
+                continue
+            frac = np.where(inside, depth[k] / np.maximum(floor, 1e-9), 1.0)
+            vsb = (400.0 + 600.0 * frac).astype(np.float32)
+            vs[k] = np.where(inside, np.minimum(vs[k], vsb), vs[k])
+    if pert_std > 0:
+        pert = correlated_field((nz, ny, nx), corr_len / dh, seed)
+        scale = (1.0 + pert_std * pert).astype(np.float32)
+    else:
+        scale = np.ones((nz, ny, nx), dtype=np.float32)
+    vs = vs * scale
+    vp = (1.73 * vs).astype(np.float32)
+    rho = (310.0 * np.power(vp.astype(np.float64), 0.25)).astype(np.float32)
+    m = np.empty((nz, ny, nx, 3), dtype=np.float32)
+    m[..., 0] = vp
+    m[..., 1] = vs
+    m[..., 2] = rho
+    return m
+
+
+def stable_dt(media: np.ndarray, dh: float, courant: float = 0.45) -> float:
+    """Time step from the CFL number vp_max*dt/dh (the CHKP stability number)."""
+    return float(courant * dh / float(media[..., 0].max()))
+
+
+# ---------------------------------------------------------------------------
+# writers
+# ---------------------------------------------------------------------------
+
+def write_media(path: str, media: np.ndarray):
+    np.ascontiguousarray(media, dtype=np.float32).tofile(path)
+
+
+def write_source_text(path: str, xyz: Sequence[int], stf: np.ndarray):
+    with open(path, "w") as f:
+        f.write("%d %d %d\n" % tuple(int(v) for v in xyz))
+        for row in np.asarray(stf, dtype=np.float32):
+            f.write(", ".join("%.9e" % float(v) for v in row) + "\n")
+
+
+def write_source_binary(path: str, xyz: Sequence[int], stf: np.ndarray):
+    with open(path, "wb") as f:
+        np.asarray(xyz, dtype=np.int32).tofile(f)
+        np.asarray(stf, dtype=np.float32).tofile(f)
+
+
+def write_cordfile(path: str, pts: np.ndarray, comment: Optional[str] = None):
+    with open(path, "w") as f:
+        if comment:
+            f.write("# %s\n" % comment)
+        f.write("%d\n" % len(pts))
+        for x, y, z in pts:
+            f.write("%d %d %d\n" % (x, y, z))
+
+
+@dataclass
+class In3d:
+    """IN3D values (io.f:327-417 order); defaults follow AWP-ODC-SGT/utils/data/IN3D.ref."""
+    igreen: int = 1
+    tmax: float = 10.0
+    dh: float = 200.0
+    dt: float = 0.01
+    npc: int = 0
+    nd: int = 20
+    arbc: float = 0.92
+    pht: float = 0.1
+    nsrc: int = 1
+    nst: int = 1000
+    nx: int = 160
+    ny: int = 160
+    nz: int = 80
+    npx: int = 1
+    npy: int = 1
+    npz: int = 1
+    ifault: int = 0
+    checkpoint: int = 0
+    isfcvlm: int = 0
+    imd5: int = 0
+    ivelocity: int = 1
+    mediarestart: int = 1
+    nvar: int = 3
+    iost: int = 1
+    partdeg: int = 1
+    io_opt: int = 1
+    perf_meas: int = 1
+    idyna: int = 0
+    socalq: int = 1
+    nve: int = 1
+    mu_s: float = 0.677
+    mu_d: float = 0.525
+    fl: float = 0.01
+    fh: float = 25.0
+    fp: float = 0.5
+    read_step: int = 1000
+    write_step: int = 100
+    write_step2: int = 100
+    rec: Tuple[int, ...] = (1, 160, 10, 1, 160, 10, 1, 80, 10)
+    ntiskp: int = 100000
+    rec2: Tuple[int, ...] = (1, 160, 10, 1, 160, 10, 1, 80, 10)
+    ntiskp2: int = 1000000
+    ntiskp_sgt: int = 10
+    chkp: str = "output_ckp/CHKP"
+    chkj: str = "output_ckp/CHKJ"
+    insrc: str = "input/src"
+    invel: str = "input/media"
+    insgt: str = "input/cordfile"
+    sxgro: str = "output_sfc/SX"
+    sygro: str = "output_sfc/SY"
+    szgro: str = "output_sfc/SZ"
+    sxgro2: str = "output_vlm/SX"
+    sygro2: str = "output_vlm/SY"
+    szgro2: str = "output_vlm/SZ"
+    sgtgro: str = "output_sgt/awp-strain"
+    sgsn: str = "output_dyn/SGSN"
+
+    def write(self, path: str):
+        names = ["NBGX", "NEDX", "NSKPX", "NBGY", "NEDY", "NSKPY", "NBGZ", "NEDZ", "NSKPZ"]
+        L = []
+        L += ["%9d igreen" % self.igreen, "%9s TMAX" % self.tmax, "",
+              "%9s DH" % self.dh, "%9s DT" % self.dt, "", "%9d NPC" % self.npc, "",
+              "%9d ND" % self.nd, "%9s ARBC" % self.arbc, "%9s PHT" % self.pht, "",
+              "%9d NSRC" % self.nsrc, "%9d NST" % self.nst, "",
+              "%9d NX" % self.nx, "%9d NY" % self.ny, "%9d NZ" % self.nz, "",
+              "%9d NPX" % self.npx, "%9d NPY" % self.npy, "%9d NPZ" % self.npz, ""]
+        L += ["%9d IFAULT" % self.ifault, "%9d CHECKPOINT" % self.checkpoint, "%9d ISFCVLM" % self.isfcvlm,
+              "%9d IMD5" % self.imd5, "%9d IVELOCITY" % self.ivelocity, "%9d MEDIARESTART" % self.mediarestart,
+              "%9d NVAR" % self.nvar, "%9d IOST" % self.iost, "%9d PARTDEG" % self.partdeg,
+              "%9d IO_OPT" % self.io_opt, "%9d PERF_MEAS" % self.perf_meas, "%9d IDYNA" % self.idyna,
+              "%9d SOCALQ" % self.socalq, "", "%9d NVE" % self.nve, "",
+              "%9s MU_S" % self.mu_s, "%9s MU_D" % self.mu_d, "",
+              "%9s FL" % self.fl, "%9s FH" % self.fh, "%9s FP" % self.fp, "",
+              "%9d READ_STEP" % self.read_step, "%9d WRITE_STEP" % self.write_step,
+              "%9d WRITE_STEP2" % self.write_step2, ""]
+        L += ["%9d %s" % (v, n) for v, n in zip(self.rec, names)]
+        L += ["", "%9d NTISKP" % self.ntiskp, ""]
+        L += ["%9d %s2" % (v, n) for v, n in zip(self.rec2, names)]
+        L += ["", "%9d NTISKP2" % self.ntiskp2, "%9d NTISKP_SGT" % self.ntiskp_sgt, ""]
+        L += ["'%s' CHKP" % self.chkp, "'%s' CHKJ" % self.chkj, "",
+              "'%s' INSRC" % self.insrc, "'%s' INVEL" % self.invel, "", "'%s' INSGT" % self.insgt, "",
+              "'%s' SXRGO" % self.sxgro, "'%s' SYRGO" % self.sygro, "'%s' SZRGO" % self.szgro, "",
+              "'%s' SXRGO2" % self.sxgro2, "'%s' SYRGO2" % self.sygro2, "'%s' SZRGO2" % self.szgro2, "",
+              "'%s' SGTGRO" % self.sgtgro, "", "'%s' SGSN" % self.sgsn]
+        with open(path, "w") as f:
+            f.write("\n".join(L) + "\n")
+
+    @property
+    def nt(self) -> int:
+        x = np.float32(self.tmax) / np.float32(self.dt)
+        return int(math.floor(float(x) + 0.5)) + 1
+
+
+# ---------------------------------------------------------------------------
+# benchmark configurations (sizes of the north-star configs)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Workload:
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    dh: float
+    dt: float
+    nst: int
+    igreen: Tuple[int, ...]
+    npts: int
+    media_kind: str = "layered"
+    src_xyz: Tuple[int, int, int] = (0, 0, 0)
+    ntiskp_sgt: int = 10
+    fl: float = 0.01
+    fh: float = 25.0
+    fp: float = 0.5
+    socalq: int = 1
+    seed: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def nt(self) -> int:
+        return self.nst + 1
+
+    def media(self) -> np.ndarray:
+        if self.media_kind == "homogeneous":
+            return homogeneous_media(self.nx, self.ny, self.nz)
+        basin = self.extra.get("basin")
+        return layered_media(self.nx, self.ny, self.nz, self.dh, self.seed, basin=basin)
+
+    def points(self) -> np.ndarray:
+        zmax = min(self.nz, max(1, int(round(10000.0 / self.dh)) + 1))
+        return sgt_points(self.nx, self.ny, zmax, self.npts, seed=0)
+
+    def stf(self, comp: int) -> np.ndarray:
+        col = {1: 0, 2: 1, 3: 2}.get(self.igreen[comp], 0)
+        return gaussian_derivative_stf(self.nst, self.dt, column=col)
+
+
+def config(n: int) -> Workload:
+    """North-star workload n (1..4) with its grid, steps and point count."""
+    if n == 1:
+        return Workload("cfg1_homog_160x160x80_fx", 160, 160, 80, 200.0, 0.01, 1000, (1,), 1000,
+                        media_kind="homogeneous", src_xyz=(80, 80, 11))
+    if n == 2:
+        return Workload("cfg2_layered_400x400x200_fxfyfz", 400, 400, 200, 100.0, 0.005, 4000, (1, 2, 3), 5000,
+                        src_xyz=(200, 200, 21))
+    if n == 3:
+        return Workload("cfg3_layered_640x640x256_fxfy", 640, 640, 256, 100.0, 0.005, 3000, (1, 2), 5000,
+                        src_xyz=(320, 320, 21))
+    if n == 4:
+        return Workload("cfg4_basin_1400x1000x400_fxfy", 1400, 1000, 400, 100.0, 0.005, 5000, (1, 2), 20000,
+                        src_xyz=(700, 500, 21),
+                        extra={"basin": {"cx": 70000.0, "cy": 50000.0, "rx": 30000.0, "ry": 20000.0,
+                                         "depth": 4000.0}})
+    raise ValueError(n)

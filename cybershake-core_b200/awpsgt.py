@@ -1,0 +1,304 @@
+"""ctypes binding of libawpsgt, the B200 AWP-ODC-SGT stepper (include/awp_sgt.h).
+
+Host-side mirror of the reference's interface for the strain-Green-tensor run:
+the same parameters as IN3D (AWP-ODC-SGT/src/io.f:327-417), the same input
+layouts (media [z][y][x][nvar] with z = 0 at the surface, source [nst][6],
+cordfile points) and the same raw SGT file image (pmcl3d.f:1589-1601).
+
+The library is the compiled CUDA path; there is no CPU fallback.  Importing this
+module on a machine without the built library raises ImportError, and creating
+a solver without a usable GPU returns AWP_ERR_CUDA as an exception.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libawpsgt.so")
+PMCL3D_PATH = os.path.join(_HERE, "lib", "pmcl3d")
+
+AWP_OK = 0
+STATUS = {0: "AWP_OK", 1: "AWP_ERR_IO", 2: "AWP_ERR_PARAM", 3: "AWP_ERR_OOM", 4: "AWP_ERR_CUDA",
+          5: "AWP_ERR_UNSTABLE", 6: "AWP_ERR_TIMEOUT", 7: "AWP_ERR_STATE", 8: "AWP_ERR_BUSY",
+          9: "AWP_ERR_CANCELLED"}
+PREC = {"f32": 0, "bf16": 1, "f16": 2}
+KERNEL = {"auto": 0, "two_sweep": 1}
+FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3", "r4", "r5", "r6",
+          "lam", "mu", "d1", "qp", "qs"]
+
+# Every symbol include/awp_sgt.h declares.
+EXPORTED = [
+    "awp_params_default", "awp_create", "awp_load_media", "awp_load_media_file", "awp_set_source",
+    "awp_set_points", "awp_run", "awp_sgt_file_floats", "awp_get_sgt", "awp_get_chkj", "awp_get_field",
+    "awp_get_stats", "awp_reset", "awp_destroy", "awp_footprint_bytes", "awp_bytes_per_cell_update",
+    "awp_status_string", "awp_last_error", "awp_read_in3d", "awp_parse_command_line",
+    "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free",
+]
+
+
+class AwpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dh", C.c_float), ("dt", C.c_float),
+        ("nt", C.c_int), ("nd", C.c_int), ("arbc", C.c_float),
+        ("fl", C.c_float), ("fh", C.c_float), ("fp", C.c_float),
+        ("socalq", C.c_int), ("nve", C.c_int), ("mediastart", C.c_int), ("nvar", C.c_int),
+        ("idyna", C.c_int), ("nst", C.c_int), ("ntiskp_sgt", C.c_int), ("write_step", C.c_int),
+        ("ncomp", C.c_int), ("igreen", C.c_int * 3), ("precision", C.c_int), ("kernel", C.c_int),
+        ("device", C.c_int), ("monitor_every", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("steps_done", C.c_int64), ("seconds_loop", C.c_double), ("gcell_updates_per_s", C.c_double),
+        ("bytes_per_cell_update", C.c_double), ("device_bytes", C.c_double),
+        ("vp_min", C.c_float), ("vp_max", C.c_float), ("vs_min", C.c_float), ("vs_max", C.c_float),
+        ("rho_min", C.c_float), ("rho_max", C.c_float), ("energy", C.c_double),
+    ]
+
+
+_S = C.c_char * 512
+
+
+class In3dC(C.Structure):
+    """awp_in3d: everything IN3D carries (AWP-ODC-SGT/src/io.f:327-417)."""
+    _fields_ = (
+        [("igreen", C.c_int), ("tmax", C.c_float), ("dh", C.c_float), ("dt", C.c_float),
+         ("npc", C.c_int), ("nd", C.c_int), ("arbc", C.c_float), ("pht", C.c_float)]
+        + [(n, C.c_int) for n in ("nsrc", "nst", "nx", "ny", "nz", "npx", "npy", "npz",
+                                   "ifault", "checkpoint", "isfcvlm", "imd5", "ivelocity", "mediarestart",
+                                   "nvar", "iost", "partdeg", "io_opt", "iperf", "idyna", "socalq", "nve")]
+        + [(n, C.c_float) for n in ("mu_s", "mu_d", "fl", "fh", "fp")]
+        + [(n, C.c_int) for n in ("read_step", "write_step", "write_step2",
+                                   "nbgx", "nedx", "nskpx", "nbgy", "nedy", "nskpy", "nbgz", "nedz", "nskpz",
+                                   "ntiskp", "nbgx2", "nedx2", "nskpx2", "nbgy2", "nedy2", "nskpy2",
+                                   "nbgz2", "nedz2", "nskpz2", "ntiskp2", "ntiskp_sgt")]
+        + [(n, _S) for n in ("chkp", "chkj", "insrc", "invel", "insgt", "sxgro", "sygro", "szgro",
+                              "sxgro2", "sygro2", "szgro2", "sgtgro", "sgsn", "out_dir")]
+        + [("gpu_cli", C.c_int), ("nt", C.c_int)]
+    )
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libawpsgt.so; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libawpsgt not built: {path} missing (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    sig = {
+        "awp_params_default": (None, [P(Params)]),
+        "awp_create": (C.c_int, [P(Params), P(C.c_void_p)]),
+        "awp_load_media": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "awp_load_media_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "awp_set_source": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+        "awp_set_points": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+        "awp_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+        "awp_sgt_file_floats": (C.c_int64, [C.c_void_p]),
+        "awp_get_sgt": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+        "awp_get_chkj": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+        "awp_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_get_stats": (C.c_int, [C.c_void_p, P(Stats)]),
+        "awp_reset": (C.c_int, [C.c_void_p]),
+        "awp_destroy": (C.c_int, [C.c_void_p]),
+        "awp_footprint_bytes": (C.c_int64, [P(Params), C.c_int]),
+        "awp_bytes_per_cell_update": (C.c_double, [P(Params)]),
+        "awp_status_string": (C.c_char_p, [C.c_int]),
+        "awp_last_error": (C.c_char_p, []),
+        "awp_read_in3d": (C.c_int, [C.c_char_p, P(In3dC)]),
+        "awp_parse_command_line": (C.c_int, [C.c_int, P(C.c_char_p), P(In3dC)]),
+        "awp_params_from_in3d": (None, [P(In3dC), P(Params)]),
+        "awp_read_source": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+        "awp_read_cordfile": (C.c_int, [C.c_char_p, P(C.c_int), P(P(C.c_int))]),
+        "awp_free": (None, [C.c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(st: int):
+    if st != AWP_OK:
+        raise AwpError(st, load_library().awp_last_error().decode())
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def make_params(nx, ny, nz, dh, dt, nt, *, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5, socalq=0, nve=1,
+                mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10, write_step=None,
+                igreen: Sequence[int] = (1,), precision="f32", kernel="auto", device=0,
+                monitor_every=0) -> Params:
+    lib = load_library()
+    p = Params()
+    lib.awp_params_default(C.byref(p))
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.dh, p.dt, p.nt = dh, dt, nt
+    p.nd, p.arbc = nd, arbc
+    p.fl, p.fh, p.fp = fl, fh, fp
+    p.socalq, p.nve, p.mediastart, p.nvar, p.idyna = socalq, nve, mediastart, nvar, idyna
+    p.nst = nt if nst is None else nst
+    p.ntiskp_sgt = ntiskp_sgt
+    p.write_step = (nt // ntiskp_sgt) if write_step is None else write_step
+    p.ncomp = len(igreen)
+    for q, g in enumerate(igreen):
+        p.igreen[q] = g
+    p.precision = PREC[precision] if isinstance(precision, str) else precision
+    p.kernel = KERNEL[kernel] if isinstance(kernel, str) else kernel
+    p.device = device
+    p.monitor_every = monitor_every
+    return p
+
+
+def nt_file(p: Params) -> int:
+    """Samples per component in the raw SGT file (pmcl3d.f:1590-1594)."""
+    return ((p.nt // p.write_step) * p.write_step) // p.ntiskp_sgt
+
+
+class Solver:
+    """One SGT solve (1-3 components sharing one medium) on one GPU."""
+
+    def __init__(self, params: Params):
+        self.lib = load_library()
+        self.p = params
+        h = C.c_void_p()
+        _check(self.lib.awp_create(C.byref(params), C.byref(h)))
+        self.h = h
+        self.npts = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.awp_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_media(self, media: Optional[np.ndarray]):
+        if media is None:
+            _check(self.lib.awp_load_media(self.h, None))
+            return
+        m = np.ascontiguousarray(media, dtype=np.float32)
+        _check(self.lib.awp_load_media(self.h, _ptr(m)))
+
+    def load_media_file(self, path: str):
+        _check(self.lib.awp_load_media_file(self.h, path.encode()))
+
+    def set_source(self, comp: int, xyz, stf: np.ndarray):
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        stf = np.ascontiguousarray(np.asarray(stf, dtype=np.float32).reshape(xyz.shape[0], -1, 6))
+        _check(self.lib.awp_set_source(self.h, comp, xyz.shape[0], _ptr(xyz), _ptr(stf)))
+
+    def set_points(self, xyz):
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        self.npts = xyz.shape[0]
+        _check(self.lib.awp_set_points(self.h, xyz.shape[0], _ptr(xyz)))
+
+    def run(self, nsteps: int, with_sgt: bool = False):
+        if with_sgt:
+            out = np.zeros((self.p.ncomp, self.sgt_file_floats()), dtype=np.float32)
+            _check(self.lib.awp_run(self.h, nsteps, _ptr(out)))
+            return out
+        _check(self.lib.awp_run(self.h, nsteps, None))
+        return None
+
+    def reset(self):
+        _check(self.lib.awp_reset(self.h))
+
+    def sgt_file_floats(self) -> int:
+        return int(self.lib.awp_sgt_file_floats(self.h))
+
+    def sgt(self, comp: int = 0) -> np.ndarray:
+        out = np.zeros(self.sgt_file_floats(), dtype=np.float32)
+        _check(self.lib.awp_get_sgt(self.h, comp, _ptr(out)))
+        return out
+
+    def chkj(self, comp: int = 0) -> np.ndarray:
+        out = np.zeros((self.p.nt, 3), dtype=np.float32)
+        _check(self.lib.awp_get_chkj(self.h, comp, _ptr(out)))
+        return out
+
+    def field(self, name: str, comp: int = 0) -> np.ndarray:
+        p = self.p
+        out = np.zeros((p.nz + 4, p.ny + 4, p.nx + 4), dtype=np.float32)
+        _check(self.lib.awp_get_field(self.h, comp, FIELDS.index(name), _ptr(out)))
+        return out
+
+    def stats(self) -> Stats:
+        s = Stats()
+        _check(self.lib.awp_get_stats(self.h, C.byref(s)))
+        return s
+
+
+def read_in3d(path: str) -> In3dC:
+    o = In3dC()
+    _check(load_library().awp_read_in3d(path.encode(), C.byref(o)))
+    return o
+
+
+def parse_command_line(argv: Sequence[str]) -> In3dC:
+    """Parses a pmcl3d command line (argv[0] is the program name)."""
+    arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+    o = In3dC()
+    _check(load_library().awp_parse_command_line(len(argv), arr, C.byref(o)))
+    return o
+
+
+def params_from_in3d(o: In3dC) -> Params:
+    p = Params()
+    load_library().awp_params_from_in3d(C.byref(o), C.byref(p))
+    return p
+
+
+def read_source(path: str, ifault: int, nsrc: int, nst: int):
+    xyz = np.zeros((nsrc, 3), dtype=np.int32)
+    stf = np.zeros((nsrc, nst, 6), dtype=np.float32)
+    _check(load_library().awp_read_source(path.encode(), ifault, nsrc, nst, _ptr(xyz), _ptr(stf)))
+    return xyz, stf
+
+
+def read_cordfile(path: str) -> np.ndarray:
+    lib = load_library()
+    n = C.c_int()
+    ptr = C.POINTER(C.c_int)()
+    _check(lib.awp_read_cordfile(path.encode(), C.byref(n), C.byref(ptr)))
+    out = np.ctypeslib.as_array(ptr, shape=(n.value * 3,)).copy().reshape(-1, 3) if n.value else np.zeros((0, 3), np.int32)
+    lib.awp_free(ptr)
+    return out
+
+
+def footprint_bytes(p: Params, npts: int) -> int:
+    return int(load_library().awp_footprint_bytes(C.byref(p), npts))
+
+
+def bytes_per_cell_update(p: Params) -> float:
+    return float(load_library().awp_bytes_per_cell_update(C.byref(p)))

@@ -1,0 +1,94 @@
+/*
+ * awp_internal.h -- device data layout shared by the kernels and the solver.
+ *
+ * HBM layout of one field (one float32 array per field per component):
+ *   x fastest, then y, then z;  element (i,j,k) of the Fortran index space
+ *   (i = -1..nx+2, j = -1..ny+2, k = -1..nz+2, k = nz the free surface) lives
+ *   at  (k+1)*plane + (j+1)*px + (i + XO - 1)  with XO = 8, so that x = 1
+ *   starts on a 32-byte sector and every row of px floats is 32-byte aligned.
+ *   px = round_up(nx + XO + 2, 8), plane = px * (ny + 4).
+ * Ghost cells hold zeros for wavefields (the boundary values of a single
+ * domain), the padded values of padmedia/afsmedia for media.
+ */
+#ifndef AWP_INTERNAL_H
+#define AWP_INTERNAL_H
+
+#include <stdint.h>
+
+#define AWP_XO 8
+#define AWP_NF_STATE 15   /* u v w xx yy zz xy xz yz r1..r6 */
+
+enum {
+    AF_U = 0, AF_V, AF_W, AF_XX, AF_YY, AF_ZZ, AF_XY, AF_XZ, AF_YZ,
+    AF_R1, AF_R2, AF_R3, AF_R4, AF_R5, AF_R6
+};
+enum { AM_LAM = 0, AM_MU, AM_D1, AM_QP, AM_QS, AM_N };
+
+struct AwpGeom {
+    int nx, ny, nz;
+    int px;      /* row pitch (floats)            */
+    int py;      /* rows per plane (ny + 4)       */
+    int plane;   /* px * py                       */
+    int64_t vol; /* plane * (nz + 4)              */
+#ifdef __CUDACC__
+    __host__ __device__ __forceinline__
+#endif
+    int idx(int i, int j, int k) const { return (k + 1) * plane + (j + 1) * px + (i + AWP_XO - 1); }
+};
+
+struct AwpComp {
+    float *f[AWP_NF_STATE];
+};
+
+template <int NC>
+struct AwpCompSet {
+    AwpComp c[NC];
+};
+
+struct AwpMedia {
+    float *m[AM_N];
+};
+
+/* relaxation coefficients tau1/tau2 indexed [itz][ity][itx] flattened */
+struct AwpTau {
+    float t1[8];
+    float t2[8];
+};
+
+/* per-component source description on the device */
+struct AwpSrcDev {
+    int igreen;
+    int nsrc;
+    const int *ijk;     /* [nsrc][3] Fortran (i,j,k), k = nz at the surface */
+    const float *stf;   /* [nsrc][nst][6]                                    */
+};
+
+struct AwpPostArgs {
+    AwpGeom g;
+    int ncomp;
+    int nst;
+    int nt;
+    float vtst, vtst1;
+    int probe;          /* (nd+2) when inside the grid, else 0 */
+    int *step;          /* device counter: completed steps      */
+    float *chkj[3];     /* [nt][3] per component                */
+    AwpSrcDev src[3];
+    AwpComp comp[3];
+    const float *d1;
+};
+
+struct AwpSgtArgs {
+    AwpGeom g;
+    int ncomp;
+    int npts;
+    int ntiskp;
+    int nsamp_written;  /* samples that land in complete chunks  */
+    int64_t nt_file;
+    const int *pt_idx;  /* [npts] linear grid index              */
+    const float *sg;    /* [npts][3] sg1 sg2 sg3                 */
+    const int *step;
+    float *file[3];     /* raw SGT file image per component      */
+    AwpComp comp[3];
+};
+
+#endif

@@ -1,0 +1,233 @@
+/*
+ * awp_sgt.h -- C ABI of libawpsgt, the B200 strain-Green-tensor (SGT) stepper.
+ *
+ * The reference has no plugin API: its boundary is the `pmcl3d` process plus
+ * its files, and inside the CUDA variant an `extern "C"` launcher layer over
+ * raw device pointers.  This header is the library form of that boundary.  The
+ * `pmcl3d` executable built beside the library is a thin C driver over it that
+ * accepts both reference command lines and writes the same files.
+ *
+ * Every entry point below names the reference code it replaces (paths are
+ * inside the reference project SCECcode/cybershake-core).
+ *
+ * Conventions shared with the reference:
+ *   - grid indices are 1-based; x = 1..NX, y = 1..NY, z = 1..NZ with z = 1 at
+ *     the free surface for every coordinate a caller passes in (source
+ *     position, cordfile points), as in the IN3D/cordfile formats;
+ *   - the media array is float32 [z][y][x][nvar], z = 0 at the surface
+ *     (file layout read by AWP-ODC-SGT/src/structure.f:142-173);
+ *   - a source time function is float32 [nst][6] with columns
+ *     axx ayy azz axz ayz axy (AWP-ODC-SGT/src/source.f:193);
+ *   - the raw SGT output is float32 [point][6][NT] with components
+ *     XX YY ZZ XY XZ YZ (AWP axes), NT = int(int(nt/WRITE_STEP)*WRITE_STEP/
+ *     NTISKP_SGT), points in cordfile order (AWP-ODC-SGT/src/pmcl3d.f:1589-1601).
+ *
+ * Ownership and threading: the library allocates and owns all device memory of
+ * a solver.  Calls on one solver must not overlap; separate solvers may be used
+ * from separate host threads.  No entry point calls exit(); failures return a
+ * status and awp_last_error() describes the latest failure of the calling
+ * thread.
+ */
+#ifndef AWP_SGT_H
+#define AWP_SGT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    AWP_OK = 0,
+    AWP_ERR_IO = 1,        /* file missing, short or malformed               */
+    AWP_ERR_PARAM = 2,     /* parameter out of range                         */
+    AWP_ERR_OOM = 3,       /* device or host allocation failed               */
+    AWP_ERR_CUDA = 4,      /* CUDA runtime error                             */
+    AWP_ERR_UNSTABLE = 5,  /* stability monitor saw NaN/Inf or runaway growth */
+    AWP_ERR_TIMEOUT = 6,   /* a bounded wait ran out                         */
+    AWP_ERR_STATE = 7,     /* call made in the wrong order                   */
+    AWP_ERR_BUSY = 8,      /* serving queue full / not enough device memory  */
+    AWP_ERR_CANCELLED = 9  /* serving request was cancelled                  */
+} awp_status;
+
+/* Storage precision of the material coefficients and of the anelastic memory
+ * variables r1..r6.  Wavefields and all stencil arithmetic stay FP32. */
+typedef enum {
+    AWP_PREC_F32 = 0,   /* plain FP32, bit-exact with the FP32 oracle        */
+    AWP_PREC_BF16 = 1,  /* media and r1..r6 stored as bfloat16               */
+    AWP_PREC_F16 = 2    /* media and r1..r6 stored as scaled binary16        */
+} awp_precision;
+
+/* Stepper implementation. */
+typedef enum {
+    AWP_KERNEL_AUTO = 0,     /* library picks (fused when available)          */
+    AWP_KERNEL_TWO_SWEEP = 1 /* velocity sweep, then stress sweep             */
+} awp_kernel;
+
+#define AWP_MAX_COMP 3
+
+/* Parameters of one solve.  Field names follow IN3D (AWP-ODC-SGT/src/io.f:327-417)
+ * and the GPU command line (AWP-GPU-SGT/src/command.c:185-230). */
+typedef struct {
+    int nx, ny, nz;          /* NX NY NZ                                     */
+    float dh, dt;            /* DH DT                                        */
+    int nt;                  /* time steps (pmcl3d.f:287: nint(TMAX/DT)+1)   */
+    int nd;                  /* ND    Cerjan sponge width                    */
+    float arbc;              /* ARBC  Cerjan coefficient                     */
+    float fl, fh, fp;        /* FL FH FP  Q band                             */
+    int socalq;              /* SOCALQ velocity dispersion correction        */
+    int nve;                 /* NVE   1 = viscoelastic, 0 = elastic          */
+    int mediastart;          /* MEDIARESTART 0 = homogeneous, else media     */
+    int nvar;                /* NVAR  3, 5 or 8                              */
+    int idyna;               /* IDYNA (homogeneous medium choice only)       */
+    int nst;                 /* NST   source time-function length            */
+    int ntiskp_sgt;          /* NTISKP_SGT                                   */
+    int write_step;          /* WRITE_STEP (SGT samples per chunk)           */
+    int ncomp;               /* components stepped together (1..3)           */
+    int igreen[AWP_MAX_COMP];/* IGREEN per component (1,2,3,-1,-2,4,5,6)     */
+    int precision;           /* awp_precision                                */
+    int kernel;              /* awp_kernel                                   */
+    int device;              /* CUDA device ordinal                          */
+    int monitor_every;       /* stability check period in steps (0 = off)    */
+} awp_params;
+
+typedef struct {
+    int64_t steps_done;
+    double seconds_loop;         /* device time of the time loop (events)    */
+    double gcell_updates_per_s;  /* nx*ny*nz*ncomp*steps / seconds_loop      */
+    double bytes_per_cell_update;/* algorithmic bytes of the chosen stepper  */
+    double device_bytes;         /* device memory held by the solver         */
+    float vp_min, vp_max, vs_min, vs_max, rho_min, rho_max;  /* for CHKP     */
+    double energy;               /* last stability-monitor value (FP64)      */
+} awp_stats;
+
+typedef struct awp_solver awp_solver;
+
+/* Fills defaults (those of AWP-GPU-SGT/src/command.c:60-115 where they apply). */
+void awp_params_default(awp_params *p);
+
+/* Allocates a solver and its device fields.
+ * Replaces: vsemem (AWP-ODC-SGT/src/memory.f:137-200), inicrj
+ * (AWP-ODC-SGT/src/cerjan.f:4-247), tausub (AWP-ODC-SGT/src/relax.f:4-39) and the
+ * device set-up of AWP-GPU-SGT/src/pmcl3d.c:640-823 and
+ * SetDeviceConstValue (AWP-GPU-SGT/src/kernel_kp1_fix_havg_ifault5.cu:23-53). */
+awp_status awp_create(const awp_params *p, awp_solver **out);
+
+/* Loads media (float32 [nz][ny][nx][nvar], z = 0 at the surface, host memory),
+ * applies the Q / SoCalQ transform and pads the ghost cells on the device.
+ * Replaces: inimesh + padmedia + afsmedia (AWP-ODC-SGT/src/structure.f:13-707),
+ * AWP-GPU-SGT/src/mesh.c:12-410.  With mediastart == 0 `media` may be NULL
+ * (inihomo, structure.f:709-765). */
+awp_status awp_load_media(awp_solver *s, const float *media);
+
+/* Same, reading the media file (structure.f:142-173 record layout). */
+awp_status awp_load_media_file(awp_solver *s, const char *path);
+
+/* Sets the sources of component `comp`: xyz [nsrc][3] (1-based, z = 1 at the
+ * surface) and stf [nsrc][nst][6].
+ * Replaces: rdsrcpos/getsrc (AWP-ODC-SGT/src/source.f:132-470) and the source
+ * upload of AWP-GPU-SGT/src/source.c:4-159. */
+awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const int *xyz, const float *stf);
+
+/* Sets the SGT output points: xyz [npts][3] cordfile coordinates (1-based,
+ * z = 1 at the surface), kept in cordfile order.
+ * Replaces: getrec SGT part (AWP-ODC-SGT/src/station.f:31-80), inisgt
+ * (AWP-GPU-SGT/src/sgt.c:4-73). */
+awp_status awp_set_points(awp_solver *s, int npts, const int *xyz);
+
+/* Advances every component by up to `nsteps` time steps (stops at nt).  When
+ * sgt_out is not NULL the raw SGT file images of all components are copied to
+ * it, one after the other ([comp][awp_sgt_file_floats()]).
+ * Replaces: the time loop AWP-ODC-SGT/src/pmcl3d.f:1183-1611 (dvelc, addcrjvel,
+ * fvelxy, fvelz, dstrqc, addcrjstr, addsrc, fstr, SGT gather) and its CUDA
+ * launchers dvelcx_H, dstrqc_H, addsrc_H, ComputeSGT
+ * (AWP-GPU-SGT/src/kernel_kp1_fix_havg_ifault5.cu:72-178, 379-419). */
+awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out);
+
+/* Number of float32 values in one component's raw SGT file image. */
+int64_t awp_sgt_file_floats(const awp_solver *s);
+
+/* Copies the raw SGT file image of one component (pmcl3d.f:1582-1604). */
+awp_status awp_get_sgt(awp_solver *s, int comp, float *out);
+
+/* Copies the CHKJ series of one component: [nt][3] u1,v1,w1 at (ND+2,ND+2,ND+2)
+ * after every step (AWP-ODC-SGT/src/pmcl3d.f:1474-1484). */
+awp_status awp_get_chkj(awp_solver *s, int comp, float *out);
+
+/* Test/diagnostic access: copies one field of one component into the padded
+ * host layout out[(k+1)][(j+1)][(i+1)], extents (nz+4, ny+4, nx+4), as float32.
+ * field: 0..8 = u1 v1 w1 xx yy zz xy xz yz, 9..14 = r1..r6,
+ * 15..19 = lam mu d1 qp qs (compliances as stored by structure.f:488-519). */
+awp_status awp_get_field(awp_solver *s, int comp, int field, float *out);
+
+/* Statistics of the solver (timers, throughput, media extremes for CHKP). */
+awp_status awp_get_stats(awp_solver *s, awp_stats *st);
+
+/* Rewinds to step 0 with zeroed wavefields, keeping media, sources and
+ * points; the next awp_run starts a new solve. */
+awp_status awp_reset(awp_solver *s);
+
+/* Frees every resource of the solver. */
+awp_status awp_destroy(awp_solver *s);
+
+/* Device memory one solver of these parameters would hold (admission). */
+int64_t awp_footprint_bytes(const awp_params *p, int npts);
+
+/* Algorithmic bytes per cell-update of the stepper these parameters select. */
+double awp_bytes_per_cell_update(const awp_params *p);
+
+const char *awp_status_string(awp_status st);
+const char *awp_last_error(void);
+
+/* ------------------------------------------------------------------------- */
+/* File formats of the drop-in driver (pmcl3d).                              */
+/* ------------------------------------------------------------------------- */
+
+/* Everything the IN3D file carries (AWP-ODC-SGT/src/io.f:327-417, in order). */
+typedef struct {
+    int igreen; float tmax, dh, dt; int npc, nd; float arbc, pht;
+    int nsrc, nst, nx, ny, nz, npx, npy, npz;
+    int ifault, checkpoint, isfcvlm, imd5, ivelocity, mediarestart, nvar, iost,
+        partdeg, io_opt, iperf, idyna, socalq, nve;
+    float mu_s, mu_d, fl, fh, fp;
+    int read_step, write_step, write_step2;
+    int nbgx, nedx, nskpx, nbgy, nedy, nskpy, nbgz, nedz, nskpz, ntiskp;
+    int nbgx2, nedx2, nskpx2, nbgy2, nedy2, nskpy2, nbgz2, nedz2, nskpz2, ntiskp2;
+    int ntiskp_sgt;
+    char chkp[512], chkj[512], insrc[512], invel[512], insgt[512];
+    char sxgro[512], sygro[512], szgro[512], sxgro2[512], sygro2[512], szgro2[512];
+    char sgtgro[512], sgsn[512];
+    char out_dir[512];   /* GPU command line -o / --OUT                      */
+    int gpu_cli;         /* 1 when parsed from the GPU getopt command line   */
+    int nt;              /* derived number of time steps                     */
+} awp_in3d;
+
+/* Reads an IN3D file: one "value NAME" per line in the fixed order of
+ * AWP-ODC-SGT/src/io.f:327-417, blank lines allowed, quoted file names. */
+awp_status awp_read_in3d(const char *path, awp_in3d *out);
+
+/* Parses a pmcl3d command line in either reference form:
+ *   pmcl3d [IN3D [SOURCE [MEDIA [CHKP [CHKJ]]]]]   (AWP-ODC-SGT/src/set_names.f:17-50)
+ *   pmcl3d -T .. --IGREEN .. --DH ..               (AWP-GPU-SGT/src/command.c:117-340) */
+awp_status awp_parse_command_line(int argc, char **argv, awp_in3d *out);
+
+/* Fills solver parameters from a parsed IN3D. */
+void awp_params_from_in3d(const awp_in3d *in, awp_params *p);
+
+/* Reads a source file: IFAULT 0 text (first line x y z, then nst lines of six
+ * comma/space separated values; AWP-ODC-SGT/src/source.f:170-198) or IFAULT 1
+ * binary (int32[3] then float32[nst*6] per source; AWP-GPU-SGT/src/source.c:52-71).
+ * xyz must hold 3*nsrc ints, stf nsrc*nst*6 floats. */
+awp_status awp_read_source(const char *path, int ifault, int nsrc, int nst, int *xyz, float *stf);
+
+/* Reads a cordfile: optional '#' lines, the point count, then "x y z" lines
+ * (AWP-ODC-SGT/src/io.f:424-434).  *xyz is malloc'ed; free with awp_free. */
+awp_status awp_read_cordfile(const char *path, int *npts, int **xyz);
+
+void awp_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AWP_SGT_H */

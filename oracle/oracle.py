@@ -1,0 +1,166 @@
+"""ctypes binding of the CPU oracle (oracle/awp_oracle.c) -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use this
+module, as the checker or as the timed CPU restatement of the reference.  The
+product path (cybershake-core_b200/) never imports it.
+
+PARITY UNPINNED: the reference ships no solver tests or golden outputs and
+cannot be built here; the oracle is a statement-by-statement restatement of the
+Fortran (see the header of awp_oracle.c), checked by known-answer tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3", "r4", "r5", "r6",
+          "lam", "mu", "d1", "qp", "qs"]
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dh", C.c_float), ("dt", C.c_float),
+        ("nd", C.c_int), ("arbc", C.c_float),
+        ("fl", C.c_float), ("fh", C.c_float), ("fp", C.c_float),
+        ("socalq", C.c_int), ("nve", C.c_int), ("mediastart", C.c_int), ("nvar", C.c_int),
+        ("idyna", C.c_int), ("nst", C.c_int), ("nt", C.c_int), ("ntiskp_sgt", C.c_int),
+        ("write_step", C.c_int), ("igreen", C.c_int),
+    ]
+
+
+_libs = {}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def load(precision: str = "f32"):
+    if precision in _libs:
+        return _libs[precision]
+    path = os.path.join(_HERE, "liborc_%s.so" % precision)
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    P, V = C.POINTER, C.c_void_p
+    lib.orc_create.restype = V
+    lib.orc_create.argtypes = [P(OrcParams)]
+    lib.orc_destroy.argtypes = [V]
+    lib.orc_set_media.restype = C.c_int
+    lib.orc_set_media.argtypes = [V, V]
+    lib.orc_set_source.restype = C.c_int
+    lib.orc_set_source.argtypes = [V, C.c_int, V, V]
+    lib.orc_set_points.restype = C.c_int
+    lib.orc_set_points.argtypes = [V, C.c_int, V]
+    lib.orc_run.restype = C.c_int
+    lib.orc_run.argtypes = [V, C.c_int]
+    lib.orc_sgt_file_floats.restype = C.c_int64
+    lib.orc_sgt_file_floats.argtypes = [V]
+    lib.orc_get_sgt_file.argtypes = [V, V]
+    lib.orc_get_chkj.argtypes = [V, V]
+    lib.orc_get_field.restype = C.c_int
+    lib.orc_get_field.argtypes = [V, C.c_int, V]
+    lib.orc_set_field.restype = C.c_int
+    lib.orc_set_field.argtypes = [V, C.c_int, V]
+    lib.orc_get_extremes.argtypes = [V, V]
+    lib.orc_real_bytes.restype = C.c_int
+    lib.orc_num_threads.restype = C.c_int
+    lib.orc_set_num_threads.argtypes = [C.c_int]
+    _libs[precision] = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    """One component of the Fortran stepper on the CPU (FP32 or FP64)."""
+
+    def __init__(self, *, nx, ny, nz, dh, dt, nt, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5,
+                 socalq=0, nve=1, mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10,
+                 write_step=None, igreen=1, precision="f32", threads=0):
+        self.lib = load(precision)
+        if threads:
+            self.lib.orc_set_num_threads(threads)
+        self.dtype = np.float32 if precision == "f32" else np.float64
+        p = OrcParams()
+        p.nx, p.ny, p.nz, p.dh, p.dt = nx, ny, nz, dh, dt
+        p.nd, p.arbc, p.fl, p.fh, p.fp = nd, arbc, fl, fh, fp
+        p.socalq, p.nve, p.mediastart, p.nvar, p.idyna = socalq, nve, mediastart, nvar, idyna
+        p.nst = nt if nst is None else nst
+        p.nt, p.ntiskp_sgt = nt, ntiskp_sgt
+        p.write_step = (nt // ntiskp_sgt) if write_step is None else write_step
+        p.igreen = igreen
+        self.p = p
+        self.h = self.lib.orc_create(C.byref(p))
+        if not self.h:
+            raise ValueError("oracle rejected the parameters")
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_media(self, media):
+        if media is None:
+            st = self.lib.orc_set_media(self.h, None)
+        else:
+            m = np.ascontiguousarray(media, dtype=np.float32)
+            st = self.lib.orc_set_media(self.h, _p(m))
+        if st != 0:
+            raise ValueError("oracle: bad media")
+
+    def set_source(self, xyz, stf):
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        stf = np.ascontiguousarray(np.asarray(stf, dtype=np.float32).reshape(xyz.shape[0], -1, 6))
+        if self.lib.orc_set_source(self.h, xyz.shape[0], _p(xyz), _p(stf)) != 0:
+            raise ValueError("oracle: source outside the grid")
+
+    def set_points(self, xyz):
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        if self.lib.orc_set_points(self.h, xyz.shape[0], _p(xyz)) != 0:
+            raise ValueError("oracle: point outside the grid")
+
+    def run(self, nsteps):
+        return self.lib.orc_run(self.h, nsteps)
+
+    def sgt(self):
+        out = np.zeros(int(self.lib.orc_sgt_file_floats(self.h)), dtype=np.float32)
+        self.lib.orc_get_sgt_file(self.h, _p(out))
+        return out
+
+    def chkj(self):
+        out = np.zeros((self.p.nt, 3), dtype=np.float32)
+        self.lib.orc_get_chkj(self.h, _p(out))
+        return out
+
+    def field(self, name):
+        p = self.p
+        out = np.zeros((p.nz + 4, p.ny + 4, p.nx + 4), dtype=self.dtype)
+        self.lib.orc_get_field(self.h, FIELDS.index(name), _p(out))
+        return out
+
+    def set_field(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=self.dtype)
+        self.lib.orc_set_field(self.h, FIELDS.index(name), _p(a))
+
+    def extremes(self):
+        out = np.zeros(6, dtype=np.float32)
+        self.lib.orc_get_extremes(self.h, _p(out))
+        return out
+
+
+def threads():
+    return load("f32").orc_num_threads()

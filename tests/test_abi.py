@@ -1,0 +1,93 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol the
+header declares, reports errors as status codes, and its host-side helpers
+(parameter defaults, algorithmic byte counts, footprints) are consistent."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import awpsgt
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "awp_sgt.h")
+
+
+def header_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(awp_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = awpsgt.load_library()
+    decl = header_functions()
+    assert len(decl) >= 20
+    missing = [n for n in decl if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(awpsgt.EXPORTED) == decl
+
+
+def test_exports_are_c_linkage():
+    out = subprocess.run(["nm", "-D", "--defined-only", awpsgt.LIB_PATH], capture_output=True, text=True).stdout
+    names = set(l.split()[-1] for l in out.splitlines() if " T " in l)
+    for n in header_functions():
+        assert n in names, n
+
+
+def test_param_defaults_match_gpu_command_defaults():
+    lib = awpsgt.load_library()
+    p = awpsgt.Params()
+    lib.awp_params_default(C.byref(p))
+    # AWP-GPU-SGT/src/command.c:60-115
+    assert (p.nx, p.ny, p.nz) == (224, 224, 1024)
+    assert p.dh == 200.0 and abs(p.dt - 0.01) < 1e-9
+    assert p.nd == 20 and abs(p.arbc - 0.92) < 1e-7
+    assert p.nst == 91 and p.write_step == 10 and p.ntiskp_sgt == 1
+    assert p.socalq == 1 and p.nve == 1
+
+
+@pytest.mark.parametrize("ncomp,prec,expect", [(1, "f32", 176.0), (2, "f32", 166.0), (3, "f32", 156.0 + 20.0 / 3)])
+def test_algorithmic_bytes_two_sweep(ncomp, prec, expect):
+    p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, igreen=(1, 2, 3)[:ncomp], precision=prec, ntiskp_sgt=1)
+    assert abs(awpsgt.bytes_per_cell_update(p) - expect) < 1e-9
+
+
+def test_footprint_grows_with_components():
+    p1 = awpsgt.make_params(400, 400, 200, 100.0, 0.005, 4001, igreen=(1,), ntiskp_sgt=10)
+    p3 = awpsgt.make_params(400, 400, 200, 100.0, 0.005, 4001, igreen=(1, 2, 3), ntiskp_sgt=10)
+    f1, f3 = awpsgt.footprint_bytes(p1, 5000), awpsgt.footprint_bytes(p3, 5000)
+    cells = 400 * 400 * 200
+    assert f1 > cells * 4 * 20
+    assert f3 > f1 + 2 * cells * 4 * 15
+
+
+def test_status_strings():
+    lib = awpsgt.load_library()
+    assert lib.awp_status_string(0) == b"AWP_OK"
+    assert lib.awp_status_string(5) == b"AWP_ERR_UNSTABLE"
+
+
+def test_bad_parameters_rejected_before_any_device_call():
+    p = awpsgt.make_params(4, 64, 64, 100.0, 0.005, 10, ntiskp_sgt=1)
+    with pytest.raises(awpsgt.AwpError) as e:
+        awpsgt.Solver(p)
+    assert e.value.status == 2
+    p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, ntiskp_sgt=1, igreen=(7,))
+    with pytest.raises(awpsgt.AwpError) as e:
+        awpsgt.Solver(p)
+    assert e.value.status == 2
+
+
+def test_create_without_gpu_fails_loudly():
+    """On a machine without a GPU the CUDA path reports AWP_ERR_CUDA; there is
+    no CPU fallback."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = awpsgt.make_params(32, 32, 32, 100.0, 0.005, 10, ntiskp_sgt=1)
+    with pytest.raises(awpsgt.AwpError) as e:
+        awpsgt.Solver(p)
+    assert e.value.status in (3, 4)

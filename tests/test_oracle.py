@@ -1,0 +1,184 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+The reference ships no solver tests or golden SGT files, so the oracle is
+pinned by properties the discrete equations must have:
+  * FP32 and FP64 builds agree to rounding level;
+  * exact linearity in the source amplitude (scaling by 2 commutes with IEEE
+    rounding, so the FP32 SGT scales bit for bit) and superposition;
+  * P waves travel at Vp: the delay between two receivers on the force axis
+    matches the analytic travel-time difference;
+  * media ingest reproduces structure.f's compliances and Q transform, the
+    unpadded qp/qs ghosts and the padmedia corner assignments.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import awp_inputs as ai
+import oracle
+
+
+def small_case(prec="f32", nt=80, stf_scale=1.0, igreen=1, src=(24, 20, 9), seed=3, **kw):
+    nx, ny, nz = 48, 40, 32
+    media = ai.layered_media(nx, ny, nz, 200.0, seed=seed, pert_std=0.05, corr_len=1000.0)
+    stf = ai.gaussian_derivative_stf(nt, 0.01, f0=1.0) * np.float32(stf_scale)
+    pts = ai.sgt_points(nx, ny, 20, 40, seed=0)
+    args = dict(nx=nx, ny=ny, nz=nz, dh=200.0, dt=0.01, nt=nt, nd=8, socalq=1, ntiskp_sgt=5, write_step=4,
+                igreen=igreen, precision=prec)
+    args.update(kw)
+    o = oracle.Oracle(**args)
+    o.load_media(media)
+    o.set_source([src], stf)
+    o.set_points(pts)
+    o.run(nt)
+    return o
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b.astype(np.float64)) / max(np.linalg.norm(b.astype(np.float64)), 1e-300))
+
+
+def test_fp32_matches_fp64():
+    a = small_case("f32").sgt()
+    b = small_case("f64").sgt()
+    assert np.abs(b).max() > 0
+    assert rel_l2(a, b) < 1e-5
+
+
+def test_linearity_exact_scaling():
+    """Doubling the source doubles every SGT value exactly, except values so
+    small that their history passed through the subnormal range, where the
+    rounding quantum is absolute rather than relative."""
+    a = small_case("f32").sgt()
+    b = small_case("f32", stf_scale=2.0).sgt()
+    big = np.abs(a) > 1e-12 * np.abs(a).max()
+    assert big.sum() > 100
+    assert np.array_equal(b[big], 2.0 * a[big])
+    assert rel_l2(b, 2.0 * a) < 1e-15
+
+
+def test_superposition_fp64():
+    nx, ny, nz, nt = 40, 36, 28, 60
+    media = ai.layered_media(nx, ny, nz, 200.0, seed=1, pert_std=0.05, corr_len=1000.0)
+    rng = np.random.default_rng(7)
+    s1 = rng.standard_normal((nt, 6)).astype(np.float32)
+    s2 = rng.standard_normal((nt, 6)).astype(np.float32)
+    pts = ai.sgt_points(nx, ny, 20, 30, seed=0)
+
+    def run(stf):
+        o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=200.0, dt=0.01, nt=nt, nd=8, ntiskp_sgt=2, write_step=10,
+                          igreen=-2, precision="f64")
+        o.load_media(media)
+        o.set_source([(20, 18, 6)], stf)
+        o.set_points(pts)
+        o.run(nt)
+        return o.sgt().astype(np.float64)
+
+    a, b, ab = run(s1), run(s2), run(s1 + s2)
+    assert rel_l2(ab, a + b) < 1e-6
+
+
+def test_p_wave_travel_time():
+    """Force along x in a homogeneous medium: the P pulse seen at two points on
+    the x axis is delayed by (r2 - r1)/Vp."""
+    nx, ny, nz, nt = 140, 48, 72, 350
+    dh, dt, f0 = 200.0, 0.01, 2.0
+    vp, vs = 6000.0, 3464.0
+    media = ai.homogeneous_media(nx, ny, nz, vp=vp, vs=vs, rho=2700.0)
+    stf = ai.gaussian_derivative_stf(nt, dt, f0=f0)
+    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=dh, dt=dt, nt=nt, nd=12, socalq=0, ntiskp_sgt=1, write_step=nt,
+                      igreen=1, precision="f64", fl=0.01, fh=25.0, fp=0.5)
+    o.load_media(media)
+    src = (30, 24, 36)
+    o.set_source([src], stf)
+    r1, r2 = 20, 60          # far field on the force axis: P only until the S wave
+    o.set_points([(src[0] + r1, 24, 36), (src[0] + r2, 24, 36)])
+    o.run(nt)
+    s = o.sgt().reshape(2, 6, -1).astype(np.float64)
+    t0 = 1.5 / f0
+    tt = np.arange(s.shape[2]) * dt + dt
+
+    def p_window(trace, r):   # keep the trace up to halfway between P and S
+        cut = t0 + 0.5 * (r * dh / vp + r * dh / vs)
+        return np.where(tt < cut, trace, 0.0)
+
+    exx1, exx2 = p_window(s[0, 0], r1), p_window(s[1, 0], r2)
+    # upsampled cross-correlation delay
+    up = 8
+    t = np.arange(exx1.size)
+    tf = np.linspace(0, exx1.size - 1, (exx1.size - 1) * up + 1)
+    a = np.interp(tf, t, exx1)
+    b = np.interp(tf, t, exx2)
+    xc = np.correlate(b, a, mode="full")
+    lag = (np.argmax(xc) - (a.size - 1)) / up * dt
+    # SoCalQ off: Vp is the medium's 6000 m/s at the Q reference frequency; the
+    # dispersion between FP and the pulse frequency (Qp ~ 350) is < 0.1 %
+    expect = (r2 - r1) * dh / 6000.0
+    assert abs(lag - expect) < 0.03 * expect, (lag, expect)
+
+
+def test_media_transform_and_padding():
+    nx, ny, nz = 12, 10, 9
+    rng = np.random.default_rng(0)
+    m = np.empty((nz, ny, nx, 5), dtype=np.float32)
+    m[..., 1] = rng.uniform(1000, 3000, (nz, ny, nx))
+    m[..., 0] = m[..., 1] * 1.8
+    m[..., 2] = rng.uniform(2000, 2800, (nz, ny, nx))
+    m[..., 4] = rng.uniform(20, 200, (nz, ny, nx))
+    m[..., 3] = 2 * m[..., 4]
+    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=100.0, dt=0.005, nt=10, nd=3, socalq=0, nvar=5, precision="f64")
+    o.load_media(m)
+    lam, mu, d1, qp, qs = (o.field(n) for n in ("lam", "mu", "d1", "qp", "qs"))
+    # interior: z flipped, compliances (structure.f:488-490)
+    vp, vs, rho = (m[..., q].astype(np.float64) for q in range(3))
+    k = nz  # Fortran k = nz is file z = 0
+    np.testing.assert_allclose(mu[k + 1, 2:ny + 2, 2:nx + 2], 1.0 / (rho[0] * vs[0] ** 2), rtol=1e-6)
+    np.testing.assert_allclose(lam[k + 1, 2:ny + 2, 2:nx + 2], 1.0 / (rho[0] * (vp[0] ** 2 - 2 * vs[0] ** 2)), rtol=1e-6)
+    np.testing.assert_allclose(d1[2, 2:ny + 2, 2:nx + 2], rho[nz - 1], rtol=1e-7)
+    # Q transform (structure.f:461-468, 515-516)
+    pi = 4 * math.atan(1.0)
+    w0, w1, w2 = 2 * pi * 0.5, 2 * pi * 0.01, 2 * pi * 25.0
+    tmax, tmin = 1 / w1, 1 / w2
+    t1, t2 = 2 / pi * math.log(tmax / tmin), 2 / pi * math.log(w0 * tmin)
+    qinv = 1.0 / m[0, ..., 4].astype(np.float64)
+    np.testing.assert_allclose(qs[k + 1, 2:ny + 2, 2:nx + 2], t1 * qinv / (1 - t2 * qinv), rtol=1e-5)
+    # qp/qs ghosts stay zero except the plane above the surface (afsmedia)
+    assert np.all(qs[1, :, :] == 0) and np.all(qs[:, 1, :] == 0) and np.all(qs[:, :, nx + 2] == 0)
+    np.testing.assert_array_equal(qs[nz + 2, 2:ny + 2, 2:nx + 2], qs[nz + 1, 2:ny + 2, 2:nx + 2])
+    # lam/mu/d1 ghosts copy the nearest interior cell
+    np.testing.assert_array_equal(mu[1, 2:ny + 2, 2:nx + 2], mu[2, 2:ny + 2, 2:nx + 2])
+    np.testing.assert_array_equal(lam[2:nz + 2, 2:ny + 2, nx + 2], lam[2:nz + 2, 2:ny + 2, nx + 1])
+    # padmedia corner (structure.f:654-655): mu and d1 at (nxt+1,0,0) take lam(nxt,1,1)
+    assert mu[1, 1, nx + 2] == lam[2, 2, nx + 1]
+    assert d1[1, 1, nx + 2] == lam[2, 2, nx + 1]
+
+
+def test_socalq_dispersion_correction():
+    nx, ny, nz = 10, 10, 10
+    m = ai.homogeneous_media(nx, ny, nz, vp=6000.0, vs=3464.0, rho=2700.0)
+    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=200.0, dt=0.01, nt=5, nd=3, socalq=1, ntiskp_sgt=1, precision="f64")
+    o.load_media(m)
+    e = o.extremes()
+    qs = 0.05 * 3464.0
+    pi = 4 * math.atan(1.0)
+    lw = math.log(25.0 / 0.5)
+    assert abs(e[2] - 3464.0 * (1 + lw / (pi * qs))) < 1e-2
+    assert abs(e[0] - 6000.0 * (1 + lw / (pi * 2 * qs))) < 1e-2
+
+
+def test_sgt_sampling_and_file_offsets():
+    """nt=81, NTISKP_SGT=5, WRITE_STEP=4: 16 samples, 4 full chunks; the file
+    holds NT = int(int(81/4)*4/5) = 16 samples per component."""
+    o = small_case("f32", nt=81)
+    s = o.sgt()
+    assert s.size == 40 * 6 * 16
+    s = s.reshape(40, 6, 16)
+    assert np.abs(s[:, :, -1]).max() > 0
+
+
+def test_chkj_series_recorded():
+    o = small_case("f32", nt=30)
+    c = o.chkj()
+    assert c.shape == (30, 3)
+    assert np.isfinite(c).all()
