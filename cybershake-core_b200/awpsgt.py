@@ -36,7 +36,7 @@ EXPORTED = [
     "awp_set_points", "awp_run", "awp_sgt_file_floats", "awp_get_sgt", "awp_get_chkj", "awp_get_field",
     "awp_get_stats", "awp_reset", "awp_destroy", "awp_footprint_bytes", "awp_bytes_per_cell_update",
     "awp_status_string", "awp_last_error", "awp_read_in3d", "awp_parse_command_line",
-    "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free",
+    "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free", "awp_profile_steps",
 ]
 
 
@@ -66,6 +66,16 @@ class Stats(C.Structure):
         ("vp_min", C.c_float), ("vp_max", C.c_float), ("vs_min", C.c_float), ("vs_max", C.c_float),
         ("rho_min", C.c_float), ("rho_max", C.c_float), ("energy", C.c_double),
     ]
+
+
+class KernelTimes(C.Structure):
+    _fields_ = [("nkernels", C.c_int), ("name", (C.c_char * 32) * 8), ("launches", C.c_int * 8),
+                ("ms_per_launch", C.c_double * 8), ("bytes_per_launch", C.c_double * 8)]
+
+    def as_dict(self):
+        return {self.name[k].value.decode(): {"launches": self.launches[k], "ms": self.ms_per_launch[k],
+                                              "bytes": self.bytes_per_launch[k]}
+                for k in range(self.nkernels)}
 
 
 _S = C.c_char * 512
@@ -127,6 +137,7 @@ def load_library(path: str = LIB_PATH):
         "awp_read_source": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
         "awp_read_cordfile": (C.c_int, [C.c_char_p, P(C.c_int), P(P(C.c_int))]),
         "awp_free": (None, [C.c_void_p]),
+        "awp_profile_steps": (C.c_int, [C.c_void_p, C.c_int, P(KernelTimes)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -252,6 +263,12 @@ class Solver:
         out = np.zeros((p.nz + 4, p.ny + 4, p.nx + 4), dtype=np.float32)
         _check(self.lib.awp_get_field(self.h, comp, FIELDS.index(name), _ptr(out)))
         return out
+
+    def profile(self, nsteps: int) -> dict:
+        """Advances nsteps steps with CUDA events around every kernel launch."""
+        kt = KernelTimes()
+        _check(self.lib.awp_profile_steps(self.h, nsteps, C.byref(kt)))
+        return kt.as_dict()
 
     def stats(self) -> Stats:
         s = Stats()

@@ -49,6 +49,22 @@ struct AwpMedia {
     float *m[AM_N];
 };
 
+/* storage type of the media arrays and of r1..r6 */
+enum { AWP_STORE_F32 = 0, AWP_STORE_BF16 = 1, AWP_STORE_F16 = 2 };
+
+/* binary16 arrays hold value * scale (a power of two); inv = 1/scale */
+struct AwpMediaScale {
+    float scale[AM_N];
+    float inv[AM_N];
+};
+
+/* media as the steppers read them: typed arrays plus their scales */
+struct AwpMediaT {
+    void *m[AM_N];
+    int type;
+    AwpMediaScale sc;
+};
+
 /* relaxation coefficients tau1/tau2 indexed [itz][ity][itx] flattened */
 struct AwpTau {
     float t1[8];
@@ -74,7 +90,9 @@ struct AwpPostArgs {
     float *chkj[3];     /* [nt][3] per component                */
     AwpSrcDev src[3];
     AwpComp comp[3];
-    const float *d1;
+    const void *d1;     /* typed density array                  */
+    int media_type;     /* AWP_STORE_*                          */
+    float d1_inv;       /* binary16 scale inverse               */
 };
 
 struct AwpSgtArgs {
@@ -89,6 +107,7 @@ struct AwpSgtArgs {
     const int *step;
     float *file[3];     /* raw SGT file image per component      */
     AwpComp comp[3];
+    int active[3];      /* 0 for moment sources (IGREEN = -1)    */
 };
 
 #endif

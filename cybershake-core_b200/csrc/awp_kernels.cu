@@ -1,19 +1,27 @@
 /*
- * awp_kernels.cu -- sm_100a kernels of the AWP-ODC-SGT stepper (two-sweep form).
+ * awp_kernels.cu -- sm_100a kernels of the AWP-ODC-SGT stepper.
  *
  * Arithmetic follows the Fortran statement by statement with the same
- * evaluation order; this translation unit is compiled with --fmad=false so
- * every product and sum is rounded once, as in the FP32 CPU reference, and the
- * FP32 stepper reproduces it bit for bit.
+ * evaluation order (awp_stencil.cuh); this translation unit is compiled with
+ * --fmad=false so every product and sum is rounded once, as in the FP32 CPU
+ * reference, and the FP32 steppers reproduce it bit for bit.
  *
  * Kernels:
  *   k_media_interior  structure.f:449-533   media -> compliances + Q transform
  *   k_media_ghosts    structure.f:563-707   padmedia / afsmedia
  *   k_media_homo      structure.f:709-765   inihomo
+ *   k_media_convert   FP32 media -> bf16 / scaled binary16 storage
  *   k_sg_coeffs       pmcl3d.f:1158-1171    sg1 sg2 sg3 at the SGT points
- *   k_vel<NC>         operator.f:92-244 + cerjan.f:292-330   velocity sweep
- *   k_fsvel<NC>       operator.f:246-306    free-surface velocity images
- *   k_str<NC>         viscoop.f:49-191 + cerjan.f:249-290 + operator.f:575-612
+ *   two-sweep stepper:
+ *     k_vel           operator.f:92-244 + cerjan.f:292-330   velocity sweep
+ *     k_fsvel         operator.f:246-306    free-surface velocity images
+ *     k_str           viscoop.f:49-191 + cerjan.f:249-290 + operator.f:575-612
+ *   fused stepper:
+ *     k_fused         one z-march per xy tile: new velocities on the tile plus
+ *                     a 2-cell halo into a 6-level shared-memory ring, then the
+ *                     stress/memory-variable update of the tile two levels
+ *                     below; free surface and fstr folded in; reads the old
+ *                     wavefield buffer and writes the other one (ping-pong)
  *   k_post            source.f:812-913, pmcl3d.f:1379-1385, 1478-1479
  *   k_sgt             pmcl3d.f:1537-1557    SGT gather into the file image
  * NC = number of unit-force components stepped together (they share media).
@@ -22,9 +30,7 @@
 #include <stdint.h>
 #include "awp_internal.h"
 #include "awp_kernels.h"
-
-#define C1 (9.0f / 8.0f)
-#define C2 (-(1.0f / 24.0f))
+#include "awp_stencil.cuh"
 
 /* ------------------------------------------------------------------ */
 /* media                                                               */
@@ -145,89 +151,102 @@ __global__ void k_media_homo(AwpGeom g, AwpMedia md, float lam, float mu, float 
     md.m[AM_D1][c] = d1;
 }
 
+/* |value| maxima and minima of the nonzero entries of each media array
+ * (for the binary16 scale and range check) */
+__global__ void k_media_range(AwpMedia md, int64_t n, unsigned *mx, unsigned *mn)
+{
+    unsigned lmx[AM_N], lmn[AM_N];
+    for (int a = 0; a < AM_N; a++) { lmx[a] = 0u; lmn[a] = 0x7f800000u; }
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        for (int a = 0; a < AM_N; a++) {
+            unsigned b = __float_as_uint(fabsf(md.m[a][t]));
+            if (b) { lmx[a] = max(lmx[a], b); lmn[a] = min(lmn[a], b); }
+        }
+    for (int a = 0; a < AM_N; a++) {
+        for (int off = 16; off > 0; off >>= 1) {
+            lmx[a] = max(lmx[a], __shfl_xor_sync(0xffffffffu, lmx[a], off));
+            lmn[a] = min(lmn[a], __shfl_xor_sync(0xffffffffu, lmn[a], off));
+        }
+        if ((threadIdx.x & 31) == 0) { atomicMax(&mx[a], lmx[a]); atomicMin(&mn[a], lmn[a]); }
+    }
+}
+
+template <class TM>
+__global__ void k_media_convert(AwpMedia src, void *d0, void *d1, void *d2, void *d3, void *d4, AwpMediaScale sc,
+                                int64_t n)
+{
+    TM *dst[AM_N] = {(TM *)d0, (TM *)d1, (TM *)d2, (TM *)d3, (TM *)d4};
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        for (int a = 0; a < AM_N; a++)
+            if (dst[a]) Store<TM>::st(dst[a], (int)t, src.m[a][t], sc.scale[a]);
+}
+
 /* pmcl3d.f:1166-1168, evaluated at the SGT points only. */
-__global__ void k_sg_coeffs(AwpGeom g, AwpMedia md, int npts, const int *__restrict__ pt_idx, float *sg)
+template <class TM>
+__global__ void k_sg_coeffs(MediaT<TM> md, int npts, const int *__restrict__ pt_idx, float *sg)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= npts) return;
     const int c = pt_idx[n];
-    const float lam = md.m[AM_LAM][c], mu = md.m[AM_MU][c];
+    const float lam = md(AM_LAM, c), mu = md(AM_MU, c);
     sg[3 * n] = (1.0f / lam + 1.0f / mu) / (1.0f / mu * (3.0f / lam + 2.0f / mu));
     sg[3 * n + 1] = -(1.0f / lam / (2.0f / mu * (3.0f / lam + 2.0f / mu)));
     sg[3 * n + 2] = mu;
 }
 
 /* ------------------------------------------------------------------ */
-/* velocity sweep                                                      */
+/* two-sweep stepper                                                   */
 /* ------------------------------------------------------------------ */
 
-template <int NC>
+__device__ __forceinline__ void zchunk(const AwpGeom &g, int kchunk, int &k0, int &k1)
+{
+    /* z chunks are aligned to the top so the top chunk always holds the
+     * levels nz-2..nz that the fused fstr reads back */
+    k1 = g.nz - ((int)gridDim.z - 1 - (int)blockIdx.z) * kchunk;
+    k0 = max(1, k1 - kchunk + 1);
+}
+
+template <int NC, class TM>
 __global__ void __launch_bounds__(256)
-k_vel(AwpGeom g, const float *__restrict__ d1, AwpCompSet<NC> cs,
-      const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
-      float dth, int kchunk)
+k_vel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
+      const float *__restrict__ cz, float dth, int kchunk)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.nx || j > g.ny) return;
-    /* z chunks are aligned to the top so the top chunk always holds the
-     * levels nz-2..nz that the fused fstr reads back */
-    const int k1 = g.nz - ((int)gridDim.z - 1 - (int)blockIdx.z) * kchunk;
-    const int k0 = max(1, k1 - kchunk + 1);
+    int k0, k1;
+    zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane;
     const float cxy = cx[i] * cy[j];
     for (int k = k0; k <= k1; ++k) {
         const int c = g.idx(i, j, k);
-        const float da = d1[c], db = d1[c - sy], dc = d1[c - sz], dd = d1[c - sy - sz];
-        const float de = d1[c + 1], df = d1[c + 1 - sz], dg = d1[c + 1 - sy];
-        /* operator.f:120-121, 171-172, 224-225 */
-        const float fu = dth / (0.25f * ((da + db) + (dc + dd)));
-        const float fv = dth / (0.25f * ((da + de) + (dc + df)));
-        const float fw = dth / (0.25f * ((da + de) + (db + dg)));
+        float fu, fv, fw;
+        vel_factors(md, c, sy, sz, dth, fu, fv, fw);
         const float crj = cxy * cz[k];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
-            float *__restrict__ u1 = cs.c[q].f[AF_U];
-            float *__restrict__ v1 = cs.c[q].f[AF_V];
-            float *__restrict__ w1 = cs.c[q].f[AF_W];
-            const float *__restrict__ xx = cs.c[q].f[AF_XX];
-            const float *__restrict__ yy = cs.c[q].f[AF_YY];
-            const float *__restrict__ zz = cs.c[q].f[AF_ZZ];
-            const float *__restrict__ xy = cs.c[q].f[AF_XY];
-            const float *__restrict__ xz = cs.c[q].f[AF_XZ];
-            const float *__restrict__ yz = cs.c[q].f[AF_YZ];
-            const float u = u1[c] + fu * (
-                C1 * (xx[c] - xx[c - 1]) + C2 * (xx[c + 1] - xx[c - 2]) +
-                C1 * (xy[c] - xy[c - sy]) + C2 * (xy[c + sy] - xy[c - 2 * sy]) +
-                C1 * (xz[c] - xz[c - sz]) + C2 * (xz[c + sz] - xz[c - 2 * sz]));
-            const float v = v1[c] + fv * (
-                C1 * (xy[c + 1] - xy[c]) + C2 * (xy[c + 2] - xy[c - 1]) +
-                C1 * (yy[c + sy] - yy[c]) + C2 * (yy[c + 2 * sy] - yy[c - sy]) +
-                C1 * (yz[c] - yz[c - sz]) + C2 * (yz[c + sz] - yz[c - 2 * sz]));
-            const float w = w1[c] + fw * (
-                C1 * (xz[c + 1] - xz[c]) + C2 * (xz[c + 2] - xz[c - 1]) +
-                C1 * (yz[c] - yz[c - sy]) + C2 * (yz[c + sy] - yz[c - 2 * sy]) +
-                C1 * (zz[c + sz] - zz[c]) + C2 * (zz[c + 2 * sz] - zz[c - sz]));
+            float u, v, w;
+            vel_one(cs.c[q], c, sy, sz, fu, fv, fw, u, v, w);
             /* Cerjan: the factor is exactly 1 outside the sponge zones */
-            u1[c] = u * crj;
-            v1[c] = v * crj;
-            w1[c] = w * crj;
+            cs.c[q].f[AF_U][c] = u * crj;
+            cs.c[q].f[AF_V][c] = v * crj;
+            cs.c[q].f[AF_W][c] = w * crj;
         }
     }
 }
 
 /* fvelxy then fvelz.  Each thread recomputes the two neighbouring fvelxy
  * values fvelz needs, so one launch covers both routines. */
-template <int NC>
-__global__ void k_fsvel(AwpGeom g, const float *__restrict__ lam, const float *__restrict__ mu, AwpCompSet<NC> cs)
+template <int NC, class TM>
+__global__ void k_fsvel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.nx || j > g.ny) return;
     const int nz = g.nz;
     const int c = g.idx(i, j, nz), sy = g.px, sz = g.plane;
-    const float xl = 1.0f / lam[c];
-    const float xl2m = 2.0f / mu[c] + xl;
+    const float xl = 1.0f / md(AM_LAM, c);
+    const float xl2m = 2.0f / md(AM_MU, c) + xl;
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
         float *u1 = cs.c[q].f[AF_U], *v1 = cs.c[q].f[AF_V], *w1 = cs.c[q].f[AF_W];
@@ -246,142 +265,47 @@ __global__ void k_fsvel(AwpGeom g, const float *__restrict__ lam, const float *_
     }
 }
 
-/* ------------------------------------------------------------------ */
-/* stress + memory-variable sweep                                      */
-/* ------------------------------------------------------------------ */
-
-template <int NC>
+template <int NC, class TM, class TR>
 __global__ void __launch_bounds__(256)
-k_str(AwpGeom g, AwpMedia md, AwpCompSet<NC> cs,
-      const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
-      const float *__restrict__ tau, float dth, float dt, float dh1, int kchunk, int nve, int fuse_fstr)
+k_str(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
+      const float *__restrict__ cz, const float *__restrict__ tau, float dth, float dt, float dh1, int kchunk,
+      int nve)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.nx || j > g.ny) return;
-    /* z chunks are aligned to the top so the top chunk always holds the
-     * levels nz-2..nz that the fused fstr reads back */
-    const int k1 = g.nz - ((int)gridDim.z - 1 - (int)blockIdx.z) * kchunk;
-    const int k0 = max(1, k1 - kchunk + 1);
+    int k0, k1;
+    zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane;
-    const float *__restrict__ lam = md.m[AM_LAM];
-    const float *__restrict__ mu = md.m[AM_MU];
-    const float *__restrict__ qp = md.m[AM_QP];
-    const float *__restrict__ qs = md.m[AM_QS];
     const float cxy = cx[i] * cy[j];
     const int itxy = ((j & 1) << 1) | (i & 1);
     for (int k = k0; k <= k1; ++k) {
         const int c = g.idx(i, j, k);
         const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
-        const float vx1 = tau[it], vx2 = tau[8 + it];
-        /* 8-cell harmonic / arithmetic averages, viscoop.f:104-124 */
-        float xl = 8.0f / (lam[c] + lam[c + 1] + lam[c - sy] + lam[c + 1 - sy] +
-                           lam[c - sz] + lam[c + 1 - sz] + lam[c - sy - sz] + lam[c + 1 - sy - sz]);
-        const float xm = 8.0f / (mu[c] + mu[c + 1] + mu[c - sy] + mu[c + 1 - sy] +
-                                 mu[c - sz] + mu[c + 1 - sz] + mu[c - sy - sz] + mu[c + 1 - sy - sz]);
-        float qpa = 0.f, qsa = 0.f;
-        if (nve == 1) {
-            qpa = 0.125f * (qp[c] + qp[c + 1] + qp[c - sy] + qp[c + 1 - sy] +
-                            qp[c - sz] + qp[c + 1 - sz] + qp[c - sy - sz] + qp[c + 1 - sy - sz]);
-            qsa = 0.125f * (qs[c] + qs[c + 1] + qs[c - sy] + qs[c + 1 - sy] +
-                            qs[c - sz] + qs[c + 1 - sz] + qs[c - sy - sz] + qs[c + 1 - sy - sz]);
-        }
-        const float xmu4 = 2.0f / (mu[c] + mu[c - sz]);
-        const float xmu5 = 2.0f / (mu[c] + mu[c - sy]);
-        const float xmu6 = 2.0f / (mu[c] + mu[c + 1]);
+        const StrCoef kc = str_coef(md, c, sy, sz, nve, tau[it], tau[8 + it]);
         const float crj = cxy * cz[k];
-        if (nve == 1) {
-            xl = xl + 2.0f * xm;
-            const float aas4 = 0.5f * (qs[c] + qs[c - sz]);
-            const float aas5 = 0.5f * (qs[c] + qs[c - sy]);
-            const float aas6 = 0.5f * (qs[c] + qs[c + 1]);
-            const float vh1 = -(xm * qsa);
-            const float vh2_r4 = -(aas4 * xmu4 / 2.0f);
-            const float vh2_r5 = -(aas5 * xmu5 / 2.0f);
-            const float vh2_r6 = -(aas6 * xmu6 / 2.0f);
 #pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                const float *__restrict__ u1 = cs.c[q].f[AF_U];
-                const float *__restrict__ v1 = cs.c[q].f[AF_V];
-                const float *__restrict__ w1 = cs.c[q].f[AF_W];
-                float *__restrict__ xx = cs.c[q].f[AF_XX];
-                float *__restrict__ yy = cs.c[q].f[AF_YY];
-                float *__restrict__ zz = cs.c[q].f[AF_ZZ];
-                float *__restrict__ xy = cs.c[q].f[AF_XY];
-                float *__restrict__ xz = cs.c[q].f[AF_XZ];
-                float *__restrict__ yz = cs.c[q].f[AF_YZ];
-                float *__restrict__ r1 = cs.c[q].f[AF_R1];
-                float *__restrict__ r2 = cs.c[q].f[AF_R2];
-                float *__restrict__ r3 = cs.c[q].f[AF_R3];
-                float *__restrict__ r4 = cs.c[q].f[AF_R4];
-                float *__restrict__ r5 = cs.c[q].f[AF_R5];
-                float *__restrict__ r6 = cs.c[q].f[AF_R6];
-                const float vt1 = C1 * (u1[c + 1] - u1[c]) + C2 * (u1[c + 2] - u1[c - 1]);
-                const float vt2 = C1 * (v1[c] - v1[c - sy]) + C2 * (v1[c + sy] - v1[c - 2 * sy]);
-                const float vt3 = C1 * (w1[c] - w1[c - sz]) + C2 * (w1[c + sz] - w1[c - 2 * sz]);
-                const float vt4 = C1 * (u1[c + sy] - u1[c]) + C2 * (u1[c + 2 * sy] - u1[c - sy]) +
-                                  C1 * (v1[c] - v1[c - 1]) + C2 * (v1[c + 1] - v1[c - 2]);
-                const float vt5 = C1 * (u1[c + sz] - u1[c]) + C2 * (u1[c + 2 * sz] - u1[c - sz]) +
-                                  C1 * (w1[c] - w1[c - 1]) + C2 * (w1[c + 1] - w1[c - 2]);
-                const float vt6 = C1 * (v1[c + sz] - v1[c]) + C2 * (v1[c + 2 * sz] - v1[c - sz]);
-                const float vt7 = C1 * (w1[c + sy] - w1[c]) + C2 * (w1[c + 2 * sy] - w1[c - sy]);
-                const float vtmp = xl * (vt1 + vt2 + vt3);
-                const float va1 = -(qpa * xl * dh1 * (vt1 + vt2 + vt3) / 2.0f);
-                const float o1 = r1[c], o2 = r2[c], o3 = r3[c], o4 = r4[c], o5 = r5[c], o6 = r6[c];
-                float sxx = xx[c] + dth * (vtmp - 2.0f * xm * (vt2 + vt3)) + dt * o1;
-                float syy = yy[c] + dth * (vtmp - 2.0f * xm * (vt1 + vt3)) + dt * o2;
-                float szz = zz[c] + dth * (vtmp - 2.0f * xm * (vt1 + vt2)) + dt * o3;
-                float sxy = xy[c] + xmu4 * dth * vt4 + dt * o4;
-                float sxz = xz[c] + xmu5 * dth * vt5 + dt * o5;
-                float syz = yz[c] + xmu6 * (dth * vt6 + dth * vt7) + dt * o6;
-                const float n1 = (vx2 * o1 - vh1 * (vt2 + vt3) * dh1 + va1) * vx1;
-                const float n2 = (vx2 * o2 - vh1 * (vt1 + vt3) * dh1 + va1) * vx1;
-                const float n3 = (vx2 * o3 - vh1 * (vt1 + vt2) * dh1 + va1) * vx1;
-                const float n4 = (vx2 * o4 + vh2_r4 * dh1 * vt4) * vx1;
-                const float n5 = (vx2 * o5 + vh2_r5 * dh1 * vt5) * vx1;
-                const float n6 = (vx2 * o6 + vh2_r6 * dh1 * (vt6 + vt7)) * vx1;
-                r1[c] = n1; r2[c] = n2; r3[c] = n3; r4[c] = n4; r5[c] = n5; r6[c] = n6;
-                sxx = sxx + dt * n1;
-                syy = syy + dt * n2;
-                szz = szz + dt * n3;
-                sxy = sxy + dt * n4;
-                sxz = sxz + dt * n5;
-                syz = syz + dt * n6;
-                xx[c] = sxx * crj; yy[c] = syy * crj; zz[c] = szz * crj;
-                xy[c] = sxy * crj; xz[c] = sxz * crj; yz[c] = syz * crj;
-            }
-        } else {
-            /* elastic, operator.f:348-571 */
-            const float a = xl + 2.0f * xm, b = xl;
+        for (int q = 0; q < NC; ++q) {
+            AwpComp &cp = cs.c[q];
+            const GVel V{cp.f[AF_U], cp.f[AF_V], cp.f[AF_W], c, sy, sz};
+            const Stress6 s{cp.f[AF_XX][c], cp.f[AF_YY][c], cp.f[AF_ZZ][c], cp.f[AF_XY][c], cp.f[AF_XZ][c], cp.f[AF_YZ][c]};
+            Stress6 o;
+            if (nve == 1) {
+                float r[6];
 #pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                const float *__restrict__ u1 = cs.c[q].f[AF_U];
-                const float *__restrict__ v1 = cs.c[q].f[AF_V];
-                const float *__restrict__ w1 = cs.c[q].f[AF_W];
-                float *__restrict__ xx = cs.c[q].f[AF_XX];
-                float *__restrict__ yy = cs.c[q].f[AF_YY];
-                float *__restrict__ zz = cs.c[q].f[AF_ZZ];
-                float *__restrict__ xy = cs.c[q].f[AF_XY];
-                float *__restrict__ xz = cs.c[q].f[AF_XZ];
-                float *__restrict__ yz = cs.c[q].f[AF_YZ];
-                const float u_a = C1 * (u1[c + 1] - u1[c]), u_b = C2 * (u1[c + 2] - u1[c - 1]);
-                const float v_a = C1 * (v1[c] - v1[c - sy]), v_b = C2 * (v1[c + sy] - v1[c - 2 * sy]);
-                const float w_a = C1 * (w1[c] - w1[c - sz]), w_b = C2 * (w1[c + sz] - w1[c - 2 * sz]);
-                const float sxx = xx[c] + dth * a * (u_a + u_b) + dth * b * (v_a + v_b + w_a + w_b);
-                const float syy = yy[c] + dth * a * (v_a + v_b) + dth * b * (u_a + u_b + w_a + w_b);
-                const float szz = zz[c] + dth * a * (w_a + w_b) + dth * b * (u_a + u_b + v_a + v_b);
-                const float sxy = xy[c] + dth * xmu4 * (C1 * (u1[c + sy] - u1[c]) + C2 * (u1[c + 2 * sy] - u1[c - sy]) +
-                                                        C1 * (v1[c] - v1[c - 1]) + C2 * (v1[c + 1] - v1[c - 2]));
-                const float sxz = xz[c] + dth * xmu5 * (C1 * (u1[c + sz] - u1[c]) + C2 * (u1[c + 2 * sz] - u1[c - sz]) +
-                                                        C1 * (w1[c] - w1[c - 1]) + C2 * (w1[c + 1] - w1[c - 2]));
-                const float syz = yz[c] + dth * xmu6 * (C1 * (v1[c + sz] - v1[c]) + C2 * (v1[c + 2 * sz] - v1[c - sz]) +
-                                                        C1 * (w1[c + sy] - w1[c]) + C2 * (w1[c + 2 * sy] - w1[c - sy]));
-                xx[c] = sxx * crj; yy[c] = syy * crj; zz[c] = szz * crj;
-                xy[c] = sxy * crj; xz[c] = sxz * crj; yz[c] = syz * crj;
+                for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
+                const VelDiff d = vel_diff(V);
+                o = str_visco(kc, d, s, r, dth, dt, dh1);
+#pragma unroll
+                for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
+            } else {
+                o = str_elastic(kc, V, s, dth);
             }
+            cp.f[AF_XX][c] = o.xx * crj; cp.f[AF_YY][c] = o.yy * crj; cp.f[AF_ZZ][c] = o.zz * crj;
+            cp.f[AF_XY][c] = o.xy * crj; cp.f[AF_XZ][c] = o.xz * crj; cp.f[AF_YZ][c] = o.yz * crj;
         }
     }
-    if (fuse_fstr && k1 == g.nz) {
+    if (k1 == g.nz) {
         /* fstr (operator.f:594-606) on this thread's own column */
         const int c = g.idx(i, j, g.nz);
 #pragma unroll
@@ -395,6 +319,174 @@ k_str(AwpGeom g, AwpMedia md, AwpCompSet<NC> cs,
             yz[c + 2 * sz] = -__ldcg(&yz[c - 2 * sz]);
             xz[c] = 0.0f;
             yz[c] = 0.0f;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* fused stepper                                                       */
+/* ------------------------------------------------------------------ */
+
+#define FX 32                      /* tile width (one warp along x)      */
+#define FSLOT 6                    /* velocity levels kept in the ring   */
+
+/* velocity accessor over the shared-memory ring (fused stress phase) */
+template <int RX>
+struct SVel {
+    const float *lat_u, *lat_v, *lat_w;   /* level k planes, at the cell    */
+    const float *zu[5], *zv[5], *zw[5];   /* levels k-2..k+2, at the cell   */
+    __device__ __forceinline__ float u(int dx, int dy, int dz) const { return dz ? zu[dz + 2][0] : lat_u[dy * RX + dx]; }
+    __device__ __forceinline__ float v(int dx, int dy, int dz) const { return dz ? zv[dz + 2][0] : lat_v[dy * RX + dx]; }
+    __device__ __forceinline__ float w(int dx, int dy, int dz) const { return dz ? zw[dz + 2][0] : lat_w[dy * RX + dx]; }
+};
+
+template <int NC, class TM, class TR, int TY>
+__global__ void __launch_bounds__(FX * TY)
+k_fused(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> old, AwpCompSet<NC> nw, const float *__restrict__ cx,
+        const float *__restrict__ cy, const float *__restrict__ cz, const float *__restrict__ tau, float dth,
+        float dt, float dh1, int kchunk, int nve)
+{
+    constexpr int RX = FX + 4, RY = TY + 4, NV = RX * RY, NT = FX * TY;
+    constexpr int PLANE = 3 * NC * NV;                 /* one ring slot      */
+    extern __shared__ float ring[];                    /* [FSLOT][NC][3][NV] */
+    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * FX + tx;
+    const int x0 = blockIdx.x * FX + 1, y0 = blockIdx.y * TY + 1;
+    int k0, k1;
+    zchunk(g, kchunk, k0, k1);
+    const int sy = g.px, sz = g.plane, nz = g.nz;
+
+    /* this thread's cell in the stress phase */
+    const int is = x0 + tx, js = y0 + ty;
+    const bool sact = is <= g.nx && js <= g.ny;
+    const int lps = (ty + 2) * RX + (tx + 2);
+    const float cxy_s = sact ? cx[is] * cy[js] : 0.f;
+    const int itxy = ((js & 1) << 1) | (is & 1);
+    float hzz[NC], hxz[NC][2], hyz[NC][2];             /* new values below k  */
+#pragma unroll
+    for (int q = 0; q < NC; ++q) { hzz[q] = 0.f; hxz[q][0] = hxz[q][1] = hyz[q][0] = hyz[q][1] = 0.f; }
+
+    for (int m = k0 - 2; m <= k1 + 2; ++m) {
+        /* ---- velocity at level m on the tile plus a 2-cell halo ---- */
+        float *sl = ring + ((m + 2 * FSLOT) % FSLOT) * PLANE;
+        for (int vcell = t; vcell < NV; vcell += NT) {
+            const int lx = vcell % RX, ly = vcell / RX;
+            const int i = x0 - 2 + lx, j = y0 - 2 + ly;
+            const bool inside = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+            const bool inter = lx >= 2 && lx < FX + 2 && ly >= 2 && ly < TY + 2;
+            float val[NC][3];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) val[q][0] = val[q][1] = val[q][2] = 0.f;
+            if (inside && m >= 1 && m <= nz) {
+                const int c = g.idx(i, j, m);
+                float fu, fv, fw;
+                vel_factors(md, c, sy, sz, dth, fu, fv, fw);
+                const float crj = (cx[i] * cy[j]) * cz[m];
+                const bool own = inter && m >= k0 && m <= k1;
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    float u, v, w;
+                    vel_one(old.c[q], c, sy, sz, fu, fv, fw, u, v, w);
+                    val[q][0] = u * crj; val[q][1] = v * crj; val[q][2] = w * crj;
+                    if (own) {
+                        nw.c[q].f[AF_U][c] = val[q][0];
+                        nw.c[q].f[AF_V][c] = val[q][1];
+                        nw.c[q].f[AF_W][c] = val[q][2];
+                    }
+                }
+            } else if (inside && inter && m == nz + 1) {
+                /* fvelxy + fvelz from level nz (and w at nz-1) of the ring */
+                const float *p0 = ring + ((nz + 2 * FSLOT) % FSLOT) * PLANE;
+                const float *p1 = ring + ((nz - 1 + 2 * FSLOT) % FSLOT) * PLANE;
+                const int ct = g.idx(i, j, nz);
+                const float xl = 1.0f / md(AM_LAM, ct);
+                const float xl2m = 2.0f / md(AM_MU, ct) + xl;
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    const float *U = p0 + (q * 3 + 0) * NV + vcell;
+                    const float *V = p0 + (q * 3 + 1) * NV + vcell;
+                    const float *W = p0 + (q * 3 + 2) * NV + vcell;
+                    const float u_fs = U[0] - (W[0] - W[-1]);
+                    const float v_fs = V[0] - (W[RX] - W[0]);
+                    const float u_fs_e = (i + 1 <= g.nx) ? (U[1] - (W[1] - W[0])) : 0.0f;
+                    const float v_fs_s = (j - 1 >= 1) ? (V[-RX] - (W[0] - W[-RX])) : 0.0f;
+                    const float w_fs = p1[(q * 3 + 2) * NV + vcell] - (xl / xl2m) * (
+                        (u_fs_e - u_fs) + (U[1] - U[0]) + (v_fs - v_fs_s) + (V[0] - V[-RX]));
+                    val[q][0] = u_fs; val[q][1] = v_fs; val[q][2] = w_fs;
+                    if (k1 == nz) {
+                        nw.c[q].f[AF_U][ct + sz] = u_fs;
+                        nw.c[q].f[AF_V][ct + sz] = v_fs;
+                        nw.c[q].f[AF_W][ct + sz] = w_fs;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                sl[(q * 3 + 0) * NV + vcell] = val[q][0];
+                sl[(q * 3 + 1) * NV + vcell] = val[q][1];
+                sl[(q * 3 + 2) * NV + vcell] = val[q][2];
+            }
+        }
+        __syncthreads();
+
+        /* ---- stress + memory variables at level k = m - 2 on the tile ---- */
+        const int k = m - 2;
+        if (k >= k0 && k <= k1 && sact) {
+            const int c = g.idx(is, js, k);
+            const int it = (((nz + 1 - k) & 1) << 2) | itxy;
+            const StrCoef kc = str_coef(md, c, sy, sz, nve, tau[it], tau[8 + it]);
+            const float crj = cxy_s * cz[k];
+            const float *lv = ring + ((k + 2 * FSLOT) % FSLOT) * PLANE + lps;
+            const float *zl[5];
+#pragma unroll
+            for (int d = 0; d < 5; ++d) zl[d] = ring + ((k - 2 + d + 2 * FSLOT) % FSLOT) * PLANE + lps;
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                SVel<RX> V;
+                V.lat_u = lv + (q * 3 + 0) * NV;
+                V.lat_v = lv + (q * 3 + 1) * NV;
+                V.lat_w = lv + (q * 3 + 2) * NV;
+#pragma unroll
+                for (int d = 0; d < 5; ++d) {
+                    V.zu[d] = zl[d] + (q * 3 + 0) * NV;
+                    V.zv[d] = zl[d] + (q * 3 + 1) * NV;
+                    V.zw[d] = zl[d] + (q * 3 + 2) * NV;
+                }
+                const AwpComp &o = old.c[q];
+                const Stress6 s{o.f[AF_XX][c], o.f[AF_YY][c], o.f[AF_ZZ][c], o.f[AF_XY][c], o.f[AF_XZ][c], o.f[AF_YZ][c]};
+                Stress6 ns;
+                if (nve == 1) {
+                    float r[6];
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)o.f[AF_R1 + a], c, 1.0f);
+                    const VelDiff d = vel_diff(V);
+                    ns = str_visco(kc, d, s, r, dth, dt, dh1);
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)o.f[AF_R1 + a], c, r[a], 1.0f);
+                } else {
+                    ns = str_elastic(kc, V, s, dth);
+                }
+                ns.xx = ns.xx * crj; ns.yy = ns.yy * crj; ns.zz = ns.zz * crj;
+                ns.xy = ns.xy * crj; ns.xz = ns.xz * crj; ns.yz = ns.yz * crj;
+                AwpComp &n = nw.c[q];
+                n.f[AF_XX][c] = ns.xx; n.f[AF_YY][c] = ns.yy; n.f[AF_ZZ][c] = ns.zz; n.f[AF_XY][c] = ns.xy;
+                if (k == nz) {
+                    /* fstr (operator.f:594-606) from this thread's own column */
+                    n.f[AF_ZZ][c + sz] = -ns.zz;
+                    n.f[AF_ZZ][c + 2 * sz] = -hzz[q];
+                    n.f[AF_XZ][c + sz] = -hxz[q][0];
+                    n.f[AF_XZ][c + 2 * sz] = -hxz[q][1];
+                    n.f[AF_YZ][c + sz] = -hyz[q][0];
+                    n.f[AF_YZ][c + 2 * sz] = -hyz[q][1];
+                    n.f[AF_XZ][c] = 0.0f;
+                    n.f[AF_YZ][c] = 0.0f;
+                } else {
+                    n.f[AF_XZ][c] = ns.xz;
+                    n.f[AF_YZ][c] = ns.yz;
+                }
+                hzz[q] = ns.zz;
+                hxz[q][1] = hxz[q][0]; hxz[q][0] = ns.xz;
+                hyz[q][1] = hyz[q][0]; hyz[q][0] = ns.yz;
+            }
         }
     }
 }
@@ -416,6 +508,15 @@ __device__ void fstr_column(const AwpGeom &g, AwpComp &cp, int i, int j)
     yz[c + 2 * sz] = -yz[c - 2 * sz];
     xz[c] = 0.0f;
     yz[c] = 0.0f;
+}
+
+__device__ __forceinline__ float d1_at(const AwpPostArgs &a, int c)
+{
+    switch (a.media_type) {
+    case 1: return __bfloat162float(((const __nv_bfloat16 *)a.d1)[c]);
+    case 2: return __half2float(((const __half *)a.d1)[c]) * a.d1_inv;
+    default: return ((const float *)a.d1)[c];
+    }
 }
 
 /* One block; thread q handles component q and walks its sources in order,
@@ -451,18 +552,18 @@ __global__ void k_post(AwpPostArgs a, int initial)
                 cp.f[AF_XY][c] = cp.f[AF_XY][c] - a.vtst * axy;
                 break;
             case 1:
-                cp.f[AF_U][c] = cp.f[AF_U][c] + axx * a.vtst / a.d1[c];
+                cp.f[AF_U][c] = cp.f[AF_U][c] + axx * a.vtst / d1_at(a, c);
                 break;
             case 2:
-                cp.f[AF_V][c] = cp.f[AF_V][c] + ayy * a.vtst / a.d1[c];
+                cp.f[AF_V][c] = cp.f[AF_V][c] + ayy * a.vtst / d1_at(a, c);
                 break;
             case 3:
-                cp.f[AF_W][c] = cp.f[AF_W][c] + azz * a.vtst / a.d1[c];
+                cp.f[AF_W][c] = cp.f[AF_W][c] + azz * a.vtst / d1_at(a, c);
                 break;
             case -2:
-                cp.f[AF_U][c] = cp.f[AF_U][c] + axx * a.vtst / a.d1[c];
-                cp.f[AF_V][c] = cp.f[AF_V][c] + ayy * a.vtst / a.d1[c];
-                cp.f[AF_W][c] = cp.f[AF_W][c] + azz * a.vtst / a.d1[c];
+                cp.f[AF_U][c] = cp.f[AF_U][c] + axx * a.vtst / d1_at(a, c);
+                cp.f[AF_V][c] = cp.f[AF_V][c] + ayy * a.vtst / d1_at(a, c);
+                cp.f[AF_W][c] = cp.f[AF_W][c] + azz * a.vtst / d1_at(a, c);
                 break;
             case 4: {
                 float *F = cp.f[AF_XZ];
@@ -513,6 +614,7 @@ __global__ void k_sgt(AwpSgtArgs a)
     const int s = n / a.ntiskp - 1;
     if (s >= a.nsamp_written) return;
     const int p = t % a.npts, q = t / a.npts;
+    if (!a.active[q]) return;   /* no SGT output for moment sources (pmcl3d.f:1536) */
     const int c = a.pt_idx[p];
     const float sg1 = a.sg[3 * p], sg2 = a.sg[3 * p + 1], sg3 = a.sg[3 * p + 2];
     const AwpComp &cp = a.comp[q];
@@ -562,36 +664,123 @@ cudaError_t awp_launch_media_homo(const AwpGeom &g, const AwpMedia &md, float la
     return cudaGetLastError();
 }
 
-cudaError_t awp_launch_sg_coeffs(const AwpGeom &g, const AwpMedia &md, int npts, const int *pt_idx, float *sg,
-                                 cudaStream_t st)
+cudaError_t awp_launch_media_range(const AwpMedia &md, int64_t n, unsigned *mx, unsigned *mn, cudaStream_t st)
+{
+    k_media_range<<<148 * 4, 256, 0, st>>>(md, n, mx, mn);
+    return cudaGetLastError();
+}
+
+cudaError_t awp_launch_media_convert(const AwpMedia &src, const AwpMediaT &dst, int64_t n, cudaStream_t st)
+{
+    if (dst.type == AWP_STORE_BF16)
+        k_media_convert<__nv_bfloat16><<<148 * 8, 256, 0, st>>>(src, dst.m[0], dst.m[1], dst.m[2], dst.m[3], dst.m[4],
+                                                               dst.sc, n);
+    else if (dst.type == AWP_STORE_F16)
+        k_media_convert<__half><<<148 * 8, 256, 0, st>>>(src, dst.m[0], dst.m[1], dst.m[2], dst.m[3], dst.m[4],
+                                                        dst.sc, n);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+template <class TM>
+static MediaT<TM> media_view(const AwpMediaT &m)
+{
+    MediaT<TM> v;
+    for (int a = 0; a < AM_N; ++a) {
+        v.m[a] = (const TM *)m.m[a];
+        v.inv[a] = m.sc.inv[a];
+    }
+    return v;
+}
+
+cudaError_t awp_launch_sg_coeffs(const AwpMediaT &md, int npts, const int *pt_idx, float *sg, cudaStream_t st)
 {
     if (npts <= 0) return cudaSuccess;
-    k_sg_coeffs<<<(npts + 255) / 256, 256, 0, st>>>(g, md, npts, pt_idx, sg);
+    const int nb = (npts + 255) / 256;
+    switch (md.type) {
+    case AWP_STORE_BF16: k_sg_coeffs<__nv_bfloat16><<<nb, 256, 0, st>>>(media_view<__nv_bfloat16>(md), npts, pt_idx, sg); break;
+    case AWP_STORE_F16: k_sg_coeffs<__half><<<nb, 256, 0, st>>>(media_view<__half>(md), npts, pt_idx, sg); break;
+    default: k_sg_coeffs<float><<<nb, 256, 0, st>>>(media_view<float>(md), npts, pt_idx, sg); break;
+    }
     return cudaGetLastError();
 }
 
 template <int NC>
-static cudaError_t launch_step_nc(const AwpStepArgs &s, cudaStream_t st)
+static void comp_sets(const AwpStepArgs &s, AwpCompSet<NC> &a, AwpCompSet<NC> &b)
 {
-    AwpCompSet<NC> cs;
-    for (int q = 0; q < NC; ++q) cs.c[q] = s.comp[q];
-    dim3 b(32, 8);
+    for (int q = 0; q < NC; ++q) { a.c[q] = s.comp[q]; b.c[q] = s.comp_new[q]; }
+}
+
+template <int TY, int NC>
+static size_t fused_smem() { return (size_t)FSLOT * 3 * NC * (FX + 4) * (TY + 4) * sizeof(float); }
+
+template <int NC, class TM, class TR>
+static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st)
+{
+    AwpCompSet<NC> cs, cn;
+    comp_sets<NC>(s, cs, cn);
+    const MediaT<TM> md = media_view<TM>(s.md);
     const int nzb = (s.g.nz + s.kchunk - 1) / s.kchunk;
-    k_vel<NC><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, s.md.m[AM_D1], cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
-    k_fsvel<NC><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, s.md.m[AM_LAM], s.md.m[AM_MU], cs);
-    k_str<NC><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, s.md, cs, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1,
-                                                     s.kchunk, s.nve, 1);
+    if (part == AWP_PART_VEL) {
+        dim3 b(32, 8);
+        k_vel<NC, TM><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
+    } else if (part == AWP_PART_FSVEL) {
+        dim3 b(32, 8);
+        k_fsvel<NC, TM><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, md, cs);
+    } else if (part == AWP_PART_STR) {
+        dim3 b(32, 8);
+        k_str<NC, TM, TR><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
+                                                                 s.dt, s.dh1, s.kchunk, s.nve);
+    } else if (part == AWP_PART_FUSED) {
+        constexpr int TY = 8;
+        dim3 b(FX, TY);
+        const size_t smem = fused_smem<TY, NC>();
+        static unsigned long long attr_done = 0;   /* per instantiation, bit per device */
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 64 || !(attr_done & (1ull << dev))) {
+            cudaError_t e = cudaFuncSetAttribute(k_fused<NC, TM, TR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            if (dev < 64) attr_done |= 1ull << dev;
+        }
+        k_fused<NC, TM, TR, TY><<<plane_grid(s.g, b, nzb), b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau,
+                                                                         s.dth, s.dt, s.dh1, s.kchunk, s.nve);
+    } else {
+        return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
+}
+
+template <int NC>
+static cudaError_t launch_part_nc(const AwpStepArgs &s, int part, cudaStream_t st)
+{
+    switch (s.md.type) {
+    case AWP_STORE_BF16: return launch_part_t<NC, __nv_bfloat16, __nv_bfloat16>(s, part, st);
+    case AWP_STORE_F16: return launch_part_t<NC, __half, __nv_bfloat16>(s, part, st);
+    default: return launch_part_t<NC, float, float>(s, part, st);
+    }
+}
+
+cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st)
+{
+    switch (s.ncomp) {
+    case 1: return launch_part_nc<1>(s, part, st);
+    case 2: return launch_part_nc<2>(s, part, st);
+    case 3: return launch_part_nc<3>(s, part, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st)
 {
-    switch (s.ncomp) {
-    case 1: return launch_step_nc<1>(s, st);
-    case 2: return launch_step_nc<2>(s, st);
-    case 3: return launch_step_nc<3>(s, st);
-    default: return cudaErrorInvalidValue;
+    if (s.fused) return awp_launch_part(s, AWP_PART_FUSED, st);
+    for (int part = 0; part < 3; ++part) {
+        cudaError_t e = awp_launch_part(s, part, st);
+        if (e != cudaSuccess) return e;
     }
+    return cudaSuccess;
 }
 
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st)

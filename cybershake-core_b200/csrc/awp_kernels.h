@@ -7,14 +7,16 @@
 
 struct AwpStepArgs {
     AwpGeom g;
-    AwpMedia md;
+    AwpMediaT md;                /* typed media                             */
     int ncomp;
-    AwpComp comp[3];
-    const float *cx, *cy, *cz;   /* sponge factors, index 1..n            */
-    const float *tau;            /* [16] tau1[8] then tau2[8]              */
+    AwpComp comp[3];             /* wavefields read (two-sweep: updated)    */
+    AwpComp comp_new[3];         /* fused: wavefields written (ping-pong)   */
+    const float *cx, *cy, *cz;   /* sponge factors, index 1..n              */
+    const float *tau;            /* [16] tau1[8] then tau2[8]               */
     float dth, dt, dh1;
-    int kchunk;                  /* z levels per thread block              */
+    int kchunk;                  /* z levels per thread block               */
     int nve;
+    int fused;                   /* 1: single-sweep stepper                 */
 };
 
 cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, const float *raw, int zf0, int nzs,
@@ -23,9 +25,14 @@ cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, cons
 cudaError_t awp_launch_media_ghosts(const AwpGeom &g, const AwpMedia &md, int nve, cudaStream_t st);
 cudaError_t awp_launch_media_homo(const AwpGeom &g, const AwpMedia &md, float lam, float mu, float d1,
                                   cudaStream_t st);
-cudaError_t awp_launch_sg_coeffs(const AwpGeom &g, const AwpMedia &md, int npts, const int *pt_idx, float *sg,
-                                 cudaStream_t st);
-/* velocity sweep, free-surface velocity, stress sweep (+ fused fstr) */
+cudaError_t awp_launch_media_range(const AwpMedia &md, int64_t n, unsigned *mx, unsigned *mn, cudaStream_t st);
+cudaError_t awp_launch_media_convert(const AwpMedia &src, const AwpMediaT &dst, int64_t n, cudaStream_t st);
+cudaError_t awp_launch_sg_coeffs(const AwpMediaT &md, int npts, const int *pt_idx, float *sg, cudaStream_t st);
+
+/* the kernels of one step */
+enum { AWP_PART_VEL = 0, AWP_PART_FSVEL = 1, AWP_PART_STR = 2, AWP_PART_FUSED = 3 };
+cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st);
+/* two-sweep: velocity, free-surface velocity, stress (+ fstr); fused: one kernel */
 cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);

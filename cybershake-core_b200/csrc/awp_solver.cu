@@ -6,6 +6,11 @@
  *   relax.f:4-39 (tausub), viscoop.f:79-88 (tau1/tau2), cerjan.f:4-247 (1-D
  *   sponge factors), structure.f:461-468 (Q-band constants), source.f:834-835,
  *   station.f:31-80 (point location), pmcl3d.f:1589-1601 (file offsets).
+ *
+ * Steppers: the fused single-sweep kernel (default) reads one wavefield
+ * buffer and writes the other, alternating every step; the two-sweep stepper
+ * updates one buffer in place.  Memory variables r1..r6 are updated in place
+ * by both.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -42,12 +47,16 @@ struct awp_solver {
     awp_params p;
     AwpGeom g;
     cudaStream_t stream;
-    AwpComp comp[AWP_MAX_COMP];
-    AwpMedia md;
+    AwpComp comp[2][AWP_MAX_COMP];   /* [buffer][component]; r1..r6 shared  */
+    int fused;
+    int store;                       /* AWP_STORE_* of media and r1..r6     */
+    AwpMedia md;                     /* FP32 media (ingest)                 */
+    AwpMediaT mdt;                   /* media as the steppers read them     */
     float *cx, *cy, *cz;
     float *tau;
     int *step;
     int *ext;
+    unsigned *rng;                   /* [2][AM_N] media |value| max / min   */
     float *chkj[AWP_MAX_COMP];
     int nsrc[AWP_MAX_COMP];
     int *src_ijk[AWP_MAX_COMP];
@@ -68,8 +77,7 @@ struct awp_solver {
     cudaEvent_t ev0, ev1;
     double loop_seconds;
     int64_t loop_steps;
-    cudaGraphExec_t graph;
-    int graph_steps;
+    cudaGraphExec_t graph[2];        /* by the parity of the first step    */
     double device_bytes;
 };
 
@@ -144,25 +152,38 @@ static int64_t file_floats_of(const awp_params *p, int npts)
     return n;
 }
 
+static int store_of(const awp_params *p)
+{
+    return p->precision == AWP_PREC_BF16 ? AWP_STORE_BF16 : p->precision == AWP_PREC_F16 ? AWP_STORE_F16 : AWP_STORE_F32;
+}
+static int fused_of(const awp_params *p) { return p->kernel != AWP_KERNEL_TWO_SWEEP; }
+static double media_word(int store) { return store == AWP_STORE_F32 ? 4.0 : 2.0; }
+
 extern "C" double awp_bytes_per_cell_update(const awp_params *p)
 {
     const int nc = p->ncomp < 1 ? 1 : p->ncomp;
-    const double mb = (p->precision == AWP_PREC_F32) ? 4.0 : 2.0;   /* media word  */
-    const double rb = (p->precision == AWP_PREC_F32) ? 4.0 : 2.0;   /* r1..r6 word */
+    const int st = store_of(p);
+    const double mb = media_word(st);
+    const double rb = mb;                              /* r1..r6 word       */
     const int nmedia = (p->nve == 1) ? 5 : 3;
-    const int nr = (p->nve == 1) ? 12 : 0;          /* r1..r6 read + write       */
-    /* two sweeps: velocity R 9 W 3 ; stress R 9 (u v w + 6 stresses) W 6 ; r R+W */
-    const double state = 12 * 4.0 + 15 * 4.0 + nr * rb;
+    const int nr = (p->nve == 1) ? 12 : 0;             /* r1..r6 read+write */
+    double state;
+    if (fused_of(p))
+        state = 18 * 4.0 + nr * rb;                    /* u v w + 6 stresses R+W */
+    else
+        state = 12 * 4.0 + 15 * 4.0 + nr * rb;         /* vel R9 W3; stress R9 W6 */
     return (nc * state + nmedia * mb) / nc;
 }
 
-static int choose_kchunk(const AwpGeom &g)
+static int choose_kchunk(const AwpGeom &g, int fused)
 {
     const int bxy = ((g.nx + 31) / 32) * ((g.ny + 7) / 8);
-    int nzb = (148 * 8 + bxy - 1) / bxy;
+    const int want = fused ? 148 * 4 : 148 * 8;
+    int nzb = (want + bxy - 1) / bxy;
     if (nzb < 1) nzb = 1;
     int kc = (g.nz + nzb - 1) / nzb;
-    if (kc < 8) kc = 8;
+    const int kmin = fused ? 24 : 8;   /* fused: 4 redundant velocity levels per chunk */
+    if (kc < kmin) kc = kmin;
     if (kc > g.nz) kc = g.nz;
     return kc;
 }
@@ -171,7 +192,12 @@ extern "C" int64_t awp_footprint_bytes(const awp_params *p, int npts)
 {
     AwpGeom g = make_geom(p);
     const int nc = p->ncomp < 1 ? 1 : p->ncomp;
-    int64_t b = (int64_t)g.vol * 4 * (AWP_NF_STATE * nc + AM_N);
+    const int st = store_of(p);
+    const double mb = media_word(st);
+    const int nbuf = fused_of(p) ? 2 : 1;
+    int64_t b = (int64_t)g.vol * (int64_t)(nc * (9 * 4 * nbuf + (p->nve == 1 ? 6 * mb : 0)));
+    b += (int64_t)g.vol * (int64_t)(AM_N * 4);                        /* FP32 media during ingest */
+    if (st != AWP_STORE_F32) b += (int64_t)g.vol * (int64_t)(AM_N * mb);
     b += file_floats_of(p, npts) * 4 * nc;
     b += (int64_t)p->nt * 12 * nc;
     b += (int64_t)npts * 16;
@@ -191,20 +217,36 @@ static float crj_high(float alpha, int nd, int n, int g)
     return expf(-(a * a));
 }
 
+static void free_media32(awp_solver *s)
+{
+    for (int m = 0; m < AM_N; m++) {
+        if (s->md.m[m] && (void *)s->md.m[m] != s->mdt.m[m]) {
+            cudaFree(s->md.m[m]);
+            s->device_bytes -= (double)s->g.vol * 4;
+        }
+        s->md.m[m] = NULL;
+    }
+}
+
 static void free_all(awp_solver *s)
 {
     if (!s) return;
-    if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (int b = 0; b < 2; b++)
+        if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
     for (int q = 0; q < AWP_MAX_COMP; q++) {
-        for (int f = 0; f < AWP_NF_STATE; f++) cudaFree(s->comp[q].f[f]);
+        for (int f = 0; f < AWP_NF_STATE; f++) {
+            cudaFree(s->comp[0][q].f[f]);
+            if (f < AF_R1 && s->comp[1][q].f[f] != s->comp[0][q].f[f]) cudaFree(s->comp[1][q].f[f]);
+        }
         cudaFree(s->chkj[q]);
         cudaFree(s->src_ijk[q]);
         cudaFree(s->src_stf[q]);
         cudaFree(s->sgt_file[q]);
     }
-    for (int m = 0; m < AM_N; m++) cudaFree(s->md.m[m]);
+    free_media32(s);
+    for (int m = 0; m < AM_N; m++) cudaFree(s->mdt.m[m]);
     cudaFree(s->cx); cudaFree(s->cy); cudaFree(s->cz);
-    cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext);
+    cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext); cudaFree(s->rng);
     cudaFree(s->pt_idx); cudaFree(s->sg);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -233,7 +275,8 @@ static awp_status check_params(const awp_params *p)
     if (p->nst < 0) return set_err(AWP_ERR_PARAM, "NST must be >= 0");
     if (p->nvar != 3 && p->nvar != 5 && p->nvar != 8) return set_err(AWP_ERR_PARAM, "NVAR must be 3, 5 or 8");
     if (p->nve != 0 && p->nve != 1) return set_err(AWP_ERR_PARAM, "NVE must be 0 or 1");
-    if (p->precision != AWP_PREC_F32) return set_err(AWP_ERR_PARAM, "precision %d not available in this build", p->precision);
+    if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_F16) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
+    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_TWO_SWEEP) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
         int ig = p->igreen[q];
@@ -248,6 +291,19 @@ static awp_status check_params(const awp_params *p)
 /* create / destroy                                                    */
 /* ------------------------------------------------------------------ */
 
+static awp_status alloc_media32(awp_solver *s)
+{
+    const size_t vb = (size_t)s->g.vol * sizeof(float);
+    for (int m = 0; m < AM_N; m++) {
+        if (s->md.m[m]) continue;
+        awp_status st = dalloc(s, (void **)&s->md.m[m], vb);
+        if (st != AWP_OK) return st;
+        CU(cudaMemsetAsync(s->md.m[m], 0, vb, s->stream));
+        if (s->store == AWP_STORE_F32) s->mdt.m[m] = s->md.m[m];
+    }
+    return AWP_OK;
+}
+
 extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
 {
     *out = NULL;
@@ -259,24 +315,43 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     memset(s, 0, sizeof *s);
     s->p = *pin;
     s->g = make_geom(pin);
+    s->fused = fused_of(pin);
+    s->store = store_of(pin);
     const awp_params *p = &s->p;
     const size_t vb = (size_t)s->g.vol * sizeof(float);
+    const size_t rb = (size_t)s->g.vol * (s->store == AWP_STORE_F32 ? 4 : 2);
 #define TRY(x) do { awp_status t_ = (x); if (t_ != AWP_OK) { free_all(s); delete s; return t_; } } while (0)
 #define TRYCU(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { free_all(s); delete s; \
     return set_err(AWP_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); } } while (0)
     TRYCU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     TRYCU(cudaEventCreate(&s->ev0));
     TRYCU(cudaEventCreate(&s->ev1));
-    for (int q = 0; q < p->ncomp; q++)
+    for (int q = 0; q < p->ncomp; q++) {
         for (int f = 0; f < AWP_NF_STATE; f++) {
-            if (p->nve == 0 && f >= AF_R1) continue;
-            TRY(dalloc(s, (void **)&s->comp[q].f[f], vb));
-            TRYCU(cudaMemsetAsync(s->comp[q].f[f], 0, vb, s->stream));
+            if (f >= AF_R1) {
+                if (p->nve == 0) continue;
+                TRY(dalloc(s, (void **)&s->comp[0][q].f[f], rb));
+                TRYCU(cudaMemsetAsync(s->comp[0][q].f[f], 0, rb, s->stream));
+                s->comp[1][q].f[f] = s->comp[0][q].f[f];
+                continue;
+            }
+            TRY(dalloc(s, (void **)&s->comp[0][q].f[f], vb));
+            TRYCU(cudaMemsetAsync(s->comp[0][q].f[f], 0, vb, s->stream));
+            if (s->fused) {
+                TRY(dalloc(s, (void **)&s->comp[1][q].f[f], vb));
+                TRYCU(cudaMemsetAsync(s->comp[1][q].f[f], 0, vb, s->stream));
+            } else {
+                s->comp[1][q].f[f] = s->comp[0][q].f[f];
+            }
         }
-    for (int m = 0; m < AM_N; m++) {
-        TRY(dalloc(s, (void **)&s->md.m[m], vb));
-        TRYCU(cudaMemsetAsync(s->md.m[m], 0, vb, s->stream));
     }
+    s->mdt.type = s->store;
+    for (int m = 0; m < AM_N; m++) { s->mdt.sc.scale[m] = 1.0f; s->mdt.sc.inv[m] = 1.0f; }
+    if (s->store != AWP_STORE_F32)
+        for (int m = 0; m < AM_N; m++) {
+            TRY(dalloc(s, &s->mdt.m[m], (size_t)s->g.vol * 2));
+            TRYCU(cudaMemsetAsync(s->mdt.m[m], 0, (size_t)s->g.vol * 2, s->stream));
+        }
     /* sponge factors (cerjan.f:19-242): separable, both lateral faces and
      * the bottom damped, the free surface not */
     {
@@ -302,6 +377,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     TRY(dalloc(s, (void **)&s->step, sizeof(int)));
     TRYCU(cudaMemsetAsync(s->step, 0, sizeof(int), s->stream));
     TRY(dalloc(s, (void **)&s->ext, 8 * sizeof(int)));
+    TRY(dalloc(s, (void **)&s->rng, 2 * AM_N * sizeof(unsigned)));
     for (int q = 0; q < p->ncomp; q++) {
         TRY(dalloc(s, (void **)&s->chkj[q], sizeof(float) * 3 * (size_t)p->nt));
         TRYCU(cudaMemsetAsync(s->chkj[q], 0, sizeof(float) * 3 * (size_t)p->nt, s->stream));
@@ -310,7 +386,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->dh1 = 1.0f / p->dh;
     s->vtst = p->dt / (p->dh * p->dh * p->dh);     /* source.f:834-835 */
     s->vtst1 = 1.0f / (p->dh * p->dh);
-    s->kchunk = choose_kchunk(s->g);
+    s->kchunk = choose_kchunk(s->g, s->fused);
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
     TRYCU(cudaStreamSynchronize(s->stream));
@@ -356,6 +432,42 @@ static awp_status upload_tau(awp_solver *s, float taumin, float taumax)
     return AWP_OK;
 }
 
+/* FP32 media -> the storage the steppers read.  binary16 arrays are scaled
+ * by a power of two chosen from the array's largest magnitude; media whose
+ * nonzero magnitudes span more than binary16's normal range are rejected. */
+static awp_status convert_media(awp_solver *s)
+{
+    if (s->store == AWP_STORE_F32) return AWP_OK;
+    if (s->store == AWP_STORE_F16) {
+        unsigned init[2 * AM_N];
+        for (int a = 0; a < AM_N; a++) { init[a] = 0u; init[AM_N + a] = 0x7f800000u; }
+        CU(cudaMemcpyAsync(s->rng, init, sizeof init, cudaMemcpyHostToDevice, s->stream));
+        CU(awp_launch_media_range(s->md, s->g.vol, s->rng, s->rng + AM_N, s->stream));
+        unsigned r[2 * AM_N];
+        CU(cudaMemcpyAsync(r, s->rng, sizeof r, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaStreamSynchronize(s->stream));
+        for (int a = 0; a < AM_N; a++) {
+            float mx, mn;
+            memcpy(&mx, &r[a], 4);
+            memcpy(&mn, &r[AM_N + a], 4);
+            int e = 0;
+            if (mx > 0) {
+                frexpf(mx, &e);                         /* mx = f * 2^e, f in [0.5,1) */
+                e = 14 - e;                             /* scaled max in [2^13, 2^14) */
+                if (mn * ldexpf(1.0f, e) < ldexpf(1.0f, -14))
+                    return set_err(AWP_ERR_PARAM, "media array %d spans %g..%g, beyond binary16 range; use BF16 or F32",
+                                   a, (double)mn, (double)mx);
+            }
+            s->mdt.sc.scale[a] = ldexpf(1.0f, e);
+            s->mdt.sc.inv[a] = ldexpf(1.0f, -e);
+        }
+    }
+    CU(awp_launch_media_convert(s->md, s->mdt, s->g.vol, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    free_media32(s);
+    return AWP_OK;
+}
+
 static awp_status finish_media(awp_solver *s)
 {
     int e[8];
@@ -365,9 +477,11 @@ static awp_status finish_media(awp_solver *s)
     memcpy(&s->ext_host[0], &e[0], 4); memcpy(&s->ext_host[1], &e[3], 4);
     memcpy(&s->ext_host[2], &e[1], 4); memcpy(&s->ext_host[3], &e[4], 4);
     memcpy(&s->ext_host[4], &e[2], 4); memcpy(&s->ext_host[5], &e[5], 4);
+    awp_status st = convert_media(s);
+    if (st != AWP_OK) return st;
     s->media_loaded = 1;
     if (s->npts > 0) {
-        CU(awp_launch_sg_coeffs(s->g, s->md, s->npts, s->pt_idx, s->sg, s->stream));
+        CU(awp_launch_sg_coeffs(s->mdt, s->npts, s->pt_idx, s->sg, s->stream));
         CU(cudaStreamSynchronize(s->stream));
     }
     return AWP_OK;
@@ -380,6 +494,8 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx)
     const awp_params *p = &s->p;
     CU(cudaSetDevice(p->device));
     if (s->started) return set_err(AWP_ERR_STATE, "media must be loaded before the first step (or after awp_reset)");
+    awp_status ast = alloc_media32(s);
+    if (ast != AWP_OK) return ast;
     const float pi = 4.0f * atanf(1.0f);
     if (p->mediastart == 0) {
         /* inihomo, structure.f:725-762 */
@@ -416,19 +532,28 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx)
     int nzs = (int)((64ull << 20) / (per_level * sizeof(float)));
     if (nzs < 1) nzs = 1;
     if (nzs > p->nz) nzs = p->nz;
-    float *hbuf = NULL, *dbuf = NULL;
-    CU(cudaMallocHost((void **)&hbuf, per_level * nzs * sizeof(float)));
-    cudaError_t e = cudaMalloc((void **)&dbuf, per_level * nzs * sizeof(float));
-    if (e != cudaSuccess) { cudaFreeHost(hbuf); return set_err(AWP_ERR_OOM, "media staging: %s", cudaGetErrorString(e)); }
+    /* two pinned staging slabs: the read of slab n+1 overlaps the copy and
+     * transform of slab n */
+    float *hbuf[2] = {NULL, NULL}, *dbuf = NULL;
+    cudaEvent_t done[2];
+    CU(cudaMallocHost((void **)&hbuf[0], per_level * nzs * sizeof(float)));
+    CU(cudaMallocHost((void **)&hbuf[1], per_level * nzs * sizeof(float)));
+    CU(cudaEventCreate(&done[0]));
+    CU(cudaEventCreate(&done[1]));
+    cudaError_t e = cudaMalloc((void **)&dbuf, per_level * nzs * sizeof(float) * 2);
     awp_status st = AWP_OK;
-    for (int z0 = 0; z0 < p->nz && st == AWP_OK; z0 += nzs) {
+    if (e != cudaSuccess) st = set_err(AWP_ERR_OOM, "media staging: %s", cudaGetErrorString(e));
+    int slab = 0;
+    for (int z0 = 0; z0 < p->nz && st == AWP_OK; z0 += nzs, slab ^= 1) {
         const int n = (z0 + nzs <= p->nz) ? nzs : p->nz - z0;
-        if (cudaStreamSynchronize(s->stream) != cudaSuccess) { st = set_err(AWP_ERR_CUDA, "media stream"); break; }
-        if (rd(ctx, hbuf, z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "media: short read at level %d", z0); break; }
-        e = cudaMemcpyAsync(dbuf, hbuf, per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+        if (z0 >= 2 * nzs && cudaEventSynchronize(done[slab]) != cudaSuccess) { st = set_err(AWP_ERR_CUDA, "media stream"); break; }
+        if (rd(ctx, hbuf[slab], z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "media: short read at level %d", z0); break; }
+        float *d = dbuf + (size_t)slab * per_level * nzs;
+        e = cudaMemcpyAsync(d, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
         if (e == cudaSuccess)
-            e = awp_launch_media_interior(s->g, s->md, dbuf, z0, n, p->nvar, var_offset, p->socalq, p->nve,
+            e = awp_launch_media_interior(s->g, s->md, d, z0, n, p->nvar, var_offset, p->socalq, p->nve,
                                           pi, lw, tmp1, tmp2, s->ext, s->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(done[slab], s->stream);
         if (e != cudaSuccess) st = set_err(AWP_ERR_CUDA, "media upload: %s", cudaGetErrorString(e));
     }
     if (st == AWP_OK) {
@@ -437,7 +562,10 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx)
     }
     cudaStreamSynchronize(s->stream);
     cudaFree(dbuf);
-    cudaFreeHost(hbuf);
+    cudaFreeHost(hbuf[0]);
+    cudaFreeHost(hbuf[1]);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
     if (st != AWP_OK) return st;
     if (p->nve == 1) {
         st = upload_tau(s, taumin, taumax);
@@ -500,6 +628,8 @@ extern "C" awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const in
         if (xyz[3 * m + 2] < 1 || xyz[3 * m + 2] > p->nz) return set_err(AWP_ERR_PARAM, "Z source coordinate %d is outside range 1-%d", xyz[3 * m + 2], p->nz);
     }
     CU(cudaSetDevice(p->device));
+    for (int b = 0; b < 2; b++)
+        if (s->graph[b]) { cudaGraphExecDestroy(s->graph[b]); s->graph[b] = NULL; }
     cudaFree(s->src_ijk[comp]); s->src_ijk[comp] = NULL;
     cudaFree(s->src_stf[comp]); s->src_stf[comp] = NULL;
     s->nsrc[comp] = nsrc;
@@ -534,6 +664,8 @@ extern "C" awp_status awp_set_points(awp_solver *s, int npts, const int *xyz)
             return set_err(AWP_ERR_PARAM, "SGT point %d (%d,%d,%d) outside the grid", n, xyz[3 * n], xyz[3 * n + 1], xyz[3 * n + 2]);
     }
     CU(cudaSetDevice(p->device));
+    for (int b = 0; b < 2; b++)
+        if (s->graph[b]) { cudaGraphExecDestroy(s->graph[b]); s->graph[b] = NULL; }
     cudaFree(s->pt_idx); s->pt_idx = NULL;
     cudaFree(s->sg); s->sg = NULL;
     for (int q = 0; q < AWP_MAX_COMP; q++) { cudaFree(s->sgt_file[q]); s->sgt_file[q] = NULL; }
@@ -545,16 +677,17 @@ extern "C" awp_status awp_set_points(awp_solver *s, int npts, const int *xyz)
         idx[n] = s->g.idx(xyz[3 * n], xyz[3 * n + 1], p->nz - xyz[3 * n + 2] + 1);
     awp_status st = dalloc(s, (void **)&s->pt_idx, sizeof(int) * (size_t)npts);
     if (st == AWP_OK) st = dalloc(s, (void **)&s->sg, sizeof(float) * 3 * (size_t)npts);
+    const size_t fb = sizeof(float) * (size_t)(s->sgt_file_floats > 0 ? s->sgt_file_floats : 1);
     for (int q = 0; q < p->ncomp && st == AWP_OK; q++) {
-        st = dalloc(s, (void **)&s->sgt_file[q], sizeof(float) * (size_t)(s->sgt_file_floats > 0 ? s->sgt_file_floats : 1));
-        if (st == AWP_OK && cudaMemset(s->sgt_file[q], 0, sizeof(float) * (size_t)(s->sgt_file_floats > 0 ? s->sgt_file_floats : 1)) != cudaSuccess)
+        st = dalloc(s, (void **)&s->sgt_file[q], fb);
+        if (st == AWP_OK && cudaMemset(s->sgt_file[q], 0, fb) != cudaSuccess)
             st = set_err(AWP_ERR_CUDA, "memset SGT file image");
     }
     if (st == AWP_OK && cudaMemcpy(s->pt_idx, idx, sizeof(int) * (size_t)npts, cudaMemcpyHostToDevice) != cudaSuccess)
         st = set_err(AWP_ERR_CUDA, "point upload");
     free(idx);
     if (st == AWP_OK && s->media_loaded) {
-        cudaError_t e = awp_launch_sg_coeffs(s->g, s->md, s->npts, s->pt_idx, s->sg, s->stream);
+        cudaError_t e = awp_launch_sg_coeffs(s->mdt, s->npts, s->pt_idx, s->sg, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) st = set_err(AWP_ERR_CUDA, "sg coefficients: %s", cudaGetErrorString(e));
     }
@@ -567,12 +700,17 @@ extern "C" int64_t awp_sgt_file_floats(const awp_solver *s) { return s ? s->sgt_
 /* time loop                                                           */
 /* ------------------------------------------------------------------ */
 
-static void fill_args(awp_solver *s, AwpStepArgs &a, AwpPostArgs &pa, AwpSgtArgs &sa)
+/* buffer holding the wavefields after `steps` steps */
+static int cur_buf(const awp_solver *s, int steps) { return s->fused ? (steps & 1) : 0; }
+
+/* arguments of the step that follows `steps` completed steps */
+static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa, AwpSgtArgs &sa)
 {
     const awp_params *p = &s->p;
+    const int rd = cur_buf(s, steps), wr = cur_buf(s, steps + 1);
     memset(&a, 0, sizeof a);
-    a.g = s->g; a.md = s->md; a.ncomp = p->ncomp;
-    for (int q = 0; q < p->ncomp; q++) a.comp[q] = s->comp[q];
+    a.g = s->g; a.md = s->mdt; a.ncomp = p->ncomp; a.fused = s->fused;
+    for (int q = 0; q < p->ncomp; q++) { a.comp[q] = s->comp[rd][q]; a.comp_new[q] = s->comp[wr][q]; }
     a.cx = s->cx; a.cy = s->cy; a.cz = s->cz; a.tau = s->tau;
     a.dth = s->dth; a.dt = p->dt; a.dh1 = s->dh1; a.kchunk = s->kchunk; a.nve = p->nve;
 
@@ -582,14 +720,16 @@ static void fill_args(awp_solver *s, AwpStepArgs &a, AwpPostArgs &pa, AwpSgtArgs
     const int q0 = p->nd + 2;
     pa.probe = (q0 <= p->nx && q0 <= p->ny && q0 <= p->nz) ? q0 : 0;
     pa.step = s->step;
-    pa.d1 = s->md.m[AM_D1];
+    pa.d1 = s->mdt.m[AM_D1];
+    pa.media_type = s->mdt.type;
+    pa.d1_inv = s->mdt.sc.inv[AM_D1];
     for (int q = 0; q < p->ncomp; q++) {
         pa.chkj[q] = s->chkj[q];
         pa.src[q].igreen = p->igreen[q];
         pa.src[q].nsrc = s->nsrc[q];
         pa.src[q].ijk = s->src_ijk[q];
         pa.src[q].stf = s->src_stf[q];
-        pa.comp[q] = s->comp[q];
+        pa.comp[q] = s->comp[wr][q];
     }
 
     memset(&sa, 0, sizeof sa);
@@ -598,49 +738,44 @@ static void fill_args(awp_solver *s, AwpStepArgs &a, AwpPostArgs &pa, AwpSgtArgs
     sa.pt_idx = s->pt_idx; sa.sg = s->sg; sa.step = s->step;
     for (int q = 0; q < p->ncomp; q++) {
         sa.file[q] = s->sgt_file[q];
-        sa.comp[q] = s->comp[q];
+        sa.comp[q] = s->comp[wr][q];
+        sa.active[q] = p->igreen[q] != -1;
     }
 }
 
-static cudaError_t enqueue_steps(awp_solver *s, int nsteps)
+/* one time step after `steps` completed steps: stepper, post, SGT gather */
+static cudaError_t enqueue_one(awp_solver *s, int steps)
 {
     AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
-    fill_args(s, a, pa, sa);
-    const bool any_sgt = s->npts > 0;
-    for (int n = 0; n < nsteps; n++) {
-        cudaError_t e = awp_launch_step(a, s->stream);
-        if (e == cudaSuccess) e = awp_launch_post(pa, 0, s->stream);
-        if (e == cudaSuccess && any_sgt && ((s->steps_done + n + 1) % s->p.ntiskp_sgt == 0))
-            e = awp_launch_sgt(sa, s->stream);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    fill_args(s, steps, a, pa, sa);
+    cudaError_t e = awp_launch_step(a, s->stream);
+    if (e == cudaSuccess) e = awp_launch_post(pa, 0, s->stream);
+    if (e == cudaSuccess && s->npts > 0 && ((steps + 1) % s->p.ntiskp_sgt == 0))
+        e = awp_launch_sgt(sa, s->stream);
+    return e;
 }
 
-/* CUDA graph of NTISKP_SGT steps followed by the SGT gather; the kernels read
- * the device step counter, so the same graph replays for every chunk. */
-static cudaError_t build_graph(awp_solver *s)
+/* CUDA graph of NTISKP_SGT steps ending with the SGT gather; kernels read the
+ * device step counter, so a graph replays for every period that starts on
+ * the same buffer parity. */
+static cudaError_t build_graph(awp_solver *s, int par)
 {
-    if (s->graph) return cudaSuccess;
+    if (s->graph[par]) return cudaSuccess;
     const int gs = s->p.ntiskp_sgt;
     cudaGraph_t graph;
     cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
-    fill_args(s, a, pa, sa);
+    /* graphs start on a period boundary; a base of gs (odd periods only)
+     * gives the steps the odd buffer parity while keeping the gather last */
+    const int base = par ? gs : 0;
     cudaError_t le = cudaSuccess;
-    for (int n = 0; n < gs && le == cudaSuccess; n++) {
-        le = awp_launch_step(a, s->stream);
-        if (le == cudaSuccess) le = awp_launch_post(pa, 0, s->stream);
-    }
-    if (le == cudaSuccess && s->npts > 0) le = awp_launch_sgt(sa, s->stream);
+    for (int n = 0; n < gs && le == cudaSuccess; n++) le = enqueue_one(s, base + n);
     e = cudaStreamEndCapture(s->stream, &graph);
     if (le != cudaSuccess) { if (e == cudaSuccess) cudaGraphDestroy(graph); return le; }
     if (e != cudaSuccess) return e;
-    e = cudaGraphInstantiate(&s->graph, graph, 0);
+    e = cudaGraphInstantiate(&s->graph[par], graph, 0);
     cudaGraphDestroy(graph);
-    if (e != cudaSuccess) { s->graph = NULL; return e; }
-    s->graph_steps = gs;
+    if (e != cudaSuccess) { s->graph[par] = NULL; return e; }
     return cudaSuccess;
 }
 
@@ -649,8 +784,8 @@ static awp_status start_if_needed(awp_solver *s)
     if (s->started) return AWP_OK;
     if (!s->media_loaded) return set_err(AWP_ERR_STATE, "media not loaded");
     AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
-    fill_args(s, a, pa, sa);
-    CU(awp_launch_post(pa, 1, s->stream));     /* addsrc(1) */
+    fill_args(s, -1, a, pa, sa);       /* addsrc(1) into the buffer step 1 reads */
+    CU(awp_launch_post(pa, 1, s->stream));
     s->started = 1;
     return AWP_OK;
 }
@@ -668,25 +803,20 @@ extern "C" awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out)
     if (todo > 0) {
         CU(cudaEventRecord(s->ev0, s->stream));
         int left = todo;
-        /* align to the graph period with single steps */
         const int gs = p->ntiskp_sgt;
         int head = (gs - (s->steps_done % gs)) % gs;
         if (head > left) head = left;
-        if (head > 0) {
-            CU(enqueue_steps(s, head));
-            s->steps_done += head; left -= head;
-        }
-        if (left >= gs && gs >= 1 && gs <= 64) {
-            CU(build_graph(s));
+        for (; head > 0; head--, left--) CU(enqueue_one(s, s->steps_done++));
+        if (left >= gs && gs <= 64) {
             while (left >= gs) {
-                CU(cudaGraphLaunch(s->graph, s->stream));
-                s->steps_done += gs; left -= gs;
+                const int par = cur_buf(s, s->steps_done);
+                CU(build_graph(s, par));
+                CU(cudaGraphLaunch(s->graph[par], s->stream));
+                s->steps_done += gs;
+                left -= gs;
             }
         }
-        if (left > 0) {
-            CU(enqueue_steps(s, left));
-            s->steps_done += left;
-        }
+        for (; left > 0; left--) CU(enqueue_one(s, s->steps_done++));
         CU(cudaEventRecord(s->ev1, s->stream));
         CU(cudaEventSynchronize(s->ev1));
         float ms = 0.f;
@@ -701,6 +831,80 @@ extern "C" awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out)
         }
     }
     return AWP_OK;
+}
+
+/* algorithmic bytes of one launch of each step kernel (compulsory traffic:
+ * every array element the kernel reads or writes counted once) */
+static double part_bytes(const awp_solver *s, int part)
+{
+    const awp_params *p = &s->p;
+    const double cells = (double)p->nx * p->ny * p->nz;
+    const double nc = p->ncomp;
+    const double mb = media_word(s->store);
+    const double rb = mb;
+    const int nr = p->nve == 1 ? 12 : 0;
+    const int nmed = p->nve == 1 ? 5 : 3;
+    switch (part) {
+    case AWP_PART_VEL: return cells * (nc * 12 * 4.0 + mb);                          /* R 9 W 3 + d1 */
+    case AWP_PART_FSVEL: return (double)p->nx * p->ny * (nc * (8 * 4.0) + 2 * mb);
+    case AWP_PART_STR: return cells * (nc * (15 * 4.0 + nr * rb) + (nmed - 1) * mb);
+    case AWP_PART_FUSED: return cells * (nc * (18 * 4.0 + nr * rb) + nmed * mb);
+    }
+    return 0.0;
+}
+
+extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_times *o)
+{
+    if (!s || !o) return set_err(AWP_ERR_PARAM, "null argument");
+    const awp_params *p = &s->p;
+    CU(cudaSetDevice(p->device));
+    memset(o, 0, sizeof *o);
+    awp_status st = start_if_needed(s);
+    if (st != AWP_OK) return st;
+    int todo = nsteps;
+    if (todo > p->nt - s->steps_done) todo = p->nt - s->steps_done;
+    /* kernel classes: the stepper kernels, then k_post, then k_sgt */
+    int parts[4], np = 0;
+    if (s->fused) parts[np++] = AWP_PART_FUSED;
+    else { parts[np++] = AWP_PART_VEL; parts[np++] = AWP_PART_FSVEL; parts[np++] = AWP_PART_STR; }
+    static const char *pname[] = {"k_vel", "k_fsvel", "k_str", "k_fused"};
+    const int nk = np + 2;
+    o->nkernels = nk;
+    for (int k = 0; k < np; k++) {
+        snprintf(o->name[k], sizeof o->name[k], "%s", pname[parts[k]]);
+        o->bytes_per_launch[k] = part_bytes(s, parts[k]);
+    }
+    snprintf(o->name[np], sizeof o->name[np], "k_post");
+    snprintf(o->name[np + 1], sizeof o->name[np + 1], "k_sgt");
+    cudaEvent_t ev[16];
+    for (int k = 0; k < 16; k++) CU(cudaEventCreate(&ev[k]));
+    double tot[8] = {0};
+    awp_status rs = AWP_OK;
+    for (int n = 0; n < todo && rs == AWP_OK; n++) {
+        AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
+        fill_args(s, s->steps_done, a, pa, sa);
+        for (int k = 0; k < nk; k++) {
+            const bool sgt_now = s->npts > 0 && ((s->steps_done + 1) % p->ntiskp_sgt == 0);
+            if (k == np + 1 && !sgt_now) continue;
+            cudaError_t e = cudaEventRecord(ev[2 * k], s->stream);
+            if (e == cudaSuccess) {
+                if (k < np) e = awp_launch_part(a, parts[k], s->stream);
+                else if (k == np) e = awp_launch_post(pa, 0, s->stream);
+                else e = awp_launch_sgt(sa, s->stream);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(ev[2 * k + 1], s->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[2 * k + 1]);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+            if (e != cudaSuccess) { rs = set_err(AWP_ERR_CUDA, "profile: %s", cudaGetErrorString(e)); break; }
+            tot[k] += ms;
+            o->launches[k]++;
+        }
+        s->steps_done++;
+    }
+    for (int k = 0; k < 16; k++) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < nk; k++) o->ms_per_launch[k] = o->launches[k] ? tot[k] / o->launches[k] : 0.0;
+    return rs;
 }
 
 extern "C" awp_status awp_get_sgt(awp_solver *s, int comp, float *out)
@@ -725,20 +929,51 @@ extern "C" awp_status awp_get_chkj(awp_solver *s, int comp, float *out)
 extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *out)
 {
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
-    const float *src = NULL;
-    if (field >= 0 && field < AWP_NF_STATE) {
-        if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
-        src = s->comp[comp].f[field];
-    } else if (field >= AWP_NF_STATE && field < AWP_NF_STATE + AM_N) {
-        src = s->md.m[field - AWP_NF_STATE];
-    }
-    if (!src) return set_err(AWP_ERR_PARAM, "field %d not held by this solver", field);
     CU(cudaSetDevice(s->p.device));
     CU(cudaStreamSynchronize(s->stream));
     const AwpGeom &g = s->g;
-    const size_t w = (size_t)(g.nx + 4);
-    CU(cudaMemcpy2D(out, w * sizeof(float), src + (AWP_XO - 2), (size_t)g.px * sizeof(float),
-                    w * sizeof(float), (size_t)(g.ny + 4) * (size_t)(g.nz + 4), cudaMemcpyDeviceToHost));
+    const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4);
+    const void *src = NULL;
+    int type = AWP_STORE_F32;
+    float inv = 1.0f;
+    if (field >= 0 && field < AWP_NF_STATE) {
+        if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
+        src = s->comp[cur_buf(s, s->steps_done)][comp].f[field];
+        if (field >= AF_R1) type = (s->store == AWP_STORE_F32) ? AWP_STORE_F32 : AWP_STORE_BF16;
+    } else if (field >= AWP_NF_STATE && field < AWP_NF_STATE + AM_N) {
+        src = s->mdt.m[field - AWP_NF_STATE];
+        type = s->mdt.type;
+        inv = s->mdt.sc.inv[field - AWP_NF_STATE];
+    }
+    if (!src) return set_err(AWP_ERR_PARAM, "field %d not held by this solver", field);
+    if (type == AWP_STORE_F32) {
+        CU(cudaMemcpy2D(out, w * sizeof(float), (const float *)src + (AWP_XO - 2), (size_t)g.px * sizeof(float),
+                        w * sizeof(float), rows, cudaMemcpyDeviceToHost));
+        return AWP_OK;
+    }
+    /* 16-bit storage: copy and widen on the host */
+    unsigned short *tmp = (unsigned short *)malloc(w * rows * 2);
+    if (!tmp) return set_err(AWP_ERR_OOM, "host buffer");
+    cudaError_t e = cudaMemcpy2D(tmp, w * 2, (const unsigned short *)src + (AWP_XO - 2), (size_t)g.px * 2, w * 2, rows,
+                                 cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { free(tmp); return set_err(AWP_ERR_CUDA, "get_field: %s", cudaGetErrorString(e)); }
+    for (size_t n = 0; n < w * rows; n++) {
+        uint32_t b = tmp[n];
+        float v;
+        if (type == AWP_STORE_BF16) {
+            b <<= 16;
+            memcpy(&v, &b, 4);
+        } else {   /* IEEE binary16 -> float */
+            uint32_t sgn = (b & 0x8000u) << 16, ex = (b >> 10) & 0x1f, man = b & 0x3ff;
+            if (ex == 0) v = ldexpf((float)man, -24);
+            else if (ex == 31) { uint32_t f = sgn | 0x7f800000u | (man << 13); memcpy(&v, &f, 4); out[n] = v; continue; }
+            else v = ldexpf((float)(man | 0x400), (int)ex - 25);
+            if (sgn) v = -v;
+            v *= inv;
+        }
+        out[n] = v;
+    }
+    free(tmp);
     return AWP_OK;
 }
 
@@ -765,9 +1000,13 @@ extern "C" awp_status awp_reset(awp_solver *s)
     CU(cudaSetDevice(p->device));
     CU(cudaStreamSynchronize(s->stream));
     const size_t vb = (size_t)s->g.vol * sizeof(float);
+    const size_t rb = (size_t)s->g.vol * (s->store == AWP_STORE_F32 ? 4 : 2);
     for (int q = 0; q < p->ncomp; q++) {
-        for (int f = 0; f < AWP_NF_STATE; f++)
-            if (s->comp[q].f[f]) CU(cudaMemsetAsync(s->comp[q].f[f], 0, vb, s->stream));
+        for (int b = 0; b < 2; b++)
+            for (int f = 0; f < AWP_NF_STATE; f++) {
+                if (!s->comp[b][q].f[f] || (b == 1 && s->comp[1][q].f[f] == s->comp[0][q].f[f])) continue;
+                CU(cudaMemsetAsync(s->comp[b][q].f[f], 0, f >= AF_R1 ? rb : vb, s->stream));
+            }
         CU(cudaMemsetAsync(s->chkj[q], 0, sizeof(float) * 3 * (size_t)p->nt, s->stream));
         if (s->sgt_file[q]) CU(cudaMemsetAsync(s->sgt_file[q], 0, sizeof(float) * (size_t)s->sgt_file_floats, s->stream));
     }

@@ -1,0 +1,216 @@
+/*
+ * awp_stencil.cuh -- the per-cell arithmetic of the stepper, shared by the
+ * two-sweep kernels and the fused kernel so every stepper evaluates the same
+ * expressions in the same order (operator.f:92-244, viscoop.f:49-191,
+ * operator.f:348-571, cerjan.f:292-330).
+ *
+ * Storage types: media arrays (lam, mu, d1, qp, qs) are TM = float, bf16 or
+ * binary16 (scaled by a power of two, so the scaling is exact); the memory
+ * variables r1..r6 are TR = float or bf16.  Every value is widened to FP32
+ * before any arithmetic.
+ */
+#ifndef AWP_STENCIL_CUH
+#define AWP_STENCIL_CUH
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include "awp_internal.h"
+
+#define C1 (9.0f / 8.0f)
+#define C2 (-(1.0f / 24.0f))
+
+template <class T> struct Store;
+template <> struct Store<float> {
+    static __device__ __forceinline__ float ld(const float *p, int c, float) { return p[c]; }
+    static __device__ __forceinline__ void st(float *p, int c, float v, float) { p[c] = v; }
+};
+template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p, int c, float) { return __bfloat162float(p[c]); }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, int c, float v, float) { p[c] = __float2bfloat16_rn(v); }
+};
+/* binary16 arrays hold value * 2^e; ld multiplies by inv = 2^-e (exact) */
+template <> struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half *p, int c, float inv) { return __half2float(p[c]) * inv; }
+    static __device__ __forceinline__ void st(__half *p, int c, float v, float scale) { p[c] = __float2half_rn(v * scale); }
+};
+
+/* typed view of the media arrays */
+template <class TM>
+struct MediaT {
+    const TM *m[AM_N];
+    float inv[AM_N];
+    __device__ __forceinline__ float operator()(int a, int c) const { return Store<TM>::ld(m[a], c, inv[a]); }
+};
+
+/* ------------------------------------------------------------------ */
+/* velocity update of one cell (all NC components)                    */
+/* ------------------------------------------------------------------ */
+
+/* d1 averages of operator.f:120-121, 171-172, 224-225 -> dth/d */
+template <class TM>
+__device__ __forceinline__ void vel_factors(const MediaT<TM> &md, int c, int sy, int sz, float dth,
+                                            float &fu, float &fv, float &fw)
+{
+    const float da = md(AM_D1, c), db = md(AM_D1, c - sy), dc = md(AM_D1, c - sz), dd = md(AM_D1, c - sy - sz);
+    const float de = md(AM_D1, c + 1), df = md(AM_D1, c + 1 - sz), dg = md(AM_D1, c + 1 - sy);
+    fu = dth / (0.25f * ((da + db) + (dc + dd)));
+    fv = dth / (0.25f * ((da + de) + (dc + df)));
+    fw = dth / (0.25f * ((da + de) + (db + dg)));
+}
+
+/* new (u, v, w) of one component, before the sponge factor */
+__device__ __forceinline__ void vel_one(const AwpComp &o, int c, int sy, int sz, float fu, float fv, float fw,
+                                        float &u, float &v, float &w)
+{
+    const float *__restrict__ xx = o.f[AF_XX];
+    const float *__restrict__ yy = o.f[AF_YY];
+    const float *__restrict__ zz = o.f[AF_ZZ];
+    const float *__restrict__ xy = o.f[AF_XY];
+    const float *__restrict__ xz = o.f[AF_XZ];
+    const float *__restrict__ yz = o.f[AF_YZ];
+    u = o.f[AF_U][c] + fu * (
+        C1 * (xx[c] - xx[c - 1]) + C2 * (xx[c + 1] - xx[c - 2]) +
+        C1 * (xy[c] - xy[c - sy]) + C2 * (xy[c + sy] - xy[c - 2 * sy]) +
+        C1 * (xz[c] - xz[c - sz]) + C2 * (xz[c + sz] - xz[c - 2 * sz]));
+    v = o.f[AF_V][c] + fv * (
+        C1 * (xy[c + 1] - xy[c]) + C2 * (xy[c + 2] - xy[c - 1]) +
+        C1 * (yy[c + sy] - yy[c]) + C2 * (yy[c + 2 * sy] - yy[c - sy]) +
+        C1 * (yz[c] - yz[c - sz]) + C2 * (yz[c + sz] - yz[c - 2 * sz]));
+    w = o.f[AF_W][c] + fw * (
+        C1 * (xz[c + 1] - xz[c]) + C2 * (xz[c + 2] - xz[c - 1]) +
+        C1 * (yz[c] - yz[c - sy]) + C2 * (yz[c + sy] - yz[c - 2 * sy]) +
+        C1 * (zz[c + sz] - zz[c]) + C2 * (zz[c + 2 * sz] - zz[c - sz]));
+}
+
+/* ------------------------------------------------------------------ */
+/* stress + memory variables of one cell                              */
+/* ------------------------------------------------------------------ */
+
+/* cell coefficients shared by all components (viscoop.f:104-124, 151-167) */
+struct StrCoef {
+    float xl, xm, qpa, vh1, xmu4, xmu5, xmu6, vh2_r4, vh2_r5, vh2_r6, vx1, vx2;
+};
+
+template <class TM>
+__device__ __forceinline__ StrCoef str_coef(const MediaT<TM> &md, int c, int sy, int sz, int nve,
+                                            float vx1, float vx2)
+{
+    StrCoef k;
+    k.xl = 8.0f / (md(AM_LAM, c) + md(AM_LAM, c + 1) + md(AM_LAM, c - sy) + md(AM_LAM, c + 1 - sy) +
+                   md(AM_LAM, c - sz) + md(AM_LAM, c + 1 - sz) + md(AM_LAM, c - sy - sz) + md(AM_LAM, c + 1 - sy - sz));
+    k.xm = 8.0f / (md(AM_MU, c) + md(AM_MU, c + 1) + md(AM_MU, c - sy) + md(AM_MU, c + 1 - sy) +
+                   md(AM_MU, c - sz) + md(AM_MU, c + 1 - sz) + md(AM_MU, c - sy - sz) + md(AM_MU, c + 1 - sy - sz));
+    const float mu0 = md(AM_MU, c);
+    k.xmu4 = 2.0f / (mu0 + md(AM_MU, c - sz));
+    k.xmu5 = 2.0f / (mu0 + md(AM_MU, c - sy));
+    k.xmu6 = 2.0f / (mu0 + md(AM_MU, c + 1));
+    k.vx1 = vx1;
+    k.vx2 = vx2;
+    if (nve == 1) {
+        k.qpa = 0.125f * (md(AM_QP, c) + md(AM_QP, c + 1) + md(AM_QP, c - sy) + md(AM_QP, c + 1 - sy) +
+                          md(AM_QP, c - sz) + md(AM_QP, c + 1 - sz) + md(AM_QP, c - sy - sz) + md(AM_QP, c + 1 - sy - sz));
+        const float qsa = 0.125f * (md(AM_QS, c) + md(AM_QS, c + 1) + md(AM_QS, c - sy) + md(AM_QS, c + 1 - sy) +
+                                    md(AM_QS, c - sz) + md(AM_QS, c + 1 - sz) + md(AM_QS, c - sy - sz) + md(AM_QS, c + 1 - sy - sz));
+        k.xl = k.xl + 2.0f * k.xm;
+        const float qs0 = md(AM_QS, c);
+        const float aas4 = 0.5f * (qs0 + md(AM_QS, c - sz));
+        const float aas5 = 0.5f * (qs0 + md(AM_QS, c - sy));
+        const float aas6 = 0.5f * (qs0 + md(AM_QS, c + 1));
+        k.vh1 = -(k.xm * qsa);
+        k.vh2_r4 = -(aas4 * k.xmu4 / 2.0f);
+        k.vh2_r5 = -(aas5 * k.xmu5 / 2.0f);
+        k.vh2_r6 = -(aas6 * k.xmu6 / 2.0f);
+    } else {
+        k.qpa = k.vh1 = k.vh2_r4 = k.vh2_r5 = k.vh2_r6 = 0.f;
+    }
+    return k;
+}
+
+/* velocity differences of viscoop.f:126-134; A provides u/v/w at offsets */
+struct VelDiff {
+    float vt1, vt2, vt3, vt4, vt5, vt6, vt7;
+};
+
+template <class A>
+__device__ __forceinline__ VelDiff vel_diff(const A &V)
+{
+    VelDiff d;
+    d.vt1 = C1 * (V.u(1, 0, 0) - V.u(0, 0, 0)) + C2 * (V.u(2, 0, 0) - V.u(-1, 0, 0));
+    d.vt2 = C1 * (V.v(0, 0, 0) - V.v(0, -1, 0)) + C2 * (V.v(0, 1, 0) - V.v(0, -2, 0));
+    d.vt3 = C1 * (V.w(0, 0, 0) - V.w(0, 0, -1)) + C2 * (V.w(0, 0, 1) - V.w(0, 0, -2));
+    d.vt4 = C1 * (V.u(0, 1, 0) - V.u(0, 0, 0)) + C2 * (V.u(0, 2, 0) - V.u(0, -1, 0)) +
+            C1 * (V.v(0, 0, 0) - V.v(-1, 0, 0)) + C2 * (V.v(1, 0, 0) - V.v(-2, 0, 0));
+    d.vt5 = C1 * (V.u(0, 0, 1) - V.u(0, 0, 0)) + C2 * (V.u(0, 0, 2) - V.u(0, 0, -1)) +
+            C1 * (V.w(0, 0, 0) - V.w(-1, 0, 0)) + C2 * (V.w(1, 0, 0) - V.w(-2, 0, 0));
+    d.vt6 = C1 * (V.v(0, 0, 1) - V.v(0, 0, 0)) + C2 * (V.v(0, 0, 2) - V.v(0, 0, -1));
+    d.vt7 = C1 * (V.w(0, 1, 0) - V.w(0, 0, 0)) + C2 * (V.w(0, 2, 0) - V.w(0, -1, 0));
+    return d;
+}
+
+struct Stress6 {
+    float xx, yy, zz, xy, xz, yz;
+};
+
+/* viscoelastic update (viscoop.f:136-185): old stresses s, old memory
+ * variables r[6] (overwritten with the new ones), returns the new stresses
+ * before the sponge factor */
+__device__ __forceinline__ Stress6 str_visco(const StrCoef &k, const VelDiff &d, const Stress6 &s, float r[6],
+                                             float dth, float dt, float dh1)
+{
+    const float vtmp = k.xl * (d.vt1 + d.vt2 + d.vt3);
+    const float va1 = -(k.qpa * k.xl * dh1 * (d.vt1 + d.vt2 + d.vt3) / 2.0f);
+    Stress6 o;
+    o.xx = s.xx + dth * (vtmp - 2.0f * k.xm * (d.vt2 + d.vt3)) + dt * r[0];
+    o.yy = s.yy + dth * (vtmp - 2.0f * k.xm * (d.vt1 + d.vt3)) + dt * r[1];
+    o.zz = s.zz + dth * (vtmp - 2.0f * k.xm * (d.vt1 + d.vt2)) + dt * r[2];
+    o.xy = s.xy + k.xmu4 * dth * d.vt4 + dt * r[3];
+    o.xz = s.xz + k.xmu5 * dth * d.vt5 + dt * r[4];
+    o.yz = s.yz + k.xmu6 * (dth * d.vt6 + dth * d.vt7) + dt * r[5];
+    r[0] = (k.vx2 * r[0] - k.vh1 * (d.vt2 + d.vt3) * dh1 + va1) * k.vx1;
+    r[1] = (k.vx2 * r[1] - k.vh1 * (d.vt1 + d.vt3) * dh1 + va1) * k.vx1;
+    r[2] = (k.vx2 * r[2] - k.vh1 * (d.vt1 + d.vt2) * dh1 + va1) * k.vx1;
+    r[3] = (k.vx2 * r[3] + k.vh2_r4 * dh1 * d.vt4) * k.vx1;
+    r[4] = (k.vx2 * r[4] + k.vh2_r5 * dh1 * d.vt5) * k.vx1;
+    r[5] = (k.vx2 * r[5] + k.vh2_r6 * dh1 * (d.vt6 + d.vt7)) * k.vx1;
+    o.xx = o.xx + dt * r[0];
+    o.yy = o.yy + dt * r[1];
+    o.zz = o.zz + dt * r[2];
+    o.xy = o.xy + dt * r[3];
+    o.xz = o.xz + dt * r[4];
+    o.yz = o.yz + dt * r[5];
+    return o;
+}
+
+/* elastic update (operator.f:389-426, 464-470, 509-515, 559-565) */
+template <class A>
+__device__ __forceinline__ Stress6 str_elastic(const StrCoef &k, const A &V, const Stress6 &s, float dth)
+{
+    const float a = k.xl + 2.0f * k.xm, b = k.xl;
+    const float u_a = C1 * (V.u(1, 0, 0) - V.u(0, 0, 0)), u_b = C2 * (V.u(2, 0, 0) - V.u(-1, 0, 0));
+    const float v_a = C1 * (V.v(0, 0, 0) - V.v(0, -1, 0)), v_b = C2 * (V.v(0, 1, 0) - V.v(0, -2, 0));
+    const float w_a = C1 * (V.w(0, 0, 0) - V.w(0, 0, -1)), w_b = C2 * (V.w(0, 0, 1) - V.w(0, 0, -2));
+    Stress6 o;
+    o.xx = s.xx + dth * a * (u_a + u_b) + dth * b * (v_a + v_b + w_a + w_b);
+    o.yy = s.yy + dth * a * (v_a + v_b) + dth * b * (u_a + u_b + w_a + w_b);
+    o.zz = s.zz + dth * a * (w_a + w_b) + dth * b * (u_a + u_b + v_a + v_b);
+    o.xy = s.xy + dth * k.xmu4 * (C1 * (V.u(0, 1, 0) - V.u(0, 0, 0)) + C2 * (V.u(0, 2, 0) - V.u(0, -1, 0)) +
+                                  C1 * (V.v(0, 0, 0) - V.v(-1, 0, 0)) + C2 * (V.v(1, 0, 0) - V.v(-2, 0, 0)));
+    o.xz = s.xz + dth * k.xmu5 * (C1 * (V.u(0, 0, 1) - V.u(0, 0, 0)) + C2 * (V.u(0, 0, 2) - V.u(0, 0, -1)) +
+                                  C1 * (V.w(0, 0, 0) - V.w(-1, 0, 0)) + C2 * (V.w(1, 0, 0) - V.w(-2, 0, 0)));
+    o.yz = s.yz + dth * k.xmu6 * (C1 * (V.v(0, 0, 1) - V.v(0, 0, 0)) + C2 * (V.v(0, 0, 2) - V.v(0, 0, -1)) +
+                                  C1 * (V.w(0, 1, 0) - V.w(0, 0, 0)) + C2 * (V.w(0, 2, 0) - V.w(0, -1, 0)));
+    return o;
+}
+
+/* velocity accessor over global arrays (two-sweep stress kernel) */
+struct GVel {
+    const float *__restrict__ U;
+    const float *__restrict__ Vv;
+    const float *__restrict__ W;
+    int c, sy, sz;
+    __device__ __forceinline__ float u(int dx, int dy, int dz) const { return U[c + dx + dy * sy + dz * sz]; }
+    __device__ __forceinline__ float v(int dx, int dy, int dz) const { return Vv[c + dx + dy * sy + dz * sz]; }
+    __device__ __forceinline__ float w(int dx, int dy, int dz) const { return W[c + dx + dy * sy + dz * sz]; }
+};
+
+#endif

@@ -171,6 +171,23 @@ awp_status awp_reset(awp_solver *s);
 /* Frees every resource of the solver. */
 awp_status awp_destroy(awp_solver *s);
 
+/* Per-kernel timing of the stepper (diagnostic, no reference counterpart).
+ * Advances the solve by `nsteps` steps exactly as awp_run does, but records
+ * CUDA events around every launch on the solver's stream and returns, per
+ * kernel class, the launch count, the average device time of one launch and
+ * the algorithmic bytes one launch moves (the compulsory traffic of its
+ * arrays; the basis of the HBM roofline). */
+#define AWP_MAX_KERNELS 8
+typedef struct {
+    int nkernels;
+    char name[AWP_MAX_KERNELS][32];
+    int launches[AWP_MAX_KERNELS];
+    double ms_per_launch[AWP_MAX_KERNELS];
+    double bytes_per_launch[AWP_MAX_KERNELS];
+} awp_kernel_times;
+
+awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_times *out);
+
 /* Device memory one solver of these parameters would hold (admission). */
 int64_t awp_footprint_bytes(const awp_params *p, int npts);
 

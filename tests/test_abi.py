@@ -49,9 +49,16 @@ def test_param_defaults_match_gpu_command_defaults():
     assert p.socalq == 1 and p.nve == 1
 
 
-@pytest.mark.parametrize("ncomp,prec,expect", [(1, "f32", 176.0), (2, "f32", 166.0), (3, "f32", 156.0 + 20.0 / 3)])
-def test_algorithmic_bytes_two_sweep(ncomp, prec, expect):
-    p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, igreen=(1, 2, 3)[:ncomp], precision=prec, ntiskp_sgt=1)
+@pytest.mark.parametrize("kernel,ncomp,prec,expect", [
+    # two sweeps: velocity R 9 W 3, stress R 9 W 6, r1..r6 R+W, media shared
+    ("two_sweep", 1, "f32", 176.0), ("two_sweep", 2, "f32", 166.0), ("two_sweep", 3, "f32", 156.0 + 20.0 / 3),
+    ("two_sweep", 2, "bf16", 137.0),
+    # fused: u v w and 6 stresses read + written once, r1..r6 R+W, media once
+    ("fused", 1, "f32", 140.0), ("fused", 2, "f16", 101.0), ("fused", 3, "f16", 96.0 + 10.0 / 3),
+])
+def test_algorithmic_bytes(kernel, ncomp, prec, expect):
+    p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, igreen=(1, 2, 3)[:ncomp], precision=prec, ntiskp_sgt=1,
+                           kernel=kernel)
     assert abs(awpsgt.bytes_per_cell_update(p) - expect) < 1e-9
 
 
