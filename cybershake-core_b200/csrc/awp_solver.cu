@@ -276,7 +276,7 @@ static awp_status check_params(const awp_params *p)
     if (p->nvar != 3 && p->nvar != 5 && p->nvar != 8) return set_err(AWP_ERR_PARAM, "NVAR must be 3, 5 or 8");
     if (p->nve != 0 && p->nve != 1) return set_err(AWP_ERR_PARAM, "NVE must be 0 or 1");
     if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_F16) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
-    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_TWO_SWEEP) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
+    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_FUSED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
         int ig = p->igreen[q];

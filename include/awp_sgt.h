@@ -61,8 +61,10 @@ typedef enum {
 
 /* Stepper implementation. */
 typedef enum {
-    AWP_KERNEL_AUTO = 0,     /* library picks (fused when available)          */
-    AWP_KERNEL_TWO_SWEEP = 1 /* velocity sweep, then stress sweep             */
+    AWP_KERNEL_AUTO = 0,      /* library picks (the fused stepper)             */
+    AWP_KERNEL_TWO_SWEEP = 1, /* velocity sweep, then stress sweep, in place   */
+    AWP_KERNEL_FUSED = 2      /* one z-march per tile: velocity on a 2-cell
+                                 halo, then stress; ping-pong wavefields       */
 } awp_kernel;
 
 #define AWP_MAX_COMP 3
