@@ -37,7 +37,13 @@ EXPORTED = [
     "awp_get_stats", "awp_reset", "awp_destroy", "awp_footprint_bytes", "awp_bytes_per_cell_update",
     "awp_status_string", "awp_last_error", "awp_read_in3d", "awp_parse_command_line",
     "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free", "awp_profile_steps",
+    "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
 ]
+
+
+class Layout(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("pitch", C.c_int), ("plane", C.c_int),
+                ("vol", C.c_int64)]
 
 
 class AwpError(RuntimeError):
@@ -138,6 +144,12 @@ def load_library(path: str = LIB_PATH):
         "awp_read_cordfile": (C.c_int, [C.c_char_p, P(C.c_int), P(P(C.c_int))]),
         "awp_free": (None, [C.c_void_p]),
         "awp_profile_steps": (C.c_int, [C.c_void_p, C.c_int, P(KernelTimes)]),
+        "awp_run_async": (C.c_int, [C.c_void_p, C.c_int]),
+        "awp_query": (C.c_int, [C.c_void_p]),
+        "awp_sync": (C.c_int, [C.c_void_p]),
+        "awp_device_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, P(C.c_void_p), P(Layout)]),
+        "awp_field_energy": (C.c_int, [P(C.c_void_p), C.c_int, P(Layout), C.c_void_p]),
+        "awp_energy": (C.c_int, [C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -264,6 +276,30 @@ class Solver:
         _check(self.lib.awp_get_field(self.h, comp, FIELDS.index(name), _ptr(out)))
         return out
 
+    def run_async(self, nsteps: int):
+        _check(self.lib.awp_run_async(self.h, nsteps))
+
+    def query(self) -> bool:
+        r = self.lib.awp_query(self.h)
+        if r < 0:
+            raise AwpError(4, self.lib.awp_last_error().decode())
+        return bool(r)
+
+    def sync(self):
+        _check(self.lib.awp_sync(self.h))
+
+    def energy(self) -> np.ndarray:
+        out = np.zeros(self.p.ncomp, dtype=np.float64)
+        _check(self.lib.awp_energy(self.h, _ptr(out)))
+        return out
+
+    def device_field(self, name: str, comp: int = 0):
+        """(device pointer, Layout) of a field of the current wavefield."""
+        ptr = C.c_void_p()
+        L = Layout()
+        _check(self.lib.awp_device_field(self.h, comp, FIELDS.index(name), C.byref(ptr), C.byref(L)))
+        return ptr.value, L
+
     def profile(self, nsteps: int) -> dict:
         """Advances nsteps steps with CUDA events around every kernel launch."""
         kt = KernelTimes()
@@ -274,6 +310,16 @@ class Solver:
         s = Stats()
         _check(self.lib.awp_get_stats(self.h, C.byref(s)))
         return s
+
+
+def field_energy(ptrs: Sequence[int], layout: Layout, ncomp: int) -> np.ndarray:
+    """awp_field_energy on device arrays (u,v,w per component); the result is
+    written to a device buffer and copied back through torch."""
+    import torch
+    arr = (C.c_void_p * len(ptrs))(*ptrs)
+    out = torch.zeros(ncomp, dtype=torch.float64, device="cuda")
+    _check(load_library().awp_field_energy(arr, ncomp, C.byref(layout), C.c_void_p(out.data_ptr())))
+    return out.cpu().numpy()
 
 
 def read_in3d(path: str) -> In3dC:

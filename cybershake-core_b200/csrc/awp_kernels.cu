@@ -630,6 +630,58 @@ __global__ void k_sgt(AwpSgtArgs a)
 }
 
 /* ------------------------------------------------------------------ */
+/* FP64 energy (stability monitor): two deterministic passes           */
+/* ------------------------------------------------------------------ */
+
+/* pass 1: block b sums u^2+v^2+w^2 over the rows r = b, b+G, ... of the
+ * interior (a row is one (j,k) line of nx cells), in a fixed order, and
+ * writes partial[b*ncomp + q] */
+__global__ void __launch_bounds__(AWP_EN_BLOCK) k_energy_partial(AwpEnergyArgs a, double *partial)
+{
+    __shared__ double sh[3][AWP_EN_BLOCK];
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int nrow = a.g.ny * a.g.nz;
+    for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
+        const int j = r % a.g.ny + 1, k = r / a.g.ny + 1;
+        const int c0 = a.g.idx(1, j, k);
+        for (int i = threadIdx.x; i < a.g.nx; i += blockDim.x) {
+            for (int q = 0; q < a.ncomp; ++q) {
+                const double u = a.f[3 * q][c0 + i], v = a.f[3 * q + 1][c0 + i], w = a.f[3 * q + 2][c0 + i];
+                acc[q] += u * u + v * v + w * w;
+            }
+        }
+    }
+    for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int s = AWP_EN_BLOCK / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < (unsigned)a.ncomp) partial[blockIdx.x * a.ncomp + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+/* pass 2: out[q] = sum of the block partials in block order; a non-finite
+ * energy raises the instability flag */
+__global__ void k_energy_final(const double *partial, int nblocks, int ncomp, double *out, int *flag)
+{
+    const int q = threadIdx.x;
+    if (q >= ncomp) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[b * ncomp + q];
+    out[q] = s;
+    if (flag && !isfinite(s)) atomicExch(flag, 1);
+}
+
+cudaError_t awp_launch_energy(const AwpEnergyArgs &a, double *partial, int nblocks, double *out, int *flag,
+                              cudaStream_t st)
+{
+    k_energy_partial<<<nblocks, AWP_EN_BLOCK, 0, st>>>(a, partial);
+    k_energy_final<<<1, 32, 0, st>>>(partial, nblocks, a.ncomp, out, flag);
+    return cudaGetLastError();
+}
+
+/* ------------------------------------------------------------------ */
 /* launchers                                                           */
 /* ------------------------------------------------------------------ */
 

@@ -37,4 +37,16 @@ cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);
 
+/* FP64 energy of (u, v, w) per component, two passes through `partial`
+ * (nblocks * ncomp doubles of scratch); flag (may be NULL) set on NaN/Inf */
+#define AWP_EN_BLOCK 256
+#define AWP_EN_GRID 592
+struct AwpEnergyArgs {
+    AwpGeom g;
+    int ncomp;
+    const float *f[9];
+};
+cudaError_t awp_launch_energy(const AwpEnergyArgs &a, double *partial, int nblocks, double *out, int *flag,
+                              cudaStream_t st);
+
 #endif

@@ -79,6 +79,13 @@ struct awp_solver {
     int64_t loop_steps;
     cudaGraphExec_t graph[2];        /* by the parity of the first step    */
     double device_bytes;
+    /* stability monitor */
+    double *en_partial;              /* scratch: AWP_EN_GRID * ncomp       */
+    double *en_out;                  /* last energy per component          */
+    int *flag;                       /* set by the monitor on NaN/Inf      */
+    int next_check;
+    int pending;                     /* asynchronous steps not yet synced  */
+    int pending_steps;
 };
 
 /* ------------------------------------------------------------------ */
@@ -248,6 +255,7 @@ static void free_all(awp_solver *s)
     cudaFree(s->cx); cudaFree(s->cy); cudaFree(s->cz);
     cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext); cudaFree(s->rng);
     cudaFree(s->pt_idx); cudaFree(s->sg);
+    cudaFree(s->en_partial); cudaFree(s->en_out); cudaFree(s->flag);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -378,6 +386,12 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     TRYCU(cudaMemsetAsync(s->step, 0, sizeof(int), s->stream));
     TRY(dalloc(s, (void **)&s->ext, 8 * sizeof(int)));
     TRY(dalloc(s, (void **)&s->rng, 2 * AM_N * sizeof(unsigned)));
+    TRY(dalloc(s, (void **)&s->en_partial, sizeof(double) * AWP_EN_GRID * AWP_MAX_COMP));
+    TRY(dalloc(s, (void **)&s->en_out, sizeof(double) * AWP_MAX_COMP));
+    TRY(dalloc(s, (void **)&s->flag, sizeof(int)));
+    TRYCU(cudaMemsetAsync(s->en_out, 0, sizeof(double) * AWP_MAX_COMP, s->stream));
+    TRYCU(cudaMemsetAsync(s->flag, 0, sizeof(int), s->stream));
+    s->next_check = p->monitor_every > 0 ? p->monitor_every : 0;
     for (int q = 0; q < p->ncomp; q++) {
         TRY(dalloc(s, (void **)&s->chkj[q], sizeof(float) * 3 * (size_t)p->nt));
         TRYCU(cudaMemsetAsync(s->chkj[q], 0, sizeof(float) * 3 * (size_t)p->nt, s->stream));
@@ -790,7 +804,27 @@ static awp_status start_if_needed(awp_solver *s)
     return AWP_OK;
 }
 
-extern "C" awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out)
+static void energy_args(awp_solver *s, AwpEnergyArgs &a)
+{
+    memset(&a, 0, sizeof a);
+    a.g = s->g;
+    a.ncomp = s->p.ncomp;
+    const int b = cur_buf(s, s->steps_done);
+    for (int q = 0; q < s->p.ncomp; q++)
+        for (int f = 0; f < 3; f++) a.f[3 * q + f] = s->comp[b][q].f[AF_U + f];
+}
+
+/* stability monitor after the steps enqueued so far, when a check is due */
+static cudaError_t maybe_monitor(awp_solver *s)
+{
+    if (s->p.monitor_every <= 0 || s->steps_done < s->next_check) return cudaSuccess;
+    while (s->next_check <= s->steps_done) s->next_check += s->p.monitor_every;
+    AwpEnergyArgs a;
+    energy_args(s, a);
+    return awp_launch_energy(a, s->en_partial, AWP_EN_GRID, s->en_out, s->flag, s->stream);
+}
+
+extern "C" awp_status awp_run_async(awp_solver *s, int nsteps)
 {
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
     const awp_params *p = &s->p;
@@ -800,30 +834,72 @@ extern "C" awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out)
     if (nsteps < 0) return set_err(AWP_ERR_PARAM, "nsteps < 0");
     int todo = nsteps;
     if (todo > p->nt - s->steps_done) todo = p->nt - s->steps_done;
-    if (todo > 0) {
-        CU(cudaEventRecord(s->ev0, s->stream));
-        int left = todo;
-        const int gs = p->ntiskp_sgt;
-        int head = (gs - (s->steps_done % gs)) % gs;
-        if (head > left) head = left;
-        for (; head > 0; head--, left--) CU(enqueue_one(s, s->steps_done++));
-        if (left >= gs && gs <= 64) {
-            while (left >= gs) {
-                const int par = cur_buf(s, s->steps_done);
-                CU(build_graph(s, par));
-                CU(cudaGraphLaunch(s->graph[par], s->stream));
-                s->steps_done += gs;
-                left -= gs;
-            }
+    if (todo <= 0) return AWP_OK;
+    if (!s->pending) CU(cudaEventRecord(s->ev0, s->stream));
+    int left = todo;
+    const int gs = p->ntiskp_sgt;
+    int head = (gs - (s->steps_done % gs)) % gs;
+    if (head > left) head = left;
+    for (; head > 0; head--, left--) { CU(enqueue_one(s, s->steps_done++)); CU(maybe_monitor(s)); }
+    if (left >= gs && gs <= 64) {
+        while (left >= gs) {
+            const int par = cur_buf(s, s->steps_done);
+            CU(build_graph(s, par));
+            CU(cudaGraphLaunch(s->graph[par], s->stream));
+            s->steps_done += gs;
+            left -= gs;
+            CU(maybe_monitor(s));
         }
-        for (; left > 0; left--) CU(enqueue_one(s, s->steps_done++));
-        CU(cudaEventRecord(s->ev1, s->stream));
+    }
+    for (; left > 0; left--) { CU(enqueue_one(s, s->steps_done++)); CU(maybe_monitor(s)); }
+    CU(cudaEventRecord(s->ev1, s->stream));
+    s->pending = 1;
+    s->pending_steps += todo;
+    return AWP_OK;
+}
+
+extern "C" int awp_query(awp_solver *s)
+{
+    if (!s) return -1;
+    if (!s->pending) return 1;
+    cudaError_t e = cudaEventQuery(s->ev1);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    set_err(AWP_ERR_CUDA, "awp_query: %s", cudaGetErrorString(e));
+    return -1;
+}
+
+extern "C" awp_status awp_sync(awp_solver *s)
+{
+    if (!s) return set_err(AWP_ERR_PARAM, "null solver");
+    CU(cudaSetDevice(s->p.device));
+    if (s->pending) {
         CU(cudaEventSynchronize(s->ev1));
         float ms = 0.f;
         CU(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
         s->loop_seconds += ms * 1e-3;
-        s->loop_steps += todo;
+        s->loop_steps += s->pending_steps;
+        s->pending = 0;
+        s->pending_steps = 0;
     }
+    if (s->p.monitor_every > 0) {
+        int flag = 0;
+        CU(cudaMemcpyAsync(&flag, s->flag, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaStreamSynchronize(s->stream));
+        if (flag) return set_err(AWP_ERR_UNSTABLE, "stability monitor: non-finite wavefield energy by step %d",
+                                 s->steps_done);
+    }
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_run(awp_solver *s, int nsteps, float *sgt_out)
+{
+    if (!s) return set_err(AWP_ERR_PARAM, "null solver");
+    const awp_params *p = &s->p;
+    awp_status st = awp_run_async(s, nsteps);
+    if (st != AWP_OK) return st;
+    st = awp_sync(s);
+    if (st != AWP_OK) return st;
     if (sgt_out) {
         for (int q = 0; q < p->ncomp; q++) {
             st = awp_get_sgt(s, q, sgt_out + (size_t)q * (size_t)s->sgt_file_floats);
@@ -1011,10 +1087,87 @@ extern "C" awp_status awp_reset(awp_solver *s)
         if (s->sgt_file[q]) CU(cudaMemsetAsync(s->sgt_file[q], 0, sizeof(float) * (size_t)s->sgt_file_floats, s->stream));
     }
     CU(cudaMemsetAsync(s->step, 0, sizeof(int), s->stream));
+    CU(cudaMemsetAsync(s->flag, 0, sizeof(int), s->stream));
     CU(cudaStreamSynchronize(s->stream));
     s->steps_done = 0;
     s->started = 0;
     s->loop_seconds = 0;
     s->loop_steps = 0;
+    s->pending = 0;
+    s->pending_steps = 0;
+    s->next_check = p->monitor_every > 0 ? p->monitor_every : 0;
+    return AWP_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* device views and the FP64 energy                                    */
+/* ------------------------------------------------------------------ */
+
+static awp_layout layout_of(const AwpGeom &g)
+{
+    awp_layout L;
+    L.nx = g.nx; L.ny = g.ny; L.nz = g.nz; L.pitch = g.px; L.plane = g.plane; L.vol = g.vol;
+    return L;
+}
+
+extern "C" awp_status awp_device_field(awp_solver *s, int comp, int field, float **ptr, awp_layout *layout)
+{
+    if (!s || !ptr) return set_err(AWP_ERR_PARAM, "null argument");
+    if (comp < 0 || comp >= s->p.ncomp || field < 0 || field >= AWP_NF_STATE + AM_N)
+        return set_err(AWP_ERR_PARAM, "bad component/field");
+    CU(cudaSetDevice(s->p.device));
+    CU(cudaStreamSynchronize(s->stream));
+    *ptr = field < AWP_NF_STATE ? s->comp[cur_buf(s, s->steps_done)][comp].f[field]
+                                : (float *)s->mdt.m[field - AWP_NF_STATE];
+    if (layout) *layout = layout_of(s->g);
+    return AWP_OK;
+}
+
+static awp_status check_layout(const float *const *fields, int ncomp, const awp_layout *L)
+{
+    if (!fields || !L) return set_err(AWP_ERR_PARAM, "null argument");
+    if (ncomp < 1 || ncomp > AWP_MAX_COMP) return set_err(AWP_ERR_PARAM, "ncomp must be 1..3");
+    if (L->nx < 1 || L->ny < 1 || L->nz < 1 || L->pitch < L->nx + AWP_XO + 2 || L->plane < L->pitch * (L->ny + 4) ||
+        L->vol < (int64_t)L->plane * (L->nz + 4) || L->vol >= ((int64_t)1 << 31))
+        return set_err(AWP_ERR_PARAM, "inconsistent layout");
+    for (int n = 0; n < 3 * ncomp; n++)
+        if (!fields[n]) return set_err(AWP_ERR_PARAM, "null field pointer %d", n);
+    return AWP_OK;
+}
+
+static void energy_args_from(const float *const *fields, int ncomp, const awp_layout *L, AwpEnergyArgs &a)
+{
+    memset(&a, 0, sizeof a);
+    a.g.nx = L->nx; a.g.ny = L->ny; a.g.nz = L->nz;
+    a.g.px = L->pitch; a.g.py = L->ny + 4; a.g.plane = L->plane; a.g.vol = L->vol;
+    a.ncomp = ncomp;
+    for (int n = 0; n < 3 * ncomp; n++) a.f[n] = fields[n];
+}
+
+extern "C" awp_status awp_field_energy(const float *const *fields, int ncomp, const awp_layout *L, double *out)
+{
+    awp_status st = check_layout(fields, ncomp, L);
+    if (st != AWP_OK) return st;
+    if (!out) return set_err(AWP_ERR_PARAM, "null output");
+    AwpEnergyArgs a;
+    energy_args_from(fields, ncomp, L, a);
+    double *partial = NULL;
+    CU(cudaMalloc((void **)&partial, sizeof(double) * AWP_EN_GRID * ncomp));
+    cudaError_t e = awp_launch_energy(a, partial, AWP_EN_GRID, out, NULL, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    cudaFree(partial);
+    if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_field_energy: %s", cudaGetErrorString(e));
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_energy(awp_solver *s, double *out)
+{
+    if (!s || !out) return set_err(AWP_ERR_PARAM, "null argument");
+    CU(cudaSetDevice(s->p.device));
+    AwpEnergyArgs a;
+    energy_args(s, a);
+    CU(awp_launch_energy(a, s->en_partial, AWP_EN_GRID, s->en_out, NULL, s->stream));
+    CU(cudaMemcpyAsync(out, s->en_out, sizeof(double) * s->p.ncomp, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
     return AWP_OK;
 }

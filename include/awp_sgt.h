@@ -173,6 +173,41 @@ awp_status awp_reset(awp_solver *s);
 /* Frees every resource of the solver. */
 awp_status awp_destroy(awp_solver *s);
 
+/* Asynchronous stepping: enqueues up to `nsteps` steps on the solver's CUDA
+ * stream and returns at once.  awp_query returns 1 when all enqueued work has
+ * finished (0 otherwise, negative on error); awp_sync waits for it and
+ * reports the stability monitor's verdict.  No reference counterpart (the
+ * reference loop is synchronous, AWP-GPU-SGT/src/pmcl3d.c:841-960). */
+awp_status awp_run_async(awp_solver *s, int nsteps);
+int awp_query(awp_solver *s);
+awp_status awp_sync(awp_solver *s);
+
+/* Device layout of the wavefield arrays (awp_internal.h): element (i,j,k)
+ * of the 1-based Fortran index space is at (k+1)*plane + (j+1)*pitch + i + 7. */
+typedef struct {
+    int nx, ny, nz;
+    int pitch;      /* floats per row                */
+    int plane;      /* floats per z level            */
+    int64_t vol;    /* floats per array              */
+} awp_layout;
+
+/* Device pointer and layout of one field of the current wavefield (field
+ * numbering as awp_get_field).  The pointer stays valid until the next step
+ * of the fused stepper, which alternates between two buffers. */
+awp_status awp_device_field(awp_solver *s, int comp, int field, float **ptr, awp_layout *layout);
+
+/* FP64 wavefield energy: out[q] = sum over interior cells of u^2 + v^2 + w^2
+ * for component q, fields = {u0, v0, w0, u1, v1, w1, ...} device arrays in
+ * the layout L, out a device array of ncomp doubles.  Two deterministic passes
+ * (per-block partial sums, then a fixed-order sum); the partial sums live in
+ * a scratch buffer this call allocates and frees on the calling thread's
+ * current device.  The quantity of the stability monitor.  No reference
+ * counterpart (the reference has no monitor). */
+awp_status awp_field_energy(const float *const *fields, int ncomp, const awp_layout *L, double *out);
+
+/* Energy of a solver's current wavefield (host output, ncomp doubles). */
+awp_status awp_energy(awp_solver *s, double *out);
+
 /* Per-kernel timing of the stepper (diagnostic, no reference counterpart).
  * Advances the solve by `nsteps` steps exactly as awp_run does, but records
  * CUDA events around every launch on the solver's stream and returns, per

@@ -1,0 +1,126 @@
+"""The pmcl3d drop-in driver end to end: reference-format inputs on disk, both
+reference command lines, reference-format outputs compared with the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import awp_inputs as ai
+import awpsgt
+import oracle
+
+NX, NY, NZ, NST = 48, 40, 32, 60
+
+
+def write_inputs(d, igreen=1, ifault=0, write_step=3, ntiskp=5):
+    media = ai.layered_media(NX, NY, NZ, 200.0, seed=4, pert_std=0.05, corr_len=1000.0)
+    stf = ai.gaussian_derivative_stf(NST, 0.01, f0=1.0, column=max(igreen, 1) - 1 if igreen in (1, 2, 3) else 0)
+    pts = ai.sgt_points(NX, NY, 20, 30, seed=0)
+    os.makedirs(d / "input", exist_ok=True)
+    ai.write_media(str(d / "input" / "media"), media)
+    if ifault == 0:
+        ai.write_source_text(str(d / "input" / "src"), (24, 20, 9), stf)
+    else:
+        ai.write_source_binary(str(d / "input" / "src"), (24, 20, 9), stf)
+    ai.write_cordfile(str(d / "input" / "cord"), pts, comment="test points")
+    return media, stf, pts
+
+
+def oracle_sgt(media, stf, pts, igreen=1, write_step=3, ntiskp=5, nt=None):
+    nt = NST + 1 if nt is None else nt
+    o = oracle.Oracle(nx=NX, ny=NY, nz=NZ, dh=200.0, dt=0.01, nt=nt, nst=NST, nd=8, fl=0.01, fh=25.0, fp=0.5,
+                      socalq=1, ntiskp_sgt=ntiskp, write_step=write_step, igreen=igreen)
+    o.load_media(media)
+    o.set_source([(24, 20, 9)], stf)
+    o.set_points(pts)
+    o.run(nt)
+    return o
+
+
+def in3d(d, igreen=1, ifault=0, write_step=3, ntiskp=5):
+    w = ai.In3d(igreen=igreen, tmax=0.6, dh=200.0, dt=0.01, nd=8, nst=NST, nx=NX, ny=NY, nz=NZ, ifault=ifault,
+                mediarestart=1, nvar=3, socalq=1, nve=1, fl=0.01, fh=25.0, fp=0.5, read_step=NST,
+                write_step=write_step, write_step2=write_step, ntiskp_sgt=ntiskp,
+                chkp="out/CHKP", chkj="out/CHKJ", insrc="input/src", invel="input/media", insgt="input/cord",
+                sgtgro="out/sgt/awp-strain")
+    w.write(str(d / "IN3D"))
+    return w
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ifault", [0, 1])
+def test_fortran_command_line(tmp_path, ifault):
+    media, stf, pts = write_inputs(tmp_path, ifault=ifault)
+    w = in3d(tmp_path, ifault=ifault)
+    assert w.nt == NST + 1
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    got = np.fromfile(tmp_path / "out" / "sgt" / "awp-strain", dtype=np.float32)
+    o = oracle_sgt(media, stf, pts)
+    ref = o.sgt()
+    assert got.size == ref.size == 30 * 6 * 12       # NT = int(int(61/3)*3/5) = 12
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    # CHKJ: (I6,3E10.3) per step, u1 v1 w1 at (ND+2, ND+2, ND+2)
+    lines = (tmp_path / "out" / "CHKJ").read_text().splitlines()
+    assert len(lines) == NST + 1
+    assert all(len(l) == 36 for l in lines)
+    cj = o.chkj()
+    last = lines[-1]
+    assert int(last[:6]) == NST + 1
+    np.testing.assert_allclose([float(last[6 + 10 * q:16 + 10 * q]) for q in range(3)], cj[-1], rtol=6e-3, atol=1e-30)
+    chkp = (tmp_path / "out" / "CHKP").read_text()
+    assert "STABILITY CRITERIA .5 > CMAX*DT/DX" in chkp and "# OF TIME STEPS  61" in chkp
+
+
+@pytest.mark.gpu
+def test_positional_overrides(tmp_path):
+    media, stf, pts = write_inputs(tmp_path)
+    in3d(tmp_path)
+    os.rename(tmp_path / "input" / "media", tmp_path / "other_media")
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D", "input/src", "other_media", "out/C1", "out/C2"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "out" / "C1").exists() and (tmp_path / "out" / "C2").exists()
+
+
+@pytest.mark.gpu
+def test_gpu_command_line_chunk_files(tmp_path):
+    """The argument list gpu_wrapper.py builds; one SGT%07d file per
+    WRITE_STEP chunk, each [point][6][WRITE_STEP] (FAST-T layout)."""
+    media, stf, pts = write_inputs(tmp_path, ifault=1)
+    argv = [awpsgt.PMCL3D_PATH, "-T", "0.6", "--IGREEN", "1", "--DH", "200.0", "--DT", "0.01", "--NSRC", "1",
+            "--NST", str(NST), "-X", str(NX), "-Y", str(NY), "-Z", str(NZ), "-x", "1", "-y", "1", "--NPC", "0",
+            "--ARBC", "0.92", "--ND", "8", "--IFAULT", "1", "--MEDIASTART", "1", "--FL", "0.01", "--FH", "25.0",
+            "--FP", "0.5", "--READ_STEP", str(NST), "--WRITE_STEP", "4", "-o", "out_sgt", "--INSGT", "input/cord",
+            "-c", "out_sgt/CHKP", "--INSRC", "input/src", "--INVEL", "input/media", "--NTISKP_SGT", "5",
+            "--NTISKP", "10"]
+    r = subprocess.run(argv, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    # nt = (int)(0.6/0.01) + 1 = 60 or 61 depending on rounding of 0.6f/0.01f
+    nt = int(np.float32(0.6) / np.float32(0.01)) + 1
+    o = oracle_sgt(media, stf, pts, write_step=4, ntiskp=5, nt=nt)
+    ref = o.sgt().reshape(30, 6, -1)
+    nchunk = (nt // 5) // 4
+    assert nchunk >= 2
+    for c in range(nchunk):
+        f = tmp_path / "out_sgt" / ("SGT%07d" % ((c + 1) * 4 * 5))
+        got = np.fromfile(f, dtype=np.float32).reshape(30, 6, 4)
+        assert np.array_equal(got, ref[:, :, c * 4:(c + 1) * 4])
+    assert (tmp_path / "out_sgt" / "CHKP").exists()
+
+
+def test_driver_reports_missing_input(tmp_path):
+    """Errors come back as a message and a nonzero exit, never a crash."""
+    in3d(tmp_path)
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0
+    assert "source" in r.stderr
+
+
+def test_driver_rejects_pml(tmp_path):
+    w = in3d(tmp_path)
+    w.npc = 1
+    w.write(str(tmp_path / "IN3D"))
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "PML" in r.stderr
