@@ -25,7 +25,7 @@ AWP_OK = 0
 STATUS = {0: "AWP_OK", 1: "AWP_ERR_IO", 2: "AWP_ERR_PARAM", 3: "AWP_ERR_OOM", 4: "AWP_ERR_CUDA",
           5: "AWP_ERR_UNSTABLE", 6: "AWP_ERR_TIMEOUT", 7: "AWP_ERR_STATE", 8: "AWP_ERR_BUSY",
           9: "AWP_ERR_CANCELLED"}
-PREC = {"f32": 0, "bf16": 1, "f16": 2}
+PREC = {"f32": 0, "bf16": 1, "f16": 2, "mixed": 3}
 KERNEL = {"auto": 0, "two_sweep": 1, "fused": 2}
 FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3", "r4", "r5", "r6",
           "lam", "mu", "d1", "qp", "qs"]
@@ -38,6 +38,8 @@ EXPORTED = [
     "awp_status_string", "awp_last_error", "awp_read_in3d", "awp_parse_command_line",
     "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free", "awp_profile_steps",
     "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
+    "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
+    "awp_server_destroy", "awp_sgt_floats_for",
 ]
 
 
@@ -150,6 +152,14 @@ def load_library(path: str = LIB_PATH):
         "awp_device_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, P(C.c_void_p), P(Layout)]),
         "awp_field_energy": (C.c_int, [P(C.c_void_p), C.c_int, P(Layout), C.c_void_p]),
         "awp_energy": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "awp_server_create": (C.c_int, [C.c_int, C.c_int64, C.c_int, C.c_int, P(C.c_void_p)]),
+        "awp_submit": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_int64)]),
+        "awp_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
+        "awp_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+        "awp_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_void_p]),
+        "awp_server_time": (C.c_double, [C.c_void_p]),
+        "awp_server_destroy": (C.c_int, [C.c_void_p]),
+        "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -310,6 +320,89 @@ class Solver:
         s = Stats()
         _check(self.lib.awp_get_stats(self.h, C.byref(s)))
         return s
+
+
+class Request(C.Structure):
+    _fields_ = [("params", Params), ("media", C.c_void_p), ("nsrc", C.c_int * 3), ("src_xyz", C.c_void_p * 3),
+                ("stf", C.c_void_p * 3), ("npts", C.c_int), ("pts", C.c_void_p), ("sgt_out", C.c_void_p)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("steps_done", C.c_int64), ("footprint", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_STATE = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class Server:
+    """Continuous-batching SGT server on one GPU (awp_server_* in the C ABI)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_active: int = 4, chunk_steps: int = 100):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.awp_server_create(device, hbm_budget, max_active, chunk_steps, C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, params: Params, media: Optional[np.ndarray], sources, points) -> int:
+        """sources: per component a (xyz [nsrc][3], stf [nsrc][nst][6]) pair."""
+        rq = Request()
+        rq.params = params
+        keep = []
+        if media is not None:
+            m = np.ascontiguousarray(media, dtype=np.float32)
+            keep.append(m)
+            rq.media = m.ctypes.data
+        for q, (xyz, stf) in enumerate(sources):
+            xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+            stf = np.ascontiguousarray(np.asarray(stf, np.float32).reshape(xyz.shape[0], -1, 6))
+            keep += [xyz, stf]
+            rq.nsrc[q] = xyz.shape[0]
+            rq.src_xyz[q] = xyz.ctypes.data
+            rq.stf[q] = stf.ctypes.data
+        pts = np.ascontiguousarray(np.asarray(points, np.int32).reshape(-1, 3))
+        keep.append(pts)
+        rq.npts = pts.shape[0]
+        rq.pts = pts.ctypes.data
+        nf = int(self.lib.awp_sgt_floats_for(C.byref(params), rq.npts))
+        out = np.zeros((params.ncomp, max(nf, 1)), dtype=np.float32)
+        keep.append(out)
+        rq.sgt_out = out.ctypes.data
+        rid = C.c_int64()
+        _check(self.lib.awp_submit(self.h, C.byref(rq), C.byref(rid)))
+        self._keep[rid.value] = (keep, out)
+        return rid.value
+
+    def poll(self, rid: int) -> dict:
+        info = RequestInfo()
+        _check(self.lib.awp_poll(self.h, rid, C.byref(info)))
+        return info.as_dict()
+
+    def wait(self, rid: int, timeout: float = 3600.0):
+        info = RequestInfo()
+        _check(self.lib.awp_wait(self.h, rid, timeout, C.byref(info)))
+        return info.as_dict(), self._keep[rid][1]
+
+    def cancel(self, rid: int):
+        _check(self.lib.awp_cancel(self.h, rid))
+
+    def time(self) -> float:
+        return float(self.lib.awp_server_time(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.awp_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def field_energy(ptrs: Sequence[int], layout: Layout, ncomp: int) -> np.ndarray:

@@ -151,17 +151,25 @@ __global__ void k_media_homo(AwpGeom g, AwpMedia md, float lam, float mu, float 
     md.m[AM_D1][c] = d1;
 }
 
-/* |value| maxima and minima of the nonzero entries of each media array
- * (for the binary16 scale and range check) */
-__global__ void k_media_range(AwpMedia md, int64_t n, unsigned *mx, unsigned *mn)
+/* |value| maxima and minima of the nonzero interior entries of each media
+ * array (for the binary16 scale and range check).  Ghost cells hold copies
+ * of interior values, except the padmedia corner (nx+1,0,0) whose d1 takes a
+ * compliance; no stencil reads that d1, so it is left out of the range. */
+__global__ void k_media_range(AwpGeom g, AwpMedia md, unsigned *mx, unsigned *mn)
 {
     unsigned lmx[AM_N], lmn[AM_N];
     for (int a = 0; a < AM_N; a++) { lmx[a] = 0u; lmn[a] = 0x7f800000u; }
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    const int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % g.nx) + 1;
+        const int j = (int)((t / g.nx) % g.ny) + 1;
+        const int k = (int)(t / ((int64_t)g.nx * g.ny)) + 1;
+        const int c = g.idx(i, j, k);
         for (int a = 0; a < AM_N; a++) {
-            unsigned b = __float_as_uint(fabsf(md.m[a][t]));
+            unsigned b = __float_as_uint(fabsf(md.m[a][c]));
             if (b) { lmx[a] = max(lmx[a], b); lmn[a] = min(lmn[a], b); }
         }
+    }
     for (int a = 0; a < AM_N; a++) {
         for (int off = 16; off > 0; off >>= 1) {
             lmx[a] = max(lmx[a], __shfl_xor_sync(0xffffffffu, lmx[a], off));
@@ -206,8 +214,8 @@ __device__ __forceinline__ void zchunk(const AwpGeom &g, int kchunk, int &k0, in
     k0 = max(1, k1 - kchunk + 1);
 }
 
-template <int NC, class TM>
-__global__ void __launch_bounds__(256)
+template <int NC, class TM, int UNR>
+__global__ void __launch_bounds__(512)
 k_vel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
       const float *__restrict__ cz, float dth, int kchunk)
 {
@@ -218,6 +226,7 @@ k_vel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx,
     zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane;
     const float cxy = cx[i] * cy[j];
+#pragma unroll (UNR)
     for (int k = k0; k <= k1; ++k) {
         const int c = g.idx(i, j, k);
         float fu, fv, fw;
@@ -265,8 +274,8 @@ __global__ void k_fsvel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs)
     }
 }
 
-template <int NC, class TM, class TR>
-__global__ void __launch_bounds__(256)
+template <int NC, class TM, class TR, int UNR>
+__global__ void __launch_bounds__(512)
 k_str(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
       const float *__restrict__ cz, const float *__restrict__ tau, float dth, float dt, float dh1, int kchunk,
       int nve)
@@ -279,6 +288,7 @@ k_str(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx,
     const int sy = g.px, sz = g.plane;
     const float cxy = cx[i] * cy[j];
     const int itxy = ((j & 1) << 1) | (i & 1);
+#pragma unroll (UNR)
     for (int k = k0; k <= k1; ++k) {
         const int c = g.idx(i, j, k);
         const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
@@ -716,9 +726,9 @@ cudaError_t awp_launch_media_homo(const AwpGeom &g, const AwpMedia &md, float la
     return cudaGetLastError();
 }
 
-cudaError_t awp_launch_media_range(const AwpMedia &md, int64_t n, unsigned *mx, unsigned *mn, cudaStream_t st)
+cudaError_t awp_launch_media_range(const AwpGeom &g, const AwpMedia &md, unsigned *mx, unsigned *mn, cudaStream_t st)
 {
-    k_media_range<<<148 * 4, 256, 0, st>>>(md, n, mx, mn);
+    k_media_range<<<148 * 4, 256, 0, st>>>(g, md, mx, mn);
     return cudaGetLastError();
 }
 
@@ -767,6 +777,26 @@ static void comp_sets(const AwpStepArgs &s, AwpCompSet<NC> &a, AwpCompSet<NC> &b
 template <int TY, int NC>
 static size_t fused_smem() { return (size_t)FSLOT * 3 * NC * (FX + 4) * (TY + 4) * sizeof(float); }
 
+template <int NC, class TM, class TR, int TY>
+static cudaError_t launch_fused(const AwpStepArgs &s, const MediaT<TM> &md, const AwpCompSet<NC> &cs,
+                                const AwpCompSet<NC> &cn, int nzb, cudaStream_t st)
+{
+    dim3 b(FX, TY);
+    const size_t smem = fused_smem<TY, NC>();
+    static unsigned long long attr_done = 0;   /* per instantiation, bit per device */
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 64 || !(attr_done & (1ull << dev))) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused<NC, TM, TR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) attr_done |= 1ull << dev;
+    }
+    k_fused<NC, TM, TR, TY><<<plane_grid(s.g, b, nzb), b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau,
+                                                                     s.dth, s.dt, s.dh1, s.kchunk, s.nve);
+    return cudaGetLastError();
+}
+
 template <int NC, class TM, class TR>
 static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st)
 {
@@ -774,31 +804,28 @@ static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st
     comp_sets<NC>(s, cs, cn);
     const MediaT<TM> md = media_view<TM>(s.md);
     const int nzb = (s.g.nz + s.kchunk - 1) / s.kchunk;
+    const int ty = (s.ty == 4 || s.ty == 16) ? s.ty : 8;
     if (part == AWP_PART_VEL) {
-        dim3 b(32, 8);
-        k_vel<NC, TM><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
+        dim3 b(32, ty);
+        if (s.unroll == 2)
+            k_vel<NC, TM, 2><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
+        else
+            k_vel<NC, TM, 1><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
     } else if (part == AWP_PART_FSVEL) {
         dim3 b(32, 8);
         k_fsvel<NC, TM><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, md, cs);
     } else if (part == AWP_PART_STR) {
-        dim3 b(32, 8);
-        k_str<NC, TM, TR><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
-                                                                 s.dt, s.dh1, s.kchunk, s.nve);
+        dim3 b(32, ty);
+        if (s.unroll == 2)
+            k_str<NC, TM, TR, 2><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
+                                                                        s.dt, s.dh1, s.kchunk, s.nve);
+        else
+            k_str<NC, TM, TR, 1><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
+                                                                        s.dt, s.dh1, s.kchunk, s.nve);
     } else if (part == AWP_PART_FUSED) {
-        constexpr int TY = 8;
-        dim3 b(FX, TY);
-        const size_t smem = fused_smem<TY, NC>();
-        static unsigned long long attr_done = 0;   /* per instantiation, bit per device */
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev >= 64 || !(attr_done & (1ull << dev))) {
-            cudaError_t e = cudaFuncSetAttribute(k_fused<NC, TM, TR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            if (dev < 64) attr_done |= 1ull << dev;
-        }
-        k_fused<NC, TM, TR, TY><<<plane_grid(s.g, b, nzb), b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau,
-                                                                         s.dth, s.dt, s.dh1, s.kchunk, s.nve);
+        if (ty == 4) return launch_fused<NC, TM, TR, 4>(s, md, cs, cn, nzb, st);
+        if (ty == 16) return launch_fused<NC, TM, TR, 16>(s, md, cs, cn, nzb, st);
+        return launch_fused<NC, TM, TR, 8>(s, md, cs, cn, nzb, st);
     } else {
         return cudaErrorInvalidValue;
     }
@@ -808,11 +835,11 @@ static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st
 template <int NC>
 static cudaError_t launch_part_nc(const AwpStepArgs &s, int part, cudaStream_t st)
 {
-    switch (s.md.type) {
-    case AWP_STORE_BF16: return launch_part_t<NC, __nv_bfloat16, __nv_bfloat16>(s, part, st);
-    case AWP_STORE_F16: return launch_part_t<NC, __half, __nv_bfloat16>(s, part, st);
-    default: return launch_part_t<NC, float, float>(s, part, st);
-    }
+    /* (media storage, r1..r6 storage) pairs of awp_precision */
+    if (s.md.type == AWP_STORE_BF16) return launch_part_t<NC, __nv_bfloat16, __nv_bfloat16>(s, part, st);
+    if (s.md.type == AWP_STORE_F16) return launch_part_t<NC, __half, __nv_bfloat16>(s, part, st);
+    if (s.rtype == AWP_STORE_BF16) return launch_part_t<NC, float, __nv_bfloat16>(s, part, st);
+    return launch_part_t<NC, float, float>(s, part, st);
 }
 
 cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st)

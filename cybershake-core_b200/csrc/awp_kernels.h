@@ -17,6 +17,9 @@ struct AwpStepArgs {
     int kchunk;                  /* z levels per thread block               */
     int nve;
     int fused;                   /* 1: single-sweep stepper                 */
+    int rtype;                   /* AWP_STORE_* of r1..r6                   */
+    int ty;                      /* thread-block rows (4, 8 or 16)          */
+    int unroll;                  /* two-sweep z-loop unroll (1 or 2)        */
 };
 
 cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, const float *raw, int zf0, int nzs,
@@ -25,7 +28,7 @@ cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, cons
 cudaError_t awp_launch_media_ghosts(const AwpGeom &g, const AwpMedia &md, int nve, cudaStream_t st);
 cudaError_t awp_launch_media_homo(const AwpGeom &g, const AwpMedia &md, float lam, float mu, float d1,
                                   cudaStream_t st);
-cudaError_t awp_launch_media_range(const AwpMedia &md, int64_t n, unsigned *mx, unsigned *mn, cudaStream_t st);
+cudaError_t awp_launch_media_range(const AwpGeom &g, const AwpMedia &md, unsigned *mx, unsigned *mn, cudaStream_t st);
 cudaError_t awp_launch_media_convert(const AwpMedia &src, const AwpMediaT &dst, int64_t n, cudaStream_t st);
 cudaError_t awp_launch_sg_coeffs(const AwpMediaT &md, int npts, const int *pt_idx, float *sg, cudaStream_t st);
 

@@ -49,7 +49,8 @@ struct awp_solver {
     cudaStream_t stream;
     AwpComp comp[2][AWP_MAX_COMP];   /* [buffer][component]; r1..r6 shared  */
     int fused;
-    int store;                       /* AWP_STORE_* of media and r1..r6     */
+    int store;                       /* AWP_STORE_* of the media arrays     */
+    int rstore;                      /* AWP_STORE_* of r1..r6               */
     AwpMedia md;                     /* FP32 media (ingest)                 */
     AwpMediaT mdt;                   /* media as the steppers read them     */
     float *cx, *cy, *cz;
@@ -72,6 +73,8 @@ struct awp_solver {
     int started;
     int media_loaded;
     int kchunk;
+    int ty;                          /* thread-block rows of the steppers   */
+    int unroll;                      /* two-sweep z-loop unroll             */
     float vtst, vtst1, dth, dh1;
     float ext_host[6];
     cudaEvent_t ev0, ev1;
@@ -159,10 +162,13 @@ static int64_t file_floats_of(const awp_params *p, int npts)
     return n;
 }
 
+/* storage of the media arrays */
 static int store_of(const awp_params *p)
 {
     return p->precision == AWP_PREC_BF16 ? AWP_STORE_BF16 : p->precision == AWP_PREC_F16 ? AWP_STORE_F16 : AWP_STORE_F32;
 }
+/* storage of r1..r6 */
+static int rstore_of(const awp_params *p) { return p->precision == AWP_PREC_F32 ? AWP_STORE_F32 : AWP_STORE_BF16; }
 static int fused_of(const awp_params *p) { return p->kernel != AWP_KERNEL_TWO_SWEEP; }
 static double media_word(int store) { return store == AWP_STORE_F32 ? 4.0 : 2.0; }
 
@@ -171,7 +177,7 @@ extern "C" double awp_bytes_per_cell_update(const awp_params *p)
     const int nc = p->ncomp < 1 ? 1 : p->ncomp;
     const int st = store_of(p);
     const double mb = media_word(st);
-    const double rb = mb;                              /* r1..r6 word       */
+    const double rb = media_word(rstore_of(p));        /* r1..r6 word       */
     const int nmedia = (p->nve == 1) ? 5 : 3;
     const int nr = (p->nve == 1) ? 12 : 0;             /* r1..r6 read+write */
     double state;
@@ -182,9 +188,18 @@ extern "C" double awp_bytes_per_cell_update(const awp_params *p)
     return (nc * state + nmedia * mb) / nc;
 }
 
-static int choose_kchunk(const AwpGeom &g, int fused)
+/* tuning overrides from the environment (AWP_TUNE_TY, AWP_TUNE_KCHUNK) */
+static int env_int(const char *name, int dflt)
 {
-    const int bxy = ((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+    const char *v = getenv(name);
+    return (v && *v) ? atoi(v) : dflt;
+}
+
+static int choose_kchunk(const AwpGeom &g, int fused, int ty)
+{
+    const int over = env_int("AWP_TUNE_KCHUNK", 0);
+    if (over > 0) return over < 8 ? 8 : (over > g.nz ? g.nz : over);
+    const int bxy = ((g.nx + 31) / 32) * ((g.ny + ty - 1) / ty);
     const int want = fused ? 148 * 4 : 148 * 8;
     int nzb = (want + bxy - 1) / bxy;
     if (nzb < 1) nzb = 1;
@@ -202,7 +217,8 @@ extern "C" int64_t awp_footprint_bytes(const awp_params *p, int npts)
     const int st = store_of(p);
     const double mb = media_word(st);
     const int nbuf = fused_of(p) ? 2 : 1;
-    int64_t b = (int64_t)g.vol * (int64_t)(nc * (9 * 4 * nbuf + (p->nve == 1 ? 6 * mb : 0)));
+    const double rb = media_word(rstore_of(p));
+    int64_t b = (int64_t)g.vol * (int64_t)(nc * (9 * 4 * nbuf + (p->nve == 1 ? 6 * rb : 0)));
     b += (int64_t)g.vol * (int64_t)(AM_N * 4);                        /* FP32 media during ingest */
     if (st != AWP_STORE_F32) b += (int64_t)g.vol * (int64_t)(AM_N * mb);
     b += file_floats_of(p, npts) * 4 * nc;
@@ -283,7 +299,7 @@ static awp_status check_params(const awp_params *p)
     if (p->nst < 0) return set_err(AWP_ERR_PARAM, "NST must be >= 0");
     if (p->nvar != 3 && p->nvar != 5 && p->nvar != 8) return set_err(AWP_ERR_PARAM, "NVAR must be 3, 5 or 8");
     if (p->nve != 0 && p->nve != 1) return set_err(AWP_ERR_PARAM, "NVE must be 0 or 1");
-    if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_F16) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
+    if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_MIXED) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
     if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_FUSED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
@@ -325,9 +341,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->g = make_geom(pin);
     s->fused = fused_of(pin);
     s->store = store_of(pin);
+    s->rstore = rstore_of(pin);
     const awp_params *p = &s->p;
     const size_t vb = (size_t)s->g.vol * sizeof(float);
-    const size_t rb = (size_t)s->g.vol * (s->store == AWP_STORE_F32 ? 4 : 2);
+    const size_t rb = (size_t)s->g.vol * (s->rstore == AWP_STORE_F32 ? 4 : 2);
 #define TRY(x) do { awp_status t_ = (x); if (t_ != AWP_OK) { free_all(s); delete s; return t_; } } while (0)
 #define TRYCU(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { free_all(s); delete s; \
     return set_err(AWP_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); } } while (0)
@@ -400,7 +417,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->dh1 = 1.0f / p->dh;
     s->vtst = p->dt / (p->dh * p->dh * p->dh);     /* source.f:834-835 */
     s->vtst1 = 1.0f / (p->dh * p->dh);
-    s->kchunk = choose_kchunk(s->g, s->fused);
+    s->ty = env_int("AWP_TUNE_TY", 8);
+    if (s->ty != 4 && s->ty != 16) s->ty = 8;
+    s->unroll = env_int("AWP_TUNE_UNROLL", 1) == 2 ? 2 : 1;
+    s->kchunk = choose_kchunk(s->g, s->fused, s->ty);
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
     TRYCU(cudaStreamSynchronize(s->stream));
@@ -456,7 +476,7 @@ static awp_status convert_media(awp_solver *s)
         unsigned init[2 * AM_N];
         for (int a = 0; a < AM_N; a++) { init[a] = 0u; init[AM_N + a] = 0x7f800000u; }
         CU(cudaMemcpyAsync(s->rng, init, sizeof init, cudaMemcpyHostToDevice, s->stream));
-        CU(awp_launch_media_range(s->md, s->g.vol, s->rng, s->rng + AM_N, s->stream));
+        CU(awp_launch_media_range(s->g, s->md, s->rng, s->rng + AM_N, s->stream));
         unsigned r[2 * AM_N];
         CU(cudaMemcpyAsync(r, s->rng, sizeof r, cudaMemcpyDeviceToHost, s->stream));
         CU(cudaStreamSynchronize(s->stream));
@@ -710,6 +730,8 @@ extern "C" awp_status awp_set_points(awp_solver *s, int npts, const int *xyz)
 
 extern "C" int64_t awp_sgt_file_floats(const awp_solver *s) { return s ? s->sgt_file_floats : 0; }
 
+extern "C" int64_t awp_sgt_floats_for(const awp_params *p, int npts) { return p ? file_floats_of(p, npts) : 0; }
+
 /* ------------------------------------------------------------------ */
 /* time loop                                                           */
 /* ------------------------------------------------------------------ */
@@ -727,6 +749,9 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     for (int q = 0; q < p->ncomp; q++) { a.comp[q] = s->comp[rd][q]; a.comp_new[q] = s->comp[wr][q]; }
     a.cx = s->cx; a.cy = s->cy; a.cz = s->cz; a.tau = s->tau;
     a.dth = s->dth; a.dt = p->dt; a.dh1 = s->dh1; a.kchunk = s->kchunk; a.nve = p->nve;
+    a.rtype = s->rstore;
+    a.ty = s->ty;
+    a.unroll = s->unroll;
 
     memset(&pa, 0, sizeof pa);
     pa.g = s->g; pa.ncomp = p->ncomp; pa.nst = p->nst; pa.nt = p->nt;
@@ -917,7 +942,7 @@ static double part_bytes(const awp_solver *s, int part)
     const double cells = (double)p->nx * p->ny * p->nz;
     const double nc = p->ncomp;
     const double mb = media_word(s->store);
-    const double rb = mb;
+    const double rb = media_word(s->rstore);
     const int nr = p->nve == 1 ? 12 : 0;
     const int nmed = p->nve == 1 ? 5 : 3;
     switch (part) {
@@ -1015,7 +1040,7 @@ extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *o
     if (field >= 0 && field < AWP_NF_STATE) {
         if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
         src = s->comp[cur_buf(s, s->steps_done)][comp].f[field];
-        if (field >= AF_R1) type = (s->store == AWP_STORE_F32) ? AWP_STORE_F32 : AWP_STORE_BF16;
+        if (field >= AF_R1) type = s->rstore;
     } else if (field >= AWP_NF_STATE && field < AWP_NF_STATE + AM_N) {
         src = s->mdt.m[field - AWP_NF_STATE];
         type = s->mdt.type;
@@ -1076,7 +1101,7 @@ extern "C" awp_status awp_reset(awp_solver *s)
     CU(cudaSetDevice(p->device));
     CU(cudaStreamSynchronize(s->stream));
     const size_t vb = (size_t)s->g.vol * sizeof(float);
-    const size_t rb = (size_t)s->g.vol * (s->store == AWP_STORE_F32 ? 4 : 2);
+    const size_t rb = (size_t)s->g.vol * (s->rstore == AWP_STORE_F32 ? 4 : 2);
     for (int q = 0; q < p->ncomp; q++) {
         for (int b = 0; b < 2; b++)
             for (int f = 0; f < AWP_NF_STATE; f++) {

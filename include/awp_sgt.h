@@ -56,7 +56,11 @@ typedef enum {
 typedef enum {
     AWP_PREC_F32 = 0,   /* plain FP32, bit-exact with the FP32 oracle        */
     AWP_PREC_BF16 = 1,  /* media and r1..r6 stored as bfloat16               */
-    AWP_PREC_F16 = 2    /* media and r1..r6 stored as scaled binary16        */
+    AWP_PREC_F16 = 2,   /* media as binary16 scaled by a power of two per
+                           array, r1..r6 as bfloat16 (binary16 lacks the
+                           exponent range for memory variables, whose size
+                           follows the source amplitude)                     */
+    AWP_PREC_MIXED = 3  /* media FP32, r1..r6 bfloat16                       */
 } awp_precision;
 
 /* Stepper implementation. */
@@ -233,6 +237,61 @@ double awp_bytes_per_cell_update(const awp_params *p);
 
 const char *awp_status_string(awp_status st);
 const char *awp_last_error(void);
+
+/* ------------------------------------------------------------------------- */
+/* Serving: continuous batching of SGT solves on one GPU.                    */
+/* No reference counterpart (the reference runs one solve per job).          */
+/*                                                                           */
+/* Requests are admitted in arrival order while their device footprint       */
+/* (awp_footprint_bytes) fits in the server's HBM budget and fewer than       */
+/* max_active solves are resident; every resident solve keeps its fields on  */
+/* the device and advances chunk_steps steps at a time on its own CUDA       */
+/* stream, so the kernels of different requests overlap on the GPU.  A       */
+/* finished request's SGT file images are copied into the caller's buffer    */
+/* and its memory is released for the next admission.  Each request's       */
+/* result is identical to running it alone (separate buffers, fixed order).  */
+/* ------------------------------------------------------------------------- */
+
+typedef struct awp_server awp_server;
+
+typedef struct {
+    awp_params params;
+    const float *media;                  /* host [nz][ny][nx][nvar]; NULL if mediastart == 0 */
+    int nsrc[AWP_MAX_COMP];
+    const int *src_xyz[AWP_MAX_COMP];    /* [nsrc][3] per component           */
+    const float *stf[AWP_MAX_COMP];      /* [nsrc][nst][6] per component      */
+    int npts;
+    const int *pts;                      /* [npts][3] cordfile coordinates    */
+    float *sgt_out;                      /* caller-owned, ncomp * awp_sgt_floats_for() floats;
+                                            must stay valid until the request ends */
+} awp_request;
+
+enum { AWP_REQ_QUEUED = 0, AWP_REQ_RUNNING = 1, AWP_REQ_DONE = 2, AWP_REQ_FAILED = 3, AWP_REQ_CANCELLED = 4 };
+
+typedef struct {
+    int state;                 /* AWP_REQ_*                                  */
+    awp_status status;         /* final status (AWP_OK when DONE)            */
+    double t_submit, t_admit, t_done;   /* seconds on the server's clock     */
+    int64_t steps_done;
+    int64_t footprint;         /* device bytes reserved for the request      */
+} awp_request_info;
+
+/* hbm_budget <= 0: 90 % of the device's free memory at creation. */
+awp_status awp_server_create(int device, int64_t hbm_budget, int max_active, int chunk_steps, awp_server **out);
+/* Copies the request description (host arrays must stay valid until the
+ * request ends); returns its id. */
+awp_status awp_submit(awp_server *sv, const awp_request *rq, int64_t *id);
+awp_status awp_poll(awp_server *sv, int64_t id, awp_request_info *info);
+/* Cancels a queued or running request; its output buffer is left as is. */
+awp_status awp_cancel(awp_server *sv, int64_t id);
+/* Waits until the request ends or timeout_s passes (AWP_ERR_TIMEOUT). */
+awp_status awp_wait(awp_server *sv, int64_t id, double timeout_s, awp_request_info *info);
+/* Seconds on the server's clock. */
+double awp_server_time(awp_server *sv);
+/* Stops the scheduler after cancelling what is still queued or running. */
+awp_status awp_server_destroy(awp_server *sv);
+/* Floats of one component's SGT file image for these parameters. */
+int64_t awp_sgt_floats_for(const awp_params *p, int npts);
 
 /* ------------------------------------------------------------------------- */
 /* File formats of the drop-in driver (pmcl3d).                              */

@@ -198,7 +198,7 @@ def test_fp64_error_budget():
     assert err <= 1e-4, err
 
 
-@pytest.mark.parametrize("precision", ["bf16", "f16"])
+@pytest.mark.parametrize("precision", ["bf16", "f16", "mixed"])
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_mixed_precision_runs_close_to_fp64(precision, kernel):
     """Media and memory variables in 16 bits, wavefields and arithmetic FP32:
