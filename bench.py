@@ -129,13 +129,35 @@ def barrier(dist):
         dist.barrier()
 
 
+def _reduce(dist, x, local, op):
+    import torch
+    dev = "cuda:%d" % local if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
 def max_over_ranks(dist, x, local):
     if dist is None:
         return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _reduce(dist, x, local, dist.ReduceOp.MAX)
+
+
+def aggregate(dist, units, seconds, local):
+    """Whole-job throughput of independent per-rank jobs: all ranks' units
+    divided by the slowest rank's time (weak scaling, no data-path
+    collective)."""
+    if dist is None:
+        return units / seconds, units, seconds
+    tot = _reduce(dist, units, local, dist.ReduceOp.SUM)
+    mx = _reduce(dist, seconds, local, dist.ReduceOp.MAX)
+    return tot / mx, tot, mx
+
+
+def shard_jobs(jobs, rank, world):
+    """Independent SGT jobs (components or requests) dealt round-robin to
+    ranks."""
+    return [j for n, j in enumerate(jobs) if n % world == rank]
 
 
 def workload():
@@ -245,9 +267,8 @@ def main():
         st1 = s.stats()
     barrier(dist)
     dev_s = st1.seconds_loop - st0.seconds_loop
-    dev_s = max_over_ranks(dist, dev_s, local)
-    updates = cells * ncomp * per_step_ts * args.steps * world
-    value = updates / dev_s * 1e-9
+    rate, updates, dev_s = aggregate(dist, float(cells * ncomp * per_step_ts * args.steps), dev_s, local)
+    value = rate * 1e-9
     ms_per_step = dev_s / args.steps * 1e3
 
     # per-kernel CUDA-event times (same solver, same stream, right after)
