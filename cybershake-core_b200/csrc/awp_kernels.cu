@@ -206,40 +206,57 @@ __global__ void k_sg_coeffs(MediaT<TM> md, int npts, const int *__restrict__ pt_
 /* two-sweep stepper                                                   */
 /* ------------------------------------------------------------------ */
 
-__device__ __forceinline__ void zchunk(const AwpGeom &g, int kchunk, int &k0, int &k1)
+/* Work items of the persistent steppers: (x tile, y tile, z chunk), x
+ * fastest so that blocks running together hold neighbouring tiles.  Every
+ * block walks items blockIdx.x, +gridDim.x, ...  z chunks are aligned to the
+ * top, so the top chunk always holds the levels nz-2..nz that fstr reads. */
+struct AwpWork {
+    int ntx, nty, nzc, kchunk, nitems;
+};
+
+__device__ __forceinline__ void work_item(const AwpGeom &g, const AwpWork &w, int item, int &bx, int &by, int &k0,
+                                          int &k1)
 {
-    /* z chunks are aligned to the top so the top chunk always holds the
-     * levels nz-2..nz that the fused fstr reads back */
-    k1 = g.nz - ((int)gridDim.z - 1 - (int)blockIdx.z) * kchunk;
-    k0 = max(1, k1 - kchunk + 1);
+    bx = item % w.ntx;
+    const int t = item / w.ntx;
+    by = t % w.nty;
+    const int bz = t / w.nty;
+    k1 = g.nz - (w.nzc - 1 - bz) * w.kchunk;
+    k0 = max(1, k1 - w.kchunk + 1);
 }
 
+/* register budgets: 256-thread blocks, more blocks per SM for one component */
+#define VEL_MINB(NC, UNR) ((UNR) == 1 ? ((NC) == 1 ? 6 : 4) : ((NC) == 1 ? 3 : 2))
+#define STR_MINB(NC, UNR) ((NC) == 1 ? 4 : ((NC) == 2 ? 3 : 2))
+
 template <int NC, class TM, int UNR>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256, VEL_MINB(NC, UNR))
 k_vel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
-      const float *__restrict__ cz, float dth, int kchunk)
+      const float *__restrict__ cz, float dth, AwpWork w)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    if (i > g.nx || j > g.ny) return;
-    int k0, k1;
-    zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane;
-    const float cxy = cx[i] * cy[j];
+    for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        int bx, by, k0, k1;
+        work_item(g, w, item, bx, by, k0, k1);
+        const int i = bx * blockDim.x + threadIdx.x + 1;
+        const int j = by * blockDim.y + threadIdx.y + 1;
+        if (i > g.nx || j > g.ny) continue;
+        const float cxy = cx[i] * cy[j];
 #pragma unroll (UNR)
-    for (int k = k0; k <= k1; ++k) {
-        const int c = g.idx(i, j, k);
-        float fu, fv, fw;
-        vel_factors(md, c, sy, sz, dth, fu, fv, fw);
-        const float crj = cxy * cz[k];
+        for (int k = k0; k <= k1; ++k) {
+            const int c = g.idx(i, j, k);
+            float fu, fv, fw;
+            vel_factors(md, c, sy, sz, dth, fu, fv, fw);
+            const float crj = cxy * cz[k];
 #pragma unroll
-        for (int q = 0; q < NC; ++q) {
-            float u, v, w;
-            vel_one(cs.c[q], c, sy, sz, fu, fv, fw, u, v, w);
-            /* Cerjan: the factor is exactly 1 outside the sponge zones */
-            cs.c[q].f[AF_U][c] = u * crj;
-            cs.c[q].f[AF_V][c] = v * crj;
-            cs.c[q].f[AF_W][c] = w * crj;
+            for (int q = 0; q < NC; ++q) {
+                float u, v, w_;
+                vel_one(cs.c[q], c, sy, sz, fu, fv, fw, u, v, w_);
+                /* Cerjan: the factor is exactly 1 outside the sponge zones */
+                cs.c[q].f[AF_U][c] = u * crj;
+                cs.c[q].f[AF_V][c] = v * crj;
+                cs.c[q].f[AF_W][c] = w_ * crj;
+            }
         }
     }
 }
@@ -275,60 +292,62 @@ __global__ void k_fsvel(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs)
 }
 
 template <int NC, class TM, class TR, int UNR>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256, STR_MINB(NC, UNR))
 k_str(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx, const float *__restrict__ cy,
-      const float *__restrict__ cz, const float *__restrict__ tau, float dth, float dt, float dh1, int kchunk,
+      const float *__restrict__ cz, const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w,
       int nve)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    if (i > g.nx || j > g.ny) return;
-    int k0, k1;
-    zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane;
-    const float cxy = cx[i] * cy[j];
-    const int itxy = ((j & 1) << 1) | (i & 1);
+    for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        int bx, by, k0, k1;
+        work_item(g, w, item, bx, by, k0, k1);
+        const int i = bx * blockDim.x + threadIdx.x + 1;
+        const int j = by * blockDim.y + threadIdx.y + 1;
+        if (i > g.nx || j > g.ny) continue;
+        const float cxy = cx[i] * cy[j];
+        const int itxy = ((j & 1) << 1) | (i & 1);
 #pragma unroll (UNR)
-    for (int k = k0; k <= k1; ++k) {
-        const int c = g.idx(i, j, k);
-        const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
-        const StrCoef kc = str_coef(md, c, sy, sz, nve, tau[it], tau[8 + it]);
-        const float crj = cxy * cz[k];
+        for (int k = k0; k <= k1; ++k) {
+            const int c = g.idx(i, j, k);
+            const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
+            const StrCoef kc = str_coef(md, c, sy, sz, nve, tau[it], tau[8 + it]);
+            const float crj = cxy * cz[k];
 #pragma unroll
-        for (int q = 0; q < NC; ++q) {
-            AwpComp &cp = cs.c[q];
-            const GVel V{cp.f[AF_U], cp.f[AF_V], cp.f[AF_W], c, sy, sz};
-            const Stress6 s{cp.f[AF_XX][c], cp.f[AF_YY][c], cp.f[AF_ZZ][c], cp.f[AF_XY][c], cp.f[AF_XZ][c], cp.f[AF_YZ][c]};
-            Stress6 o;
-            if (nve == 1) {
-                float r[6];
+            for (int q = 0; q < NC; ++q) {
+                AwpComp &cp = cs.c[q];
+                const GVel V{cp.f[AF_U], cp.f[AF_V], cp.f[AF_W], c, sy, sz};
+                const Stress6 s{cp.f[AF_XX][c], cp.f[AF_YY][c], cp.f[AF_ZZ][c], cp.f[AF_XY][c], cp.f[AF_XZ][c], cp.f[AF_YZ][c]};
+                Stress6 o;
+                if (nve == 1) {
+                    float r[6];
 #pragma unroll
-                for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
-                const VelDiff d = vel_diff(V);
-                o = str_visco(kc, d, s, r, dth, dt, dh1);
+                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
+                    const VelDiff d = vel_diff(V);
+                    o = str_visco(kc, d, s, r, dth, dt, dh1);
 #pragma unroll
-                for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
-            } else {
-                o = str_elastic(kc, V, s, dth);
+                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
+                } else {
+                    o = str_elastic(kc, V, s, dth);
+                }
+                cp.f[AF_XX][c] = o.xx * crj; cp.f[AF_YY][c] = o.yy * crj; cp.f[AF_ZZ][c] = o.zz * crj;
+                cp.f[AF_XY][c] = o.xy * crj; cp.f[AF_XZ][c] = o.xz * crj; cp.f[AF_YZ][c] = o.yz * crj;
             }
-            cp.f[AF_XX][c] = o.xx * crj; cp.f[AF_YY][c] = o.yy * crj; cp.f[AF_ZZ][c] = o.zz * crj;
-            cp.f[AF_XY][c] = o.xy * crj; cp.f[AF_XZ][c] = o.xz * crj; cp.f[AF_YZ][c] = o.yz * crj;
         }
-    }
-    if (k1 == g.nz) {
-        /* fstr (operator.f:594-606) on this thread's own column */
-        const int c = g.idx(i, j, g.nz);
+        if (k1 == g.nz) {
+            /* fstr (operator.f:594-606) on this thread's own column */
+            const int c = g.idx(i, j, g.nz);
 #pragma unroll
-        for (int q = 0; q < NC; ++q) {
-            float *zz = cs.c[q].f[AF_ZZ], *xz = cs.c[q].f[AF_XZ], *yz = cs.c[q].f[AF_YZ];
-            zz[c + sz] = -__ldcg(&zz[c]);
-            zz[c + 2 * sz] = -__ldcg(&zz[c - sz]);
-            xz[c + sz] = -__ldcg(&xz[c - sz]);
-            xz[c + 2 * sz] = -__ldcg(&xz[c - 2 * sz]);
-            yz[c + sz] = -__ldcg(&yz[c - sz]);
-            yz[c + 2 * sz] = -__ldcg(&yz[c - 2 * sz]);
-            xz[c] = 0.0f;
-            yz[c] = 0.0f;
+            for (int q = 0; q < NC; ++q) {
+                float *zz = cs.c[q].f[AF_ZZ], *xz = cs.c[q].f[AF_XZ], *yz = cs.c[q].f[AF_YZ];
+                zz[c + sz] = -__ldcg(&zz[c]);
+                zz[c + 2 * sz] = -__ldcg(&zz[c - sz]);
+                xz[c + sz] = -__ldcg(&xz[c - sz]);
+                xz[c + 2 * sz] = -__ldcg(&xz[c - 2 * sz]);
+                yz[c + sz] = -__ldcg(&yz[c - sz]);
+                yz[c + 2 * sz] = -__ldcg(&yz[c - 2 * sz]);
+                xz[c] = 0.0f;
+                yz[c] = 0.0f;
+            }
         }
     }
 }
@@ -354,16 +373,18 @@ template <int NC, class TM, class TR, int TY>
 __global__ void __launch_bounds__(FX * TY)
 k_fused(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> old, AwpCompSet<NC> nw, const float *__restrict__ cx,
         const float *__restrict__ cy, const float *__restrict__ cz, const float *__restrict__ tau, float dth,
-        float dt, float dh1, int kchunk, int nve)
+        float dt, float dh1, AwpWork wk, int nve)
 {
     constexpr int RX = FX + 4, RY = TY + 4, NV = RX * RY, NT = FX * TY;
     constexpr int PLANE = 3 * NC * NV;                 /* one ring slot      */
     extern __shared__ float ring[];                    /* [FSLOT][NC][3][NV] */
     const int tx = threadIdx.x, ty = threadIdx.y, t = ty * FX + tx;
-    const int x0 = blockIdx.x * FX + 1, y0 = blockIdx.y * TY + 1;
-    int k0, k1;
-    zchunk(g, kchunk, k0, k1);
     const int sy = g.px, sz = g.plane, nz = g.nz;
+    (void)RY;
+    for (int item = blockIdx.x; item < wk.nitems; item += gridDim.x) {
+    int bx, by, k0, k1;
+    work_item(g, wk, item, bx, by, k0, k1);
+    const int x0 = bx * FX + 1, y0 = by * TY + 1;
 
     /* this thread's cell in the stress phase */
     const int is = x0 + tx, js = y0 + ty;
@@ -498,6 +519,8 @@ k_fused(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> old, AwpCompSet<NC> nw, const f
                 hyz[q][1] = hyz[q][0]; hyz[q][0] = ns.yz;
             }
         }
+    }
+    __syncthreads();   /* the next item's first velocity levels reuse the ring */
     }
 }
 
@@ -777,9 +800,32 @@ static void comp_sets(const AwpStepArgs &s, AwpCompSet<NC> &a, AwpCompSet<NC> &b
 template <int TY, int NC>
 static size_t fused_smem() { return (size_t)FSLOT * 3 * NC * (FX + 4) * (TY + 4) * sizeof(float); }
 
+static AwpWork make_work(const AwpGeom &g, int ty, int kchunk)
+{
+    AwpWork w;
+    w.ntx = (g.nx + 31) / 32;
+    w.nty = (g.ny + ty - 1) / ty;
+    w.kchunk = kchunk;
+    w.nzc = (g.nz + kchunk - 1) / kchunk;
+    w.nitems = w.ntx * w.nty * w.nzc;
+    return w;
+}
+
+/* persistent grid: every SM filled to its occupancy, capped by the items */
+template <class K>
+static int persistent_grid(K kernel, int threads, size_t smem, int nitems)
+{
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) per = 1;
+    const int grid = nsm * per;
+    return grid < nitems ? grid : nitems;
+}
+
 template <int NC, class TM, class TR, int TY>
 static cudaError_t launch_fused(const AwpStepArgs &s, const MediaT<TM> &md, const AwpCompSet<NC> &cs,
-                                const AwpCompSet<NC> &cn, int nzb, cudaStream_t st)
+                                const AwpCompSet<NC> &cn, cudaStream_t st)
 {
     dim3 b(FX, TY);
     const size_t smem = fused_smem<TY, NC>();
@@ -792,8 +838,31 @@ static cudaError_t launch_fused(const AwpStepArgs &s, const MediaT<TM> &md, cons
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_done |= 1ull << dev;
     }
-    k_fused<NC, TM, TR, TY><<<plane_grid(s.g, b, nzb), b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau,
-                                                                     s.dth, s.dt, s.dh1, s.kchunk, s.nve);
+    const AwpWork w = make_work(s.g, TY, s.kchunk);
+    const int grid = persistent_grid(k_fused<NC, TM, TR, TY>, FX * TY, smem, w.nitems);
+    k_fused<NC, TM, TR, TY><<<grid, b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w,
+                                                   s.nve);
+    return cudaGetLastError();
+}
+
+template <int NC, class TM, int UNR>
+static cudaError_t launch_vel(const AwpStepArgs &s, const MediaT<TM> &md, const AwpCompSet<NC> &cs, int ty,
+                              cudaStream_t st)
+{
+    const AwpWork w = make_work(s.g, ty, s.kchunk_sweep);
+    const int grid = persistent_grid(k_vel<NC, TM, UNR>, 32 * ty, 0, w.nitems);
+    k_vel<NC, TM, UNR><<<grid, dim3(32, ty), 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, w);
+    return cudaGetLastError();
+}
+
+template <int NC, class TM, class TR, int UNR>
+static cudaError_t launch_str(const AwpStepArgs &s, const MediaT<TM> &md, const AwpCompSet<NC> &cs, int ty,
+                              cudaStream_t st)
+{
+    const AwpWork w = make_work(s.g, ty, s.kchunk_sweep);
+    const int grid = persistent_grid(k_str<NC, TM, TR, UNR>, 32 * ty, 0, w.nitems);
+    k_str<NC, TM, TR, UNR><<<grid, dim3(32, ty), 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1,
+                                                          w, s.nve);
     return cudaGetLastError();
 }
 
@@ -803,29 +872,19 @@ static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st
     AwpCompSet<NC> cs, cn;
     comp_sets<NC>(s, cs, cn);
     const MediaT<TM> md = media_view<TM>(s.md);
-    const int nzb = (s.g.nz + s.kchunk - 1) / s.kchunk;
-    const int ty = (s.ty == 4 || s.ty == 16) ? s.ty : 8;
     if (part == AWP_PART_VEL) {
-        dim3 b(32, ty);
-        if (s.unroll == 2)
-            k_vel<NC, TM, 2><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
-        else
-            k_vel<NC, TM, 1><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, s.kchunk);
+        const int ty = s.ty == 4 ? 4 : 8;
+        return s.unroll == 2 ? launch_vel<NC, TM, 2>(s, md, cs, ty, st) : launch_vel<NC, TM, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FSVEL) {
         dim3 b(32, 8);
         k_fsvel<NC, TM><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, md, cs);
     } else if (part == AWP_PART_STR) {
-        dim3 b(32, ty);
-        if (s.unroll == 2)
-            k_str<NC, TM, TR, 2><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
-                                                                        s.dt, s.dh1, s.kchunk, s.nve);
-        else
-            k_str<NC, TM, TR, 1><<<plane_grid(s.g, b, nzb), b, 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth,
-                                                                        s.dt, s.dh1, s.kchunk, s.nve);
+        const int ty = s.ty == 4 ? 4 : 8;
+        return s.unroll == 2 ? launch_str<NC, TM, TR, 2>(s, md, cs, ty, st) : launch_str<NC, TM, TR, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FUSED) {
-        if (ty == 4) return launch_fused<NC, TM, TR, 4>(s, md, cs, cn, nzb, st);
-        if (ty == 16) return launch_fused<NC, TM, TR, 16>(s, md, cs, cn, nzb, st);
-        return launch_fused<NC, TM, TR, 8>(s, md, cs, cn, nzb, st);
+        if (s.ty == 4) return launch_fused<NC, TM, TR, 4>(s, md, cs, cn, st);
+        if (s.ty == 16) return launch_fused<NC, TM, TR, 16>(s, md, cs, cn, st);
+        return launch_fused<NC, TM, TR, 8>(s, md, cs, cn, st);
     } else {
         return cudaErrorInvalidValue;
     }

@@ -14,7 +14,8 @@ struct AwpStepArgs {
     const float *cx, *cy, *cz;   /* sponge factors, index 1..n              */
     const float *tau;            /* [16] tau1[8] then tau2[8]               */
     float dth, dt, dh1;
-    int kchunk;                  /* z levels per thread block               */
+    int kchunk;                  /* z levels per fused work item            */
+    int kchunk_sweep;            /* z levels per two-sweep work item        */
     int nve;
     int fused;                   /* 1: single-sweep stepper                 */
     int rtype;                   /* AWP_STORE_* of r1..r6                   */

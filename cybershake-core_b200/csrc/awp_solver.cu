@@ -72,7 +72,8 @@ struct awp_solver {
     int steps_done;
     int started;
     int media_loaded;
-    int kchunk;
+    int kchunk;                      /* z levels per fused work item        */
+    int kchunk_sweep;                /* z levels per two-sweep work item    */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
     float vtst, vtst1, dth, dh1;
@@ -195,17 +196,22 @@ static int env_int(const char *name, int dflt)
     return (v && *v) ? atoi(v) : dflt;
 }
 
+/* z levels per work item of the persistent steppers: enough items to keep
+ * every SM busy (about eight per SM), but chunks no shorter than kmin -- the
+ * fused stepper recomputes four velocity levels per chunk -- nor longer than
+ * kmax; a top chunk always holds at least the three levels fstr reads. */
 static int choose_kchunk(const AwpGeom &g, int fused, int ty)
 {
-    const int over = env_int("AWP_TUNE_KCHUNK", 0);
+    const int over = env_int(fused ? "AWP_TUNE_KCHUNK" : "AWP_TUNE_KSWEEP", 0);
     if (over > 0) return over < 8 ? 8 : (over > g.nz ? g.nz : over);
-    const int bxy = ((g.nx + 31) / 32) * ((g.ny + ty - 1) / ty);
-    const int want = fused ? 148 * 4 : 148 * 8;
-    int nzb = (want + bxy - 1) / bxy;
-    if (nzb < 1) nzb = 1;
-    int kc = (g.nz + nzb - 1) / nzb;
-    const int kmin = fused ? 24 : 8;   /* fused: 4 redundant velocity levels per chunk */
+    const int tiles = ((g.nx + 31) / 32) * ((g.ny + ty - 1) / ty);
+    const int want = 148 * 8;
+    int nzc = (want + tiles - 1) / tiles;
+    if (nzc < 1) nzc = 1;
+    int kc = (g.nz + nzc - 1) / nzc;
+    const int kmin = fused ? 16 : 8, kmax = fused ? 64 : 32;
     if (kc < kmin) kc = kmin;
+    if (kc > kmax) kc = kmax;
     if (kc > g.nz) kc = g.nz;
     return kc;
 }
@@ -420,7 +426,8 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->ty = env_int("AWP_TUNE_TY", 8);
     if (s->ty != 4 && s->ty != 16) s->ty = 8;
     s->unroll = env_int("AWP_TUNE_UNROLL", 1) == 2 ? 2 : 1;
-    s->kchunk = choose_kchunk(s->g, s->fused, s->ty);
+    s->kchunk = choose_kchunk(s->g, 1, s->ty);
+    s->kchunk_sweep = choose_kchunk(s->g, 0, 8);
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
     TRYCU(cudaStreamSynchronize(s->stream));
@@ -749,6 +756,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     for (int q = 0; q < p->ncomp; q++) { a.comp[q] = s->comp[rd][q]; a.comp_new[q] = s->comp[wr][q]; }
     a.cx = s->cx; a.cy = s->cy; a.cz = s->cz; a.tau = s->tau;
     a.dth = s->dth; a.dt = p->dt; a.dh1 = s->dh1; a.kchunk = s->kchunk; a.nve = p->nve;
+    a.kchunk_sweep = s->kchunk_sweep;
     a.rtype = s->rstore;
     a.ty = s->ty;
     a.unroll = s->unroll;

@@ -70,7 +70,7 @@ def test_fortran_command_line(tmp_path, ifault):
     assert int(last[:6]) == NST + 1
     np.testing.assert_allclose([float(last[6 + 10 * q:16 + 10 * q]) for q in range(3)], cj[-1], rtol=6e-3, atol=1e-30)
     chkp = (tmp_path / "out" / "CHKP").read_text()
-    assert "STABILITY CRITERIA .5 > CMAX*DT/DX" in chkp and "# OF TIME STEPS  61" in chkp
+    assert "STABILITY CRITERIA .5 > CMAX*DT/DX" in chkp and "# OF TIME STEPS   61" in chkp   # I5
 
 
 @pytest.mark.gpu
