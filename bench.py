@@ -160,8 +160,19 @@ def shard_jobs(jobs, rank, world):
     return [j for n, j in enumerate(jobs) if n % world == rank]
 
 
-def workload():
+def workload(args=None):
+    """The config-2 job, or a reduced grid / component set for small profiling
+    captures (--grid, --components); the name records any change."""
     w = ai.config(CONFIG_N)
+    if args is None:
+        return w
+    import dataclasses
+    if args.grid:
+        nx, ny, nz = (int(v) for v in args.grid.split(","))
+        w = dataclasses.replace(w, name="layered_%dx%dx%d" % (nx, ny, nz), nx=nx, ny=ny, nz=nz,
+                                src_xyz=(nx // 2, ny // 2, min(21, nz)), npts=min(w.npts, nx * ny // 4))
+    if args.components:
+        w = dataclasses.replace(w, name=w.name + "_c%d" % args.components, igreen=w.igreen[:args.components])
     return w
 
 
@@ -209,7 +220,7 @@ def run_reference(args):
     """--impl reference: the CPU path on the host cores, rank 0 only."""
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    w = workload()
+    w = workload(args)
     media = w.media()
     stf = w.stf(0)
     rate, threads, times = cpu_oracle_rate(w, media, stf, nsteps=max(args.steps, 1), warm=max(args.warmup, 1))
@@ -241,13 +252,15 @@ def main():
     ap.add_argument("--e2e-solves", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", default="", help="nx,ny,nz: reduced grid for profiling captures")
+    ap.add_argument("--components", type=int, default=0, help="first n of the fx, fy, fz components")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
 
     dist, rank, world, local = dist_setup(args.gpus)
     import awpsgt
-    w = workload()
+    w = workload(args)
     media = w.media()
     pts = w.points()
     stfs = [w.stf(q) for q in range(len(w.igreen))]

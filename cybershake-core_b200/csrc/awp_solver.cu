@@ -170,7 +170,7 @@ static int store_of(const awp_params *p)
 }
 /* storage of r1..r6 */
 static int rstore_of(const awp_params *p) { return p->precision == AWP_PREC_F32 ? AWP_STORE_F32 : AWP_STORE_BF16; }
-static int fused_of(const awp_params *p) { return p->kernel != AWP_KERNEL_TWO_SWEEP; }
+static int fused_of(const awp_params *p) { return p->kernel == AWP_KERNEL_FUSED; }
 static double media_word(int store) { return store == AWP_STORE_F32 ? 4.0 : 2.0; }
 
 extern "C" double awp_bytes_per_cell_update(const awp_params *p)
@@ -209,7 +209,7 @@ static int choose_kchunk(const AwpGeom &g, int fused, int ty)
     int nzc = (want + tiles - 1) / tiles;
     if (nzc < 1) nzc = 1;
     int kc = (g.nz + nzc - 1) / nzc;
-    const int kmin = fused ? 16 : 8, kmax = fused ? 64 : 32;
+    const int kmin = fused ? 16 : 8, kmax = fused ? 64 : 8;
     if (kc < kmin) kc = kmin;
     if (kc > kmax) kc = kmax;
     if (kc > g.nz) kc = g.nz;
@@ -427,7 +427,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     if (s->ty != 4 && s->ty != 16) s->ty = 8;
     s->unroll = env_int("AWP_TUNE_UNROLL", 1) == 2 ? 2 : 1;
     s->kchunk = choose_kchunk(s->g, 1, s->ty);
-    s->kchunk_sweep = choose_kchunk(s->g, 0, 8);
+    s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
     TRYCU(cudaStreamSynchronize(s->stream));

@@ -65,7 +65,7 @@ typedef enum {
 
 /* Stepper implementation. */
 typedef enum {
-    AWP_KERNEL_AUTO = 0,      /* library picks (the fused stepper)             */
+    AWP_KERNEL_AUTO = 0,      /* library picks (the two-sweep stepper)         */
     AWP_KERNEL_TWO_SWEEP = 1, /* velocity sweep, then stress sweep, in place   */
     AWP_KERNEL_FUSED = 2      /* one z-march per tile: velocity on a 2-cell
                                  halo, then stress; ping-pong wavefields       */
