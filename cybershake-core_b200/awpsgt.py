@@ -39,7 +39,7 @@ EXPORTED = [
     "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free", "awp_profile_steps",
     "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
-    "awp_server_destroy", "awp_sgt_floats_for",
+    "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc",
 ]
 
 
@@ -151,6 +151,7 @@ def load_library(path: str = LIB_PATH):
         "awp_sync": (C.c_int, [C.c_void_p]),
         "awp_device_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, P(C.c_void_p), P(Layout)]),
         "awp_field_energy": (C.c_int, [P(C.c_void_p), C.c_int, P(Layout), C.c_void_p]),
+        "awp_field_energy_noalloc": (C.c_int, [P(C.c_void_p), C.c_int, P(Layout), C.c_void_p, C.c_void_p]),
         "awp_energy": (C.c_int, [C.c_void_p, C.c_void_p]),
         "awp_server_create": (C.c_int, [C.c_int, C.c_int64, C.c_int, C.c_int, P(C.c_void_p)]),
         "awp_submit": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_int64)]),
@@ -413,6 +414,15 @@ def field_energy(ptrs: Sequence[int], layout: Layout, ncomp: int) -> np.ndarray:
     out = torch.zeros(ncomp, dtype=torch.float64, device="cuda")
     _check(load_library().awp_field_energy(arr, ncomp, C.byref(layout), C.c_void_p(out.data_ptr())))
     return out.cpu().numpy()
+
+
+def field_energy_noalloc(ptrs: Sequence[int], layout: Layout, ncomp: int, out, stream: int = 0) -> None:
+    """awp_field_energy_noalloc: enqueues the energy of the device arrays into
+    the caller's device buffer `out` (a torch float64 tensor of >= ncomp
+    elements) on `stream` (a raw cudaStream_t handle) and returns at once."""
+    arr = (C.c_void_p * len(ptrs))(*ptrs)
+    _check(load_library().awp_field_energy_noalloc(arr, ncomp, C.byref(layout), C.c_void_p(out.data_ptr()),
+                                                   C.c_void_p(stream)))
 
 
 def read_in3d(path: str) -> In3dC:

@@ -18,6 +18,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <mutex>
 #include <new>
 
 #include "awp_internal.h"
@@ -1190,6 +1191,60 @@ extern "C" awp_status awp_field_energy(const float *const *fields, int ncomp, co
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     cudaFree(partial);
     if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_field_energy: %s", cudaGetErrorString(e));
+    return AWP_OK;
+}
+
+/* Scratch of awp_field_energy_noalloc: the pass-1 partial sums, one FP64
+ * value per block and component (592 x 3 doubles, 14,208 bytes), in static
+ * device memory of this module so that the call itself allocates nothing.
+ * Every slot pass 2 reads is written by pass 1 of the same call, so nothing
+ * has to start at zero.  Calls on one device share it: two of them that
+ * overlap in time (other streams or threads) race on it. */
+#define AWP_NOALLOC_PARTIALS (AWP_EN_GRID * AWP_MAX_COMP)
+#define AWP_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) double g_energy_scratch[AWP_NOALLOC_PARTIALS];
+static double *g_energy_scratch_addr[AWP_NOALLOC_MAX_DEVICES];
+static std::mutex g_energy_scratch_mu;
+
+/* Device address of the scratch on the current device: looked up once per
+ * device (cudaGetSymbolAddress, which may load this module onto the device --
+ * the reason the first call on a device is the set-up call), then cached. */
+static awp_status energy_scratch(double **addr)
+{
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= AWP_NOALLOC_MAX_DEVICES)
+        return set_err(AWP_ERR_PARAM, "awp_field_energy_noalloc: device %d beyond the %d it keeps scratch for", dev,
+                       AWP_NOALLOC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_energy_scratch_mu);
+    if (!g_energy_scratch_addr[dev]) {
+        void *a = NULL;
+        const cudaError_t e = cudaGetSymbolAddress(&a, g_energy_scratch);
+        if (e != cudaSuccess || !a)
+            return set_err(AWP_ERR_CUDA, "awp_field_energy_noalloc: scratch address on device %d: %s", dev,
+                           cudaGetErrorString(e));
+        g_energy_scratch_addr[dev] = (double *)a;
+    }
+    *addr = g_energy_scratch_addr[dev];
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_field_energy_noalloc(const float *const *fields, int ncomp, const awp_layout *L,
+                                               double *out, void *stream)
+{
+    if (ncomp > AWP_MAX_COMP || (int64_t)ncomp * AWP_EN_GRID > AWP_NOALLOC_PARTIALS)
+        return set_err(AWP_ERR_PARAM, "awp_field_energy_noalloc: %d components exceed the static scratch "
+                       "(%d partial sums: at most %d components)", ncomp, AWP_NOALLOC_PARTIALS, AWP_MAX_COMP);
+    awp_status st = check_layout(fields, ncomp, L);
+    if (st != AWP_OK) return st;
+    if (!out) return set_err(AWP_ERR_PARAM, "null output");
+    double *partial = NULL;
+    st = energy_scratch(&partial);
+    if (st != AWP_OK) return st;
+    AwpEnergyArgs a;
+    energy_args_from(fields, ncomp, L, a);
+    const cudaError_t e = awp_launch_energy(a, partial, AWP_EN_GRID, out, NULL, (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_field_energy_noalloc: %s", cudaGetErrorString(e));
     return AWP_OK;
 }
 

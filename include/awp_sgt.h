@@ -209,6 +209,23 @@ awp_status awp_device_field(awp_solver *s, int comp, int field, float **ptr, awp
  * counterpart (the reference has no monitor). */
 awp_status awp_field_energy(const float *const *fields, int ncomp, const awp_layout *L, double *out);
 
+/* awp_field_energy without any allocation (no counterpart in the reference).
+ * For callers that must not allocate device memory mid-run: a host that runs
+ * several solves side by side on one device (cudaFree waits for the whole
+ * device, stalling every other solve's stream) or that admits work against a
+ * fixed device-memory budget (an allocation here could fail or overrun it).
+ * Same passes and result as awp_field_energy, enqueued on `stream` (a
+ * cudaStream_t; NULL = the default stream) without synchronizing: `out` is
+ * ready once that stream's work completes.  The partial sums live in a static
+ * device array of the library (592 x 3 doubles), so ncomp is at most 3 and a
+ * larger count is rejected with AWP_ERR_PARAM.  The first call on a device
+ * does a one-time set-up (looks up that array's device address) and should
+ * come before any stream capture.  Calls on one device share the array: calls
+ * that overlap in time, from other streams or threads, race and must be
+ * serialized by the caller. */
+awp_status awp_field_energy_noalloc(const float *const *fields, int ncomp, const awp_layout *L, double *out,
+                                    void *stream);
+
 /* Energy of a solver's current wavefield (host output, ncomp doubles). */
 awp_status awp_energy(awp_solver *s, double *out);
 
