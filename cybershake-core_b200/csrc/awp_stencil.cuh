@@ -46,40 +46,61 @@ struct MediaT {
 /* velocity update of one cell (all NC components)                    */
 /* ------------------------------------------------------------------ */
 
-/* d1 averages of operator.f:120-121, 171-172, 224-225 -> dth/d */
+/* d1 averages of operator.f:120-121, 171-172, 224-225 -> dth/d, from the
+ * seven d1 values around the cell: a (0,0,0) b (0,-1,0) c (0,0,-1)
+ * d (0,-1,-1) e (1,0,0) f (1,0,-1) g (1,-1,0) */
+__device__ __forceinline__ void vel_factors7(float da, float db, float dc, float dd, float de, float df, float dg,
+                                             float dth, float &fu, float &fv, float &fw)
+{
+    fu = dth / (0.25f * ((da + db) + (dc + dd)));
+    fv = dth / (0.25f * ((da + de) + (dc + df)));
+    fw = dth / (0.25f * ((da + de) + (db + dg)));
+}
+
 template <class TM>
 __device__ __forceinline__ void vel_factors(const MediaT<TM> &md, int c, int sy, int sz, float dth,
                                             float &fu, float &fv, float &fw)
 {
     const float da = md(AM_D1, c), db = md(AM_D1, c - sy), dc = md(AM_D1, c - sz), dd = md(AM_D1, c - sy - sz);
     const float de = md(AM_D1, c + 1), df = md(AM_D1, c + 1 - sz), dg = md(AM_D1, c + 1 - sy);
-    fu = dth / (0.25f * ((da + db) + (dc + dd)));
-    fv = dth / (0.25f * ((da + de) + (dc + df)));
-    fw = dth / (0.25f * ((da + de) + (db + dg)));
+    vel_factors7(da, db, dc, dd, de, df, dg, dth, fu, fv, fw);
 }
 
-/* new (u, v, w) of one component, before the sponge factor */
+/* stress indices of the accessors below */
+enum { S_XX = 0, S_YY = 1, S_ZZ = 2, S_XY = 3, S_XZ = 4, S_YZ = 5 };
+
+/* new (u, v, w) of one component, before the sponge factor; A::s(f, dx, dy,
+ * dz) is stress f at the offset (operator.f:122-132, 173-183, 226-236) */
+template <class A>
+__device__ __forceinline__ void vel_one_t(const A &S, float u0, float v0, float w0, float fu, float fv, float fw,
+                                          float &u, float &v, float &w)
+{
+    u = u0 + fu * (
+        C1 * (S.s(S_XX, 0, 0, 0) - S.s(S_XX, -1, 0, 0)) + C2 * (S.s(S_XX, 1, 0, 0) - S.s(S_XX, -2, 0, 0)) +
+        C1 * (S.s(S_XY, 0, 0, 0) - S.s(S_XY, 0, -1, 0)) + C2 * (S.s(S_XY, 0, 1, 0) - S.s(S_XY, 0, -2, 0)) +
+        C1 * (S.s(S_XZ, 0, 0, 0) - S.s(S_XZ, 0, 0, -1)) + C2 * (S.s(S_XZ, 0, 0, 1) - S.s(S_XZ, 0, 0, -2)));
+    v = v0 + fv * (
+        C1 * (S.s(S_XY, 1, 0, 0) - S.s(S_XY, 0, 0, 0)) + C2 * (S.s(S_XY, 2, 0, 0) - S.s(S_XY, -1, 0, 0)) +
+        C1 * (S.s(S_YY, 0, 1, 0) - S.s(S_YY, 0, 0, 0)) + C2 * (S.s(S_YY, 0, 2, 0) - S.s(S_YY, 0, -1, 0)) +
+        C1 * (S.s(S_YZ, 0, 0, 0) - S.s(S_YZ, 0, 0, -1)) + C2 * (S.s(S_YZ, 0, 0, 1) - S.s(S_YZ, 0, 0, -2)));
+    w = w0 + fw * (
+        C1 * (S.s(S_XZ, 1, 0, 0) - S.s(S_XZ, 0, 0, 0)) + C2 * (S.s(S_XZ, 2, 0, 0) - S.s(S_XZ, -1, 0, 0)) +
+        C1 * (S.s(S_YZ, 0, 0, 0) - S.s(S_YZ, 0, -1, 0)) + C2 * (S.s(S_YZ, 0, 1, 0) - S.s(S_YZ, 0, -2, 0)) +
+        C1 * (S.s(S_ZZ, 0, 0, 1) - S.s(S_ZZ, 0, 0, 0)) + C2 * (S.s(S_ZZ, 0, 0, 2) - S.s(S_ZZ, 0, 0, -1)));
+}
+
+/* stresses of one component in global memory */
+struct GStr {
+    const float *__restrict__ f[6];
+    int c, sy, sz;
+    __device__ __forceinline__ float s(int a, int dx, int dy, int dz) const { return f[a][c + dx + dy * sy + dz * sz]; }
+};
+
 __device__ __forceinline__ void vel_one(const AwpComp &o, int c, int sy, int sz, float fu, float fv, float fw,
                                         float &u, float &v, float &w)
 {
-    const float *__restrict__ xx = o.f[AF_XX];
-    const float *__restrict__ yy = o.f[AF_YY];
-    const float *__restrict__ zz = o.f[AF_ZZ];
-    const float *__restrict__ xy = o.f[AF_XY];
-    const float *__restrict__ xz = o.f[AF_XZ];
-    const float *__restrict__ yz = o.f[AF_YZ];
-    u = o.f[AF_U][c] + fu * (
-        C1 * (xx[c] - xx[c - 1]) + C2 * (xx[c + 1] - xx[c - 2]) +
-        C1 * (xy[c] - xy[c - sy]) + C2 * (xy[c + sy] - xy[c - 2 * sy]) +
-        C1 * (xz[c] - xz[c - sz]) + C2 * (xz[c + sz] - xz[c - 2 * sz]));
-    v = o.f[AF_V][c] + fv * (
-        C1 * (xy[c + 1] - xy[c]) + C2 * (xy[c + 2] - xy[c - 1]) +
-        C1 * (yy[c + sy] - yy[c]) + C2 * (yy[c + 2 * sy] - yy[c - sy]) +
-        C1 * (yz[c] - yz[c - sz]) + C2 * (yz[c + sz] - yz[c - 2 * sz]));
-    w = o.f[AF_W][c] + fw * (
-        C1 * (xz[c + 1] - xz[c]) + C2 * (xz[c + 2] - xz[c - 1]) +
-        C1 * (yz[c] - yz[c - sy]) + C2 * (yz[c + sy] - yz[c - 2 * sy]) +
-        C1 * (zz[c + sz] - zz[c]) + C2 * (zz[c + 2 * sz] - zz[c - sz]));
+    const GStr S{{o.f[AF_XX], o.f[AF_YY], o.f[AF_ZZ], o.f[AF_XY], o.f[AF_XZ], o.f[AF_YZ]}, c, sy, sz};
+    vel_one_t(S, o.f[AF_U][c], o.f[AF_V][c], o.f[AF_W][c], fu, fv, fw, u, v, w);
 }
 
 /* ------------------------------------------------------------------ */
@@ -91,31 +112,32 @@ struct StrCoef {
     float xl, xm, qpa, vh1, xmu4, xmu5, xmu6, vh2_r4, vh2_r5, vh2_r6, vx1, vx2;
 };
 
-template <class TM>
-__device__ __forceinline__ StrCoef str_coef(const MediaT<TM> &md, int c, int sy, int sz, int nve,
-                                            float vx1, float vx2)
+/* A::m(a, dx, dy, dz) is media array a at the offset */
+template <class A>
+__device__ __forceinline__ StrCoef str_coef_t(const A &M, int nve, float vx1, float vx2)
 {
     StrCoef k;
-    k.xl = 8.0f / (md(AM_LAM, c) + md(AM_LAM, c + 1) + md(AM_LAM, c - sy) + md(AM_LAM, c + 1 - sy) +
-                   md(AM_LAM, c - sz) + md(AM_LAM, c + 1 - sz) + md(AM_LAM, c - sy - sz) + md(AM_LAM, c + 1 - sy - sz));
-    k.xm = 8.0f / (md(AM_MU, c) + md(AM_MU, c + 1) + md(AM_MU, c - sy) + md(AM_MU, c + 1 - sy) +
-                   md(AM_MU, c - sz) + md(AM_MU, c + 1 - sz) + md(AM_MU, c - sy - sz) + md(AM_MU, c + 1 - sy - sz));
-    const float mu0 = md(AM_MU, c);
-    k.xmu4 = 2.0f / (mu0 + md(AM_MU, c - sz));
-    k.xmu5 = 2.0f / (mu0 + md(AM_MU, c - sy));
-    k.xmu6 = 2.0f / (mu0 + md(AM_MU, c + 1));
+    k.xl = 8.0f / (M.m(AM_LAM, 0, 0, 0) + M.m(AM_LAM, 1, 0, 0) + M.m(AM_LAM, 0, -1, 0) + M.m(AM_LAM, 1, -1, 0) +
+                   M.m(AM_LAM, 0, 0, -1) + M.m(AM_LAM, 1, 0, -1) + M.m(AM_LAM, 0, -1, -1) + M.m(AM_LAM, 1, -1, -1));
+    k.xm = 8.0f / (M.m(AM_MU, 0, 0, 0) + M.m(AM_MU, 1, 0, 0) + M.m(AM_MU, 0, -1, 0) + M.m(AM_MU, 1, -1, 0) +
+                   M.m(AM_MU, 0, 0, -1) + M.m(AM_MU, 1, 0, -1) + M.m(AM_MU, 0, -1, -1) + M.m(AM_MU, 1, -1, -1));
+    const float mu0 = M.m(AM_MU, 0, 0, 0);
+    k.xmu4 = 2.0f / (mu0 + M.m(AM_MU, 0, 0, -1));
+    k.xmu5 = 2.0f / (mu0 + M.m(AM_MU, 0, -1, 0));
+    k.xmu6 = 2.0f / (mu0 + M.m(AM_MU, 1, 0, 0));
     k.vx1 = vx1;
     k.vx2 = vx2;
     if (nve == 1) {
-        k.qpa = 0.125f * (md(AM_QP, c) + md(AM_QP, c + 1) + md(AM_QP, c - sy) + md(AM_QP, c + 1 - sy) +
-                          md(AM_QP, c - sz) + md(AM_QP, c + 1 - sz) + md(AM_QP, c - sy - sz) + md(AM_QP, c + 1 - sy - sz));
-        const float qsa = 0.125f * (md(AM_QS, c) + md(AM_QS, c + 1) + md(AM_QS, c - sy) + md(AM_QS, c + 1 - sy) +
-                                    md(AM_QS, c - sz) + md(AM_QS, c + 1 - sz) + md(AM_QS, c - sy - sz) + md(AM_QS, c + 1 - sy - sz));
+        k.qpa = 0.125f * (M.m(AM_QP, 0, 0, 0) + M.m(AM_QP, 1, 0, 0) + M.m(AM_QP, 0, -1, 0) + M.m(AM_QP, 1, -1, 0) +
+                          M.m(AM_QP, 0, 0, -1) + M.m(AM_QP, 1, 0, -1) + M.m(AM_QP, 0, -1, -1) + M.m(AM_QP, 1, -1, -1));
+        const float qsa = 0.125f * (M.m(AM_QS, 0, 0, 0) + M.m(AM_QS, 1, 0, 0) + M.m(AM_QS, 0, -1, 0) +
+                                    M.m(AM_QS, 1, -1, 0) + M.m(AM_QS, 0, 0, -1) + M.m(AM_QS, 1, 0, -1) +
+                                    M.m(AM_QS, 0, -1, -1) + M.m(AM_QS, 1, -1, -1));
         k.xl = k.xl + 2.0f * k.xm;
-        const float qs0 = md(AM_QS, c);
-        const float aas4 = 0.5f * (qs0 + md(AM_QS, c - sz));
-        const float aas5 = 0.5f * (qs0 + md(AM_QS, c - sy));
-        const float aas6 = 0.5f * (qs0 + md(AM_QS, c + 1));
+        const float qs0 = M.m(AM_QS, 0, 0, 0);
+        const float aas4 = 0.5f * (qs0 + M.m(AM_QS, 0, 0, -1));
+        const float aas5 = 0.5f * (qs0 + M.m(AM_QS, 0, -1, 0));
+        const float aas6 = 0.5f * (qs0 + M.m(AM_QS, 1, 0, 0));
         k.vh1 = -(k.xm * qsa);
         k.vh2_r4 = -(aas4 * k.xmu4 / 2.0f);
         k.vh2_r5 = -(aas5 * k.xmu5 / 2.0f);
@@ -124,6 +146,22 @@ __device__ __forceinline__ StrCoef str_coef(const MediaT<TM> &md, int c, int sy,
         k.qpa = k.vh1 = k.vh2_r4 = k.vh2_r5 = k.vh2_r6 = 0.f;
     }
     return k;
+}
+
+/* media in global memory around cell c */
+template <class TM>
+struct GMed {
+    const MediaT<TM> &md;
+    int c, sy, sz;
+    __device__ __forceinline__ float m(int a, int dx, int dy, int dz) const { return md(a, c + dx + dy * sy + dz * sz); }
+};
+
+template <class TM>
+__device__ __forceinline__ StrCoef str_coef(const MediaT<TM> &md, int c, int sy, int sz, int nve,
+                                            float vx1, float vx2)
+{
+    const GMed<TM> M{md, c, sy, sz};
+    return str_coef_t(M, nve, vx1, vx2);
 }
 
 /* velocity differences of viscoop.f:126-134; A provides u/v/w at offsets */
