@@ -206,25 +206,6 @@ __global__ void k_sg_coeffs(MediaT<TM> md, int npts, const int *__restrict__ pt_
 /* two-sweep stepper                                                   */
 /* ------------------------------------------------------------------ */
 
-/* Work items of the persistent steppers: (x tile, y tile, z chunk), x
- * fastest so that blocks running together hold neighbouring tiles.  Every
- * block walks items blockIdx.x, +gridDim.x, ...  z chunks are aligned to the
- * top, so the top chunk always holds the levels nz-2..nz that fstr reads. */
-struct AwpWork {
-    int ntx, nty, nzc, kchunk, nitems;
-};
-
-__device__ __forceinline__ void work_item(const AwpGeom &g, const AwpWork &w, int item, int &bx, int &by, int &k0,
-                                          int &k1)
-{
-    bx = item % w.ntx;
-    const int t = item / w.ntx;
-    by = t % w.nty;
-    const int bz = t / w.nty;
-    k1 = g.nz - (w.nzc - 1 - bz) * w.kchunk;
-    k0 = max(1, k1 - w.kchunk + 1);
-}
-
 /* register budgets: 256-thread blocks, more blocks per SM for one component */
 #define VEL_MINB(NC, UNR) ((UNR) == 1 ? ((NC) == 1 ? 6 : 4) : ((NC) == 1 ? 3 : 2))
 #define STR_MINB(NC, UNR) ((NC) == 1 ? 4 : ((NC) == 2 ? 3 : 2))
@@ -873,12 +854,14 @@ static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st
     comp_sets<NC>(s, cs, cn);
     const MediaT<TM> md = media_view<TM>(s.md);
     if (part == AWP_PART_VEL) {
+        if (s.staged) return awp_launch_vel_staged(s.staged, s, st);
         const int ty = s.ty == 4 ? 4 : 8;
         return s.unroll == 2 ? launch_vel<NC, TM, 2>(s, md, cs, ty, st) : launch_vel<NC, TM, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FSVEL) {
         dim3 b(32, 8);
         k_fsvel<NC, TM><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, md, cs);
     } else if (part == AWP_PART_STR) {
+        if (s.staged) return awp_launch_str_staged(s.staged, s, st);
         const int ty = s.ty == 4 ? 4 : 8;
         return s.unroll == 2 ? launch_str<NC, TM, TR, 2>(s, md, cs, ty, st) : launch_str<NC, TM, TR, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FUSED) {

@@ -5,6 +5,12 @@
 #include <cuda_runtime.h>
 #include "awp_internal.h"
 
+/* tensor maps of the TMA-staged stepper (awp_staged.cu) */
+struct AwpStaged;
+
+/* error word bits the steppers set */
+#define AWP_KERR_TMA_WAIT 1          /* a staged-tile barrier wait ran out */
+
 struct AwpStepArgs {
     AwpGeom g;
     AwpMediaT md;                /* typed media                             */
@@ -21,6 +27,9 @@ struct AwpStepArgs {
     int rtype;                   /* AWP_STORE_* of r1..r6                   */
     int ty;                      /* thread-block rows (4, 8 or 16)          */
     int unroll;                  /* two-sweep z-loop unroll (1 or 2)        */
+    const AwpStaged *staged;     /* non-NULL: TMA-staged velocity/stress    */
+    int kchunk_staged;           /* z levels per staged work item           */
+    int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 
 cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, const float *raw, int zf0, int nzs,
@@ -38,6 +47,11 @@ enum { AWP_PART_VEL = 0, AWP_PART_FSVEL = 1, AWP_PART_STR = 2, AWP_PART_FUSED = 
 cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st);
 /* two-sweep: velocity, free-surface velocity, stress (+ fstr); fused: one kernel */
 cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st);
+/* TMA-staged sweeps: FP32 media; maps built once over fixed device arrays */
+cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md);
+void awp_staged_destroy(AwpStaged *s);
+cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
+cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);
 

@@ -75,6 +75,9 @@ struct awp_solver {
     int media_loaded;
     int kchunk;                      /* z levels per fused work item        */
     int kchunk_sweep;                /* z levels per two-sweep work item    */
+    int staged_on;                   /* TMA-staged velocity/stress sweeps   */
+    int kchunk_staged;               /* z levels per staged work item       */
+    AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
     float vtst, vtst1, dth, dh1;
@@ -274,6 +277,7 @@ static void free_all(awp_solver *s)
         cudaFree(s->sgt_file[q]);
     }
     free_media32(s);
+    awp_staged_destroy(s->staged);
     for (int m = 0; m < AM_N; m++) cudaFree(s->mdt.m[m]);
     cudaFree(s->cx); cudaFree(s->cy); cudaFree(s->cz);
     cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext); cudaFree(s->rng);
@@ -307,7 +311,9 @@ static awp_status check_params(const awp_params *p)
     if (p->nvar != 3 && p->nvar != 5 && p->nvar != 8) return set_err(AWP_ERR_PARAM, "NVAR must be 3, 5 or 8");
     if (p->nve != 0 && p->nve != 1) return set_err(AWP_ERR_PARAM, "NVE must be 0 or 1");
     if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_MIXED) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
-    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_FUSED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
+    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_STAGED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
+    if (p->kernel == AWP_KERNEL_STAGED && store_of(p) != AWP_STORE_F32)
+        return set_err(AWP_ERR_PARAM, "the staged stepper reads FP32 media (precision f32 or mixed)");
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
         int ig = p->igreen[q];
@@ -412,9 +418,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     TRY(dalloc(s, (void **)&s->rng, 2 * AM_N * sizeof(unsigned)));
     TRY(dalloc(s, (void **)&s->en_partial, sizeof(double) * AWP_EN_GRID * AWP_MAX_COMP));
     TRY(dalloc(s, (void **)&s->en_out, sizeof(double) * AWP_MAX_COMP));
-    TRY(dalloc(s, (void **)&s->flag, sizeof(int)));
+    TRY(dalloc(s, (void **)&s->flag, 2 * sizeof(int)));   /* [0] monitor, [1] AWP_KERR_* */
     TRYCU(cudaMemsetAsync(s->en_out, 0, sizeof(double) * AWP_MAX_COMP, s->stream));
-    TRYCU(cudaMemsetAsync(s->flag, 0, sizeof(int), s->stream));
+    TRYCU(cudaMemsetAsync(s->flag, 0, 2 * sizeof(int), s->stream));
     s->next_check = p->monitor_every > 0 ? p->monitor_every : 0;
     for (int q = 0; q < p->ncomp; q++) {
         TRY(dalloc(s, (void **)&s->chkj[q], sizeof(float) * 3 * (size_t)p->nt));
@@ -429,6 +435,11 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->unroll = env_int("AWP_TUNE_UNROLL", 1) == 2 ? 2 : 1;
     s->kchunk = choose_kchunk(s->g, 1, s->ty);
     s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
+    s->staged_on = p->kernel == AWP_KERNEL_STAGED || (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
+    {
+        const int kc = env_int("AWP_TUNE_KSTAGE", 32);
+        s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
+    }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
     TRYCU(cudaStreamSynchronize(s->stream));
@@ -761,6 +772,9 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.rtype = s->rstore;
     a.ty = s->ty;
     a.unroll = s->unroll;
+    a.staged = s->staged_on ? s->staged : NULL;
+    a.kchunk_staged = s->kchunk_staged;
+    a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);
     pa.g = s->g; pa.ncomp = p->ncomp; pa.nst = p->nst; pa.nt = p->nt;
@@ -831,6 +845,11 @@ static awp_status start_if_needed(awp_solver *s)
 {
     if (s->started) return AWP_OK;
     if (!s->media_loaded) return set_err(AWP_ERR_STATE, "media not loaded");
+    if (s->staged_on && !s->staged) {
+        /* the arrays are fixed from here on: u v w, the stresses, FP32 media */
+        const cudaError_t e = awp_staged_create(&s->staged, s->g, s->p.ncomp, s->comp[0], s->mdt);
+        if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "staged stepper: tensor maps: %s", cudaGetErrorString(e));
+    }
     AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
     fill_args(s, -1, a, pa, sa);       /* addsrc(1) into the buffer step 1 reads */
     CU(awp_launch_post(pa, 1, s->stream));
@@ -916,12 +935,14 @@ extern "C" awp_status awp_sync(awp_solver *s)
         s->pending = 0;
         s->pending_steps = 0;
     }
-    if (s->p.monitor_every > 0) {
-        int flag = 0;
-        CU(cudaMemcpyAsync(&flag, s->flag, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
+    if (s->p.monitor_every > 0 || s->staged_on) {
+        int flag[2] = {0, 0};
+        CU(cudaMemcpyAsync(flag, s->flag, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
         CU(cudaStreamSynchronize(s->stream));
-        if (flag) return set_err(AWP_ERR_UNSTABLE, "stability monitor: non-finite wavefield energy by step %d",
-                                 s->steps_done);
+        if (flag[1]) return set_err(AWP_ERR_CUDA, "staged stepper: a tile barrier wait ran out (error word %d)",
+                                    flag[1]);
+        if (flag[0]) return set_err(AWP_ERR_UNSTABLE, "stability monitor: non-finite wavefield energy by step %d",
+                                    s->steps_done);
     }
     return AWP_OK;
 }
@@ -978,10 +999,11 @@ extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_ti
     if (s->fused) parts[np++] = AWP_PART_FUSED;
     else { parts[np++] = AWP_PART_VEL; parts[np++] = AWP_PART_FSVEL; parts[np++] = AWP_PART_STR; }
     static const char *pname[] = {"k_vel", "k_fsvel", "k_str", "k_fused"};
+    static const char *pname_staged[] = {"k_vel_tma", "k_fsvel", "k_str_tma", "k_fused"};
     const int nk = np + 2;
     o->nkernels = nk;
     for (int k = 0; k < np; k++) {
-        snprintf(o->name[k], sizeof o->name[k], "%s", pname[parts[k]]);
+        snprintf(o->name[k], sizeof o->name[k], "%s", (s->staged_on ? pname_staged : pname)[parts[k]]);
         o->bytes_per_launch[k] = part_bytes(s, parts[k]);
     }
     snprintf(o->name[np], sizeof o->name[np], "k_post");
@@ -1121,7 +1143,7 @@ extern "C" awp_status awp_reset(awp_solver *s)
         if (s->sgt_file[q]) CU(cudaMemsetAsync(s->sgt_file[q], 0, sizeof(float) * (size_t)s->sgt_file_floats, s->stream));
     }
     CU(cudaMemsetAsync(s->step, 0, sizeof(int), s->stream));
-    CU(cudaMemsetAsync(s->flag, 0, sizeof(int), s->stream));
+    CU(cudaMemsetAsync(s->flag, 0, 2 * sizeof(int), s->stream));
     CU(cudaStreamSynchronize(s->stream));
     s->steps_done = 0;
     s->started = 0;

@@ -1,0 +1,570 @@
+/*
+ * awp_staged.cu -- the two-sweep stepper with TMA-staged xy tiles (2.5D blocking).
+ *
+ * A thread block owns a 32 x 8 column tile of one component and marches up a
+ * chunk of z levels.  For every level one thread issues TMA tile loads
+ * (cp.async.bulk.tensor over 3D tensor maps of the padded volume) of the
+ * arrays that are read with x/y neighbours -- stencil tiles with a 4-column
+ * and 2-row halo, media tiles with the one row below -- into a ring of shared
+ * memory slots, D levels ahead of the level being computed; one mbarrier per
+ * slot counts the bytes in.  Values needed only along the cell's own column
+ * (z neighbours) travel in a per-thread register queue fed by one load per
+ * level, and the point-wise state (u, v, w in the velocity sweep; six
+ * stresses and six memory variables in the stress sweep) is read and written
+ * once per cell with coalesced accesses.  So the bytes in flight per SM are
+ * set by the ring depth, not by registers or resident warps.
+ *
+ * Work items (x tile, y tile, z chunk, component) are spread over a
+ * persistent grid; the components of one tile are neighbouring items, so
+ * their common media tiles are read from HBM once and from L2 after.
+ *
+ * The per-cell arithmetic is the shared code of awp_stencil.cuh, evaluated in
+ * the same order as the other steppers (bit-identical results).  FP32 media
+ * only; memory variables FP32 or bf16.
+ *
+ * Every wait on an mbarrier is bounded (2 s of %globaltimer); on expiry the
+ * block records AWP_KERR_TMA_WAIT in the error word, waits (bounded again)
+ * for its own copies in flight and returns.
+ */
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/awp_sgt.h"
+#include "awp_internal.h"
+#include "awp_kernels.h"
+#include "awp_stencil.cuh"
+
+#define ST_X 32                      /* tile width: one warp along x            */
+#define ST_Y 8                       /* tile rows                               */
+#define ST_W 40                      /* staged row: 4 halo + 32 + 4 halo        */
+#define ST_HR (ST_Y + 4)             /* stencil tile rows: 2 below, 2 above     */
+#define ST_MR (ST_Y + 1)             /* media tile rows: 1 below                */
+#define ST_VT (ST_W * ST_HR)         /* floats of a stencil tile (1920 B)       */
+#define ST_MT (ST_W * ST_MR)         /* floats a media tile receives (1440 B)   */
+#define ST_MP 384                    /* floats reserved per media tile (1536 B) */
+#define ST_WAIT_NS 2000000000ull     /* bound of one barrier wait               */
+#define ST_VEL_D 3                   /* levels in flight, velocity sweep        */
+#define ST_STR_D 2                   /* levels in flight, stress sweep          */
+
+struct AwpStagedVelMaps {
+    CUtensorMap st[AWP_MAX_COMP][5]; /* xx yy xy xz yz, box 40 x 12           */
+    CUtensorMap d1;                  /* box 40 x 9                             */
+};
+struct AwpStagedStrMaps {
+    CUtensorMap v[AWP_MAX_COMP][3];  /* u v w, box 40 x 12                     */
+    CUtensorMap med[4];              /* lam mu qp qs, box 40 x 9               */
+};
+struct AwpStaged {
+    AwpStagedVelMaps vm;
+    AwpStagedStrMaps sm;
+};
+
+/* ------------------------------------------------------------------ */
+/* mbarrier / TMA primitives (PTX ISA: mbarrier, cp.async.bulk.tensor) */
+/* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ uint32_t s_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mb_init(uint64_t *b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mb_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mb_expect(uint64_t *b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mb_try(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(s_addr(b)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* true once the phase of the given parity has completed; false after the bound */
+__device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity)
+{
+    if (mb_try(b, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t n = 0; n < (1u << 26); ++n) {
+        if (mb_try(b, parity)) return true;
+        if ((n & 63) == 63 && global_ns() - t0 > ST_WAIT_NS) return false;
+    }
+    return false;
+}
+
+/* generic-proxy accesses to a slot are ordered before the async-proxy refill */
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_3d(void *dst, const CUtensorMap *map, uint64_t *b, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(s_addr(dst)),
+                 "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(s_addr(b))
+                 : "memory");
+}
+
+/* memory coordinates of a tile: column of cell i0 - 4 (a multiple of 4, so
+ * the copy starts on a 16-byte boundary), row of cell j0 - 2 (stencil) or
+ * j0 - 1 (media), level k */
+__device__ __forceinline__ int tile_x(int i0) { return i0 + AWP_XO - 1 - 4; }
+
+__device__ __forceinline__ float *pick(const AwpCompSet<AWP_MAX_COMP> &cs, int q, int f)
+{
+    return q == 0 ? cs.c[0].f[f] : (q == 1 ? cs.c[1].f[f] : cs.c[2].f[f]);
+}
+
+/* ------------------------------------------------------------------ */
+/* velocity sweep                                                      */
+/* ------------------------------------------------------------------ */
+
+/* slot layout: xx yy xy xz yz stencil tiles, then the d1 media tile */
+#define VEL_SLOT (5 * ST_VT + ST_MP)
+#define VEL_TXB ((5 * ST_VT + ST_MT) * 4)
+
+/* stresses of plane k from the slot (in-plane) and from the register queue (z) */
+struct TStr {
+    const float *t; /* slot + cell offset */
+    float xz_m2, xz_m1, xz_p1, yz_m2, yz_m1, yz_p1, zz_m1, zz_0, zz_p1, zz_p2;
+    __device__ __forceinline__ float s(int a, int dx, int dy, int dz) const
+    {
+        if (a == S_ZZ) return dz == -1 ? zz_m1 : (dz == 0 ? zz_0 : (dz == 1 ? zz_p1 : zz_p2));
+        if (dz == 0) {
+            const int n = a == S_XX ? 0 : (a == S_YY ? 1 : (a == S_XY ? 2 : (a == S_XZ ? 3 : 4)));
+            return t[n * ST_VT + dy * ST_W + dx];
+        }
+        if (a == S_XZ) return dz == -2 ? xz_m2 : (dz == -1 ? xz_m1 : xz_p1);
+        return dz == -2 ? yz_m2 : (dz == -1 ? yz_m1 : yz_p1);
+    }
+};
+
+template <int S>
+__device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorMap *md1, float *ring, uint64_t *bar,
+                                          uint32_t use, int i0, int j0, int k)
+{
+    float *sl = ring + (use % S) * VEL_SLOT;
+    uint64_t *b = &bar[use % S];
+    fence_async_smem();
+    mb_expect(b, VEL_TXB);
+    const int x = tile_x(i0);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) tma_3d(sl + a * ST_VT, ms + a, b, x, j0 - 1, k + 1);
+    tma_3d(sl + 5 * ST_VT, md1, b, x, j0, k + 1);
+}
+
+template <int D>
+__global__ void __launch_bounds__(ST_X * ST_Y, 4)
+k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
+          const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
+          const float *__restrict__ cz, float dth, AwpWork w, int *err)
+{
+    constexpr int S = 1 + D;          /* plane k resident, D in flight */
+    extern __shared__ unsigned char st_smem[];
+    float *ring = (float *)(((uintptr_t)st_smem + 127) & ~(uintptr_t)127);
+    uint64_t *bar = (uint64_t *)(ring + S * VEL_SLOT);
+    __shared__ int abort_s;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * ST_X + tx;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mb_init(&bar[s], 1);
+        mb_fence_init();
+        abort_s = 0;
+    }
+    __syncthreads();
+    const int sy = g.px, sz = g.plane;
+    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
+    uint32_t used = 0;                /* ring uses so far (same in every thread) */
+    for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        const int q = item % ncomp;
+        int bx, by, k0, k1;
+        work_item(g, w, item / ncomp, bx, by, k0, k1);
+        const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1, i = i0 + tx, j = j0 + ty;
+        const bool live = i <= g.nx && j <= g.ny;
+        const int np = k1 - k0 + 1;
+        const uint32_t g0 = used;
+        used += np;
+        const CUtensorMap *ms = maps.st[q];
+        int issued = 0;               /* meaningful in thread 0 only */
+        if (tid == 0)
+            for (; issued < S && issued < np; ++issued) vel_issue<S>(ms, &maps.d1, ring, bar, g0 + issued, i0, j0, k0 + issued);
+        float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
+        const float *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ), *ZZ = pick(cs, q, AF_ZZ);
+        float xz_m2 = 0.f, xz_m1 = 0.f, yz_m2 = 0.f, yz_m1 = 0.f, zz_m1 = 0.f, zz_0 = 0.f, zz_p1 = 0.f;
+        float dA = 0.f, dB = 0.f, dE = 0.f, cxy = 0.f;
+        int c = g.idx(i, j, k0);
+        if (live) {
+            xz_m2 = XZ[c - 2 * sz]; xz_m1 = XZ[c - sz];
+            yz_m2 = YZ[c - 2 * sz]; yz_m1 = YZ[c - sz];
+            zz_m1 = ZZ[c - sz]; zz_0 = ZZ[c]; zz_p1 = ZZ[c + sz];
+            dA = d1[c - sz]; dB = d1[c - sy - sz]; dE = d1[c + 1 - sz];
+            cxy = cx[i] * cy[j];
+        }
+        int k = k0;
+        for (; k <= k1; ++k, c += sz) {
+            const uint32_t use = g0 + (uint32_t)(k - k0);
+            float u0 = 0.f, v0 = 0.f, w0 = 0.f, xz_p1 = 0.f, yz_p1 = 0.f, zz_p2 = 0.f, czk = 0.f;
+            if (live) {
+                u0 = U[c]; v0 = V[c]; w0 = W[c];
+                xz_p1 = XZ[c + sz]; yz_p1 = YZ[c + sz]; zz_p2 = ZZ[c + 2 * sz];
+                czk = cz[k];
+            }
+            const bool ok = mb_wait(&bar[use % S], (use / S) & 1);
+            if (!ok) {
+                abort_s = 1;
+                atomicOr(err, AWP_KERR_TMA_WAIT);
+            }
+            if (live && ok) {
+                const float *sl = ring + (use % S) * VEL_SLOT;
+                const float *t1 = sl + 5 * ST_VT + cm;
+                const float da = t1[0], db = t1[-ST_W], de = t1[1], dg = t1[1 - ST_W];
+                float fu, fv, fw;
+                vel_factors7(da, db, dA, dB, de, dE, dg, dth, fu, fv, fw);
+                const TStr A{sl + cv, xz_m2, xz_m1, xz_p1, yz_m2, yz_m1, yz_p1, zz_m1, zz_0, zz_p1, zz_p2};
+                float u, v, w_;
+                vel_one_t(A, u0, v0, w0, fu, fv, fw, u, v, w_);
+                const float crj = cxy * czk;
+                U[c] = u * crj;
+                V[c] = v * crj;
+                W[c] = w_ * crj;
+                xz_m2 = xz_m1; xz_m1 = sl[3 * ST_VT + cv];
+                yz_m2 = yz_m1; yz_m1 = sl[4 * ST_VT + cv];
+                zz_m1 = zz_0; zz_0 = zz_p1; zz_p1 = zz_p2;
+                dA = da; dB = db; dE = de;
+            }
+            __syncthreads();
+            if (abort_s) break;
+            if (tid == 0 && issued < np) {
+                vel_issue<S>(ms, &maps.d1, ring, bar, g0 + issued, i0, j0, k0 + issued);
+                ++issued;
+            }
+        }
+        if (abort_s) {
+            if (tid == 0)
+                for (int n = k - k0; n < issued; ++n)
+                    if (!mb_wait(&bar[(g0 + n) % S], ((g0 + n) / S) & 1)) break;
+            return;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* stress sweep                                                        */
+/* ------------------------------------------------------------------ */
+
+/* slot layout: u v w stencil tiles, then lam mu qp qs media tiles */
+#define STR_SLOT (3 * ST_VT + 4 * ST_MP)
+
+/* media of planes k and k-1 at the cell */
+struct TMed {
+    const float *p0, *pm; /* media tiles (lam first) of planes k and k-1, at the cell */
+    __device__ __forceinline__ float m(int a, int dx, int dy, int dz) const
+    {
+        const int n = a == AM_LAM ? 0 : (a == AM_MU ? 1 : (a == AM_QP ? 2 : 3));
+        return (dz == 0 ? p0 : pm)[n * ST_MP + dy * ST_W + dx];
+    }
+};
+
+/* velocities: plane k from the slot, the column from registers */
+struct TVel {
+    const float *t;   /* u tile of plane k at the cell; v and w tiles follow */
+    float um1, vm1, wm1, up1, up2, vp1, vp2, wm2, wp1;
+    __device__ __forceinline__ float u(int dx, int dy, int dz) const
+    {
+        return dz == 0 ? t[dy * ST_W + dx] : (dz == -1 ? um1 : (dz == 1 ? up1 : up2));
+    }
+    __device__ __forceinline__ float v(int dx, int dy, int dz) const
+    {
+        return dz == 0 ? t[ST_VT + dy * ST_W + dx] : (dz == -1 ? vm1 : (dz == 1 ? vp1 : vp2));
+    }
+    __device__ __forceinline__ float w(int dx, int dy, int dz) const
+    {
+        return dz == 0 ? t[2 * ST_VT + dy * ST_W + dx] : (dz == -1 ? wm1 : (dz == -2 ? wm2 : wp1));
+    }
+};
+
+template <int S>
+__device__ __forceinline__ void str_issue(const CUtensorMap *mv, const CUtensorMap *mm, int nmed, uint32_t txb,
+                                          float *ring, uint64_t *bar, uint32_t use, int i0, int j0, int k)
+{
+    float *sl = ring + (use % S) * STR_SLOT;
+    uint64_t *b = &bar[use % S];
+    fence_async_smem();
+    mb_expect(b, txb);
+    const int x = tile_x(i0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, mv + a, b, x, j0 - 1, k + 1);
+    for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * ST_VT + a * ST_MP, mm + a, b, x, j0, k + 1);
+}
+
+template <class TR, int D>
+__global__ void __launch_bounds__(ST_X * ST_Y, 4)
+k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
+          const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
+          const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
+{
+    constexpr int S = 2 + D;          /* planes k-1 and k resident, D in flight */
+    const int nmed = nve == 1 ? 4 : 2;
+    const uint32_t txb = (uint32_t)(3 * ST_VT + nmed * ST_MT) * 4u;
+    extern __shared__ unsigned char st_smem[];
+    float *ring = (float *)(((uintptr_t)st_smem + 127) & ~(uintptr_t)127);
+    uint64_t *bar = (uint64_t *)(ring + S * STR_SLOT);
+    __shared__ int abort_s;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * ST_X + tx;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mb_init(&bar[s], 1);
+        mb_fence_init();
+        abort_s = 0;
+    }
+    __syncthreads();
+    const int sy = g.px, sz = g.plane;
+    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
+    uint32_t used = 0;
+    for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        const int q = item % ncomp;
+        int bx, by, k0, k1;
+        work_item(g, w, item / ncomp, bx, by, k0, k1);
+        const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1, i = i0 + tx, j = j0 + ty;
+        const bool live = i <= g.nx && j <= g.ny;
+        const int pb = k0 - 1;        /* first staged plane */
+        const int np = k1 - pb + 1;
+        const uint32_t g0 = used;
+        used += np;
+        const CUtensorMap *mv = maps.v[q];
+        int issued = 0;
+        if (tid == 0)
+            for (; issued < S && issued < np; ++issued)
+                str_issue<S>(mv, maps.med, nmed, txb, ring, bar, g0 + issued, i0, j0, pb + issued);
+        const float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
+        float *XX = pick(cs, q, AF_XX), *YY = pick(cs, q, AF_YY), *ZZ = pick(cs, q, AF_ZZ);
+        float *XY = pick(cs, q, AF_XY), *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ);
+        TR *Rr[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) Rr[a] = (TR *)pick(cs, q, AF_R1 + a);
+        float up1 = 0.f, vp1 = 0.f, wm2 = 0.f, cxy = 0.f;
+        const int itxy = ((j & 1) << 1) | (i & 1);
+        int c = g.idx(i, j, k0);
+        if (live) {
+            up1 = U[c + sz]; vp1 = V[c + sz]; wm2 = W[c - 2 * sz];
+            cxy = cx[i] * cy[j];
+        }
+        int k = k0;
+        for (; k <= k1; ++k, c += sz) {
+            const uint32_t use = g0 + (uint32_t)(k - pb), usem = use - 1;
+            float up2 = 0.f, vp2 = 0.f, wp1 = 0.f, czk = 0.f;
+            Stress6 s0{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float r[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (live) {
+                s0 = Stress6{XX[c], YY[c], ZZ[c], XY[c], XZ[c], YZ[c]};
+                if (nve == 1) {
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(Rr[a], c, 1.0f);
+                }
+                up2 = U[c + 2 * sz]; vp2 = V[c + 2 * sz]; wp1 = W[c + sz];
+                czk = cz[k];
+            }
+            bool ok = true;
+            if (k == k0) ok = mb_wait(&bar[usem % S], (usem / S) & 1);
+            if (ok) ok = mb_wait(&bar[use % S], (use / S) & 1);
+            if (!ok) {
+                abort_s = 1;
+                atomicOr(err, AWP_KERR_TMA_WAIT);
+            }
+            if (live && ok) {
+                const float *sk = ring + (use % S) * STR_SLOT, *sm = ring + (usem % S) * STR_SLOT;
+                const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
+                const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
+                const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
+                const float wm1 = sm[2 * ST_VT + cv];
+                const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1, up2, vp1, vp2, wm2, wp1};
+                Stress6 o;
+                if (nve == 1) {
+                    const VelDiff dd = vel_diff(Vq);
+                    o = str_visco(kc, dd, s0, r, dth, dt, dh1);
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) Store<TR>::st(Rr[a], c, r[a], 1.0f);
+                } else {
+                    o = str_elastic(kc, Vq, s0, dth);
+                }
+                const float crj = cxy * czk;
+                XX[c] = o.xx * crj; YY[c] = o.yy * crj; ZZ[c] = o.zz * crj;
+                XY[c] = o.xy * crj; XZ[c] = o.xz * crj; YZ[c] = o.yz * crj;
+                wm2 = wm1;
+            }
+            up1 = up2;
+            vp1 = vp2;
+            __syncthreads();
+            if (abort_s) break;
+            if (tid == 0 && issued < np) {
+                str_issue<S>(mv, maps.med, nmed, txb, ring, bar, g0 + issued, i0, j0, pb + issued);
+                ++issued;
+            }
+        }
+        if (abort_s) {
+            if (tid == 0)
+                for (int n = k - pb - (k == k0 ? 1 : 0); n < issued; ++n)
+                    if (!mb_wait(&bar[(g0 + n) % S], ((g0 + n) / S) & 1)) break;
+            return;
+        }
+        if (live && k1 == g.nz) {
+            /* fstr (operator.f:594-606) on this thread's own column; the top
+             * chunk holds at least levels nz-2..nz, all written by this thread */
+            const int ct = g.idx(i, j, g.nz);
+            ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+            ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+            XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+            XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+            YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+            YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+            XZ[ct] = 0.0f;
+            YZ[ct] = 0.0f;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* host side                                                           */
+/* ------------------------------------------------------------------ */
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = NULL;
+    if (!fn) {
+        void *p = NULL;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+/* tensor map of one padded FP32 volume: (pitch, ny + 4, nz + 4), box 40 x rows x 1 */
+static bool make_map(CUtensorMap *m, const AwpGeom &g, const void *base, int rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || !base || ((uintptr_t)base & 15)) return false;
+    const cuuint64_t dim[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.nz + 4};
+    const cuuint64_t stride[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.plane * 4};
+    const cuuint32_t box[3] = {ST_W, (cuuint32_t)rows, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dim, stride, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md)
+{
+    *out = NULL;
+    if (md.type != AWP_STORE_F32 || ncomp < 1 || ncomp > AWP_MAX_COMP) return cudaErrorInvalidValue;
+    if (g.px % 4 != 0) return cudaErrorInvalidValue;
+    AwpStaged *s = (AwpStaged *)aligned_alloc(64, sizeof(AwpStaged));
+    if (!s) return cudaErrorMemoryAllocation;
+    memset(s, 0, sizeof *s);
+    static const int vel_f[5] = {AF_XX, AF_YY, AF_XY, AF_XZ, AF_YZ};
+    static const int med_f[4] = {AM_LAM, AM_MU, AM_QP, AM_QS};
+    bool ok = make_map(&s->vm.d1, g, md.m[AM_D1], ST_MR);
+    for (int q = 0; q < ncomp; ++q) {
+        for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_HR);
+        for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->sm.v[q][a], g, comp[q].f[AF_U + a], ST_HR);
+    }
+    for (int a = 0; a < 4; ++a) ok = ok && make_map(&s->sm.med[a], g, md.m[med_f[a]], ST_MR);
+    if (!ok) {
+        free(s);
+        return cudaErrorInvalidValue;
+    }
+    *out = s;
+    return cudaSuccess;
+}
+
+void awp_staged_destroy(AwpStaged *s) { free(s); }
+
+static AwpWork staged_work(const AwpGeom &g, int kchunk, int ncomp)
+{
+    AwpWork w;
+    w.ntx = (g.nx + ST_X - 1) / ST_X;
+    w.nty = (g.ny + ST_Y - 1) / ST_Y;
+    w.kchunk = kchunk;
+    w.nzc = (g.nz + kchunk - 1) / kchunk;
+    w.nitems = w.ntx * w.nty * w.nzc * ncomp;
+    return w;
+}
+
+template <class K>
+static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid)
+{
+    int dev = 0, nsm = 148, per = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, ST_X * ST_Y, smem);
+    if (e != cudaSuccess) return e;
+    if (per < 1) return cudaErrorInvalidConfiguration;
+    *grid = nsm * per < nitems ? nsm * per : nitems;
+    return cudaSuccess;
+}
+
+static AwpCompSet<AWP_MAX_COMP> comp_set3(const AwpStepArgs &s)
+{
+    AwpCompSet<AWP_MAX_COMP> cs;
+    memset(&cs, 0, sizeof cs);
+    for (int q = 0; q < s.ncomp; ++q) cs.c[q] = s.comp[q];
+    return cs;
+}
+
+cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
+    constexpr int S = 1 + ST_VEL_D;
+    const size_t smem = 128 + (size_t)S * VEL_SLOT * 4 + S * 8;
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
+    int grid = 0;
+    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D>, smem, w.nitems, &grid);
+    if (e != cudaSuccess) return e;
+    k_vel_tma<ST_VEL_D><<<grid, dim3(ST_X, ST_Y), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp,
+                                                                   (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz,
+                                                                   s.dth, w, s.kerr);
+    return cudaGetLastError();
+}
+
+template <class TR>
+static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    constexpr int S = 2 + ST_STR_D;
+    const size_t smem = 128 + (size_t)S * STR_SLOT * 4 + S * 8;
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
+    int grid = 0;
+    cudaError_t e = staged_grid(k_str_tma<TR, ST_STR_D>, smem, w.nitems, &grid);
+    if (e != cudaSuccess) return e;
+    k_str_tma<TR, ST_STR_D><<<grid, dim3(ST_X, ST_Y), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.cx, s.cy,
+                                                                       s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve,
+                                                                       s.kerr);
+    return cudaGetLastError();
+}
+
+cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
+    if (s.rtype == AWP_STORE_BF16) return launch_str_tr<__nv_bfloat16>(st, s, stream);
+    return launch_str_tr<float>(st, s, stream);
+}

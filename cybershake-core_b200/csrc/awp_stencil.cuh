@@ -16,6 +16,25 @@
 #include <cuda_fp16.h>
 #include "awp_internal.h"
 
+/* Work items of the persistent steppers: (x tile, y tile, z chunk), x
+ * fastest so that blocks running together hold neighbouring tiles.  Every
+ * block walks items blockIdx.x, +gridDim.x, ...  z chunks are aligned to the
+ * top, so the top chunk always holds the levels nz-2..nz that fstr reads. */
+struct AwpWork {
+    int ntx, nty, nzc, kchunk, nitems;
+};
+
+__device__ __forceinline__ void work_item(const AwpGeom &g, const AwpWork &w, int item, int &bx, int &by, int &k0,
+                                          int &k1)
+{
+    bx = item % w.ntx;
+    const int t = item / w.ntx;
+    by = t % w.nty;
+    const int bz = t / w.nty;
+    k1 = g.nz - (w.nzc - 1 - bz) * w.kchunk;
+    k0 = max(1, k1 - w.kchunk + 1);
+}
+
 #define C1 (9.0f / 8.0f)
 #define C2 (-(1.0f / 24.0f))
 

@@ -65,10 +65,13 @@ typedef enum {
 
 /* Stepper implementation. */
 typedef enum {
-    AWP_KERNEL_AUTO = 0,      /* library picks (the two-sweep stepper)         */
+    AWP_KERNEL_AUTO = 0,      /* library picks: the staged stepper for FP32
+                                 media, else the two-sweep stepper           */
     AWP_KERNEL_TWO_SWEEP = 1, /* velocity sweep, then stress sweep, in place   */
-    AWP_KERNEL_FUSED = 2      /* one z-march per tile: velocity on a 2-cell
+    AWP_KERNEL_FUSED = 2,     /* one z-march per tile: velocity on a 2-cell
                                  halo, then stress; ping-pong wavefields       */
+    AWP_KERNEL_STAGED = 3     /* the two sweeps with TMA-staged xy tiles and a
+                                 z register queue (FP32 media only)           */
 } awp_kernel;
 
 #define AWP_MAX_COMP 3

@@ -52,7 +52,7 @@ def test_param_defaults_match_gpu_command_defaults():
 @pytest.mark.parametrize("kernel,ncomp,prec,expect", [
     # two sweeps: velocity R 9 W 3, stress R 9 W 6, r1..r6 R+W, media shared
     ("two_sweep", 1, "f32", 176.0), ("two_sweep", 2, "f32", 166.0), ("two_sweep", 3, "f32", 156.0 + 20.0 / 3),
-    ("two_sweep", 2, "bf16", 137.0),
+    ("two_sweep", 2, "bf16", 137.0), ("staged", 1, "f32", 176.0), ("staged", 3, "mixed", 132.0 + 20.0 / 3),
     # fused: u v w and 6 stresses read + written once, r1..r6 R+W, media once
     ("fused", 1, "f32", 140.0), ("fused", 2, "f16", 101.0), ("fused", 3, "f16", 96.0 + 10.0 / 3),
 ])
@@ -86,6 +86,11 @@ def test_bad_parameters_rejected_before_any_device_call():
     with pytest.raises(awpsgt.AwpError) as e:
         awpsgt.Solver(p)
     assert e.value.status == 2
+    for prec in ("bf16", "f16"):           # the staged stepper reads FP32 media only
+        p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, ntiskp_sgt=1, precision=prec, kernel="staged")
+        with pytest.raises(awpsgt.AwpError) as e:
+            awpsgt.Solver(p)
+        assert e.value.status == 2 and "FP32 media" in str(e.value)
 
 
 def test_create_without_gpu_fails_loudly():

@@ -104,7 +104,7 @@ def assert_same_state(s, o, q=0, fields=ALL_FIELDS):
     assert bits_equal(s.sgt(q), o.sgt())
 
 
-KERNELS = ["fused", "two_sweep"]
+KERNELS = ["fused", "two_sweep", "staged"]
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -140,11 +140,26 @@ def test_odd_sizes_and_boundary_points(kernel):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-def test_multi_tile_multi_chunk_grid():
-    """Several x/y tiles and z chunks of the fused stepper (halo recompute at
-    tile seams and redundant levels at chunk seams)."""
+@pytest.mark.parametrize("kernel,kstage", [("fused", None), ("staged", None), ("staged", "8")])
+def test_multi_tile_multi_chunk_grid(kernel, kstage, monkeypatch):
+    """Several x/y tiles (partial ones at the high edges) and z chunks: halo
+    recompute at the fused stepper's tile seams and redundant levels at its
+    chunk seams; the staged stepper's tile halos, chunk prologues and ring
+    reuse across many work items per block."""
+    if kstage:
+        monkeypatch.setenv("AWP_TUNE_KSTAGE", kstage)
     c = Case(nx=100, ny=30, nz=80, nt=25, nd=6, srcs=[[(50, 15, 40)]], ntiskp=5, write_step=5)
-    assert_same_state(c.gpu(kernel="fused"), c.oracle())
+    assert_same_state(c.gpu(kernel=kernel), c.oracle())
+
+
+def test_staged_batched_components_many_items(monkeypatch):
+    """Three components as neighbouring work items, 8-level chunks."""
+    monkeypatch.setenv("AWP_TUNE_KSTAGE", "8")
+    c = Case(nx=70, ny=20, nz=41, nt=30, igreen=(1, 2, 3),
+             srcs=[[(35, 10, 20)], [(34, 9, 20)], [(36, 11, 21)]])
+    s = c.gpu(kernel="staged")
+    for q in range(3):
+        assert_same_state(s, c.oracle(q), q)
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -204,6 +219,8 @@ def test_mixed_precision_runs_close_to_fp64(precision, kernel):
     """Media and memory variables in 16 bits, wavefields and arithmetic FP32:
     the SGT stays close to the FP64 oracle (the bound here is loose; the
     measured errors are reported by the error study)."""
+    if kernel == "staged" and precision != "mixed":
+        pytest.skip("the staged stepper reads FP32 media")
     c = Case(nt=80, stf_seed=11)
     s = c.gpu(precision=precision, kernel=kernel)
     o64 = c.oracle(precision="f64")
@@ -211,6 +228,13 @@ def test_mixed_precision_runs_close_to_fp64(precision, kernel):
     assert np.isfinite(g).all()
     err = rel_l2(g, o64.sgt())
     assert err <= 2e-2, err
+
+
+def test_mixed_mode_same_result_staged_and_two_sweep():
+    c = Case(nt=40)
+    a = c.gpu(precision="mixed", kernel="staged").sgt()
+    b = c.gpu(precision="mixed", kernel="two_sweep").sgt()
+    assert bits_equal(a, b)
 
 
 def test_mixed_precision_same_result_both_kernels():
