@@ -133,6 +133,71 @@ __device__ __forceinline__ float *pick(const AwpCompSet<AWP_MAX_COMP> &cs, int q
 }
 
 /* ------------------------------------------------------------------ */
+/* warp roles and the ring                                             */
+/* ------------------------------------------------------------------ */
+
+/* Eight consumer warps (one tile row each) and one producer warp whose lane
+ * 0 issues the copies.  Ring slot s has a "full" barrier (the producer's
+ * expect_tx arrival plus the bytes) and an "empty" barrier (one arrival per
+ * consumer warp once it is done with the slot's level); the producer refills
+ * a slot only after its empty phase completes, so no block-wide barrier
+ * stands in the level loop and warps drift within the ring depth. */
+#define ST_CW 8
+#define ST_THREADS (32 * (ST_CW + 1))
+
+__device__ __forceinline__ void mb_arrive(uint64_t *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s_addr(b)) : "memory");
+}
+
+/* bounded wait that also gives up once another thread has flagged an abort */
+__device__ __forceinline__ bool mb_wait_or_abort(uint64_t *b, uint32_t parity, const volatile int *abort)
+{
+    if (mb_try(b, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t n = 0; n < (1u << 26); ++n) {
+        if (mb_try(b, parity)) return true;
+        if ((n & 63) == 63 && (*abort || global_ns() - t0 > ST_WAIT_NS)) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float *ring_base(unsigned char *raw)
+{
+    return (float *)(((uintptr_t)raw + 127) & ~(uintptr_t)127);
+}
+
+template <int S>
+__device__ __forceinline__ void ring_init(uint64_t *full, uint64_t *empty, volatile int *abort)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        for (int s = 0; s < S; ++s) {
+            mb_init(&full[s], 1);
+            mb_init(&empty[s], ST_CW);
+        }
+        mb_fence_init();
+        *abort = 0;
+    }
+    __syncthreads();
+}
+
+/* the producer's last act: the most recent use of every slot has landed, so
+ * no copy into this block's shared memory is still in flight when it exits */
+template <int S>
+__device__ __forceinline__ void ring_drain(uint64_t *full, uint32_t uses)
+{
+    for (uint32_t u = uses > (uint32_t)S ? uses - S : 0; u < uses; ++u)
+        if (!mb_wait(&full[u % S], (u / S) & 1)) return;
+}
+
+/* producer: wait until use `use` of its slot may be refilled */
+template <int S>
+__device__ __forceinline__ bool ring_acquire(uint64_t *empty, uint32_t use, const volatile int *abort)
+{
+    return use < (uint32_t)S || mb_wait_or_abort(&empty[use % S], ((use / S) - 1) & 1, abort);
+}
+
+/* ------------------------------------------------------------------ */
 /* velocity sweep                                                      */
 /* ------------------------------------------------------------------ */
 
@@ -157,11 +222,11 @@ struct TStr {
 };
 
 template <int S>
-__device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorMap *md1, float *ring, uint64_t *bar,
+__device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorMap *md1, float *ring, uint64_t *full,
                                           uint32_t use, int i0, int j0, int k)
 {
     float *sl = ring + (use % S) * VEL_SLOT;
-    uint64_t *b = &bar[use % S];
+    uint64_t *b = &full[use % S];
     fence_async_smem();
     mb_expect(b, VEL_TXB);
     const int x = tile_x(i0);
@@ -170,40 +235,52 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
     tma_3d(sl + 5 * ST_VT, md1, b, x, j0, k + 1);
 }
 
+/* work items: (x tile, y tile, z chunk, component), component fastest */
 template <int D>
-__global__ void __launch_bounds__(ST_X * ST_Y, 4)
+__global__ void __launch_bounds__(ST_THREADS, 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
           const float *__restrict__ cz, float dth, AwpWork w, int *err)
 {
-    constexpr int S = 1 + D;          /* plane k resident, D in flight */
+    constexpr int S = 1 + D;          /* level k in use, D in flight */
     extern __shared__ unsigned char st_smem[];
-    float *ring = (float *)(((uintptr_t)st_smem + 127) & ~(uintptr_t)127);
-    uint64_t *bar = (uint64_t *)(ring + S * VEL_SLOT);
-    __shared__ int abort_s;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * ST_X + tx;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mb_init(&bar[s], 1);
-        mb_fence_init();
-        abort_s = 0;
+    float *ring = ring_base(st_smem);
+    uint64_t *full = (uint64_t *)(ring + S * VEL_SLOT), *empty = full + S;
+    __shared__ volatile int abort_s;
+    ring_init<S>(full, empty, &abort_s);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+
+    if (ty == ST_CW) {                /* producer warp */
+        if (tx != 0) return;
+        uint32_t use = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
+            const int q = item % ncomp;
+            int bx, by, k0, k1;
+            work_item(g, w, item / ncomp, bx, by, k0, k1);
+            for (int k = k0; k <= k1; ++k, ++use) {
+                ok = ring_acquire<S>(empty, use, &abort_s);
+                if (!ok) break;
+                vel_issue<S>(maps.st[q], &maps.d1, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+            }
+        }
+        if (!ok) {
+            abort_s = 1;
+            atomicOr(err, AWP_KERR_TMA_WAIT);
+        }
+        ring_drain<S>(full, use);
+        return;
     }
-    __syncthreads();
+
     const int sy = g.px, sz = g.plane;
     const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
-    uint32_t used = 0;                /* ring uses so far (same in every thread) */
+    uint32_t use = 0;
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
         const int q = item % ncomp;
         int bx, by, k0, k1;
         work_item(g, w, item / ncomp, bx, by, k0, k1);
-        const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1, i = i0 + tx, j = j0 + ty;
+        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
-        const int np = k1 - k0 + 1;
-        const uint32_t g0 = used;
-        used += np;
-        const CUtensorMap *ms = maps.st[q];
-        int issued = 0;               /* meaningful in thread 0 only */
-        if (tid == 0)
-            for (; issued < S && issued < np; ++issued) vel_issue<S>(ms, &maps.d1, ring, bar, g0 + issued, i0, j0, k0 + issued);
         float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
         const float *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ), *ZZ = pick(cs, q, AF_ZZ);
         float xz_m2 = 0.f, xz_m1 = 0.f, yz_m2 = 0.f, yz_m1 = 0.f, zz_m1 = 0.f, zz_0 = 0.f, zz_p1 = 0.f;
@@ -216,21 +293,20 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             dA = d1[c - sz]; dB = d1[c - sy - sz]; dE = d1[c + 1 - sz];
             cxy = cx[i] * cy[j];
         }
-        int k = k0;
-        for (; k <= k1; ++k, c += sz) {
-            const uint32_t use = g0 + (uint32_t)(k - k0);
+        for (int k = k0; k <= k1; ++k, c += sz, ++use) {
             float u0 = 0.f, v0 = 0.f, w0 = 0.f, xz_p1 = 0.f, yz_p1 = 0.f, zz_p2 = 0.f, czk = 0.f;
             if (live) {
                 u0 = U[c]; v0 = V[c]; w0 = W[c];
                 xz_p1 = XZ[c + sz]; yz_p1 = YZ[c + sz]; zz_p2 = ZZ[c + 2 * sz];
                 czk = cz[k];
             }
-            const bool ok = mb_wait(&bar[use % S], (use / S) & 1);
-            if (!ok) {
+            /* warp-uniform outcome, so a warp leaves together or not at all */
+            if (!__all_sync(0xffffffffu, mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s))) {
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
+                return;
             }
-            if (live && ok) {
+            if (live) {
                 const float *sl = ring + (use % S) * VEL_SLOT;
                 const float *t1 = sl + 5 * ST_VT + cm;
                 const float da = t1[0], db = t1[-ST_W], de = t1[1], dg = t1[1 - ST_W];
@@ -248,18 +324,8 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
                 zz_m1 = zz_0; zz_0 = zz_p1; zz_p1 = zz_p2;
                 dA = da; dB = db; dE = de;
             }
-            __syncthreads();
-            if (abort_s) break;
-            if (tid == 0 && issued < np) {
-                vel_issue<S>(ms, &maps.d1, ring, bar, g0 + issued, i0, j0, k0 + issued);
-                ++issued;
-            }
-        }
-        if (abort_s) {
-            if (tid == 0)
-                for (int n = k - k0; n < issued; ++n)
-                    if (!mb_wait(&bar[(g0 + n) % S], ((g0 + n) / S) & 1)) break;
-            return;
+            __syncwarp();
+            if (tx == 0) mb_arrive(&empty[use % S]);
         }
     }
 }
@@ -268,8 +334,8 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
 /* stress sweep                                                        */
 /* ------------------------------------------------------------------ */
 
-/* slot layout: u v w stencil tiles, then lam mu qp qs media tiles */
-#define STR_SLOT (3 * ST_VT + 4 * ST_MP)
+/* slot layout: u v w stencil tiles of every component, then lam mu qp qs */
+#define STR_SLOT(NC) (3 * (NC) * ST_VT + 4 * ST_MP)
 
 /* media of planes k and k-1 at the cell */
 struct TMed {
@@ -299,141 +365,172 @@ struct TVel {
     }
 };
 
-template <int S>
-__device__ __forceinline__ void str_issue(const CUtensorMap *mv, const CUtensorMap *mm, int nmed, uint32_t txb,
-                                          float *ring, uint64_t *bar, uint32_t use, int i0, int j0, int k)
+template <int NC, int S>
+__device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int nmed, uint32_t txb, float *ring,
+                                          uint64_t *full, uint32_t use, int i0, int j0, int k)
 {
-    float *sl = ring + (use % S) * STR_SLOT;
-    uint64_t *b = &bar[use % S];
+    float *sl = ring + (use % S) * STR_SLOT(NC);
+    uint64_t *b = &full[use % S];
     fence_async_smem();
     mb_expect(b, txb);
     const int x = tile_x(i0);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, mv + a, b, x, j0 - 1, k + 1);
-    for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * ST_VT + a * ST_MP, mm + a, b, x, j0, k + 1);
+    for (int q = 0; q < NC; ++q)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) tma_3d(sl + (3 * q + a) * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
+    for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * NC * ST_VT + a * ST_MP, &maps.med[a], b, x, j0, k + 1);
 }
 
-template <class TR, int D>
-__global__ void __launch_bounds__(ST_X * ST_Y, 4)
-k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
+#define STR_MINB(NC) ((NC) == 3 ? 2 : 3)
+
+/* work items: (x tile, y tile, z chunk); every component of the tile in the
+ * block, so the media tiles and the cell coefficients serve all of them */
+template <class TR, int NC, int D>
+__global__ void __launch_bounds__(ST_THREADS, STR_MINB(NC))
+k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
-    constexpr int S = 2 + D;          /* planes k-1 and k resident, D in flight */
-    const int nmed = nve == 1 ? 4 : 2;
-    const uint32_t txb = (uint32_t)(3 * ST_VT + nmed * ST_MT) * 4u;
+    constexpr int S = 2 + D;          /* levels k-1 and k in use, D in flight */
+    constexpr int SLOT = STR_SLOT(NC);
     extern __shared__ unsigned char st_smem[];
-    float *ring = (float *)(((uintptr_t)st_smem + 127) & ~(uintptr_t)127);
-    uint64_t *bar = (uint64_t *)(ring + S * STR_SLOT);
-    __shared__ int abort_s;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * ST_X + tx;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mb_init(&bar[s], 1);
-        mb_fence_init();
-        abort_s = 0;
+    float *ring = ring_base(st_smem);
+    uint64_t *full = (uint64_t *)(ring + S * SLOT), *empty = full + S;
+    __shared__ volatile int abort_s;
+    ring_init<S>(full, empty, &abort_s);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+
+    if (ty == ST_CW) {                /* producer warp */
+        if (tx != 0) return;
+        const int nmed = nve == 1 ? 4 : 2;
+        const uint32_t txb = (uint32_t)(3 * NC * ST_VT + nmed * ST_MT) * 4u;
+        uint32_t use = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
+            int bx, by, k0, k1;
+            work_item(g, w, item, bx, by, k0, k1);
+            for (int k = k0 - 1; k <= k1; ++k, ++use) {
+                ok = ring_acquire<S>(empty, use, &abort_s);
+                if (!ok) break;
+                str_issue<NC, S>(maps, nmed, txb, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+            }
+        }
+        if (!ok) {
+            abort_s = 1;
+            atomicOr(err, AWP_KERR_TMA_WAIT);
+        }
+        ring_drain<S>(full, use);
+        return;
     }
-    __syncthreads();
-    const int sy = g.px, sz = g.plane;
+
+    const int sz = g.plane;
     const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
-    uint32_t used = 0;
+    uint32_t use0 = 0;                /* ring use of the item's first level */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
-        const int q = item % ncomp;
         int bx, by, k0, k1;
-        work_item(g, w, item / ncomp, bx, by, k0, k1);
-        const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1, i = i0 + tx, j = j0 + ty;
+        work_item(g, w, item, bx, by, k0, k1);
+        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
-        const int pb = k0 - 1;        /* first staged plane */
-        const int np = k1 - pb + 1;
-        const uint32_t g0 = used;
-        used += np;
-        const CUtensorMap *mv = maps.v[q];
-        int issued = 0;
-        if (tid == 0)
-            for (; issued < S && issued < np; ++issued)
-                str_issue<S>(mv, maps.med, nmed, txb, ring, bar, g0 + issued, i0, j0, pb + issued);
-        const float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
-        float *XX = pick(cs, q, AF_XX), *YY = pick(cs, q, AF_YY), *ZZ = pick(cs, q, AF_ZZ);
-        float *XY = pick(cs, q, AF_XY), *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ);
-        TR *Rr[6];
-#pragma unroll
-        for (int a = 0; a < 6; ++a) Rr[a] = (TR *)pick(cs, q, AF_R1 + a);
-        float up1 = 0.f, vp1 = 0.f, wm2 = 0.f, cxy = 0.f;
+        const int np = k1 - k0 + 2;   /* levels k0-1 .. k1 */
+        float up1[NC], vp1[NC], wm2[NC], cxy = 0.f;
         const int itxy = ((j & 1) << 1) | (i & 1);
         int c = g.idx(i, j, k0);
-        if (live) {
-            up1 = U[c + sz]; vp1 = V[c + sz]; wm2 = W[c - 2 * sz];
-            cxy = cx[i] * cy[j];
-        }
-        int k = k0;
-        for (; k <= k1; ++k, c += sz) {
-            const uint32_t use = g0 + (uint32_t)(k - pb), usem = use - 1;
-            float up2 = 0.f, vp2 = 0.f, wp1 = 0.f, czk = 0.f;
-            Stress6 s0{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            float r[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (live) {
-                s0 = Stress6{XX[c], YY[c], ZZ[c], XY[c], XZ[c], YZ[c]};
-                if (nve == 1) {
 #pragma unroll
-                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(Rr[a], c, 1.0f);
+        for (int q = 0; q < NC; ++q) {
+            up1[q] = vp1[q] = wm2[q] = 0.f;
+            if (live) {
+                up1[q] = cs.c[q].f[AF_U][c + sz];
+                vp1[q] = cs.c[q].f[AF_V][c + sz];
+                wm2[q] = cs.c[q].f[AF_W][c - 2 * sz];
+            }
+        }
+        if (live) cxy = cx[i] * cy[j];
+        for (int k = k0; k <= k1; ++k, c += sz) {
+            const uint32_t use = use0 + (uint32_t)(k - k0 + 1), usem = use - 1;
+            float up2[NC], vp2[NC], wp1[NC], czk = 0.f;
+            Stress6 s0{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                up2[q] = vp2[q] = wp1[q] = 0.f;
+                if (live) {
+                    up2[q] = cs.c[q].f[AF_U][c + 2 * sz];
+                    vp2[q] = cs.c[q].f[AF_V][c + 2 * sz];
+                    wp1[q] = cs.c[q].f[AF_W][c + sz];
                 }
-                up2 = U[c + 2 * sz]; vp2 = V[c + 2 * sz]; wp1 = W[c + sz];
+            }
+            if (live) {
+                const AwpComp &c0 = cs.c[0];
+                s0 = Stress6{c0.f[AF_XX][c], c0.f[AF_YY][c], c0.f[AF_ZZ][c], c0.f[AF_XY][c], c0.f[AF_XZ][c],
+                             c0.f[AF_YZ][c]};
                 czk = cz[k];
             }
             bool ok = true;
-            if (k == k0) ok = mb_wait(&bar[usem % S], (usem / S) & 1);
-            if (ok) ok = mb_wait(&bar[use % S], (use / S) & 1);
-            if (!ok) {
+            if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s);
+            if (ok) ok = mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s);
+            if (!__all_sync(0xffffffffu, ok)) {   /* warp-uniform outcome */
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
+                return;
             }
-            if (live && ok) {
-                const float *sk = ring + (use % S) * STR_SLOT, *sm = ring + (usem % S) * STR_SLOT;
+            if (live) {
+                const float *sk = ring + (use % S) * SLOT, *sm = ring + (usem % S) * SLOT;
                 const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
-                const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
+                const TMed M{sk + 3 * NC * ST_VT + cm, sm + 3 * NC * ST_VT + cm};
                 const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
-                const float wm1 = sm[2 * ST_VT + cv];
-                const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1, up2, vp1, vp2, wm2, wp1};
-                Stress6 o;
-                if (nve == 1) {
-                    const VelDiff dd = vel_diff(Vq);
-                    o = str_visco(kc, dd, s0, r, dth, dt, dh1);
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) Store<TR>::st(Rr[a], c, r[a], 1.0f);
-                } else {
-                    o = str_elastic(kc, Vq, s0, dth);
-                }
                 const float crj = cxy * czk;
-                XX[c] = o.xx * crj; YY[c] = o.yy * crj; ZZ[c] = o.zz * crj;
-                XY[c] = o.xy * crj; XZ[c] = o.xz * crj; YZ[c] = o.yz * crj;
-                wm2 = wm1;
+#pragma unroll
+                for (int q = 0; q < NC; ++q) {
+                    const AwpComp &cp = cs.c[q];
+                    const Stress6 sq = q == 0 ? s0
+                                              : Stress6{cp.f[AF_XX][c], cp.f[AF_YY][c], cp.f[AF_ZZ][c], cp.f[AF_XY][c],
+                                                        cp.f[AF_XZ][c], cp.f[AF_YZ][c]};
+                    const float *tq = sk + 3 * q * ST_VT + cv, *mq = sm + 3 * q * ST_VT + cv;
+                    const float wm1 = mq[2 * ST_VT];
+                    const TVel Vq{tq, mq[0], mq[ST_VT], wm1, up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
+                    Stress6 o;
+                    if (nve == 1) {
+                        float r[6];
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
+                        const VelDiff dd = vel_diff(Vq);
+                        o = str_visco(kc, dd, sq, r, dth, dt, dh1);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
+                    } else {
+                        o = str_elastic(kc, Vq, sq, dth);
+                    }
+                    cp.f[AF_XX][c] = o.xx * crj; cp.f[AF_YY][c] = o.yy * crj; cp.f[AF_ZZ][c] = o.zz * crj;
+                    cp.f[AF_XY][c] = o.xy * crj; cp.f[AF_XZ][c] = o.xz * crj; cp.f[AF_YZ][c] = o.yz * crj;
+                    wm2[q] = wm1;
+                }
             }
-            up1 = up2;
-            vp1 = vp2;
-            __syncthreads();
-            if (abort_s) break;
-            if (tid == 0 && issued < np) {
-                str_issue<S>(mv, maps.med, nmed, txb, ring, bar, g0 + issued, i0, j0, pb + issued);
-                ++issued;
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                up1[q] = up2[q];
+                vp1[q] = vp2[q];
             }
+            __syncwarp();
+            if (tx == 0) mb_arrive(&empty[usem % S]);
         }
-        if (abort_s) {
-            if (tid == 0)
-                for (int n = k - pb - (k == k0 ? 1 : 0); n < issued; ++n)
-                    if (!mb_wait(&bar[(g0 + n) % S], ((g0 + n) / S) & 1)) break;
-            return;
-        }
+        __syncwarp();
+        if (tx == 0) mb_arrive(&empty[(use0 + np - 1) % S]);
+        use0 += np;
         if (live && k1 == g.nz) {
             /* fstr (operator.f:594-606) on this thread's own column; the top
              * chunk holds at least levels nz-2..nz, all written by this thread */
             const int ct = g.idx(i, j, g.nz);
-            ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
-            ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
-            XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
-            XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
-            YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
-            YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
-            XZ[ct] = 0.0f;
-            YZ[ct] = 0.0f;
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                float *ZZ = cs.c[q].f[AF_ZZ], *XZ = cs.c[q].f[AF_XZ], *YZ = cs.c[q].f[AF_YZ];
+                ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+                ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+                XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+                XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+                YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+                YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+                XZ[ct] = 0.0f;
+                YZ[ct] = 0.0f;
+            }
         }
     }
 }
@@ -517,7 +614,7 @@ static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid)
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, ST_X * ST_Y, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, ST_THREADS, smem);
     if (e != cudaSuccess) return e;
     if (per < 1) return cudaErrorInvalidConfiguration;
     *grid = nsm * per < nitems ? nsm * per : nitems;
@@ -532,34 +629,45 @@ static AwpCompSet<AWP_MAX_COMP> comp_set3(const AwpStepArgs &s)
     return cs;
 }
 
+/* dynamic shared memory of a ring: alignment slack, slots, full + empty barriers */
+static size_t ring_bytes(int slots, int slot_floats) { return 128 + (size_t)slots * slot_floats * 4 + 2 * 8 * slots; }
+
 cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
-    constexpr int S = 1 + ST_VEL_D;
-    const size_t smem = 128 + (size_t)S * VEL_SLOT * 4 + S * 8;
+    const size_t smem = ring_bytes(1 + ST_VEL_D, VEL_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
     cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
-    k_vel_tma<ST_VEL_D><<<grid, dim3(ST_X, ST_Y), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp,
-                                                                   (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz,
-                                                                   s.dth, w, s.kerr);
+    k_vel_tma<ST_VEL_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp,
+                                                                      (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz,
+                                                                      s.dth, w, s.kerr);
+    return cudaGetLastError();
+}
+
+template <class TR, int NC>
+static cudaError_t launch_str_nc(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    const size_t smem = ring_bytes(2 + ST_STR_D, STR_SLOT(NC));
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
+    int grid = 0;
+    cudaError_t e = staged_grid(k_str_tma<TR, NC, ST_STR_D>, smem, w.nitems, &grid);
+    if (e != cudaSuccess) return e;
+    k_str_tma<TR, NC, ST_STR_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
+        st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
 }
 
 template <class TR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
-    constexpr int S = 2 + ST_STR_D;
-    const size_t smem = 128 + (size_t)S * STR_SLOT * 4 + S * 8;
-    const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
-    int grid = 0;
-    cudaError_t e = staged_grid(k_str_tma<TR, ST_STR_D>, smem, w.nitems, &grid);
-    if (e != cudaSuccess) return e;
-    k_str_tma<TR, ST_STR_D><<<grid, dim3(ST_X, ST_Y), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.cx, s.cy,
-                                                                       s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve,
-                                                                       s.kerr);
-    return cudaGetLastError();
+    switch (s.ncomp) {
+    case 1: return launch_str_nc<TR, 1>(st, s, stream);
+    case 2: return launch_str_nc<TR, 2>(st, s, stream);
+    case 3: return launch_str_nc<TR, 3>(st, s, stream);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
