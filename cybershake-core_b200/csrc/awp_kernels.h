@@ -29,6 +29,7 @@ struct AwpStepArgs {
     int unroll;                  /* two-sweep z-loop unroll (1 or 2)        */
     const AwpStaged *staged;     /* non-NULL: TMA-staged velocity/stress    */
     int kchunk_staged;           /* z levels per staged work item           */
+    int staged_group;            /* 1: stress blocks carry every component  */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

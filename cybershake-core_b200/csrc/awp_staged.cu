@@ -366,7 +366,7 @@ struct TVel {
 };
 
 template <int NC, int S>
-__device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int nmed, uint32_t txb, float *ring,
+__device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q0, int nmed, uint32_t txb, float *ring,
                                           uint64_t *full, uint32_t use, int i0, int j0, int k)
 {
     float *sl = ring + (use % S) * STR_SLOT(NC);
@@ -377,17 +377,27 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int nmed
 #pragma unroll
     for (int q = 0; q < NC; ++q)
 #pragma unroll
-        for (int a = 0; a < 3; ++a) tma_3d(sl + (3 * q + a) * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
+        for (int a = 0; a < 3; ++a) tma_3d(sl + (3 * q + a) * ST_VT, &maps.v[NC > 1 ? q : q0][a], b, x, j0 - 1, k + 1);
     for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * NC * ST_VT + a * ST_MP, &maps.med[a], b, x, j0, k + 1);
 }
 
 #define STR_MINB(NC) ((NC) == 3 ? 2 : 3)
 
-/* work items: (x tile, y tile, z chunk); every component of the tile in the
- * block, so the media tiles and the cell coefficients serve all of them */
+/* field f of component q of the block's group: a compile-time parameter
+ * access when the block carries every component (q0 = 0), a select on the
+ * item's component when it carries one */
+template <int NC>
+__device__ __forceinline__ float *gp(const AwpCompSet<AWP_MAX_COMP> &cs, int q0, int q, int f)
+{
+    return NC > 1 ? cs.c[q].f[f] : pick(cs, q0, f);
+}
+
+/* work items: (x tile, y tile, z chunk, component group), group fastest; a
+ * block carries NC components of the tile (NC = 1: one component per item,
+ * NC = ncomp: the media tiles and cell coefficients serve all of them) */
 template <class TR, int NC, int D>
 __global__ void __launch_bounds__(ST_THREADS, STR_MINB(NC))
-k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
+k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ngroup,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
@@ -407,12 +417,13 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
         uint32_t use = 0;
         bool ok = true;
         for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
+            const int q0 = (item % ngroup) * NC;
             int bx, by, k0, k1;
-            work_item(g, w, item, bx, by, k0, k1);
+            work_item(g, w, item / ngroup, bx, by, k0, k1);
             for (int k = k0 - 1; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
-                str_issue<NC, S>(maps, nmed, txb, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+                str_issue<NC, S>(maps, q0, nmed, txb, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
         }
         if (!ok) {
@@ -427,8 +438,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
     uint32_t use0 = 0;                /* ring use of the item's first level */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        const int q0 = (item % ngroup) * NC;
         int bx, by, k0, k1;
-        work_item(g, w, item, bx, by, k0, k1);
+        work_item(g, w, item / ngroup, bx, by, k0, k1);
         const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
         const int np = k1 - k0 + 2;   /* levels k0-1 .. k1 */
@@ -439,9 +451,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
         for (int q = 0; q < NC; ++q) {
             up1[q] = vp1[q] = wm2[q] = 0.f;
             if (live) {
-                up1[q] = cs.c[q].f[AF_U][c + sz];
-                vp1[q] = cs.c[q].f[AF_V][c + sz];
-                wm2[q] = cs.c[q].f[AF_W][c - 2 * sz];
+                up1[q] = gp<NC>(cs, q0, q, AF_U)[c + sz];
+                vp1[q] = gp<NC>(cs, q0, q, AF_V)[c + sz];
+                wm2[q] = gp<NC>(cs, q0, q, AF_W)[c - 2 * sz];
             }
         }
         if (live) cxy = cx[i] * cy[j];
@@ -453,15 +465,14 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             for (int q = 0; q < NC; ++q) {
                 up2[q] = vp2[q] = wp1[q] = 0.f;
                 if (live) {
-                    up2[q] = cs.c[q].f[AF_U][c + 2 * sz];
-                    vp2[q] = cs.c[q].f[AF_V][c + 2 * sz];
-                    wp1[q] = cs.c[q].f[AF_W][c + sz];
+                    up2[q] = gp<NC>(cs, q0, q, AF_U)[c + 2 * sz];
+                    vp2[q] = gp<NC>(cs, q0, q, AF_V)[c + 2 * sz];
+                    wp1[q] = gp<NC>(cs, q0, q, AF_W)[c + sz];
                 }
             }
             if (live) {
-                const AwpComp &c0 = cs.c[0];
-                s0 = Stress6{c0.f[AF_XX][c], c0.f[AF_YY][c], c0.f[AF_ZZ][c], c0.f[AF_XY][c], c0.f[AF_XZ][c],
-                             c0.f[AF_YZ][c]};
+                s0 = Stress6{gp<NC>(cs, q0, 0, AF_XX)[c], gp<NC>(cs, q0, 0, AF_YY)[c], gp<NC>(cs, q0, 0, AF_ZZ)[c],
+                             gp<NC>(cs, q0, 0, AF_XY)[c], gp<NC>(cs, q0, 0, AF_XZ)[c], gp<NC>(cs, q0, 0, AF_YZ)[c]};
                 czk = cz[k];
             }
             bool ok = true;
@@ -480,10 +491,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                 const float crj = cxy * czk;
 #pragma unroll
                 for (int q = 0; q < NC; ++q) {
-                    const AwpComp &cp = cs.c[q];
                     const Stress6 sq = q == 0 ? s0
-                                              : Stress6{cp.f[AF_XX][c], cp.f[AF_YY][c], cp.f[AF_ZZ][c], cp.f[AF_XY][c],
-                                                        cp.f[AF_XZ][c], cp.f[AF_YZ][c]};
+                                              : Stress6{gp<NC>(cs, q0, q, AF_XX)[c], gp<NC>(cs, q0, q, AF_YY)[c], gp<NC>(cs, q0, q, AF_ZZ)[c], gp<NC>(cs, q0, q, AF_XY)[c],
+                                                        gp<NC>(cs, q0, q, AF_XZ)[c], gp<NC>(cs, q0, q, AF_YZ)[c]};
                     const float *tq = sk + 3 * q * ST_VT + cv, *mq = sm + 3 * q * ST_VT + cv;
                     const float wm1 = mq[2 * ST_VT];
                     const TVel Vq{tq, mq[0], mq[ST_VT], wm1, up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
@@ -491,16 +501,16 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                     if (nve == 1) {
                         float r[6];
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
+                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)gp<NC>(cs, q0, q, AF_R1 + a), c, 1.0f);
                         const VelDiff dd = vel_diff(Vq);
                         o = str_visco(kc, dd, sq, r, dth, dt, dh1);
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
+                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)gp<NC>(cs, q0, q, AF_R1 + a), c, r[a], 1.0f);
                     } else {
                         o = str_elastic(kc, Vq, sq, dth);
                     }
-                    cp.f[AF_XX][c] = o.xx * crj; cp.f[AF_YY][c] = o.yy * crj; cp.f[AF_ZZ][c] = o.zz * crj;
-                    cp.f[AF_XY][c] = o.xy * crj; cp.f[AF_XZ][c] = o.xz * crj; cp.f[AF_YZ][c] = o.yz * crj;
+                    gp<NC>(cs, q0, q, AF_XX)[c] = o.xx * crj; gp<NC>(cs, q0, q, AF_YY)[c] = o.yy * crj; gp<NC>(cs, q0, q, AF_ZZ)[c] = o.zz * crj;
+                    gp<NC>(cs, q0, q, AF_XY)[c] = o.xy * crj; gp<NC>(cs, q0, q, AF_XZ)[c] = o.xz * crj; gp<NC>(cs, q0, q, AF_YZ)[c] = o.yz * crj;
                     wm2[q] = wm1;
                 }
             }
@@ -521,7 +531,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             const int ct = g.idx(i, j, g.nz);
 #pragma unroll
             for (int q = 0; q < NC; ++q) {
-                float *ZZ = cs.c[q].f[AF_ZZ], *XZ = cs.c[q].f[AF_XZ], *YZ = cs.c[q].f[AF_YZ];
+                float *ZZ = gp<NC>(cs, q0, q, AF_ZZ), *XZ = gp<NC>(cs, q0, q, AF_XZ), *YZ = gp<NC>(cs, q0, q, AF_YZ);
                 ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
                 ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
                 XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
@@ -650,20 +660,22 @@ template <class TR, int NC>
 static cudaError_t launch_str_nc(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     const size_t smem = ring_bytes(2 + ST_STR_D, STR_SLOT(NC));
-    const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
+    const int ngroup = s.ncomp / NC;
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, ngroup);
     int grid = 0;
     cudaError_t e = staged_grid(k_str_tma<TR, NC, ST_STR_D>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
     k_str_tma<TR, NC, ST_STR_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
-        st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+        st->sm, s.g, comp_set3(s), ngroup, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
 }
 
 template <class TR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
+    /* one component per block unless the caller asks for whole-tile blocks */
+    if (!s.staged_group || s.ncomp == 1) return launch_str_nc<TR, 1>(st, s, stream);
     switch (s.ncomp) {
-    case 1: return launch_str_nc<TR, 1>(st, s, stream);
     case 2: return launch_str_nc<TR, 2>(st, s, stream);
     case 3: return launch_str_nc<TR, 3>(st, s, stream);
     default: return cudaErrorInvalidValue;
