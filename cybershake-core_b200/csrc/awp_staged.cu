@@ -384,12 +384,12 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q0, 
 #define STR_MINB(NC) ((NC) == 3 ? 2 : 3)
 
 /* field f of component q of the block's group: a compile-time parameter
- * access when the block carries every component (q0 = 0), a select on the
- * item's component when it carries one */
+ * access when the block carries every component (q0 = 0); one shared-memory
+ * load from the block's pointer table when it carries the item's component */
 template <int NC>
-__device__ __forceinline__ float *gp(const AwpCompSet<AWP_MAX_COMP> &cs, int q0, int q, int f)
+__device__ __forceinline__ float *gp(const AwpCompSet<AWP_MAX_COMP> &cs, const AwpComp *tab, int q0, int q, int f)
 {
-    return NC > 1 ? cs.c[q].f[f] : pick(cs, q0, f);
+    return NC > 1 ? cs.c[q].f[f] : tab[q0].f[f];
 }
 
 /* work items: (x tile, y tile, z chunk, component group), group fastest; a
@@ -407,6 +407,11 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     float *ring = ring_base(st_smem);
     uint64_t *full = (uint64_t *)(ring + S * SLOT), *empty = full + S;
     __shared__ volatile int abort_s;
+    __shared__ AwpComp tab[AWP_MAX_COMP];
+    if (NC == 1 && threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
+#pragma unroll
+        for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
+    }
     ring_init<S>(full, empty, &abort_s);
     const int tx = threadIdx.x, ty = threadIdx.y;
 
@@ -451,9 +456,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
         for (int q = 0; q < NC; ++q) {
             up1[q] = vp1[q] = wm2[q] = 0.f;
             if (live) {
-                up1[q] = gp<NC>(cs, q0, q, AF_U)[c + sz];
-                vp1[q] = gp<NC>(cs, q0, q, AF_V)[c + sz];
-                wm2[q] = gp<NC>(cs, q0, q, AF_W)[c - 2 * sz];
+                up1[q] = gp<NC>(cs, tab, q0, q, AF_U)[c + sz];
+                vp1[q] = gp<NC>(cs, tab, q0, q, AF_V)[c + sz];
+                wm2[q] = gp<NC>(cs, tab, q0, q, AF_W)[c - 2 * sz];
             }
         }
         if (live) cxy = cx[i] * cy[j];
@@ -465,14 +470,14 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             for (int q = 0; q < NC; ++q) {
                 up2[q] = vp2[q] = wp1[q] = 0.f;
                 if (live) {
-                    up2[q] = gp<NC>(cs, q0, q, AF_U)[c + 2 * sz];
-                    vp2[q] = gp<NC>(cs, q0, q, AF_V)[c + 2 * sz];
-                    wp1[q] = gp<NC>(cs, q0, q, AF_W)[c + sz];
+                    up2[q] = gp<NC>(cs, tab, q0, q, AF_U)[c + 2 * sz];
+                    vp2[q] = gp<NC>(cs, tab, q0, q, AF_V)[c + 2 * sz];
+                    wp1[q] = gp<NC>(cs, tab, q0, q, AF_W)[c + sz];
                 }
             }
             if (live) {
-                s0 = Stress6{gp<NC>(cs, q0, 0, AF_XX)[c], gp<NC>(cs, q0, 0, AF_YY)[c], gp<NC>(cs, q0, 0, AF_ZZ)[c],
-                             gp<NC>(cs, q0, 0, AF_XY)[c], gp<NC>(cs, q0, 0, AF_XZ)[c], gp<NC>(cs, q0, 0, AF_YZ)[c]};
+                s0 = Stress6{gp<NC>(cs, tab, q0, 0, AF_XX)[c], gp<NC>(cs, tab, q0, 0, AF_YY)[c], gp<NC>(cs, tab, q0, 0, AF_ZZ)[c],
+                             gp<NC>(cs, tab, q0, 0, AF_XY)[c], gp<NC>(cs, tab, q0, 0, AF_XZ)[c], gp<NC>(cs, tab, q0, 0, AF_YZ)[c]};
                 czk = cz[k];
             }
             bool ok = true;
@@ -492,8 +497,8 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
 #pragma unroll
                 for (int q = 0; q < NC; ++q) {
                     const Stress6 sq = q == 0 ? s0
-                                              : Stress6{gp<NC>(cs, q0, q, AF_XX)[c], gp<NC>(cs, q0, q, AF_YY)[c], gp<NC>(cs, q0, q, AF_ZZ)[c], gp<NC>(cs, q0, q, AF_XY)[c],
-                                                        gp<NC>(cs, q0, q, AF_XZ)[c], gp<NC>(cs, q0, q, AF_YZ)[c]};
+                                              : Stress6{gp<NC>(cs, tab, q0, q, AF_XX)[c], gp<NC>(cs, tab, q0, q, AF_YY)[c], gp<NC>(cs, tab, q0, q, AF_ZZ)[c], gp<NC>(cs, tab, q0, q, AF_XY)[c],
+                                                        gp<NC>(cs, tab, q0, q, AF_XZ)[c], gp<NC>(cs, tab, q0, q, AF_YZ)[c]};
                     const float *tq = sk + 3 * q * ST_VT + cv, *mq = sm + 3 * q * ST_VT + cv;
                     const float wm1 = mq[2 * ST_VT];
                     const TVel Vq{tq, mq[0], mq[ST_VT], wm1, up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
@@ -501,16 +506,16 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                     if (nve == 1) {
                         float r[6];
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)gp<NC>(cs, q0, q, AF_R1 + a), c, 1.0f);
+                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)gp<NC>(cs, tab, q0, q, AF_R1 + a), c, 1.0f);
                         const VelDiff dd = vel_diff(Vq);
                         o = str_visco(kc, dd, sq, r, dth, dt, dh1);
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)gp<NC>(cs, q0, q, AF_R1 + a), c, r[a], 1.0f);
+                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)gp<NC>(cs, tab, q0, q, AF_R1 + a), c, r[a], 1.0f);
                     } else {
                         o = str_elastic(kc, Vq, sq, dth);
                     }
-                    gp<NC>(cs, q0, q, AF_XX)[c] = o.xx * crj; gp<NC>(cs, q0, q, AF_YY)[c] = o.yy * crj; gp<NC>(cs, q0, q, AF_ZZ)[c] = o.zz * crj;
-                    gp<NC>(cs, q0, q, AF_XY)[c] = o.xy * crj; gp<NC>(cs, q0, q, AF_XZ)[c] = o.xz * crj; gp<NC>(cs, q0, q, AF_YZ)[c] = o.yz * crj;
+                    gp<NC>(cs, tab, q0, q, AF_XX)[c] = o.xx * crj; gp<NC>(cs, tab, q0, q, AF_YY)[c] = o.yy * crj; gp<NC>(cs, tab, q0, q, AF_ZZ)[c] = o.zz * crj;
+                    gp<NC>(cs, tab, q0, q, AF_XY)[c] = o.xy * crj; gp<NC>(cs, tab, q0, q, AF_XZ)[c] = o.xz * crj; gp<NC>(cs, tab, q0, q, AF_YZ)[c] = o.yz * crj;
                     wm2[q] = wm1;
                 }
             }
@@ -531,7 +536,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             const int ct = g.idx(i, j, g.nz);
 #pragma unroll
             for (int q = 0; q < NC; ++q) {
-                float *ZZ = gp<NC>(cs, q0, q, AF_ZZ), *XZ = gp<NC>(cs, q0, q, AF_XZ), *YZ = gp<NC>(cs, q0, q, AF_YZ);
+                float *ZZ = gp<NC>(cs, tab, q0, q, AF_ZZ), *XZ = gp<NC>(cs, tab, q0, q, AF_XZ), *YZ = gp<NC>(cs, tab, q0, q, AF_YZ);
                 ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
                 ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
                 XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
