@@ -29,7 +29,6 @@ struct AwpStepArgs {
     int unroll;                  /* two-sweep z-loop unroll (1 or 2)        */
     const AwpStaged *staged;     /* non-NULL: TMA-staged velocity/stress    */
     int kchunk_staged;           /* z levels per staged work item           */
-    int staged_group;            /* 1: stress blocks carry every component  */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 
@@ -49,7 +48,8 @@ cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st);
 /* two-sweep: velocity, free-surface velocity, stress (+ fstr); fused: one kernel */
 cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st);
 /* TMA-staged sweeps: FP32 media; maps built once over fixed device arrays */
-cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md);
+cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md,
+                              int rtype);
 void awp_staged_destroy(AwpStaged *s);
 cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);

@@ -77,7 +77,6 @@ struct awp_solver {
     int kchunk_sweep;                /* z levels per two-sweep work item    */
     int staged_on;                   /* TMA-staged velocity/stress sweeps   */
     int kchunk_staged;               /* z levels per staged work item       */
-    int staged_group;                /* stress blocks carry all components  */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -440,7 +439,6 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     {
         const int kc = env_int("AWP_TUNE_KSTAGE", 32);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
-        s->staged_group = env_int("AWP_TUNE_STRGROUP", 0) != 0;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -776,7 +774,6 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.unroll = s->unroll;
     a.staged = s->staged_on ? s->staged : NULL;
     a.kchunk_staged = s->kchunk_staged;
-    a.staged_group = s->staged_group;
     a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);
@@ -850,7 +847,7 @@ static awp_status start_if_needed(awp_solver *s)
     if (!s->media_loaded) return set_err(AWP_ERR_STATE, "media not loaded");
     if (s->staged_on && !s->staged) {
         /* the arrays are fixed from here on: u v w, the stresses, FP32 media */
-        const cudaError_t e = awp_staged_create(&s->staged, s->g, s->p.ncomp, s->comp[0], s->mdt);
+        const cudaError_t e = awp_staged_create(&s->staged, s->g, s->p.ncomp, s->comp[0], s->mdt, s->rstore);
         if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "staged stepper: tensor maps: %s", cudaGetErrorString(e));
     }
     AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;

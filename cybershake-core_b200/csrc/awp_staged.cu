@@ -47,7 +47,6 @@
 #define ST_MP 384                    /* floats reserved per media tile (1536 B) */
 #define ST_WAIT_NS 2000000000ull     /* bound of one barrier wait               */
 #define ST_VEL_D 3                   /* levels in flight, velocity sweep        */
-#define ST_STR_D 2                   /* levels in flight, stress sweep          */
 
 struct AwpStagedVelMaps {
     CUtensorMap st[AWP_MAX_COMP][5]; /* xx yy xy xz yz, box 40 x 12           */
@@ -56,6 +55,8 @@ struct AwpStagedVelMaps {
 struct AwpStagedStrMaps {
     CUtensorMap v[AWP_MAX_COMP][3];  /* u v w, box 40 x 12                     */
     CUtensorMap med[4];              /* lam mu qp qs, box 40 x 9               */
+    CUtensorMap s[AWP_MAX_COMP][6];  /* xx yy zz xy xz yz, box 32 x 8          */
+    CUtensorMap r[AWP_MAX_COMP][6];  /* r1..r6 (FP32 or bf16), box 32 x 8      */
 };
 struct AwpStaged {
     AwpStagedVelMaps vm;
@@ -334,8 +335,14 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
 /* stress sweep                                                        */
 /* ------------------------------------------------------------------ */
 
-/* slot layout: u v w stencil tiles of every component, then lam mu qp qs */
-#define STR_SLOT(NC) (3 * (NC) * ST_VT + 4 * ST_MP)
+/* Slot layout (floats): u v w stencil tiles, lam mu qp qs media tiles, the
+ * six stresses and the six memory variables of the tile (32 x 8 each; the
+ * memory variables in their storage type).  Levels k-1 and k are in use
+ * while level k+1 is in flight. */
+#define STR_D 1
+#define STR_ST (3 * ST_VT + 4 * ST_MP)           /* first stress tile        */
+#define STR_PT (ST_X * ST_Y)                      /* floats of a point tile   */
+#define STR_SLOT (STR_ST + 12 * STR_PT)           /* r tiles fit in 6 x 256   */
 
 /* media of planes k and k-1 at the cell */
 struct TMed {
@@ -365,50 +372,52 @@ struct TVel {
     }
 };
 
-template <int NC, int S>
-__device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q0, int nmed, uint32_t txb, float *ring,
-                                          uint64_t *full, uint32_t use, int i0, int j0, int k)
+/* bytes one level brings in */
+__host__ __device__ __forceinline__ uint32_t str_txb(int nve, int rsize)
 {
-    float *sl = ring + (use % S) * STR_SLOT(NC);
+    return (uint32_t)((3 * ST_VT + (nve == 1 ? 4 : 2) * ST_MT + 6 * STR_PT) * 4 + (nve == 1 ? 6 * STR_PT * rsize : 0));
+}
+
+template <int S, int RSIZE>
+__device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, int nve, float *ring, uint64_t *full,
+                                          uint32_t use, int i0, int j0, int k)
+{
+    float *sl = ring + (use % S) * STR_SLOT;
     uint64_t *b = &full[use % S];
     fence_async_smem();
-    mb_expect(b, txb);
+    mb_expect(b, str_txb(nve, RSIZE));
     const int x = tile_x(i0);
 #pragma unroll
-    for (int q = 0; q < NC; ++q)
+    for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
+    const int nmed = nve == 1 ? 4 : 2;
+    for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * ST_VT + a * ST_MP, &maps.med[a], b, x, j0, k + 1);
+    /* point tiles start at cell (i0, j0): memory column i0 + 7 (a multiple of 8) */
+    const int xp = i0 + AWP_XO - 1;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) tma_3d(sl + (3 * q + a) * ST_VT, &maps.v[NC > 1 ? q : q0][a], b, x, j0 - 1, k + 1);
-    for (int a = 0; a < nmed; ++a) tma_3d(sl + 3 * NC * ST_VT + a * ST_MP, &maps.med[a], b, x, j0, k + 1);
+    for (int a = 0; a < 6; ++a) tma_3d(sl + STR_ST + a * STR_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
+    if (nve == 1) {
+        unsigned char *rb = (unsigned char *)(sl + STR_ST + 6 * STR_PT);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) tma_3d(rb + a * STR_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
+    }
 }
 
-#define STR_MINB(NC) ((NC) == 3 ? 2 : 3)
-
-/* field f of component q of the block's group: a compile-time parameter
- * access when the block carries every component (q0 = 0); one shared-memory
- * load from the block's pointer table when it carries the item's component */
-template <int NC>
-__device__ __forceinline__ float *gp(const AwpCompSet<AWP_MAX_COMP> &cs, const AwpComp *tab, int q0, int q, int f)
-{
-    return NC > 1 ? cs.c[q].f[f] : tab[q0].f[f];
-}
-
-/* work items: (x tile, y tile, z chunk, component group), group fastest; a
- * block carries NC components of the tile (NC = 1: one component per item,
- * NC = ncomp: the media tiles and cell coefficients serve all of them) */
-template <class TR, int NC, int D>
-__global__ void __launch_bounds__(ST_THREADS, STR_MINB(NC))
-k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ngroup,
+/* work items: (x tile, y tile, z chunk, component), component fastest, so
+ * the components of a tile run side by side and share its media through L2 */
+template <class TR>
+__global__ void __launch_bounds__(ST_THREADS, 3)
+k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
-    constexpr int S = 2 + D;          /* levels k-1 and k in use, D in flight */
-    constexpr int SLOT = STR_SLOT(NC);
+    constexpr int S = 2 + STR_D;      /* levels k-1 and k in use, STR_D in flight */
+    constexpr int RSIZE = (int)sizeof(TR);
     extern __shared__ unsigned char st_smem[];
     float *ring = ring_base(st_smem);
-    uint64_t *full = (uint64_t *)(ring + S * SLOT), *empty = full + S;
+    uint64_t *full = (uint64_t *)(ring + S * STR_SLOT), *empty = full + S;
     __shared__ volatile int abort_s;
     __shared__ AwpComp tab[AWP_MAX_COMP];
-    if (NC == 1 && threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
+    if (threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
 #pragma unroll
         for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
@@ -417,18 +426,16 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
 
     if (ty == ST_CW) {                /* producer warp */
         if (tx != 0) return;
-        const int nmed = nve == 1 ? 4 : 2;
-        const uint32_t txb = (uint32_t)(3 * NC * ST_VT + nmed * ST_MT) * 4u;
         uint32_t use = 0;
         bool ok = true;
         for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
-            const int q0 = (item % ngroup) * NC;
+            const int q = item % ncomp;
             int bx, by, k0, k1;
-            work_item(g, w, item / ngroup, bx, by, k0, k1);
+            work_item(g, w, item / ncomp, bx, by, k0, k1);
             for (int k = k0 - 1; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
-                str_issue<NC, S>(maps, q0, nmed, txb, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+                str_issue<S, RSIZE>(maps, q, nve, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
         }
         if (!ok) {
@@ -440,44 +447,31 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     }
 
     const int sz = g.plane;
-    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
+    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
     uint32_t use0 = 0;                /* ring use of the item's first level */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
-        const int q0 = (item % ngroup) * NC;
+        const int q = item % ncomp;
         int bx, by, k0, k1;
-        work_item(g, w, item / ngroup, bx, by, k0, k1);
+        work_item(g, w, item / ncomp, bx, by, k0, k1);
         const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
         const int np = k1 - k0 + 2;   /* levels k0-1 .. k1 */
-        float up1[NC], vp1[NC], wm2[NC], cxy = 0.f;
+        const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
+        /* column queues: u, v at k+1, k+2 (and k+3 loaded one level ahead), w at k-2 and k+1 (k+2 ahead) */
+        float up1 = 0.f, up2 = 0.f, vp1 = 0.f, vp2 = 0.f, wm2 = 0.f, wp1 = 0.f, cxy = 0.f;
         const int itxy = ((j & 1) << 1) | (i & 1);
         int c = g.idx(i, j, k0);
-#pragma unroll
-        for (int q = 0; q < NC; ++q) {
-            up1[q] = vp1[q] = wm2[q] = 0.f;
-            if (live) {
-                up1[q] = gp<NC>(cs, tab, q0, q, AF_U)[c + sz];
-                vp1[q] = gp<NC>(cs, tab, q0, q, AF_V)[c + sz];
-                wm2[q] = gp<NC>(cs, tab, q0, q, AF_W)[c - 2 * sz];
-            }
+        if (live) {
+            up1 = U[c + sz]; up2 = U[c + 2 * sz];
+            vp1 = V[c + sz]; vp2 = V[c + 2 * sz];
+            wm2 = W[c - 2 * sz]; wp1 = W[c + sz];
+            cxy = cx[i] * cy[j];
         }
-        if (live) cxy = cx[i] * cy[j];
         for (int k = k0; k <= k1; ++k, c += sz) {
             const uint32_t use = use0 + (uint32_t)(k - k0 + 1), usem = use - 1;
-            float up2[NC], vp2[NC], wp1[NC], czk = 0.f;
-            Stress6 s0{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                up2[q] = vp2[q] = wp1[q] = 0.f;
-                if (live) {
-                    up2[q] = gp<NC>(cs, tab, q0, q, AF_U)[c + 2 * sz];
-                    vp2[q] = gp<NC>(cs, tab, q0, q, AF_V)[c + 2 * sz];
-                    wp1[q] = gp<NC>(cs, tab, q0, q, AF_W)[c + sz];
-                }
-            }
+            float up3 = 0.f, vp3 = 0.f, wp2 = 0.f, czk = 0.f;
             if (live) {
-                s0 = Stress6{gp<NC>(cs, tab, q0, 0, AF_XX)[c], gp<NC>(cs, tab, q0, 0, AF_YY)[c], gp<NC>(cs, tab, q0, 0, AF_ZZ)[c],
-                             gp<NC>(cs, tab, q0, 0, AF_XY)[c], gp<NC>(cs, tab, q0, 0, AF_XZ)[c], gp<NC>(cs, tab, q0, 0, AF_YZ)[c]};
+                if (k < k1) { up3 = U[c + 3 * sz]; vp3 = V[c + 3 * sz]; wp2 = W[c + 2 * sz]; }
                 czk = cz[k];
             }
             bool ok = true;
@@ -488,42 +482,35 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                 atomicOr(err, AWP_KERR_TMA_WAIT);
                 return;
             }
+            const float *sk = ring + (use % S) * STR_SLOT, *sm = ring + (usem % S) * STR_SLOT;
+            const float wm1 = sm[2 * ST_VT + cv];
             if (live) {
-                const float *sk = ring + (use % S) * SLOT, *sm = ring + (usem % S) * SLOT;
                 const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
-                const TMed M{sk + 3 * NC * ST_VT + cm, sm + 3 * NC * ST_VT + cm};
+                const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
                 const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
-                const float crj = cxy * czk;
+                const float *ps = sk + STR_ST + cp;
+                const Stress6 s0{ps[0], ps[STR_PT], ps[2 * STR_PT], ps[3 * STR_PT], ps[4 * STR_PT], ps[5 * STR_PT]};
+                const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1, up2, vp1, vp2, wm2, wp1};
+                Stress6 o;
+                if (nve == 1) {
+                    const TR *pr = (const TR *)(sk + STR_ST + 6 * STR_PT) + cp;
+                    float r[6];
 #pragma unroll
-                for (int q = 0; q < NC; ++q) {
-                    const Stress6 sq = q == 0 ? s0
-                                              : Stress6{gp<NC>(cs, tab, q0, q, AF_XX)[c], gp<NC>(cs, tab, q0, q, AF_YY)[c], gp<NC>(cs, tab, q0, q, AF_ZZ)[c], gp<NC>(cs, tab, q0, q, AF_XY)[c],
-                                                        gp<NC>(cs, tab, q0, q, AF_XZ)[c], gp<NC>(cs, tab, q0, q, AF_YZ)[c]};
-                    const float *tq = sk + 3 * q * ST_VT + cv, *mq = sm + 3 * q * ST_VT + cv;
-                    const float wm1 = mq[2 * ST_VT];
-                    const TVel Vq{tq, mq[0], mq[ST_VT], wm1, up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
-                    Stress6 o;
-                    if (nve == 1) {
-                        float r[6];
+                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(pr, a * STR_PT, 1.0f);
+                    const VelDiff dd = vel_diff(Vq);
+                    o = str_visco(kc, dd, s0, r, dth, dt, dh1);
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)gp<NC>(cs, tab, q0, q, AF_R1 + a), c, 1.0f);
-                        const VelDiff dd = vel_diff(Vq);
-                        o = str_visco(kc, dd, sq, r, dth, dt, dh1);
-#pragma unroll
-                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)gp<NC>(cs, tab, q0, q, AF_R1 + a), c, r[a], 1.0f);
-                    } else {
-                        o = str_elastic(kc, Vq, sq, dth);
-                    }
-                    gp<NC>(cs, tab, q0, q, AF_XX)[c] = o.xx * crj; gp<NC>(cs, tab, q0, q, AF_YY)[c] = o.yy * crj; gp<NC>(cs, tab, q0, q, AF_ZZ)[c] = o.zz * crj;
-                    gp<NC>(cs, tab, q0, q, AF_XY)[c] = o.xy * crj; gp<NC>(cs, tab, q0, q, AF_XZ)[c] = o.xz * crj; gp<NC>(cs, tab, q0, q, AF_YZ)[c] = o.yz * crj;
-                    wm2[q] = wm1;
+                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, r[a], 1.0f);
+                } else {
+                    o = str_elastic(kc, Vq, s0, dth);
                 }
+                const float crj = cxy * czk;
+                tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj; tab[q].f[AF_ZZ][c] = o.zz * crj;
+                tab[q].f[AF_XY][c] = o.xy * crj; tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
             }
-#pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                up1[q] = up2[q];
-                vp1[q] = vp2[q];
-            }
+            up1 = up2; up2 = up3;
+            vp1 = vp2; vp2 = vp3;
+            wm2 = wm1; wp1 = wp2;
             __syncwarp();
             if (tx == 0) mb_arrive(&empty[usem % S]);
         }
@@ -534,18 +521,15 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             /* fstr (operator.f:594-606) on this thread's own column; the top
              * chunk holds at least levels nz-2..nz, all written by this thread */
             const int ct = g.idx(i, j, g.nz);
-#pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                float *ZZ = gp<NC>(cs, tab, q0, q, AF_ZZ), *XZ = gp<NC>(cs, tab, q0, q, AF_XZ), *YZ = gp<NC>(cs, tab, q0, q, AF_YZ);
-                ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
-                ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
-                XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
-                XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
-                YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
-                YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
-                XZ[ct] = 0.0f;
-                YZ[ct] = 0.0f;
-            }
+            float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
+            ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+            ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+            XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+            XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+            YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+            YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+            XZ[ct] = 0.0f;
+            YZ[ct] = 0.0f;
         }
     }
 }
@@ -571,36 +555,41 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-/* tensor map of one padded FP32 volume: (pitch, ny + 4, nz + 4), box 40 x rows x 1 */
-static bool make_map(CUtensorMap *m, const AwpGeom &g, const void *base, int rows)
+/* tensor map of one padded volume (pitch, ny + 4, nz + 4) of 4- or 2-byte
+ * elements, box w x rows x 1 */
+static bool make_map(CUtensorMap *m, const AwpGeom &g, const void *base, int w, int rows, int esize = 4)
 {
     EncodeTiledFn fn = encode_fn();
-    if (!fn || !base || ((uintptr_t)base & 15)) return false;
+    if (!fn || !base || ((uintptr_t)base & 15) || (g.px * esize) % 16 || (w * esize) % 16) return false;
     const cuuint64_t dim[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.nz + 4};
-    const cuuint64_t stride[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.plane * 4};
-    const cuuint32_t box[3] = {ST_W, (cuuint32_t)rows, 1};
+    const cuuint64_t stride[2] = {(cuuint64_t)g.px * esize, (cuuint64_t)g.plane * esize};
+    const cuuint32_t box[3] = {(cuuint32_t)w, (cuuint32_t)rows, 1};
     const cuuint32_t es[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dim, stride, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    const CUtensorMapDataType t = esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    return fn(m, t, 3, (void *)base, dim, stride, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md)
+cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, const AwpComp *comp, const AwpMediaT &md,
+                              int rtype)
 {
     *out = NULL;
     if (md.type != AWP_STORE_F32 || ncomp < 1 || ncomp > AWP_MAX_COMP) return cudaErrorInvalidValue;
-    if (g.px % 4 != 0) return cudaErrorInvalidValue;
+    if (g.px % 8 != 0) return cudaErrorInvalidValue;
     AwpStaged *s = (AwpStaged *)aligned_alloc(64, sizeof(AwpStaged));
     if (!s) return cudaErrorMemoryAllocation;
     memset(s, 0, sizeof *s);
     static const int vel_f[5] = {AF_XX, AF_YY, AF_XY, AF_XZ, AF_YZ};
     static const int med_f[4] = {AM_LAM, AM_MU, AM_QP, AM_QS};
-    bool ok = make_map(&s->vm.d1, g, md.m[AM_D1], ST_MR);
+    const int rsize = rtype == AWP_STORE_BF16 ? 2 : 4;
+    bool ok = make_map(&s->vm.d1, g, md.m[AM_D1], ST_W, ST_MR);
     for (int q = 0; q < ncomp; ++q) {
-        for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_HR);
-        for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->sm.v[q][a], g, comp[q].f[AF_U + a], ST_HR);
+        for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_W, ST_HR);
+        for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->sm.v[q][a], g, comp[q].f[AF_U + a], ST_W, ST_HR);
+        for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.s[q][a], g, comp[q].f[AF_XX + a], ST_X, ST_Y);
+        for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.r[q][a], g, comp[q].f[AF_R1 + a], ST_X, ST_Y, rsize);
     }
-    for (int a = 0; a < 4; ++a) ok = ok && make_map(&s->sm.med[a], g, md.m[med_f[a]], ST_MR);
+    for (int a = 0; a < 4; ++a) ok = ok && make_map(&s->sm.med[a], g, md.m[med_f[a]], ST_W, ST_MR);
     if (!ok) {
         free(s);
         return cudaErrorInvalidValue;
@@ -661,30 +650,17 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
     return cudaGetLastError();
 }
 
-template <class TR, int NC>
-static cudaError_t launch_str_nc(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
-{
-    const size_t smem = ring_bytes(2 + ST_STR_D, STR_SLOT(NC));
-    const int ngroup = s.ncomp / NC;
-    const AwpWork w = staged_work(s.g, s.kchunk_staged, ngroup);
-    int grid = 0;
-    cudaError_t e = staged_grid(k_str_tma<TR, NC, ST_STR_D>, smem, w.nitems, &grid);
-    if (e != cudaSuccess) return e;
-    k_str_tma<TR, NC, ST_STR_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
-        st->sm, s.g, comp_set3(s), ngroup, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
-    return cudaGetLastError();
-}
-
 template <class TR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
-    /* one component per block unless the caller asks for whole-tile blocks */
-    if (!s.staged_group || s.ncomp == 1) return launch_str_nc<TR, 1>(st, s, stream);
-    switch (s.ncomp) {
-    case 2: return launch_str_nc<TR, 2>(st, s, stream);
-    case 3: return launch_str_nc<TR, 3>(st, s, stream);
-    default: return cudaErrorInvalidValue;
-    }
+    const size_t smem = ring_bytes(2 + STR_D, STR_SLOT);
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
+    int grid = 0;
+    cudaError_t e = staged_grid(k_str_tma<TR>, smem, w.nitems, &grid);
+    if (e != cudaSuccess) return e;
+    k_str_tma<TR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.cx, s.cy, s.cz,
+                                                                s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+    return cudaGetLastError();
 }
 
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)

@@ -152,12 +152,9 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, monkeypatch):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-@pytest.mark.parametrize("group", ["0", "1"])
-def test_staged_batched_components_many_items(group, monkeypatch):
-    """Three components as neighbouring work items (or all three in one
-    stress block), 8-level chunks."""
+def test_staged_batched_components_many_items(monkeypatch):
+    """Three components as neighbouring work items, 8-level chunks."""
     monkeypatch.setenv("AWP_TUNE_KSTAGE", "8")
-    monkeypatch.setenv("AWP_TUNE_STRGROUP", group)
     c = Case(nx=70, ny=20, nz=41, nt=30, igreen=(1, 2, 3),
              srcs=[[(35, 10, 20)], [(34, 9, 20)], [(36, 11, 21)]])
     s = c.gpu(kernel="staged")
