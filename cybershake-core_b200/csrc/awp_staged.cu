@@ -587,7 +587,8 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
         for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_W, ST_HR);
         for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->sm.v[q][a], g, comp[q].f[AF_U + a], ST_W, ST_HR);
         for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.s[q][a], g, comp[q].f[AF_XX + a], ST_X, ST_Y);
-        for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.r[q][a], g, comp[q].f[AF_R1 + a], ST_X, ST_Y, rsize);
+        for (int a = 0; a < 6; ++a)     /* absent in the elastic scheme, which never loads them */
+            if (comp[q].f[AF_R1 + a]) ok = ok && make_map(&s->sm.r[q][a], g, comp[q].f[AF_R1 + a], ST_X, ST_Y, rsize);
     }
     for (int a = 0; a < 4; ++a) ok = ok && make_map(&s->sm.med[a], g, md.m[med_f[a]], ST_W, ST_MR);
     if (!ok) {
