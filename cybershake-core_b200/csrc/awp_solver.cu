@@ -437,7 +437,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
     s->staged_on = p->kernel == AWP_KERNEL_STAGED || (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
     {
-        const int kc = env_int("AWP_TUNE_KSTAGE", 32);
+        const int kc = env_int("AWP_TUNE_KSTAGE", 16);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
     }
     s->nt_file = nt_file_of(p);

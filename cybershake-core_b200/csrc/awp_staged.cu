@@ -45,12 +45,14 @@
 #define ST_VT (ST_W * ST_HR)         /* floats of a stencil tile (1920 B)       */
 #define ST_MT (ST_W * ST_MR)         /* floats a media tile receives (1440 B)   */
 #define ST_MP 384                    /* floats reserved per media tile (1536 B) */
+#define ST_PT (ST_X * ST_Y)          /* floats of a point tile (no halo)        */
 #define ST_WAIT_NS 2000000000ull     /* bound of one barrier wait               */
 #define ST_VEL_D 3                   /* levels in flight, velocity sweep        */
 
 struct AwpStagedVelMaps {
     CUtensorMap st[AWP_MAX_COMP][5]; /* xx yy xy xz yz, box 40 x 12           */
     CUtensorMap d1;                  /* box 40 x 9                             */
+    CUtensorMap p[AWP_MAX_COMP][3];  /* u v w, box 32 x 8                      */
 };
 struct AwpStagedStrMaps {
     CUtensorMap v[AWP_MAX_COMP][3];  /* u v w, box 40 x 12                     */
@@ -202,9 +204,11 @@ __device__ __forceinline__ bool ring_acquire(uint64_t *empty, uint32_t use, cons
 /* velocity sweep                                                      */
 /* ------------------------------------------------------------------ */
 
-/* slot layout: xx yy xy xz yz stencil tiles, then the d1 media tile */
-#define VEL_SLOT (5 * ST_VT + ST_MP)
-#define VEL_TXB ((5 * ST_VT + ST_MT) * 4)
+/* slot layout: xx yy xy xz yz stencil tiles, the d1 media tile, then the
+ * u v w point tiles */
+#define VEL_PT (5 * ST_VT + ST_MP)
+#define VEL_SLOT (VEL_PT + 3 * ST_PT)
+#define VEL_TXB ((5 * ST_VT + ST_MT + 3 * ST_PT) * 4)
 
 /* stresses of plane k from the slot (in-plane) and from the register queue (z) */
 struct TStr {
@@ -223,8 +227,8 @@ struct TStr {
 };
 
 template <int S>
-__device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorMap *md1, float *ring, uint64_t *full,
-                                          uint32_t use, int i0, int j0, int k)
+__device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorMap *md1, const CUtensorMap *mp,
+                                          float *ring, uint64_t *full, uint32_t use, int i0, int j0, int k)
 {
     float *sl = ring + (use % S) * VEL_SLOT;
     uint64_t *b = &full[use % S];
@@ -234,6 +238,8 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
 #pragma unroll
     for (int a = 0; a < 5; ++a) tma_3d(sl + a * ST_VT, ms + a, b, x, j0 - 1, k + 1);
     tma_3d(sl + 5 * ST_VT, md1, b, x, j0, k + 1);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) tma_3d(sl + VEL_PT + a * ST_PT, mp + a, b, i0 + AWP_XO - 1, j0 + 1, k + 1);
 }
 
 /* work items: (x tile, y tile, z chunk, component), component fastest */
@@ -262,7 +268,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             for (int k = k0; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
-                vel_issue<S>(maps.st[q], &maps.d1, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+                vel_issue<S>(maps.st[q], &maps.d1, maps.p[q], ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
         }
         if (!ok) {
@@ -274,7 +280,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
     }
 
     const int sy = g.px, sz = g.plane;
-    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4;
+    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
     uint32_t use = 0;
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
         const int q = item % ncomp;
@@ -284,21 +290,22 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
         const bool live = i <= g.nx && j <= g.ny;
         float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
         const float *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ), *ZZ = pick(cs, q, AF_ZZ);
-        float xz_m2 = 0.f, xz_m1 = 0.f, yz_m2 = 0.f, yz_m1 = 0.f, zz_m1 = 0.f, zz_0 = 0.f, zz_p1 = 0.f;
+        /* column queues, each loaded one level before it is needed */
+        float xz_m2 = 0.f, xz_m1 = 0.f, xz_p1 = 0.f, yz_m2 = 0.f, yz_m1 = 0.f, yz_p1 = 0.f;
+        float zz_m1 = 0.f, zz_0 = 0.f, zz_p1 = 0.f, zz_p2 = 0.f;
         float dA = 0.f, dB = 0.f, dE = 0.f, cxy = 0.f;
         int c = g.idx(i, j, k0);
         if (live) {
-            xz_m2 = XZ[c - 2 * sz]; xz_m1 = XZ[c - sz];
-            yz_m2 = YZ[c - 2 * sz]; yz_m1 = YZ[c - sz];
-            zz_m1 = ZZ[c - sz]; zz_0 = ZZ[c]; zz_p1 = ZZ[c + sz];
+            xz_m2 = XZ[c - 2 * sz]; xz_m1 = XZ[c - sz]; xz_p1 = XZ[c + sz];
+            yz_m2 = YZ[c - 2 * sz]; yz_m1 = YZ[c - sz]; yz_p1 = YZ[c + sz];
+            zz_m1 = ZZ[c - sz]; zz_0 = ZZ[c]; zz_p1 = ZZ[c + sz]; zz_p2 = ZZ[c + 2 * sz];
             dA = d1[c - sz]; dB = d1[c - sy - sz]; dE = d1[c + 1 - sz];
             cxy = cx[i] * cy[j];
         }
         for (int k = k0; k <= k1; ++k, c += sz, ++use) {
-            float u0 = 0.f, v0 = 0.f, w0 = 0.f, xz_p1 = 0.f, yz_p1 = 0.f, zz_p2 = 0.f, czk = 0.f;
+            float xz_n = 0.f, yz_n = 0.f, zz_n = 0.f, czk = 0.f;
             if (live) {
-                u0 = U[c]; v0 = V[c]; w0 = W[c];
-                xz_p1 = XZ[c + sz]; yz_p1 = YZ[c + sz]; zz_p2 = ZZ[c + 2 * sz];
+                if (k < k1) { xz_n = XZ[c + 2 * sz]; yz_n = YZ[c + 2 * sz]; zz_n = ZZ[c + 3 * sz]; }
                 czk = cz[k];
             }
             /* warp-uniform outcome, so a warp leaves together or not at all */
@@ -309,6 +316,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             }
             if (live) {
                 const float *sl = ring + (use % S) * VEL_SLOT;
+                const float u0 = sl[VEL_PT + cp], v0 = sl[VEL_PT + ST_PT + cp], w0 = sl[VEL_PT + 2 * ST_PT + cp];
                 const float *t1 = sl + 5 * ST_VT + cm;
                 const float da = t1[0], db = t1[-ST_W], de = t1[1], dg = t1[1 - ST_W];
                 float fu, fv, fw;
@@ -322,7 +330,8 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
                 W[c] = w_ * crj;
                 xz_m2 = xz_m1; xz_m1 = sl[3 * ST_VT + cv];
                 yz_m2 = yz_m1; yz_m1 = sl[4 * ST_VT + cv];
-                zz_m1 = zz_0; zz_0 = zz_p1; zz_p1 = zz_p2;
+                zz_m1 = zz_0; zz_0 = zz_p1; zz_p1 = zz_p2; zz_p2 = zz_n;
+                xz_p1 = xz_n; yz_p1 = yz_n;
                 dA = da; dB = db; dE = de;
             }
             __syncwarp();
@@ -341,8 +350,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
  * while level k+1 is in flight. */
 #define STR_D 1
 #define STR_ST (3 * ST_VT + 4 * ST_MP)           /* first stress tile        */
-#define STR_PT (ST_X * ST_Y)                      /* floats of a point tile   */
-#define STR_SLOT (STR_ST + 12 * STR_PT)           /* r tiles fit in 6 x 256   */
+#define STR_SLOT (STR_ST + 12 * ST_PT)           /* r tiles fit in 6 x 256   */
 
 /* media of planes k and k-1 at the cell */
 struct TMed {
@@ -375,7 +383,7 @@ struct TVel {
 /* bytes one level brings in */
 __host__ __device__ __forceinline__ uint32_t str_txb(int nve, int rsize)
 {
-    return (uint32_t)((3 * ST_VT + (nve == 1 ? 4 : 2) * ST_MT + 6 * STR_PT) * 4 + (nve == 1 ? 6 * STR_PT * rsize : 0));
+    return (uint32_t)((3 * ST_VT + (nve == 1 ? 4 : 2) * ST_MT + 6 * ST_PT) * 4 + (nve == 1 ? 6 * ST_PT * rsize : 0));
 }
 
 template <int S, int RSIZE>
@@ -394,11 +402,11 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
     /* point tiles start at cell (i0, j0): memory column i0 + 7 (a multiple of 8) */
     const int xp = i0 + AWP_XO - 1;
 #pragma unroll
-    for (int a = 0; a < 6; ++a) tma_3d(sl + STR_ST + a * STR_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
+    for (int a = 0; a < 6; ++a) tma_3d(sl + STR_ST + a * ST_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
     if (nve == 1) {
-        unsigned char *rb = (unsigned char *)(sl + STR_ST + 6 * STR_PT);
+        unsigned char *rb = (unsigned char *)(sl + STR_ST + 6 * ST_PT);
 #pragma unroll
-        for (int a = 0; a < 6; ++a) tma_3d(rb + a * STR_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
+        for (int a = 0; a < 6; ++a) tma_3d(rb + a * ST_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
     }
 }
 
@@ -489,14 +497,14 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                 const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
                 const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
                 const float *ps = sk + STR_ST + cp;
-                const Stress6 s0{ps[0], ps[STR_PT], ps[2 * STR_PT], ps[3 * STR_PT], ps[4 * STR_PT], ps[5 * STR_PT]};
+                const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
                 const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1, up2, vp1, vp2, wm2, wp1};
                 Stress6 o;
                 if (nve == 1) {
-                    const TR *pr = (const TR *)(sk + STR_ST + 6 * STR_PT) + cp;
+                    const TR *pr = (const TR *)(sk + STR_ST + 6 * ST_PT) + cp;
                     float r[6];
 #pragma unroll
-                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(pr, a * STR_PT, 1.0f);
+                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
                     const VelDiff dd = vel_diff(Vq);
                     o = str_visco(kc, dd, s0, r, dth, dt, dh1);
 #pragma unroll
@@ -585,6 +593,7 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
     bool ok = make_map(&s->vm.d1, g, md.m[AM_D1], ST_W, ST_MR);
     for (int q = 0; q < ncomp; ++q) {
         for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_W, ST_HR);
+        for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->vm.p[q][a], g, comp[q].f[AF_U + a], ST_X, ST_Y);
         for (int a = 0; a < 3; ++a) ok = ok && make_map(&s->sm.v[q][a], g, comp[q].f[AF_U + a], ST_W, ST_HR);
         for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.s[q][a], g, comp[q].f[AF_XX + a], ST_X, ST_Y);
         for (int a = 0; a < 6; ++a)     /* absent in the elastic scheme, which never loads them */
