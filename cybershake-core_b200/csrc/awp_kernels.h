@@ -29,6 +29,7 @@ struct AwpStepArgs {
     int unroll;                  /* two-sweep z-loop unroll (1 or 2)        */
     const AwpStaged *staged;     /* non-NULL: TMA-staged velocity/stress    */
     int kchunk_staged;           /* z levels per staged work item           */
+    int staged_qslow;            /* staged items: one component at a time   */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

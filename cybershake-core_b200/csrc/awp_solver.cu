@@ -77,6 +77,7 @@ struct awp_solver {
     int kchunk_sweep;                /* z levels per two-sweep work item    */
     int staged_on;                   /* TMA-staged velocity/stress sweeps   */
     int kchunk_staged;               /* z levels per staged work item       */
+    int staged_qslow;                /* staged items: component slowest     */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -439,6 +440,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     {
         const int kc = env_int("AWP_TUNE_KSTAGE", 16);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
+        s->staged_qslow = env_int("AWP_TUNE_QSLOW", 0) != 0;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -774,6 +776,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.unroll = s->unroll;
     a.staged = s->staged_on ? s->staged : NULL;
     a.kchunk_staged = s->kchunk_staged;
+    a.staged_qslow = s->staged_qslow;
     a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);

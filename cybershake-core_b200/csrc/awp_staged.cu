@@ -130,6 +130,20 @@ __device__ __forceinline__ void tma_3d(void *dst, const CUtensorMap *map, uint64
  * j0 - 1 (media), level k */
 __device__ __forceinline__ int tile_x(int i0) { return i0 + AWP_XO - 1 - 4; }
 
+/* component q and tile item t of work item `item`: the components of one
+ * tile side by side (qslow = 0; their common media tiles come from L2) or one
+ * component over all tiles at a time (qslow = 1; fewer arrays streamed at once) */
+__device__ __forceinline__ void split_item(int item, int ncomp, int ntile, int qslow, int &q, int &t)
+{
+    if (qslow) {
+        q = item / ntile;
+        t = item - q * ntile;
+    } else {
+        q = item % ncomp;
+        t = item / ncomp;
+    }
+}
+
 __device__ __forceinline__ float *pick(const AwpCompSet<AWP_MAX_COMP> &cs, int q, int f)
 {
     return q == 0 ? cs.c[0].f[f] : (q == 1 ? cs.c[1].f[f] : cs.c[2].f[f]);
@@ -245,7 +259,7 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
 /* work items: (x tile, y tile, z chunk, component), component fastest */
 template <int D>
 __global__ void __launch_bounds__(ST_THREADS, 3)
-k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
+k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
           const float *__restrict__ cz, float dth, AwpWork w, int *err)
 {
@@ -262,9 +276,10 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
         uint32_t use = 0;
         bool ok = true;
         for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
-            const int q = item % ncomp;
+            int q, t;
+            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
             int bx, by, k0, k1;
-            work_item(g, w, item / ncomp, bx, by, k0, k1);
+            work_item(g, w, t, bx, by, k0, k1);
             for (int k = k0; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
@@ -283,9 +298,10 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
     const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
     uint32_t use = 0;
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
-        const int q = item % ncomp;
+        int q, t;
+            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
         int bx, by, k0, k1;
-        work_item(g, w, item / ncomp, bx, by, k0, k1);
+        work_item(g, w, t, bx, by, k0, k1);
         const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
         float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
@@ -414,7 +430,7 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
  * the components of a tile run side by side and share its media through L2 */
 template <class TR>
 __global__ void __launch_bounds__(ST_THREADS, 3)
-k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp,
+k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
@@ -437,9 +453,10 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
         uint32_t use = 0;
         bool ok = true;
         for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
-            const int q = item % ncomp;
+            int q, t;
+            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
             int bx, by, k0, k1;
-            work_item(g, w, item / ncomp, bx, by, k0, k1);
+            work_item(g, w, t, bx, by, k0, k1);
             for (int k = k0 - 1; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
@@ -458,9 +475,10 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
     uint32_t use0 = 0;                /* ring use of the item's first level */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
-        const int q = item % ncomp;
+        int q, t;
+            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
         int bx, by, k0, k1;
-        work_item(g, w, item / ncomp, bx, by, k0, k1);
+        work_item(g, w, t, bx, by, k0, k1);
         const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
         const bool live = i <= g.nx && j <= g.ny;
         const int np = k1 - k0 + 2;   /* levels k0-1 .. k1 */
@@ -654,7 +672,7 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
     int grid = 0;
     cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
-    k_vel_tma<ST_VEL_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp,
+    k_vel_tma<ST_VEL_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow,
                                                                       (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz,
                                                                       s.dth, w, s.kerr);
     return cudaGetLastError();
@@ -668,7 +686,7 @@ static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cuda
     int grid = 0;
     cudaError_t e = staged_grid(k_str_tma<TR>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
-    k_str_tma<TR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.cx, s.cy, s.cz,
+    k_str_tma<TR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, s.cx, s.cy, s.cz,
                                                                 s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
 }

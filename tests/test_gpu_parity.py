@@ -152,9 +152,12 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, monkeypatch):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-def test_staged_batched_components_many_items(monkeypatch):
-    """Three components as neighbouring work items, 8-level chunks."""
+@pytest.mark.parametrize("qslow", ["0", "1"])
+def test_staged_batched_components_many_items(qslow, monkeypatch):
+    """Three components as neighbouring work items (or one component over
+    all tiles at a time), 8-level chunks."""
     monkeypatch.setenv("AWP_TUNE_KSTAGE", "8")
+    monkeypatch.setenv("AWP_TUNE_QSLOW", qslow)
     c = Case(nx=70, ny=20, nz=41, nt=30, igreen=(1, 2, 3),
              srcs=[[(35, 10, 20)], [(34, 9, 20)], [(36, 11, 21)]])
     s = c.gpu(kernel="staged")
