@@ -433,10 +433,12 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->vtst1 = 1.0f / (p->dh * p->dh);
     s->ty = env_int("AWP_TUNE_TY", 8);
     if (s->ty != 4 && s->ty != 16) s->ty = 8;
-    s->unroll = env_int("AWP_TUNE_UNROLL", 1) == 2 ? 2 : 1;
+    s->staged_on = p->kernel == AWP_KERNEL_STAGED || (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
+    /* z-loop unroll: 1 or 2 (default 1 for the two-sweep kernels, 2 for the staged ones) */
+    s->unroll = env_int("AWP_TUNE_UNROLL", 0);
+    if (s->unroll != 1 && s->unroll != 2) s->unroll = s->staged_on ? 2 : 1;
     s->kchunk = choose_kchunk(s->g, 1, s->ty);
     s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
-    s->staged_on = p->kernel == AWP_KERNEL_STAGED || (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
     {
         const int kc = env_int("AWP_TUNE_KSTAGE", 16);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);

@@ -257,7 +257,7 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
 }
 
 /* work items: (x tile, y tile, z chunk, component), component fastest */
-template <int D>
+template <int D, int UNR>
 __global__ void __launch_bounds__(ST_THREADS, 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
@@ -318,6 +318,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             dA = d1[c - sz]; dB = d1[c - sy - sz]; dE = d1[c + 1 - sz];
             cxy = cx[i] * cy[j];
         }
+#pragma unroll (UNR)
         for (int k = k0; k <= k1; ++k, c += sz, ++use) {
             float xz_n = 0.f, yz_n = 0.f, zz_n = 0.f, czk = 0.f;
             if (live) {
@@ -428,7 +429,7 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
 
 /* work items: (x tile, y tile, z chunk, component), component fastest, so
  * the components of a tile run side by side and share its media through L2 */
-template <class TR>
+template <class TR, int UNR>
 __global__ void __launch_bounds__(ST_THREADS, 3)
 k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
@@ -493,6 +494,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             wm2 = W[c - 2 * sz]; wp1 = W[c + sz];
             cxy = cx[i] * cy[j];
         }
+#pragma unroll (UNR)
         for (int k = k0; k <= k1; ++k, c += sz) {
             const uint32_t use = use0 + (uint32_t)(k - k0 + 1), usem = use - 1;
             float up3 = 0.f, vp3 = 0.f, wp2 = 0.f, czk = 0.f;
@@ -664,36 +666,47 @@ static AwpCompSet<AWP_MAX_COMP> comp_set3(const AwpStepArgs &s)
 /* dynamic shared memory of a ring: alignment slack, slots, full + empty barriers */
 static size_t ring_bytes(int slots, int slot_floats) { return 128 + (size_t)slots * slot_floats * 4 + 2 * 8 * slots; }
 
-cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+template <int UNR>
+static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
-    if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
     const size_t smem = ring_bytes(1 + ST_VEL_D, VEL_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, UNR>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
-    k_vel_tma<ST_VEL_D><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow,
-                                                                      (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz,
-                                                                      s.dth, w, s.kerr);
+    k_vel_tma<ST_VEL_D, UNR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
+        st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w,
+        s.kerr);
     return cudaGetLastError();
 }
 
-template <class TR>
+template <class TR, int UNR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     const size_t smem = ring_bytes(2 + STR_D, STR_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_str_tma<TR>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_str_tma<TR, UNR>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
-    k_str_tma<TR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, s.cx, s.cy, s.cz,
-                                                                s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+    k_str_tma<TR, UNR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
+                                                                     s.staged_qslow, s.cx, s.cy, s.cz, s.tau, s.dth,
+                                                                     s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
+}
+
+/* level loops unrolled twice unless asked otherwise: the column queues then
+ * rotate by register renaming instead of moves that wait for loads in flight */
+cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
+    return s.unroll == 1 ? launch_vel_u<1>(st, s, stream) : launch_vel_u<2>(st, s, stream);
 }
 
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
-    if (s.rtype == AWP_STORE_BF16) return launch_str_tr<__nv_bfloat16>(st, s, stream);
-    return launch_str_tr<float>(st, s, stream);
+    if (s.rtype == AWP_STORE_BF16)
+        return s.unroll == 1 ? launch_str_tr<__nv_bfloat16, 1>(st, s, stream)
+                             : launch_str_tr<__nv_bfloat16, 2>(st, s, stream);
+    return s.unroll == 1 ? launch_str_tr<float, 1>(st, s, stream) : launch_str_tr<float, 2>(st, s, stream);
 }

@@ -140,14 +140,17 @@ def test_odd_sizes_and_boundary_points(kernel):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-@pytest.mark.parametrize("kernel,kstage", [("fused", None), ("staged", None), ("staged", "8")])
-def test_multi_tile_multi_chunk_grid(kernel, kstage, monkeypatch):
+@pytest.mark.parametrize("kernel,kstage,unroll", [("fused", None, None), ("staged", None, None), ("staged", "8", "1"),
+                                                  ("staged", "9", "2")])
+def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, monkeypatch):
     """Several x/y tiles (partial ones at the high edges) and z chunks: halo
     recompute at the fused stepper's tile seams and redundant levels at its
     chunk seams; the staged stepper's tile halos, chunk prologues and ring
     reuse across many work items per block."""
     if kstage:
         monkeypatch.setenv("AWP_TUNE_KSTAGE", kstage)
+    if unroll:
+        monkeypatch.setenv("AWP_TUNE_UNROLL", unroll)
     c = Case(nx=100, ny=30, nz=80, nt=25, nd=6, srcs=[[(50, 15, 40)]], ntiskp=5, write_step=5)
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
