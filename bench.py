@@ -241,6 +241,130 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# serving stream (--serve): continuous batching against serial solves
+# ---------------------------------------------------------------------------
+
+def serve_requests(n, seed, nst_scale):
+    """n request specs: sizes log-uniform 100x100x50 .. 500x500x250, DH 100-200,
+    NST 1000-4000 (times nst_scale), a random non-empty component set, media
+    seeded per request; Poisson arrivals are drawn later from the measured
+    serial service rate."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for r in range(n):
+        f = float(np.exp(rng.uniform(0.0, np.log(5.0))))
+        nx = ny = int(round(100 * f))
+        nz = int(round(50 * f))
+        dh = float(rng.choice([100.0, 150.0, 200.0]))
+        nst = max(20, int(round(int(rng.integers(1000, 4001)) * nst_scale)))
+        comps = [c for c in (1, 2, 3) if rng.random() < 0.5] or [int(rng.integers(1, 4))]
+        specs.append({"id": r, "nx": nx, "ny": ny, "nz": nz, "dh": dh, "nst": nst, "igreen": tuple(comps),
+                      "seed": 1000 + r})
+    return specs
+
+
+def build_request(sp):
+    """Host inputs of one request (media, sources, points) and its params."""
+    import awpsgt
+    nx, ny, nz, dh, nst = sp["nx"], sp["ny"], sp["nz"], sp["dh"], sp["nst"]
+    media = ai.layered_media(nx, ny, nz, dh, seed=sp["seed"], pert_std=0.05, corr_len=20 * dh)
+    dt = ai.stable_dt(media, dh, 0.35)
+    nt = nst + 1
+    p = awpsgt.make_params(nx, ny, nz, dh, dt, nt, nst=nst, igreen=sp["igreen"], nd=20, arbc=0.92, socalq=1,
+                           ntiskp_sgt=10, write_step=max(1, nt // 10))
+    src = (nx // 2, ny // 2, max(1, min(nz, int(round(2000.0 / dh)) + 1)))
+    sources = [([src], ai.gaussian_derivative_stf(nst, dt, f0=0.5, column=c - 1)) for c in sp["igreen"]]
+    pts = ai.sgt_points(nx, ny, min(nz, int(10000.0 / dh) + 1), 1000, seed=sp["seed"])
+    return p, media, sources, pts
+
+
+def pct(x, q):
+    return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
+
+
+def run_serve(args):
+    """Serial solves (one at a time) give the service times; the same requests
+    then arrive as a Poisson stream at `--serve-load` times the serial service
+    rate and go through the continuous-batching server.  Latency = completion
+    minus arrival.  The serial latencies are those of a FIFO single server fed
+    the same arrival times with the measured service times."""
+    import queue
+    import awpsgt
+    specs = serve_requests(args.serve_requests, 1, args.serve_nst_scale)
+    work = [sp["nx"] * sp["ny"] * sp["nz"] * len(sp["igreen"]) * (sp["nst"] + 1) for sp in specs]
+
+    def producer(out_q):
+        for sp in specs:
+            out_q.put(build_request(sp))
+
+    # serial solves
+    q1 = queue.Queue(maxsize=2)
+    th = threading.Thread(target=producer, args=(q1,), daemon=True)
+    th.start()
+    service = []
+    for sp in specs:
+        p, media, sources, pts = q1.get()
+        t0 = time.perf_counter()
+        with awpsgt.Solver(p) as s:
+            s.load_media(media)
+            for qq, (xyz, stf) in enumerate(sources):
+                s.set_source(qq, xyz, stf)
+            s.set_points(pts)
+            s.run(p.nt, with_sgt=True)
+        service.append(time.perf_counter() - t0)
+    th.join()
+    total_serial = float(sum(service))
+    rate = args.serve_load * len(specs) / total_serial
+    arr = np.cumsum(np.random.default_rng(1).exponential(1.0 / rate, size=len(specs)))
+    arr -= arr[0]
+    free_at, serial_lat = 0.0, []
+    for a, sv in zip(arr, service):
+        start = max(a, free_at)
+        free_at = start + sv
+        serial_lat.append(free_at - a)
+
+    # served stream
+    q2 = queue.Queue(maxsize=3)
+    th = threading.Thread(target=producer, args=(q2,), daemon=True)
+    th.start()
+    lat, ids, late = [], [], []
+    with awpsgt.Server(device=0, max_active=args.serve_active, chunk_steps=100) as sv:
+        t_start = sv.time()
+        for k, sp in enumerate(specs):
+            req = q2.get()
+            while sv.time() - t_start < arr[k]:
+                time.sleep(0.0005)
+            ids.append(sv.submit(*req))
+            late.append(sv.time() - t_start - arr[k])
+        t_sub = {}
+        for rid in ids:
+            info, _ = sv.wait(rid, timeout=7200)
+            if awpsgt.REQ_STATE[info["state"]] != "done":
+                raise RuntimeError("request %d: %s" % (rid, info))
+            t_sub[rid] = info
+        t_end = max(i["t_done"] for i in t_sub.values())
+    th.join()
+    for k, rid in enumerate(ids):
+        lat.append(t_sub[rid]["t_done"] - (t_start + arr[k]))
+    span = t_end - t_start
+    line = {
+        "metric": "served-solve latency p50/p99", "value": pct(lat, 50), "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
+        "throughput": {"value": sum(work) / span * 1e-9, "unit": METRIC, "span_s": span},
+        "serial": {"p50_s": pct(serial_lat, 50), "p99_s": pct(serial_lat, 99),
+                   "throughput": {"value": sum(work) / total_serial * 1e-9, "unit": METRIC,
+                                  "busy_s": total_serial}},
+        "offered_load": args.serve_load, "arrival_rate_per_s": rate, "requests": len(specs),
+        "max_submit_lateness_s": float(max(late)),
+        "max_active": args.serve_active, "dtype": "f32", "data": "synthetic (seeded layered media, seeded arrivals)",
+        "config": {"workload": "serving stream: %d requests, sizes 100x100x50..500x500x250, NST 1000-4000 x %g"
+                               % (len(specs), args.serve_nst_scale), "cell_updates": int(sum(work))},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,7 +378,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", default="", help="nx,ny,nz: reduced grid for profiling captures")
     ap.add_argument("--components", type=int, default=0, help="first n of the fx, fy, fz components")
+    ap.add_argument("--serve", action="store_true", help="serving stream: p50/p99 latency against serial solves")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-load", type=float, default=1.2, help="offered load / serial service rate")
+    ap.add_argument("--serve-active", type=int, default=4, help="requests on the GPU at once")
+    ap.add_argument("--serve-nst-scale", type=float, default=1.0, help="scales every request's NST")
     args = ap.parse_args()
+    if args.serve:
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
 
