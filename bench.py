@@ -329,7 +329,8 @@ def run_serve(args):
     th = threading.Thread(target=producer, args=(q2,), daemon=True)
     th.start()
     lat, ids, late = [], [], []
-    with awpsgt.Server(device=0, max_active=args.serve_active, chunk_steps=100) as sv:
+    with awpsgt.Server(device=0, max_active=args.serve_active, chunk_steps=10) as sv:
+        sv.configure(args.serve_policy, args.serve_fill, 0.0)
         t_start = sv.time()
         for k, sp in enumerate(specs):
             req = q2.get()
@@ -357,7 +358,7 @@ def run_serve(args):
                                   "busy_s": total_serial}},
         "offered_load": args.serve_load, "arrival_rate_per_s": rate, "requests": len(specs),
         "max_submit_lateness_s": float(max(late)),
-        "max_active": args.serve_active, "dtype": "f32", "data": "synthetic (seeded layered media, seeded arrivals)",
+        "max_active": args.serve_active, "policy": args.serve_policy, "dtype": "f32", "data": "synthetic (seeded layered media, seeded arrivals)",
         "config": {"workload": "serving stream: %d requests, sizes 100x100x50..500x500x250, NST 1000-4000 x %g"
                                % (len(specs), args.serve_nst_scale), "cell_updates": int(sum(work))},
     }
@@ -383,6 +384,8 @@ def main():
     ap.add_argument("--serve-load", type=float, default=1.2, help="offered load / serial service rate")
     ap.add_argument("--serve-active", type=int, default=4, help="requests on the GPU at once")
     ap.add_argument("--serve-nst-scale", type=float, default=1.0, help="scales every request's NST")
+    ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="admission order")
+    ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
     args = ap.parse_args()
     if args.serve:
         return run_serve(args)

@@ -39,7 +39,7 @@ EXPORTED = [
     "awp_params_from_in3d", "awp_read_source", "awp_read_cordfile", "awp_free", "awp_profile_steps",
     "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
-    "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc",
+    "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
 ]
 
 
@@ -160,6 +160,7 @@ def load_library(path: str = LIB_PATH):
         "awp_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_void_p]),
         "awp_server_time": (C.c_double, [C.c_void_p]),
         "awp_server_destroy": (C.c_int, [C.c_void_p]),
+        "awp_server_configure": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
     }
     for name, (res, args) in sig.items():
@@ -377,6 +378,11 @@ class Server:
         _check(self.lib.awp_submit(self.h, C.byref(rq), C.byref(rid)))
         self._keep[rid.value] = (keep, out)
         return rid.value
+
+    def configure(self, policy: str = "fifo", fill_cells: float = 0.0, chunk_cells: float = 0.0):
+        """Admission order ("fifo" or "sjf"), GPU-fill threshold and chunk size
+        in cell-updates (<= 0 keeps the current value)."""
+        _check(self.lib.awp_server_configure(self.h, {"fifo": 0, "sjf": 1}[policy], fill_cells, chunk_cells))
 
     def poll(self, rid: int) -> dict:
         info = RequestInfo()

@@ -1,17 +1,24 @@
 /*
  * awp_serve.cpp -- continuous batching of SGT solves on one GPU.
  *
- * One scheduler thread owns every resident solver.  It admits queued
- * requests in arrival order while their footprint fits in the HBM budget,
- * keeps one chunk of steps in flight per resident solver (each on its own
- * CUDA stream, so kernels of different requests overlap), finishes requests
- * whose last chunk completed (SGT images copied to the caller's buffer,
- * device memory released) and honours cancellations.  Host threads talk to
- * it through a mutex-protected table of requests.
+ * Three host threads share a mutex-protected table of requests:
+ *  - the admitter takes queued requests (arrival order, or shortest total
+ *    work first) while their footprint fits in the HBM budget, fewer than
+ *    max_active solves are resident and the resident solves do not already
+ *    fill the GPU, and builds each one (device allocation, media, sources,
+ *    points) while the others keep stepping;
+ *  - the scheduler keeps one chunk of steps in flight per resident solve,
+ *    each on its own CUDA stream, so kernels of different requests overlap;
+ *    a chunk is sized to about chunk_cells cell-updates, so small solves are
+ *    not stepped in slivers;
+ *  - the reaper copies a finished request's SGT file images to the caller's
+ *    buffer and releases its device memory (a device-wide synchronisation,
+ *    kept off the scheduler's path).
  */
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -31,8 +38,10 @@ struct Req {
     awp_request rq;
     awp_request_info info;
     awp_solver *s = nullptr;
-    bool cancel = false;
+    std::atomic<bool> cancel{false};
     bool in_flight = false;
+    double cells = 0;      /* cells x components: work of one step */
+    double work = 0;       /* cells x components x steps           */
 };
 
 awp_status fail(awp_status st, const char *msg)
@@ -48,42 +57,63 @@ struct awp_server {
     int64_t budget;
     int64_t reserved = 0;
     int max_active;
-    int chunk;
+    int chunk;                       /* fewest steps per chunk         */
+    int policy = AWP_SERVE_FIFO;
+    double fill_cells = 32.0e6;      /* resident cells x comps that fill the GPU */
+    double chunk_cells = 4.0e8;      /* cell-updates per chunk (target) */
     std::mutex mu;
-    std::condition_variable cv;      /* scheduler wake-up   */
-    std::condition_variable done_cv; /* request ended       */
+    std::condition_variable cv;      /* scheduler, admitter and reaper wake-up */
+    std::condition_variable done_cv; /* a request ended                       */
     std::deque<int64_t> queue;
     std::map<int64_t, Req *> reqs;
-    std::vector<Req *> active;
+    std::vector<Req *> active;       /* resident and stepping            */
+    std::deque<Req *> reap;          /* finished stepping, to be released */
+    int admitting = 0;
     int64_t next_id = 1;
     bool stop = false;
-    std::thread th;
+    bool reap_stop = false;          /* set once nothing can reach the reaper */
+    std::thread th_sched, th_admit, th_reap;
     std::chrono::steady_clock::time_point t0;
 
     double now() const
     {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
-    void loop();
-    void finish(Req *r, int state, awp_status st);
-    awp_status admit(Req *r);
+    void sched_loop();
+    void admit_loop();
+    void reap_loop();
+    void end(Req *r, int state, awp_status st);
+    awp_status build(Req *r);
+    double resident_cells() const
+    {
+        double c = 0;
+        for (const Req *r : active) c += r->cells;
+        return c;
+    }
+    /* memory first (released solves still held by the reaper count), then
+     * the number of resident solves and how much of the GPU they fill */
+    bool can_admit(const Req *r) const
+    {
+        if (reserved > 0 && reserved + r->info.footprint > budget) return false;
+        const int resident = (int)active.size() + admitting;
+        if (resident == 0) return true;
+        if (resident >= max_active) return false;
+        return resident_cells() + r->cells <= fill_cells;
+    }
 };
 
-void awp_server::finish(Req *r, int state, awp_status st)
+/* called with mu held; the solver is already destroyed */
+void awp_server::end(Req *r, int state, awp_status st)
 {
-    /* called with mu held */
-    if (r->s) {
-        awp_destroy(r->s);
-        r->s = nullptr;
-    }
     reserved -= r->info.footprint;
     r->info.state = state;
     r->info.status = st;
     r->info.t_done = now();
     done_cv.notify_all();
+    cv.notify_all();
 }
 
-awp_status awp_server::admit(Req *r)
+awp_status awp_server::build(Req *r)
 {
     awp_solver *s = nullptr;
     awp_status st = awp_create(&r->rq.params, &s);
@@ -99,88 +129,132 @@ awp_status awp_server::admit(Req *r)
     return AWP_OK;
 }
 
-void awp_server::loop()
+/* steps of the next chunk: about chunk_cells cell-updates, at least `chunk`,
+ * a whole number of SGT periods so that the solve keeps replaying graphs */
+static int chunk_steps_for(const awp_server *sv, const Req *r)
+{
+    const double want = sv->chunk_cells / (r->cells > 1 ? r->cells : 1);
+    int steps = want > 1e9 ? 1000000000 : (int)want;
+    if (steps < sv->chunk) steps = sv->chunk;
+    const int gs = r->rq.params.ntiskp_sgt > 0 ? r->rq.params.ntiskp_sgt : 1;
+    return ((steps + gs - 1) / gs) * gs;
+}
+
+void awp_server::admit_loop()
 {
     cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
     while (!stop) {
-        bool busy = false;
-        /* admissions, in arrival order */
-        while (!queue.empty() && (int)active.size() < max_active) {
-            Req *r = reqs[queue.front()];
+        for (auto it = queue.begin(); it != queue.end();) {
+            Req *r = reqs[*it];
             if (r->cancel) {
-                queue.pop_front();
                 r->info.footprint = 0;
-                finish(r, AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
-                continue;
+                end(r, AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
+                it = queue.erase(it);
+            } else {
+                ++it;
             }
-            if (reserved + r->info.footprint > budget && !active.empty()) break;
-            queue.pop_front();
-            reserved += r->info.footprint;
-            r->info.state = AWP_REQ_RUNNING;
-            r->info.t_admit = now();
-            lk.unlock();
-            awp_status st = admit(r);
+        }
+        auto pit = queue.begin();
+        if (policy == AWP_SERVE_SJF)
+            for (auto it = queue.begin(); it != queue.end(); ++it)
+                if (reqs[*it]->work < reqs[*pit]->work) pit = it;
+        Req *r = pit == queue.end() ? nullptr : reqs[*pit];
+        if (!r || !can_admit(r)) {
+            cv.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        queue.erase(pit);
+        reserved += r->info.footprint;
+        r->info.state = AWP_REQ_RUNNING;
+        r->info.t_admit = now();
+        admitting++;
+        lk.unlock();
+        const awp_status st = build(r);
+        lk.lock();
+        admitting--;
+        if (st != AWP_OK) end(r, AWP_REQ_FAILED, st);
+        else active.push_back(r);
+        cv.notify_all();
+    }
+}
+
+void awp_server::sched_loop()
+{
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    std::vector<Req *> snap, done;
+    while (!stop) {
+        snap = active;
+        lk.unlock();
+        bool busy = false;
+        done.clear();
+        for (Req *r : snap) {
+            const int q = r->in_flight ? awp_query(r->s) : 1;
+            if (q == 0 && !r->cancel) continue;
+            awp_status st = AWP_OK;
+            int64_t steps = r->info.steps_done;
+            if (r->in_flight) {
+                st = awp_sync(r->s);
+                r->in_flight = false;
+                awp_stats stt;
+                if (awp_get_stats(r->s, &stt) == AWP_OK) steps = stt.steps_done;
+            }
+            if (q < 0 && st == AWP_OK) st = AWP_ERR_CUDA;
+            if (st == AWP_OK && !r->cancel && steps < r->rq.params.nt) {
+                st = awp_run_async(r->s, chunk_steps_for(this, r));
+                r->in_flight = st == AWP_OK;
+            }
             lk.lock();
-            if (st != AWP_OK) finish(r, AWP_REQ_FAILED, st);
-            else active.push_back(r);
+            r->info.steps_done = steps;
+            if (!r->in_flight) {                 /* finished, failed or cancelled */
+                r->info.status = st;
+                done.push_back(r);
+            }
+            lk.unlock();
             busy = true;
         }
-        /* progress of the resident solves */
-        for (size_t n = 0; n < active.size();) {
-            Req *r = active[n];
-            const int q = r->in_flight ? awp_query(r->s) : 1;
-            if (q < 0 || r->cancel) {
-                if (r->in_flight) awp_sync(r->s);
-                finish(r, r->cancel ? AWP_REQ_CANCELLED : AWP_REQ_FAILED, r->cancel ? AWP_ERR_CANCELLED : AWP_ERR_CUDA);
-                active.erase(active.begin() + n);
-                busy = true;
-                continue;
-            }
-            if (q == 1) {
-                awp_status st = AWP_OK;
-                if (r->in_flight) {
-                    st = awp_sync(r->s);
-                    r->in_flight = false;
-                    awp_stats stt;
-                    awp_get_stats(r->s, &stt);
-                    r->info.steps_done = stt.steps_done;
-                }
-                if (st == AWP_OK && r->info.steps_done < r->rq.params.nt) {
-                    st = awp_run_async(r->s, chunk);
-                    r->in_flight = (st == AWP_OK);
-                } else if (st == AWP_OK) {
-                    const int64_t nf = awp_sgt_file_floats(r->s);
-                    for (int c = 0; c < r->rq.params.ncomp && st == AWP_OK; c++)
-                        if (r->rq.sgt_out) st = awp_get_sgt(r->s, c, r->rq.sgt_out + (size_t)c * (size_t)nf);
-                    finish(r, st == AWP_OK ? AWP_REQ_DONE : AWP_REQ_FAILED, st);
+        lk.lock();
+        for (Req *r : done) {
+            for (size_t n = 0; n < active.size(); n++)
+                if (active[n] == r) {
                     active.erase(active.begin() + n);
-                    busy = true;
-                    continue;
+                    break;
                 }
-                if (st != AWP_OK) {
-                    finish(r, AWP_REQ_FAILED, st);
-                    active.erase(active.begin() + n);
-                    busy = true;
-                    continue;
-                }
-                busy = true;
-            }
-            n++;
+            reap.push_back(r);
         }
-        if (!busy) cv.wait_for(lk, std::chrono::microseconds(200));
+        if (!done.empty()) cv.notify_all();
+        if (!busy) cv.wait_for(lk, std::chrono::microseconds(100));
     }
-    /* shutdown: cancel what is left */
-    for (Req *r : active) {
-        if (r->in_flight) awp_sync(r->s);
-        finish(r, AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
+}
+
+void awp_server::reap_loop()
+{
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        if (reap.empty()) {
+            if (reap_stop) break;
+            cv.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        Req *r = reap.front();
+        reap.pop_front();
+        const bool complete = r->info.status == AWP_OK && r->info.steps_done >= r->rq.params.nt;
+        awp_status st = r->info.status;
+        lk.unlock();
+        if (complete && r->rq.sgt_out) {
+            const int64_t nf = awp_sgt_file_floats(r->s);
+            for (int c = 0; c < r->rq.params.ncomp && st == AWP_OK; c++)
+                st = awp_get_sgt(r->s, c, r->rq.sgt_out + (size_t)c * (size_t)nf);
+        }
+        awp_destroy(r->s);
+        lk.lock();
+        r->s = nullptr;
+        if (complete) end(r, st == AWP_OK ? AWP_REQ_DONE : AWP_REQ_FAILED, st);
+        else if (r->cancel) end(r, AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
+        else end(r, AWP_REQ_FAILED, st == AWP_OK ? AWP_ERR_CUDA : st);
     }
-    active.clear();
-    for (int64_t id : queue) {
-        reqs[id]->info.footprint = 0;
-        finish(reqs[id], AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
-    }
-    queue.clear();
 }
 
 extern "C" awp_status awp_server_create(int device, int64_t hbm_budget, int max_active, int chunk_steps,
@@ -197,8 +271,22 @@ extern "C" awp_status awp_server_create(int device, int64_t hbm_budget, int max_
     sv->max_active = max_active;
     sv->chunk = chunk_steps;
     sv->t0 = std::chrono::steady_clock::now();
-    sv->th = std::thread([sv] { sv->loop(); });
+    sv->th_reap = std::thread([sv] { sv->reap_loop(); });
+    sv->th_sched = std::thread([sv] { sv->sched_loop(); });
+    sv->th_admit = std::thread([sv] { sv->admit_loop(); });
     *out = sv;
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_server_configure(awp_server *sv, int policy, double fill_cells, double chunk_cells)
+{
+    if (!sv) return fail(AWP_ERR_PARAM, "null server");
+    if (policy != AWP_SERVE_FIFO && policy != AWP_SERVE_SJF) return fail(AWP_ERR_PARAM, "unknown admission policy");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->policy = policy;
+    if (fill_cells > 0) sv->fill_cells = fill_cells;
+    if (chunk_cells > 0) sv->chunk_cells = chunk_cells;
+    sv->cv.notify_all();
     return AWP_OK;
 }
 
@@ -211,6 +299,9 @@ extern "C" awp_status awp_submit(awp_server *sv, const awp_request *rq, int64_t 
     memset(&r->info, 0, sizeof r->info);
     r->info.state = AWP_REQ_QUEUED;
     r->info.footprint = fp;
+    const awp_params &p = rq->params;
+    r->cells = (double)p.nx * p.ny * p.nz * (p.ncomp > 0 ? p.ncomp : 1);
+    r->work = r->cells * p.nt;
     std::lock_guard<std::mutex> lk(sv->mu);
     if (fp > sv->budget) {
         delete r;
@@ -272,7 +363,26 @@ extern "C" awp_status awp_server_destroy(awp_server *sv)
         sv->stop = true;
         sv->cv.notify_all();
     }
-    sv->th.join();
+    sv->th_admit.join();            /* a request being built ends up resident */
+    sv->th_sched.join();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (Req *r : sv->active) {  /* resident solves: cancelled, released by the reaper */
+            r->cancel = true;
+            r->info.status = AWP_ERR_CANCELLED;
+            sv->reap.push_back(r);
+        }
+        sv->active.clear();
+        for (int64_t id : sv->queue) {
+            Req *r = sv->reqs[id];
+            r->info.footprint = 0;
+            sv->end(r, AWP_REQ_CANCELLED, AWP_ERR_CANCELLED);
+        }
+        sv->queue.clear();
+        sv->reap_stop = true;
+        sv->cv.notify_all();
+    }
+    sv->th_reap.join();
     for (auto &kv : sv->reqs) delete kv.second;
     delete sv;
     return AWP_OK;

@@ -262,14 +262,17 @@ const char *awp_last_error(void);
 /* Serving: continuous batching of SGT solves on one GPU.                    */
 /* No reference counterpart (the reference runs one solve per job).          */
 /*                                                                           */
-/* Requests are admitted in arrival order while their device footprint       */
-/* (awp_footprint_bytes) fits in the server's HBM budget and fewer than       */
-/* max_active solves are resident; every resident solve keeps its fields on  */
-/* the device and advances chunk_steps steps at a time on its own CUDA       */
-/* stream, so the kernels of different requests overlap on the GPU.  A       */
-/* finished request's SGT file images are copied into the caller's buffer    */
-/* and its memory is released for the next admission.  Each request's       */
-/* result is identical to running it alone (separate buffers, fixed order).  */
+/* A request is admitted (arrival order, or shortest total work first) when  */
+/* its device footprint (awp_footprint_bytes) fits in the server's HBM       */
+/* budget, fewer than max_active solves are resident and the resident solves */
+/* do not already fill the GPU; it is built (allocation, media, sources,     */
+/* points) while the resident solves keep stepping.  Every resident solve    */
+/* keeps its fields on the device and advances a chunk of steps at a time on */
+/* its own CUDA stream, so the kernels of different requests overlap on the  */
+/* GPU.  A finished request's SGT file images are copied into the caller's   */
+/* buffer and its memory is released for the next admission.  Each          */
+/* request's result is identical to running it alone (separate buffers,      */
+/* fixed order).                                                             */
 /* ------------------------------------------------------------------------- */
 
 typedef struct awp_server awp_server;
@@ -296,8 +299,18 @@ typedef struct {
     int64_t footprint;         /* device bytes reserved for the request      */
 } awp_request_info;
 
-/* hbm_budget <= 0: 90 % of the device's free memory at creation. */
+/* hbm_budget <= 0: 90 % of the device's free memory at creation.
+ * chunk_steps: fewest steps a resident solve advances per chunk. */
 awp_status awp_server_create(int device, int64_t hbm_budget, int max_active, int chunk_steps, awp_server **out);
+
+enum { AWP_SERVE_FIFO = 0, AWP_SERVE_SJF = 1 };
+/* Admission order (AWP_SERVE_FIFO: arrival; AWP_SERVE_SJF: least total work,
+ * cells x components x steps, first); fill_cells: resident cells x components
+ * at which the GPU counts as full, so that a request is admitted next to
+ * others only while their sum stays below it (default 32e6); chunk_cells:
+ * cell-updates per chunk (default 4e8; at least chunk_steps steps).  Values
+ * <= 0 keep the current setting. */
+awp_status awp_server_configure(awp_server *sv, int policy, double fill_cells, double chunk_cells);
 /* Copies the request description (host arrays must stay valid until the
  * request ends); returns its id. */
 awp_status awp_submit(awp_server *sv, const awp_request *rq, int64_t *id);

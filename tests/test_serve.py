@@ -38,10 +38,12 @@ REQS = [(1, (64, 48, 40), (1,), 120), (2, (96, 80, 48), (1, 2), 90), (3, (40, 40
         (4, (128, 96, 64), (2,), 60), (5, (50, 60, 36), (3, 1), 100), (6, (72, 72, 40), (1,), 80)]
 
 
-def test_mix_equals_alone():
+@pytest.mark.parametrize("policy,fill", [("fifo", 0.0), ("sjf", 1.0e6)])
+def test_mix_equals_alone(policy, fill):
     reqs = [make_request(*r) for r in REQS]
     alone = [run_alone(*r) for r in reqs]
     with awpsgt.Server(max_active=4, chunk_steps=20) as sv:
+        sv.configure(policy, fill, 2.0e6)
         ids = []
         for r in reqs:
             ids.append(sv.submit(*r))
@@ -85,3 +87,23 @@ def test_cancel_queued_and_running():
         ib, _ = sv.wait(b, timeout=120)
     assert awpsgt.REQ_STATE[ia["state"]] == "cancelled"
     assert awpsgt.REQ_STATE[ib["state"]] == "cancelled"
+
+
+def test_sjf_admits_least_work_first():
+    blocker = make_request(9, (160, 160, 80), (1,), 1500)
+    big = make_request(10, (96, 96, 64), (1, 2), 400)
+    small = make_request(11, (40, 40, 32), (1,), 40)
+    with awpsgt.Server(max_active=1, chunk_steps=10) as sv:
+        sv.configure("sjf")
+        ids = [sv.submit(*r) for r in (blocker, big, small)]
+        infos = [sv.wait(i, timeout=600)[0] for i in ids]
+    assert all(awpsgt.REQ_STATE[i["state"]] == "done" for i in infos)
+    assert infos[2]["t_admit"] < infos[1]["t_admit"]       # the small one overtook the big one
+    assert infos[2]["t_admit"] >= infos[0]["t_done"] - 1e-6
+
+
+def test_configure_rejects_unknown_policy():
+    with awpsgt.Server() as sv:
+        with pytest.raises(awpsgt.AwpError) as e:
+            sv.lib.awp_server_configure(sv.h, 7, 0.0, 0.0) and awpsgt._check(sv.lib.awp_server_configure(sv.h, 7, 0.0, 0.0))
+        assert e.value.status == 2
