@@ -163,7 +163,7 @@ def shard_jobs(jobs, rank, world):
 def workload(args=None):
     """The config-2 job, or a reduced grid / component set for small profiling
     captures (--grid, --components); the name records any change."""
-    w = ai.config(CONFIG_N)
+    w = ai.config(args.config if args is not None and args.config else CONFIG_N)
     if args is None:
         return w
     import dataclasses
@@ -377,6 +377,7 @@ def main():
     ap.add_argument("--e2e-solves", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", type=int, default=0, help="workload 1..4 (default 2: 400x400x200 fx+fy+fz)")
     ap.add_argument("--grid", default="", help="nx,ny,nz: reduced grid for profiling captures")
     ap.add_argument("--components", type=int, default=0, help="first n of the fx, fy, fz components")
     ap.add_argument("--serve", action="store_true", help="serving stream: p50/p99 latency against serial solves")
@@ -426,12 +427,13 @@ def main():
     # ---------------- end to end through the C ABI ----------------
     e2e_vals, h2d, d2h = [], 0, 0
     media_pinned = media
-    try:
-        import torch
-        mt = torch.from_numpy(media).pin_memory()
-        media_pinned = mt.numpy()
-    except Exception:
-        pass
+    if not args.no_e2e:
+        try:
+            import torch
+            mt = torch.from_numpy(media).pin_memory()
+            media_pinned = mt.numpy()
+        except Exception:
+            pass
     for it in range(0 if args.no_e2e else 1 + args.e2e_solves):
         barrier(dist)
         t0 = time.perf_counter()

@@ -126,6 +126,85 @@ def correlated_field(shape: Tuple[int, int, int], corr_cells: float, seed: int) 
     return np.ascontiguousarray(out.astype(np.float32))
 
 
+def _field_slab(coarse: np.ndarray, cf: int, shape, z0: int, z1: int) -> np.ndarray:
+    """Planes z0..z1-1 of the trilinear interpolation of a coarse field (the
+    interpolation of correlated_field, before normalisation)."""
+    out = coarse
+    sl = [(z0, z1), (0, shape[1]), (0, shape[2])]
+    for ax in range(3):
+        lo, hi = sl[ax]
+        pos = np.arange(lo, hi, dtype=np.float64) / cf + 0.5
+        i0 = np.floor(pos).astype(np.int64)
+        wgt = (pos - i0).astype(np.float32)
+        a = np.take(out, i0, axis=ax)
+        b = np.take(out, i0 + 1, axis=ax)
+        bshape = [1, 1, 1]
+        bshape[ax] = hi - lo
+        wgt = wgt.reshape(bshape)
+        out = a * (1 - wgt) + b * wgt
+    return out.astype(np.float32)
+
+
+def _layered_media_slabs(nx, ny, nz, dh, seed, nlayers, vs_top, vs_bot, pert_std, corr_len, basin, slab=16):
+    """layered_media for grids too large to hold several full-size temporaries:
+    the same recipe evaluated z-slab by z-slab (the correlated field is
+    normalised with statistics gathered over all slabs first)."""
+    depth = (np.arange(nz, dtype=np.float64) + 0.5) * dh
+    thick = nz * dh / nlayers
+    layer = np.minimum((depth // thick).astype(np.int64), nlayers - 1)
+    vs_l = vs_top * (vs_bot / vs_top) ** (np.arange(nlayers) / max(nlayers - 1, 1))
+    shape = (nz, ny, nx)
+    coarse, cf = None, 1
+    mean, std = 0.0, 1.0
+    if pert_std > 0:
+        sigma = (corr_len / dh) / 2.0
+        cf = max(1, int(sigma // 2))
+        cshape = tuple(int(math.ceil(n / cf)) + 2 for n in shape)
+        rng = np.random.default_rng(seed)
+        w = rng.standard_normal(cshape).astype(np.float32)
+        sc = sigma / cf
+        kz = np.fft.fftfreq(cshape[0])[:, None, None]
+        ky = np.fft.fftfreq(cshape[1])[None, :, None]
+        kx = np.fft.rfftfreq(cshape[2])[None, None, :]
+        g = np.exp(-2.0 * (math.pi * sc) ** 2 * (kx * kx + ky * ky + kz * kz))
+        coarse = np.fft.irfftn(np.fft.rfftn(w) * g, s=cshape, axes=(0, 1, 2)).astype(np.float32)
+        coarse -= coarse.mean()
+        coarse /= max(float(coarse.std()), 1e-30)
+        s1 = s2 = 0.0
+        for z0 in range(0, nz, slab):
+            f = _field_slab(coarse, cf, shape, z0, min(nz, z0 + slab)).astype(np.float64)
+            s1 += float(f.sum())
+            s2 += float((f * f).sum())
+        n = float(nx) * ny * nz
+        mean = s1 / n
+        std = max(math.sqrt(max(s2 / n - mean * mean, 0.0)), 1e-30)
+    if basin is not None:
+        x = (np.arange(nx) + 0.5) * dh
+        y = (np.arange(ny) + 0.5) * dh
+        r2 = ((x[None, :] - basin["cx"]) / basin["rx"]) ** 2 + ((y[:, None] - basin["cy"]) / basin["ry"]) ** 2
+        floor = basin["depth"] * np.sqrt(np.clip(1.0 - r2, 0.0, None))
+    m = np.empty((nz, ny, nx, 3), dtype=np.float32)
+    for z0 in range(0, nz, slab):
+        z1 = min(nz, z0 + slab)
+        vs = np.empty((z1 - z0, ny, nx), dtype=np.float32)
+        for k in range(z0, z1):
+            vs[k - z0] = np.float32(vs_l[layer[k]])
+            if basin is not None:
+                inside = depth[k] < floor
+                if inside.any():
+                    frac = np.where(inside, depth[k] / np.maximum(floor, 1e-9), 1.0)
+                    vsb = (400.0 + 600.0 * frac).astype(np.float32)
+                    vs[k - z0] = np.where(inside, np.minimum(vs[k - z0], vsb), vs[k - z0])
+        if coarse is not None:
+            pert = ((_field_slab(coarse, cf, shape, z0, z1) - mean) / std).astype(np.float32)
+            vs *= (1.0 + pert_std * pert).astype(np.float32)
+        vp = (1.73 * vs).astype(np.float32)
+        m[z0:z1, ..., 0] = vp
+        m[z0:z1, ..., 1] = vs
+        m[z0:z1, ..., 2] = (310.0 * np.power(vp.astype(np.float64), 0.25)).astype(np.float32)
+    return m
+
+
 def layered_media(nx: int, ny: int, nz: int, dh: float, seed: int, nlayers: int = 8,
                   vs_top: float = 500.0, vs_bot: float = 4000.0, pert_std: float = 0.05,
                   corr_len: float = 2000.0,
@@ -134,7 +213,10 @@ def layered_media(nx: int, ny: int, nz: int, dh: float, seed: int, nlayers: int 
     vs_bot), Vp = 1.73 Vs, rho = 310 Vp^0.25 (Gardner, SI units), times
     (1 + pert_std * correlated field) on Vp and Vs.  Optional basin: ellipsoid
     {cx, cy, rx, ry, depth} (metres) where Vs ramps from 400 m/s at the surface
-    to 1000 m/s at its floor."""
+    to 1000 m/s at its floor.  Grids above 2e8 cells are built z-slab by
+    z-slab (same recipe, bounded host memory)."""
+    if float(nx) * ny * nz > 2.0e8:
+        return _layered_media_slabs(nx, ny, nz, dh, seed, nlayers, vs_top, vs_bot, pert_std, corr_len, basin)
     depth = (np.arange(nz, dtype=np.float64) + 0.5) * dh
     thick = nz * dh / nlayers
     layer = np.minimum((depth // thick).astype(np.int64), nlayers - 1)
