@@ -440,9 +440,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->kchunk = choose_kchunk(s->g, 1, s->ty);
     s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
     {
-        const int kc = env_int("AWP_TUNE_KSTAGE", 16);
+        const int kc = env_int("AWP_TUNE_KSTAGE", 32);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
-        s->staged_qslow = env_int("AWP_TUNE_QSLOW", 0) != 0;
+        s->staged_qslow = env_int("AWP_TUNE_QSLOW", 1) != 0;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;

@@ -2,29 +2,28 @@
  * awp_staged.cu -- the two-sweep stepper with TMA-staged xy tiles (2.5D blocking).
  *
  * A thread block owns a 32 x 8 column tile of one component and marches up a
- * chunk of z levels.  For every level one thread issues TMA tile loads
- * (cp.async.bulk.tensor over 3D tensor maps of the padded volume) of the
- * arrays that are read with x/y neighbours -- stencil tiles with a 4-column
- * and 2-row halo, media tiles with the one row below -- into a ring of shared
- * memory slots, D levels ahead of the level being computed; one mbarrier per
- * slot counts the bytes in.  Values needed only along the cell's own column
- * (z neighbours) travel in a per-thread register queue fed by one load per
- * level, and the point-wise state (u, v, w in the velocity sweep; six
- * stresses and six memory variables in the stress sweep) is read and written
- * once per cell with coalesced accesses.  So the bytes in flight per SM are
- * set by the ring depth, not by registers or resident warps.
+ * chunk of z levels.  A producer warp issues, for every level, TMA tile loads
+ * (cp.async.bulk.tensor over 3D tensor maps of the padded volume) into a ring
+ * of shared-memory slots ahead of the level being computed: stencil tiles
+ * with a 4-column and 2-row halo, media tiles with the row below, and the
+ * point-wise state as 32 x 8 tiles.  A "full" mbarrier per slot counts the
+ * bytes in; the eight consumer warps release a slot through its "empty"
+ * mbarrier.  Values needed only along the cell's own column (z neighbours)
+ * travel in per-thread register queues, loaded one level ahead.  Results are
+ * written with coalesced stores.  The bytes in flight per SM are set by the
+ * ring depth, not by registers or resident warps.
  *
  * Work items (x tile, y tile, z chunk, component) are spread over a
- * persistent grid; the components of one tile are neighbouring items, so
- * their common media tiles are read from HBM once and from L2 after.
+ * persistent grid, one component after the other or the components of a
+ * tile side by side (split_item).
  *
  * The per-cell arithmetic is the shared code of awp_stencil.cuh, evaluated in
  * the same order as the other steppers (bit-identical results).  FP32 media
  * only; memory variables FP32 or bf16.
  *
  * Every wait on an mbarrier is bounded (2 s of %globaltimer); on expiry the
- * block records AWP_KERR_TMA_WAIT in the error word, waits (bounded again)
- * for its own copies in flight and returns.
+ * block records AWP_KERR_TMA_WAIT in the error word and its warps leave; the
+ * producer first waits (bounded again) for its own copies in flight.
  */
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -256,7 +255,7 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
     for (int a = 0; a < 3; ++a) tma_3d(sl + VEL_PT + a * ST_PT, mp + a, b, i0 + AWP_XO - 1, j0 + 1, k + 1);
 }
 
-/* work items: (x tile, y tile, z chunk, component), component fastest */
+/* work items: (x tile, y tile, z chunk, component); see split_item for the order */
 template <int D, int UNR>
 __global__ void __launch_bounds__(ST_THREADS, 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
@@ -427,8 +426,7 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
     }
 }
 
-/* work items: (x tile, y tile, z chunk, component), component fastest, so
- * the components of a tile run side by side and share its media through L2 */
+/* work items: (x tile, y tile, z chunk, component); see split_item for the order */
 template <class TR, int UNR>
 __global__ void __launch_bounds__(ST_THREADS, 3)
 k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
