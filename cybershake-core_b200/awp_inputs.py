@@ -442,3 +442,50 @@ def config(n: int) -> Workload:
                         extra={"basin": {"cx": 70000.0, "cy": 50000.0, "rx": 30000.0, "ry": 20000.0,
                                          "depth": 4000.0}})
     raise ValueError(n)
+
+
+# ---------------------------------------------------------------------------
+# SGT header inputs (the files SgtHead's write_head reads)
+# ---------------------------------------------------------------------------
+
+def write_sgthead_inputs(d: str, nx: int, ny: int, nz: int, h_km: float, npts: int, seed: int = 0,
+                         site=(None, None), mlon: float = -118.2, mlat: float = 34.05, mrot: float = -55.0,
+                         edge_points: bool = True) -> dict:
+    """Model box, RWG coordinate file, site location, grid file and AWP media
+    file ([z][x][y][vp vs rho], y fastest, m/s and kg/m^3) for an nx x ny x nz
+    RWG grid; returns the paths.  Points are distinct, seeded, and (with
+    edge_points) include the special cases of the header writer: y = 0,
+    x = nx-1, z = 0, z = 1 and z = nz-1."""
+    os.makedirs(d, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    paths = {k: os.path.join(d, k) for k in ("modelbox", "coordfile", "fdloc", "gridout", "media")}
+    with open(paths["modelbox"], "w") as f:
+        f.write("synthetic model box\nline 2\nline 3\nline 4\n")
+        f.write("mlon= %.5f mlat= %.5f mrot= %.2f\n" % (mlon, mlat, mrot))
+    xs, ys = site
+    xs = nx // 2 if xs is None else xs
+    ys = ny // 3 if ys is None else ys
+    with open(paths["fdloc"], "w") as f:
+        f.write("%d %d\n" % (xs, ys))
+    with open(paths["gridout"], "w") as f:
+        for name, n in (("x", nx), ("y", ny), ("z", nz)):
+            f.write("%slen=%.6e\n%s=%d\n" % (name, n * h_km, "n" + name, n))
+            for i in range(n):
+                f.write("%d %12.5e %12.5e\n" % (i, i * h_km, h_km))
+    pts = set()
+    if edge_points:
+        for p in ((0, 0, 0), (nx - 1, 3 % ny, 1), (2 % nx, 0, nz - 1), (nx - 1, ny - 1, nz - 1), (1, 1, 0)):
+            pts.add(p)
+    while len(pts) < npts:
+        pts.add((int(rng.integers(0, nx)), int(rng.integers(0, ny)), int(rng.integers(0, nz))))
+    pts = sorted(pts, key=lambda p: (p[1], p[0], p[2]))[:npts]
+    with open(paths["coordfile"], "w") as f:
+        f.write("# synthetic SGT coordinates\n# x y z indx lon lat dep\n%d\n" % len(pts))
+        for x, y, z in pts:
+            f.write("%d %d %d %d %.5f %.5f %.4f\n" % (x, y, z, x * 1000000000000 + y * 1000000 + z,
+                                                     mlon + 0.01 * x, mlat + 0.01 * y, z * h_km))
+    vs = (500.0 + 3500.0 * rng.random((nz, nx, ny))).astype(np.float32)
+    vp = (1.73 * vs * (1.0 + 0.05 * rng.random((nz, nx, ny)))).astype(np.float32)
+    rho = (310.0 * np.power(vp.astype(np.float64), 0.25)).astype(np.float32)
+    np.stack([vp, vs, rho], axis=-1).astype(np.float32).tofile(paths["media"])
+    return paths

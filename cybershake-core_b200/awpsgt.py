@@ -19,6 +19,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libawpsgt.so")
+WRITE_HEAD_PATH = os.path.join(_HERE, "lib", "write_head")
+REFORMAT_AWP_PATH = os.path.join(_HERE, "lib", "reformat_awp")
 PMCL3D_PATH = os.path.join(_HERE, "lib", "pmcl3d")
 
 AWP_OK = 0
@@ -40,6 +42,7 @@ EXPORTED = [
     "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
+    "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header",
 ]
 
 
@@ -111,6 +114,56 @@ class In3dC(C.Structure):
 _lib = None
 
 
+class SgtHeadArgs(C.Structure):
+    """awp_sgthead_args: the arguments of SgtHead's write_head."""
+    _fields_ = [("modelbox", C.c_char_p), ("coordfile", C.c_char_p), ("fdloc", C.c_char_p),
+                ("gridout", C.c_char_p), ("spacing", C.c_float), ("nt", C.c_int), ("dt", C.c_float),
+                ("sgt_tinc", C.c_int), ("component", C.c_char_p), ("moment", C.c_float), ("flo", C.c_float),
+                ("media_file", C.c_char_p), ("mu_corr", C.c_int)]
+
+
+SGTMASTER = np.dtype([("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"), ("modelrot", "<f4"),
+                      ("xshift", "<f4"), ("yshift", "<f4"), ("globnp", "<i4"), ("localnp", "<i4"), ("nt", "<i4")])
+SGTINDEX = np.dtype([("indx", "<i8"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"), ("h", "<f4")])
+SGTHEADER = np.dtype([("indx", "<i8"), ("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"),
+                      ("modelrot", "<f4"), ("xshift", "<f4"), ("yshift", "<f4"), ("nt", "<i4"), ("xazim", "<f4"),
+                      ("dt", "<f4"), ("tst", "<f4"), ("h", "<f4"), ("src_lat", "<f4"), ("src_lon", "<f4"),
+                      ("src_dep", "<f4"), ("xsrc", "<i4"), ("ysrc", "<i4"), ("zsrc", "<i4"), ("sgt_lat", "<f4"),
+                      ("sgt_lon", "<f4"), ("sgt_dep", "<f4"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"),
+                      ("cdist", "<f4"), ("lam", "<f4"), ("mu", "<f4"), ("rho", "<f4"), ("xmom", "<f4"),
+                      ("ymom", "<f4"), ("zmom", "<f4")])
+
+
+def write_sgt_header(outfile: str, modelbox: str, coordfile: str, fdloc: str, gridout: str, spacing: float,
+                     nt: int, dt: float, sgt_tinc: int, component: str, moment: float, flo: float,
+                     media_file: str, mu_corr: bool = False) -> None:
+    """awp_write_sgt_header: the .sgthead file of one SGT component."""
+    a = SgtHeadArgs(modelbox.encode(), coordfile.encode(), fdloc.encode(), gridout.encode(), spacing, nt, dt,
+                    sgt_tinc, component.encode(), moment, flo, media_file.encode(), int(bool(mu_corr)))
+    _check(load_library().awp_write_sgt_header(C.byref(a), outfile.encode()))
+
+
+def read_sgt_header(path: str):
+    """(sgtmaster, sgtindex[np], sgtheader[np]) records of a header file."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    m = raw[:SGTMASTER.itemsize].view(SGTMASTER)[0]
+    npts = int(m["globnp"])
+    o = SGTMASTER.itemsize
+    ix = raw[o:o + npts * SGTINDEX.itemsize].view(SGTINDEX)
+    o += npts * SGTINDEX.itemsize
+    hd = raw[o:o + npts * SGTHEADER.itemsize].view(SGTHEADER)
+    return m, ix, hd
+
+
+def sgt_reorder_rwg(sgt: np.ndarray, nt: int, z_source: bool = False) -> np.ndarray:
+    """awp_sgt_reorder_rwg on a host SGT file image (points x [6][nt])."""
+    a = np.ascontiguousarray(sgt, dtype=np.float32)
+    npts = a.size // (6 * nt)
+    out = np.empty(npts * 6 * nt, dtype=np.float32)
+    _check(load_library().awp_sgt_reorder_rwg(_ptr(a), npts, nt, int(bool(z_source)), _ptr(out)))
+    return out
+
+
 def load_library(path: str = LIB_PATH):
     """Loads libawpsgt.so; raises ImportError when it has not been built."""
     global _lib
@@ -161,6 +214,9 @@ def load_library(path: str = LIB_PATH):
         "awp_server_time": (C.c_double, [C.c_void_p]),
         "awp_server_destroy": (C.c_int, [C.c_void_p]),
         "awp_server_configure": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
+        "awp_get_sgt_rwg": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_sgt_reorder_rwg": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p]),
+        "awp_write_sgt_header": (C.c_int, [P(SgtHeadArgs), C.c_char_p]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
     }
     for name, (res, args) in sig.items():
@@ -275,6 +331,12 @@ class Solver:
     def sgt(self, comp: int = 0) -> np.ndarray:
         out = np.zeros(self.sgt_file_floats(), dtype=np.float32)
         _check(self.lib.awp_get_sgt(self.h, comp, _ptr(out)))
+        return out
+
+    def sgt_rwg(self, comp: int = 0, z_source: bool = False) -> np.ndarray:
+        """SGT file image of one component in RWG order (awp_get_sgt_rwg)."""
+        out = np.empty(max(int(self.lib.awp_sgt_file_floats(self.h)), 0), dtype=np.float32)
+        _check(self.lib.awp_get_sgt_rwg(self.h, comp, int(bool(z_source)), _ptr(out)))
         return out
 
     def chkj(self, comp: int = 0) -> np.ndarray:

@@ -910,6 +910,35 @@ cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st)
     return cudaGetLastError();
 }
 
+/* RWG order of SGT file images, per point [6][nt]: XX <- YY, YY <- XX, ZZ,
+ * XY, XZ <- -YZ, YZ <- -XZ, every value first scaled by -2 for the z-force
+ * run (SgtHead/src/reformat_awp_mpi.c:85-122).  Scaling by -2 and -1 is
+ * exact in FP32, so the result matches the reference's double products. */
+__global__ void k_sgt_rwg(const float *__restrict__ in, float *__restrict__ out, int64_t total, int nt, int zsrc)
+{
+    const int64_t per = (int64_t)6 * nt;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = e / per;
+        const int r = (int)(e - p * per);
+        const int c = r / nt, t = r - c * nt;
+        const int src = c == 0 ? 1 : (c == 1 ? 0 : (c == 4 ? 5 : (c == 5 ? 4 : c)));
+        float v = in[p * per + (int64_t)src * nt + t];
+        if (zsrc) v = -2.0f * v;
+        if (c >= 4) v = -1.0f * v;
+        out[e] = v;
+    }
+}
+
+cudaError_t awp_launch_sgt_rwg(const float *in, float *out, int64_t npts, int nt, int zsrc, cudaStream_t st)
+{
+    const int64_t total = npts * 6 * (int64_t)nt;
+    if (total <= 0) return cudaSuccess;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_sgt_rwg<<<(unsigned)blocks, 256, 0, st>>>(in, out, total, nt, zsrc);
+    return cudaGetLastError();
+}
+
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st)
 {
     const int n = a.npts * a.ncomp;

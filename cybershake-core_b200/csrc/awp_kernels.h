@@ -56,6 +56,8 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);
+/* SGT file images [point][6][nt] in RWG component order (z-force runs x -2) */
+cudaError_t awp_launch_sgt_rwg(const float *in, float *out, int64_t npts, int nt, int zsrc, cudaStream_t st);
 
 /* FP64 energy of (u, v, w) per component, two passes through `partial`
  * (nblocks * ncomp doubles of scratch); flag (may be NULL) set on NaN/Inf */

@@ -1054,6 +1054,40 @@ extern "C" awp_status awp_get_sgt(awp_solver *s, int comp, float *out)
     return AWP_OK;
 }
 
+extern "C" awp_status awp_get_sgt_rwg(awp_solver *s, int comp, int z_source, float *out)
+{
+    if (!s || !out || comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad solver/component/output");
+    if (s->sgt_file_floats <= 0) return AWP_OK;
+    CU(cudaSetDevice(s->p.device));
+    CU(cudaStreamSynchronize(s->stream));
+    float *tmp = NULL;
+    CU(cudaMalloc((void **)&tmp, sizeof(float) * (size_t)s->sgt_file_floats));
+    cudaError_t e = awp_launch_sgt_rwg(s->sgt_file[comp], tmp, s->npts, s->nt_file, z_source != 0, s->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, tmp, sizeof(float) * (size_t)s->sgt_file_floats, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_get_sgt_rwg: %s", cudaGetErrorString(e));
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_sgt_reorder_rwg(const float *in, int64_t npts, int nt, int z_source, float *out)
+{
+    if (!in || !out || npts < 0 || nt < 0) return set_err(AWP_ERR_PARAM, "awp_sgt_reorder_rwg: bad argument");
+    const size_t bytes = sizeof(float) * 6 * (size_t)npts * (size_t)nt;
+    if (bytes == 0) return AWP_OK;
+    float *d_in = NULL, *d_out = NULL;
+    cudaError_t e = cudaMalloc((void **)&d_in, bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_out, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(d_in, in, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = awp_launch_sgt_rwg(d_in, d_out, npts, nt, z_source != 0, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_sgt_reorder_rwg: %s", cudaGetErrorString(e));
+    return AWP_OK;
+}
+
 extern "C" awp_status awp_get_chkj(awp_solver *s, int comp, float *out)
 {
     if (!s || comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad solver/component");

@@ -10,7 +10,10 @@
  *   GPU form:  OUT/SGT%07d per WRITE_STEP chunk, layout [point][6][WRITE_STEP]
  *              (AWP-GPU-SGT/src/pmcl3d.c:462-492, 932-958), and CHKFILE
  *              (AWP-GPU-SGT/src/io.c:7-35).
- * Everything runs on one GPU; NPX/NPY/NPZ are read and ignored.
+ * Everything runs on one GPU; NPX/NPY/NPZ are read and ignored.  With
+ * AWP_RWG_SGT=x|y|z in the environment the SGTs are written in RWG component
+ * order (SgtHead/src/reformat_awp_mpi.c:104-122), so no separate reformat
+ * pass is needed.
  */
 #include <math.h>
 #include <stdio.h>
@@ -205,7 +208,12 @@ int main(int argc, char **argv)
     if (npts > 0 && in.io_opt == 1) {
         const int64_t nf = awp_sgt_file_floats(s);
         float *img = (float *)malloc(sizeof(float) * (size_t)(nf > 0 ? nf : 1));
-        if ((st = awp_get_sgt(s, 0, img)) != AWP_OK) return fail(st, "reading the SGTs");
+        /* AWP_RWG_SGT=x|y|z: the file image in RWG order (the z-force run scaled
+         * by -2), which folds SgtHead's reformat_awp pass into the run */
+        const char *rwg = getenv("AWP_RWG_SGT");
+        if (rwg && *rwg) st = awp_get_sgt_rwg(s, 0, rwg[0] == 'z', img);
+        else st = awp_get_sgt(s, 0, img);
+        if (st != AWP_OK) return fail(st, "reading the SGTs");
         if (!in.gpu_cli) {
             mkdir_for(in.sgtgro);
             FILE *f = fopen(in.sgtgro, "wb");

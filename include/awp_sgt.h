@@ -259,6 +259,66 @@ const char *awp_status_string(awp_status st);
 const char *awp_last_error(void);
 
 /* ------------------------------------------------------------------------- */
+/* SGT post-processing formats (SgtHead).                                    */
+/* ------------------------------------------------------------------------- */
+
+/* One component's SGT file image in RWG order, straight from the device
+ * image: per point [6][NT] with XX <- YY, YY <- XX, ZZ, XY, XZ <- -YZ,
+ * YZ <- -XZ, and for the z-force run every value first scaled by -2
+ * (z_source = 1).  Replaces the separate reformat_awp / reformat_awp_mpi
+ * pass (SgtHead/src/reformat_awp_mpi.c:104-122); `out` holds
+ * awp_sgt_file_floats() floats. */
+awp_status awp_get_sgt_rwg(awp_solver *s, int comp, int z_source, float *out);
+
+/* The same reordering of a host SGT file image of npts points x [6][nt],
+ * done on the current device (the reformat_awp tool's transform). */
+awp_status awp_sgt_reorder_rwg(const float *in, int64_t npts, int nt, int z_source, float *out);
+
+/* Records of the RWG SGT header file (SgtHead/src/structure.h:164-220). */
+typedef struct {
+    int geoproj;
+    float modellon, modellat, modelrot, xshift, yshift;
+    int globnp, localnp, nt;
+} awp_sgtmaster;
+typedef struct {
+    long long indx;
+    int xsgt, ysgt, zsgt;
+    float h;
+} awp_sgtindex;
+typedef struct {
+    long long indx;
+    int geoproj;
+    float modellon, modellat, modelrot, xshift, yshift;
+    int nt;
+    float xazim, dt, tst, h, src_lat, src_lon, src_dep;
+    int xsrc, ysrc, zsrc;
+    float sgt_lat, sgt_lon, sgt_dep;
+    int xsgt, ysgt, zsgt;
+    float cdist, lam, mu, rho, xmom, ymom, zmom;
+} awp_sgtheader;
+
+/* Inputs of the header writer, the arguments of SgtHead's write_head. */
+typedef struct {
+    const char *modelbox;    /* model box file; line 5: "mlon= . mlat= . mrot= ." */
+    const char *coordfile;   /* RWG SGT coordinate file: x y z indx lon lat dep   */
+    const char *fdloc;       /* "xsrc ysrc" of the site (the reciprocal source)   */
+    const char *gridout;     /* grid file with nx=, ny=, nz=                      */
+    float spacing;           /* grid spacing (km)                                 */
+    int nt;                  /* time steps of the run                             */
+    float dt;                /* time step (s)                                     */
+    int sgt_tinc;            /* SGT time decimation                               */
+    const char *component;   /* "x", "y" or "z"                                   */
+    float moment;            /* force moment of the run                           */
+    float flo;               /* source filter frequency (Hz)                      */
+    const char *media_file;  /* AWP media file (vp vs rho, m/s and kg/m^3)        */
+    int mu_corr;             /* 1: unrelaxed mu (the -c option)                   */
+} awp_sgthead_args;
+
+/* Writes sgtmaster, sgtindex[np] and sgtheader[np] (the .sgthead file),
+ * byte-identical to write_head (SgtHead/src/write_head.c:48-469). */
+awp_status awp_write_sgt_header(const awp_sgthead_args *a, const char *outfile);
+
+/* ------------------------------------------------------------------------- */
 /* Serving: continuous batching of SGT solves on one GPU.                    */
 /* No reference counterpart (the reference runs one solve per job).          */
 /*                                                                           */

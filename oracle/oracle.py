@@ -164,3 +164,15 @@ class Oracle:
 
 def threads():
     return load("f32").orc_num_threads()
+
+
+def reorder_rwg(sgt: np.ndarray, nt: int, z_source: bool = False) -> np.ndarray:
+    """RWG component order of an AWP SGT file image, points x [6][nt]
+    (SgtHead/src/reformat_awp.c:39-63, reformat_awp_mpi.c:85-122): XX <- YY,
+    YY <- XX, ZZ, XY, XZ <- -YZ, YZ <- -XZ; for the z-force run every value is
+    first multiplied by -2.0 in double precision and stored as float."""
+    x = np.asarray(sgt, dtype=np.float32).reshape(-1, 6, nt)
+    if z_source:
+        x = (-2.0 * x.astype(np.float64)).astype(np.float32)
+    neg = lambda a: (-1.0 * a.astype(np.float64)).astype(np.float32)
+    return np.stack([x[:, 1], x[:, 0], x[:, 2], x[:, 3], neg(x[:, 5]), neg(x[:, 4])], axis=1).reshape(-1)

@@ -124,3 +124,18 @@ def test_driver_rejects_pml(tmp_path):
     w.write(str(tmp_path / "IN3D"))
     r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "PML" in r.stderr
+
+
+@pytest.mark.gpu
+def test_rwg_order_output(tmp_path):
+    """AWP_RWG_SGT=x: the SGT file comes out in RWG component order, as
+    SgtHead's reformat_awp would write it."""
+    media, stf, pts = write_inputs(tmp_path)
+    in3d(tmp_path)
+    env = dict(os.environ, AWP_RWG_SGT="x")
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=300,
+                       env=env)
+    assert r.returncode == 0, r.stderr + r.stdout
+    got = np.fromfile(tmp_path / "out" / "sgt" / "awp-strain", dtype=np.float32)
+    ref = oracle.reorder_rwg(oracle_sgt(media, stf, pts).sgt(), 12)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
