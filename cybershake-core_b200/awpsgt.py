@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libawpsgt.so")
 WRITE_HEAD_PATH = os.path.join(_HERE, "lib", "write_head")
 REFORMAT_AWP_PATH = os.path.join(_HERE, "lib", "reformat_awp")
+REFORMAT_VELOCITY_PATH = os.path.join(_HERE, "lib", "reformat_velocity")
 PMCL3D_PATH = os.path.join(_HERE, "lib", "pmcl3d")
 
 AWP_OK = 0
@@ -42,7 +43,8 @@ EXPORTED = [
     "awp_run_async", "awp_query", "awp_sync", "awp_device_field", "awp_field_energy", "awp_energy",
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
-    "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header",
+    "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
+    "awp_reformat_velocity",
 ]
 
 
@@ -217,6 +219,8 @@ def load_library(path: str = LIB_PATH):
         "awp_get_sgt_rwg": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
         "awp_sgt_reorder_rwg": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p]),
         "awp_write_sgt_header": (C.c_int, [P(SgtHeadArgs), C.c_char_p]),
+        "awp_load_media_rwg": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "awp_reformat_velocity": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
     }
     for name, (res, args) in sig.items():
@@ -332,6 +336,10 @@ class Solver:
         out = np.zeros(self.sgt_file_floats(), dtype=np.float32)
         _check(self.lib.awp_get_sgt(self.h, comp, _ptr(out)))
         return out
+
+    def load_media_rwg(self, prefix: str):
+        """Media from RWG volumes prefix.p / .s / .d (awp_load_media_rwg)."""
+        _check(self.lib.awp_load_media_rwg(self.h, prefix.encode()))
 
     def sgt_rwg(self, comp: int = 0, z_source: bool = False) -> np.ndarray:
         """SGT file image of one component in RWG order (awp_get_sgt_rwg)."""

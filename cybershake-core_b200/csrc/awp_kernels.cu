@@ -939,6 +939,45 @@ cudaError_t awp_launch_sgt_rwg(const float *in, float *out, int64_t npts, int nt
     return cudaGetLastError();
 }
 
+/* RWG velocity volumes to the AWP media layout, one z-slab of n levels
+ * (SgtHead/src/reformat_velocity.c:30-80): input [3][ny][n][nx] (p, s, d;
+ * x fastest, then z, then y; km/s and g/cm^3), output [n][nx][ny][3] (y
+ * fastest; m/s and kg/m^3, values times 1000).  A 32 x 32 (x, y) tile of all
+ * three variables goes through shared memory so reads and writes coalesce.
+ * The float product is the exact product rounded once, as the reference's
+ * double product stored to float. */
+__global__ void __launch_bounds__(256) k_rwg_slab(const float *__restrict__ rwg, float *__restrict__ awp, int nx,
+                                                  int ny, int n)
+{
+    __shared__ float t[3][32][33];
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32, kk = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int v = 0; v < 3; ++v)
+        for (int jj = ty; jj < 32; jj += 8) {
+            const int i = i0 + tx, j = j0 + jj;
+            if (i < nx && j < ny) t[v][jj][tx] = rwg[(((size_t)v * ny + j) * n + kk) * nx + i];
+        }
+    __syncthreads();
+    /* one output row per x: 32 y values x 3 variables, contiguous */
+    for (int ii = ty; ii < 32; ii += 8) {
+        const int i = i0 + ii;
+        if (i >= nx) continue;
+        float *row = awp + (((size_t)kk * nx + i) * ny + j0) * 3;
+        const int nyr = min(32, ny - j0);
+        for (int e = tx; e < 3 * nyr; e += 32) {
+            const int jj = e / 3, v = e - 3 * jj;
+            row[e] = t[v][jj][ii] * 1000.0f;
+        }
+    }
+}
+
+cudaError_t awp_launch_rwg_slab(const float *rwg, float *awp, int nx, int ny, int n, cudaStream_t st)
+{
+    if (nx <= 0 || ny <= 0 || n <= 0) return cudaSuccess;
+    k_rwg_slab<<<dim3((nx + 31) / 32, (ny + 31) / 32, n), dim3(32, 8), 0, st>>>(rwg, awp, nx, ny, n);
+    return cudaGetLastError();
+}
+
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st)
 {
     const int n = a.npts * a.ncomp;

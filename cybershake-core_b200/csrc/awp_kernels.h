@@ -56,6 +56,9 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);
+/* one z-slab of RWG p/s/d volumes ([3][ny][n][nx]) to AWP media order
+ * ([n][nx][ny][3], x 1000) */
+cudaError_t awp_launch_rwg_slab(const float *rwg, float *awp, int nx, int ny, int n, cudaStream_t st);
 /* SGT file images [point][6][nt] in RWG component order (z-force runs x -2) */
 cudaError_t awp_launch_sgt_rwg(const float *in, float *out, int64_t npts, int nt, int zsrc, cudaStream_t st);
 

@@ -546,7 +546,10 @@ static awp_status finish_media(awp_solver *s)
 
 typedef int (*slab_reader)(void *ctx, float *dst, int zf0, int nzs, size_t floats_per_level);
 
-static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx)
+/* rwg_nx > 0: the reader delivers z-slabs of RWG p/s/d volumes ([3][ny][n][nx],
+ * rwg_nx x rwg_ny = ny x nx of the AWP grid), turned into AWP media order on
+ * the device before the transform */
+static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, int rwg_nx = 0, int rwg_ny = 0)
 {
     const awp_params *p = &s->p;
     CU(cudaSetDevice(p->device));
@@ -597,16 +600,22 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx)
     CU(cudaMallocHost((void **)&hbuf[1], per_level * nzs * sizeof(float)));
     CU(cudaEventCreate(&done[0]));
     CU(cudaEventCreate(&done[1]));
-    cudaError_t e = cudaMalloc((void **)&dbuf, per_level * nzs * sizeof(float) * 2);
+    cudaError_t e = cudaMalloc((void **)&dbuf, per_level * nzs * sizeof(float) * (rwg_nx > 0 ? 3 : 2));
     awp_status st = AWP_OK;
     if (e != cudaSuccess) st = set_err(AWP_ERR_OOM, "media staging: %s", cudaGetErrorString(e));
+    float *draw = rwg_nx > 0 && dbuf ? dbuf + 2 * per_level * nzs : NULL;
     int slab = 0;
     for (int z0 = 0; z0 < p->nz && st == AWP_OK; z0 += nzs, slab ^= 1) {
         const int n = (z0 + nzs <= p->nz) ? nzs : p->nz - z0;
         if (z0 >= 2 * nzs && cudaEventSynchronize(done[slab]) != cudaSuccess) { st = set_err(AWP_ERR_CUDA, "media stream"); break; }
         if (rd(ctx, hbuf[slab], z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "media: short read at level %d", z0); break; }
         float *d = dbuf + (size_t)slab * per_level * nzs;
-        e = cudaMemcpyAsync(d, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+        if (draw) {
+            e = cudaMemcpyAsync(draw, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+            if (e == cudaSuccess) e = awp_launch_rwg_slab(draw, d, rwg_nx, rwg_ny, n, s->stream);
+        } else {
+            e = cudaMemcpyAsync(d, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+        }
         if (e == cudaSuccess)
             e = awp_launch_media_interior(s->g, s->md, d, z0, n, p->nvar, var_offset, p->socalq, p->nve,
                                           pi, lw, tmp1, tmp2, s->ext, s->stream);
@@ -664,6 +673,96 @@ extern "C" awp_status awp_load_media_file(awp_solver *s, const char *path)
     file_ctx fc = {f};
     awp_status st = load_media_common(s, file_reader, &fc);
     fclose(f);
+    return st;
+}
+
+/* z-slabs of RWG velocity volumes prefix.p / .s / .d: float, x fastest, then
+ * z (surface first), then y; a slab of AWP levels z0..z0+n-1 is, per file and
+ * per y plane, one contiguous run of n * nx values */
+struct rwg_ctx { FILE *f[3]; int nx, ny, nz; };
+static int rwg_reader(void *ctx, float *dst, int zf0, int nzs, size_t per_level)
+{
+    rwg_ctx *r = (rwg_ctx *)ctx;
+    (void)per_level;
+    const size_t run = (size_t)nzs * r->nx;
+    for (int v = 0; v < 3; v++)
+        for (int j = 0; j < r->ny; j++) {
+            const long long off = ((long long)j * r->nz + zf0) * r->nx * (long long)sizeof(float);
+            if (fseeko(r->f[v], (off_t)off, SEEK_SET) != 0) return -1;
+            if (fread(dst + ((size_t)v * r->ny + j) * run, sizeof(float), run, r->f[v]) != run) return -1;
+        }
+    return 0;
+}
+
+static awp_status open_rwg(rwg_ctx *r, const char *prefix)
+{
+    static const char sfx[3] = {'p', 's', 'd'};
+    for (int v = 0; v < 3; v++) r->f[v] = NULL;
+    for (int v = 0; v < 3; v++) {
+        char name[1100];
+        snprintf(name, sizeof name, "%s.%c", prefix, sfx[v]);
+        r->f[v] = fopen(name, "rb");
+        if (!r->f[v]) {
+            for (int u = 0; u < v; u++) fclose(r->f[u]);
+            return set_err(AWP_ERR_IO, "cannot open velocity volume %s", name);
+        }
+    }
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_load_media_rwg(awp_solver *s, const char *prefix)
+{
+    if (!s || !prefix) return set_err(AWP_ERR_PARAM, "null argument");
+    if (s->p.mediastart == 0) return set_err(AWP_ERR_PARAM, "MEDIARESTART 0 reads no media");
+    if (s->p.nvar != 3) return set_err(AWP_ERR_PARAM, "RWG volumes carry vp, vs, rho: NVAR must be 3");
+    rwg_ctx r;
+    awp_status st = open_rwg(&r, prefix);
+    if (st != AWP_OK) return st;
+    r.nx = s->p.ny;            /* RWG x is AWP y */
+    r.ny = s->p.nx;
+    r.nz = s->p.nz;
+    st = load_media_common(s, rwg_reader, &r, r.nx, r.ny);
+    for (int v = 0; v < 3; v++) fclose(r.f[v]);
+    return st;
+}
+
+extern "C" awp_status awp_reformat_velocity(int nx, int ny, int nz, const char *prefix, const char *out)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !prefix || !out) return set_err(AWP_ERR_PARAM, "bad argument");
+    rwg_ctx r;
+    awp_status st = open_rwg(&r, prefix);
+    if (st != AWP_OK) return st;
+    r.nx = nx; r.ny = ny; r.nz = nz;
+    FILE *fo = fopen(out, "wb");
+    if (!fo) {
+        for (int v = 0; v < 3; v++) fclose(r.f[v]);
+        return set_err(AWP_ERR_IO, "cannot create %s", out);
+    }
+    const size_t per_level = (size_t)3 * nx * ny;
+    int nzs = (int)((256ull << 20) / (per_level * sizeof(float)));
+    if (nzs < 1) nzs = 1;
+    if (nzs > nz) nzs = nz;
+    const size_t bytes = per_level * nzs * sizeof(float);
+    float *h = NULL, *d_in = NULL, *d_out = NULL;
+    cudaError_t e = cudaMallocHost((void **)&h, bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_in, bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_out, bytes);
+    if (e != cudaSuccess) st = set_err(AWP_ERR_OOM, "reformat_velocity buffers: %s", cudaGetErrorString(e));
+    for (int z0 = 0; z0 < nz && st == AWP_OK; z0 += nzs) {
+        const int n = z0 + nzs <= nz ? nzs : nz - z0;
+        const size_t sz = per_level * n * sizeof(float);
+        if (rwg_reader(&r, h, z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "velocity volumes: short read at z %d", z0); break; }
+        e = cudaMemcpy(d_in, h, sz, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = awp_launch_rwg_slab(d_in, d_out, nx, ny, n, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(h, d_out, sz, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { st = set_err(AWP_ERR_CUDA, "reformat_velocity: %s", cudaGetErrorString(e)); break; }
+        if (fwrite(h, 1, sz, fo) != sz) { st = set_err(AWP_ERR_IO, "cannot write %s", out); break; }
+    }
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFreeHost(h);
+    for (int v = 0; v < 3; v++) fclose(r.f[v]);
+    if (fclose(fo) != 0 && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", out);
     return st;
 }
 

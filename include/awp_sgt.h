@@ -274,6 +274,19 @@ awp_status awp_get_sgt_rwg(awp_solver *s, int comp, int z_source, float *out);
  * done on the current device (the reformat_awp tool's transform). */
 awp_status awp_sgt_reorder_rwg(const float *in, int64_t npts, int nt, int z_source, float *out);
 
+/* Media from RWG velocity volumes prefix.p, prefix.s, prefix.d (float,
+ * x fastest, then z from the surface, then y; km/s and g/cm^3), transposed
+ * to the AWP order on the device slab by slab and then transformed as
+ * awp_load_media does; NVAR must be 3, RWG (nx, ny) = AWP (ny, nx).  Replaces
+ * SgtHead's reformat_velocity pass plus the media read
+ * (SgtHead/src/reformat_velocity.c:30-80, structure.f:107-116). */
+awp_status awp_load_media_rwg(awp_solver *s, const char *prefix);
+
+/* The AWP media file ([z][x][y][vp vs rho], y fastest, values x 1000) written
+ * from RWG volumes of nx x ny x nz, the transpose done on the current device:
+ * the reformat_velocity tool (SgtHead/src/reformat_velocity.c). */
+awp_status awp_reformat_velocity(int nx, int ny, int nz, const char *prefix, const char *out);
+
 /* Records of the RWG SGT header file (SgtHead/src/structure.h:164-220). */
 typedef struct {
     int geoproj;

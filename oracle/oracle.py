@@ -176,3 +176,15 @@ def reorder_rwg(sgt: np.ndarray, nt: int, z_source: bool = False) -> np.ndarray:
         x = (-2.0 * x.astype(np.float64)).astype(np.float32)
     neg = lambda a: (-1.0 * a.astype(np.float64)).astype(np.float32)
     return np.stack([x[:, 1], x[:, 0], x[:, 2], x[:, 3], neg(x[:, 5]), neg(x[:, 4])], axis=1).reshape(-1)
+
+
+def rwg_to_awp_media(p: np.ndarray, s: np.ndarray, d: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
+    """AWP media file order from RWG velocity volumes (SgtHead/src/
+    reformat_velocity.c:55-80): input x fastest, then z, then y (km/s, g/cm^3);
+    output [z][x][y][vp vs rho], y fastest, each value times 1000.0 (double
+    product stored as float)."""
+    out = np.empty((nz, nx, ny, 3), dtype=np.float32)
+    for v, a in enumerate((p, s, d)):
+        a = np.asarray(a, dtype=np.float32).reshape(ny, nz, nx)
+        out[..., v] = (a.transpose(1, 2, 0).astype(np.float64) * 1000.0).astype(np.float32)
+    return out.reshape(-1)

@@ -32,6 +32,7 @@ HEADERS = [
                                                         corr=True)),
 ]
 REFORMAT = [("sgt_x", 30, 37, 0, False), ("sgt_z", 30, 37, 1, True)]   # name, points, nt, seed, -z
+VELOCITY = [("vel_20x17x9", 20, 17, 9, 5), ("vel_33x8x5", 33, 8, 5, 6)]   # name, nx, ny, nz, seed
 
 
 def main():
@@ -54,6 +55,18 @@ def main():
         subprocess.run([os.path.join(REF, "reformat_awp"), "in.sgt", str(nt), "expected.sgt"] + (["-z"] if z else []),
                        cwd=d, check=True, capture_output=True)
         meta["reformat"].append({"name": name, "nt": nt, "z": z})
+    meta["velocity"] = []
+    for name, nx, ny, nz, seed in VELOCITY:
+        d = os.path.join(OUT, name)
+        os.makedirs(d, exist_ok=True)
+        rng = np.random.default_rng(seed)
+        vs = (0.4 + 3.6 * rng.random(ny * nz * nx)).astype(np.float32)          # km/s, RWG order y, z, x
+        (1.73 * vs).astype(np.float32).tofile(os.path.join(d, "v.p"))
+        vs.tofile(os.path.join(d, "v.s"))
+        (1.6 + rng.random(ny * nz * nx)).astype(np.float32).tofile(os.path.join(d, "v.d"))   # g/cm^3
+        subprocess.run([os.path.join(REF, "reformat_velocity"), str(nx), str(ny), str(nz), "v", "expected.media"],
+                       cwd=d, check=True, capture_output=True)
+        meta["velocity"].append({"name": name, "nx": nx, "ny": ny, "nz": nz})
     with open(os.path.join(OUT, "cases.json"), "w") as f:
         json.dump(meta, f, indent=1)
 

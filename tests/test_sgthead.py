@@ -1,11 +1,13 @@
-"""SGT post-processing formats: the RWG header file and the RWG component order.
+"""SgtHead formats on either side of the stepper: the RWG header file, the RWG
+component order of the SGTs, and AWP media built from RWG velocity volumes.
 
-Golden fixtures (tests/golden/sgthead, made by the reference's own write_head
-and reformat_awp, see make_sgthead_golden.py) pin the header writer byte for
-byte and the reorder restatement of the oracle; where the reference tools have
-been built into oracle/_ref, more cases are compared live.  The GPU tests check
-the device reordering (awp_get_sgt_rwg, the reformat_awp tool and pmcl3d's
-AWP_RWG_SGT output) against the oracle restatement."""
+Golden fixtures (tests/golden/sgthead, made by the reference's own write_head,
+reformat_awp and reformat_velocity, see make_sgthead_golden.py) pin the header
+writer byte for byte and the oracle's restatements of the two transforms;
+where the reference tools have been built into oracle/_ref, more header cases
+are compared live.  The GPU tests check the device transforms (awp_get_sgt_rwg,
+the reformat_awp and reformat_velocity tools, awp_load_media_rwg) against
+those fixtures and restatements."""
 import json
 import os
 import shutil
@@ -128,3 +130,39 @@ def test_device_rwg_image_matches_oracle_reorder(z):
     assert np.array_equal(rwg.view(np.uint32), oracle.reorder_rwg(awp, ntf, z).view(np.uint32))
     host = awpsgt.sgt_reorder_rwg(awp, ntf, z)
     assert np.array_equal(host.view(np.uint32), rwg.view(np.uint32))
+
+
+@pytest.mark.parametrize("case", CASES["velocity"], ids=lambda c: c["name"])
+def test_oracle_velocity_reformat_matches_reference_tool(case):
+    d = os.path.join(GOLD, case["name"])
+    vol = [np.fromfile(os.path.join(d, "v." + c), np.float32) for c in "psd"]
+    got = oracle.rwg_to_awp_media(*vol, case["nx"], case["ny"], case["nz"])
+    ref = np.fromfile(os.path.join(d, "expected.media"), np.float32)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES["velocity"], ids=lambda c: c["name"])
+def test_reformat_velocity_tool_on_gpu_matches_reference(case, tmp_path):
+    d = os.path.join(GOLD, case["name"])
+    r = subprocess.run([awpsgt.REFORMAT_VELOCITY_PATH, str(case["nx"]), str(case["ny"]), str(case["nz"]),
+                        os.path.join(d, "v"), str(tmp_path / "m")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(tmp_path / "m", np.float32)
+    ref = np.fromfile(os.path.join(d, "expected.media"), np.float32)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_solver_media_from_rwg_volumes_equals_awp_file():
+    case = CASES["velocity"][0]
+    d = os.path.join(GOLD, case["name"])
+    nx, ny, nz = case["ny"], case["nx"], case["nz"]          # AWP x is RWG y
+    p = awpsgt.make_params(nx, ny, nz, 100.0, 0.005, 10, igreen=(1,), nd=3, socalq=1, ntiskp_sgt=1, write_step=5)
+    fields = ("lam", "mu", "d1", "qp", "qs")
+    with awpsgt.Solver(p) as a, awpsgt.Solver(p) as b:
+        awpsgt._check(a.lib.awp_load_media_file(a.h, os.path.join(d, "expected.media").encode()))
+        b.load_media_rwg(os.path.join(d, "v"))
+        for f in fields:
+            fa, fb = a.field(f), b.field(f)
+            assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32)), f
