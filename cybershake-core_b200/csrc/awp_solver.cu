@@ -76,6 +76,9 @@ struct awp_solver {
     int kchunk;                      /* z levels per fused work item        */
     int kchunk_sweep;                /* z levels per two-sweep work item    */
     int staged_on;                   /* TMA-staged velocity/stress sweeps   */
+    size_t stagger;                  /* base-address offset step of the field arrays */
+    int nstag;
+    struct { void *user, *raw; } stag[128];
     int kchunk_staged;               /* z levels per staged work item       */
     int staged_qslow;                /* staged items: component slowest     */
     AwpStaged *staged;               /* their tensor maps (first step)      */
@@ -251,11 +254,13 @@ static float crj_high(float alpha, int nd, int n, int g)
     return expf(-(a * a));
 }
 
+static void dfree_field(awp_solver *s, void *p);
+
 static void free_media32(awp_solver *s)
 {
     for (int m = 0; m < AM_N; m++) {
         if (s->md.m[m] && (void *)s->md.m[m] != s->mdt.m[m]) {
-            cudaFree(s->md.m[m]);
+            dfree_field(s, s->md.m[m]);
             s->device_bytes -= (double)s->g.vol * 4;
         }
         s->md.m[m] = NULL;
@@ -269,8 +274,8 @@ static void free_all(awp_solver *s)
         if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
     for (int q = 0; q < AWP_MAX_COMP; q++) {
         for (int f = 0; f < AWP_NF_STATE; f++) {
-            cudaFree(s->comp[0][q].f[f]);
-            if (f < AF_R1 && s->comp[1][q].f[f] != s->comp[0][q].f[f]) cudaFree(s->comp[1][q].f[f]);
+            dfree_field(s, s->comp[0][q].f[f]);
+            if (f < AF_R1 && s->comp[1][q].f[f] != s->comp[0][q].f[f]) dfree_field(s, s->comp[1][q].f[f]);
         }
         cudaFree(s->chkj[q]);
         cudaFree(s->src_ijk[q]);
@@ -298,6 +303,36 @@ static awp_status dalloc(awp_solver *s, void **ptr, size_t bytes)
     }
     s->device_bytes += (double)bytes;
     return AWP_OK;
+}
+
+/* field arrays with staggered base addresses (AWP_TUNE_STAGGER bytes times the
+ * array's ordinal, modulo 32 ordinals), so that the same cell of different
+ * arrays does not always fall on the same DRAM channel */
+static awp_status dalloc_field(awp_solver *s, void **ptr, size_t bytes)
+{
+    const size_t off = s->stagger * (size_t)(s->nstag % 32);
+    void *raw = NULL;
+    awp_status st = dalloc(s, &raw, bytes + off);
+    if (st != AWP_OK) return st;
+    *ptr = (char *)raw + off;
+    if (off && s->nstag < 128) {
+        s->stag[s->nstag].user = *ptr;
+        s->stag[s->nstag].raw = raw;
+    }
+    s->nstag++;
+    return AWP_OK;
+}
+
+static void dfree_field(awp_solver *s, void *p)
+{
+    if (!p) return;
+    for (int n = 0; n < s->nstag && n < 128; n++)
+        if (s->stag[n].user == p && s->stag[n].raw) {
+            cudaFree(s->stag[n].raw);
+            s->stag[n].raw = NULL;
+            return;
+        }
+    cudaFree(p);
 }
 
 static awp_status check_params(const awp_params *p)
@@ -334,7 +369,7 @@ static awp_status alloc_media32(awp_solver *s)
     const size_t vb = (size_t)s->g.vol * sizeof(float);
     for (int m = 0; m < AM_N; m++) {
         if (s->md.m[m]) continue;
-        awp_status st = dalloc(s, (void **)&s->md.m[m], vb);
+        awp_status st = dalloc_field(s, (void **)&s->md.m[m], vb);
         if (st != AWP_OK) return st;
         CU(cudaMemsetAsync(s->md.m[m], 0, vb, s->stream));
         if (s->store == AWP_STORE_F32) s->mdt.m[m] = s->md.m[m];
@@ -356,6 +391,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->fused = fused_of(pin);
     s->store = store_of(pin);
     s->rstore = rstore_of(pin);
+    {
+        const int sg = env_int("AWP_TUNE_STAGGER", 0);
+        s->stagger = sg > 0 ? ((size_t)sg + 255) / 256 * 256 : 0;
+    }
     const awp_params *p = &s->p;
     const size_t vb = (size_t)s->g.vol * sizeof(float);
     const size_t rb = (size_t)s->g.vol * (s->rstore == AWP_STORE_F32 ? 4 : 2);
@@ -369,15 +408,15 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         for (int f = 0; f < AWP_NF_STATE; f++) {
             if (f >= AF_R1) {
                 if (p->nve == 0) continue;
-                TRY(dalloc(s, (void **)&s->comp[0][q].f[f], rb));
+                TRY(dalloc_field(s, (void **)&s->comp[0][q].f[f], rb));
                 TRYCU(cudaMemsetAsync(s->comp[0][q].f[f], 0, rb, s->stream));
                 s->comp[1][q].f[f] = s->comp[0][q].f[f];
                 continue;
             }
-            TRY(dalloc(s, (void **)&s->comp[0][q].f[f], vb));
+            TRY(dalloc_field(s, (void **)&s->comp[0][q].f[f], vb));
             TRYCU(cudaMemsetAsync(s->comp[0][q].f[f], 0, vb, s->stream));
             if (s->fused) {
-                TRY(dalloc(s, (void **)&s->comp[1][q].f[f], vb));
+                TRY(dalloc_field(s, (void **)&s->comp[1][q].f[f], vb));
                 TRYCU(cudaMemsetAsync(s->comp[1][q].f[f], 0, vb, s->stream));
             } else {
                 s->comp[1][q].f[f] = s->comp[0][q].f[f];

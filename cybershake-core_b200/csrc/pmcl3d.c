@@ -184,7 +184,10 @@ int main(int argc, char **argv)
 
     awp_solver *s = NULL;
     if ((st = awp_create(&p, &s)) != AWP_OK) return fail(st, "creating the solver");
-    if ((st = awp_load_media_file(s, in.invel)) != AWP_OK) return fail(st, "loading the media");
+    /* MEDIASTART 1 and 2 read INVEL; 3 reads the rank's partition file, which
+     * on one GPU is the whole domain (AWP-GPU-SGT/src/mesh.c:97-118) */
+    const char *media_path = p.mediastart == 3 ? "input_rst/mediapart/media0000000.bin" : in.invel;
+    if ((st = awp_load_media_file(s, media_path)) != AWP_OK) return fail(st, "loading the media");
     if ((st = awp_set_source(s, 0, in.nsrc, sxyz, stf)) != AWP_OK) return fail(st, "setting the source");
     if ((st = awp_set_points(s, npts, pxyz)) != AWP_OK) return fail(st, "setting the SGT points");
 
