@@ -284,7 +284,7 @@ static void free_all(awp_solver *s)
     }
     free_media32(s);
     awp_staged_destroy(s->staged);
-    for (int m = 0; m < AM_N; m++) cudaFree(s->mdt.m[m]);
+    for (int m = 0; m < AM_N; m++) dfree_field(s, s->mdt.m[m]);
     cudaFree(s->cx); cudaFree(s->cy); cudaFree(s->cz);
     cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext); cudaFree(s->rng);
     cudaFree(s->pt_idx); cudaFree(s->sg);
