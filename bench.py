@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 AWP-ODC-SGT stepper (Gcell-updates/s).
+"""Benchmark of the B200 AWP-ODC-SGT stepper (Gcell-updates/s), default
+TMA-staged two-sweep kernels (k_vel_tma, k_fsvel, k_str_tma).
 
 Workload: the batched fx+fy+fz SGT solve on a 400x400x200 grid (h = 100 m,
 dt = 0.005 s, 4000 source steps, 5000 SGT points every 10 steps), seeded
@@ -24,6 +25,10 @@ ranks' cell-updates / max-over-ranks time; scaling "weak".
 --impl reference: the reference's CPU path (the FP32 oracle; the Fortran/MPI
 reference cannot be built in this image) on rank 0, all host threads, one
 time step of one component of the same grid per bench step.
+
+Other modes: --config N (workloads 1-4), --grid / --components (reduced
+grids for profiling captures), --serve (the 64-request serving stream:
+p50/p99 latency and throughput against serial solves).
 """
 import argparse
 import json
