@@ -68,7 +68,7 @@ class Params(C.Structure):
         ("socalq", C.c_int), ("nve", C.c_int), ("mediastart", C.c_int), ("nvar", C.c_int),
         ("idyna", C.c_int), ("nst", C.c_int), ("ntiskp_sgt", C.c_int), ("write_step", C.c_int),
         ("ncomp", C.c_int), ("igreen", C.c_int * 3), ("precision", C.c_int), ("kernel", C.c_int),
-        ("device", C.c_int), ("monitor_every", C.c_int),
+        ("device", C.c_int), ("monitor_every", C.c_int), ("kinematic", C.c_int),
     ]
 
 
@@ -243,7 +243,7 @@ def _ptr(a: np.ndarray):
 def make_params(nx, ny, nz, dh, dt, nt, *, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5, socalq=0, nve=1,
                 mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10, write_step=None,
                 igreen: Sequence[int] = (1,), precision="f32", kernel="auto", device=0,
-                monitor_every=0) -> Params:
+                monitor_every=0, kinematic=0) -> Params:
     lib = load_library()
     p = Params()
     lib.awp_params_default(C.byref(p))
@@ -262,6 +262,7 @@ def make_params(nx, ny, nz, dh, dt, nt, *, nd=20, arbc=0.92, fl=0.01, fh=25.0, f
     p.kernel = KERNEL[kernel] if isinstance(kernel, str) else kernel
     p.device = device
     p.monitor_every = monitor_every
+    p.kinematic = kinematic
     return p
 
 

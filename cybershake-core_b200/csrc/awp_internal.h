@@ -93,6 +93,11 @@ struct AwpPostArgs {
     const void *d1;     /* typed density array                  */
     int media_type;     /* AWP_STORE_*                          */
     float d1_inv;       /* binary16 scale inverse               */
+    int kinematic;      /* IFAULT=5 subfault sources            */
+    float dt;
+    const void *mu;     /* typed compliance 1/mu (kinematic)     */
+    float mu_inv;
+    float *kin[3];      /* [nsrc][6] per-step stress increments  */
 };
 
 struct AwpSgtArgs {

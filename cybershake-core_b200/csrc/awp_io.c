@@ -252,6 +252,7 @@ void awp_params_from_in3d(const awp_in3d *in, awp_params *p)
     p->fl = in->fl; p->fh = in->fh; p->fp = in->fp;
     p->socalq = in->socalq; p->nve = in->nve;
     p->mediastart = in->mediarestart; p->nvar = in->nvar; p->idyna = in->idyna;
+    p->kinematic = in->ifault == 5;
     p->nst = in->nst; p->ntiskp_sgt = in->ntiskp_sgt; p->write_step = in->write_step;
     p->ncomp = 1; p->igreen[0] = in->igreen;
 }
@@ -276,7 +277,9 @@ static int next_number(FILE *f, double *v)
 
 awp_status awp_read_source(const char *path, int ifault, int nsrc, int nst, int *xyz, float *stf)
 {
-    if (ifault != 0 && ifault != 1) return ioerr(AWP_ERR_PARAM, "IFAULT %s: only 0 (text) and 1 (binary) sources are read", "");
+    if (ifault != 0 && ifault != 1 && ifault != 5)
+        return ioerr(AWP_ERR_PARAM, "IFAULT %s: only 0 (text), 1 and 5 (binary) sources are read", "");
+    if (ifault == 5) ifault = 1;   /* the subfault table has the binary IFAULT=1 layout (source.c:42-71) */
     FILE *f = fopen(path, ifault == 1 ? "rb" : "r");
     if (!f) return ioerr(AWP_ERR_IO, "cannot open source file %s", path);
     for (int s = 0; s < nsrc; s++) {

@@ -545,7 +545,7 @@ __global__ void k_post(AwpPostArgs a, int initial)
     const int q = threadIdx.x;
     const int n = initial ? 0 : (*a.step + 1);
     const int sample = initial ? 1 : n + 1;
-    if (q < a.ncomp && sample <= a.nst) {
+    if (q < a.ncomp && sample <= a.nst && !a.kinematic) {
         const AwpSrcDev &s = a.src[q];
         AwpComp &cp = a.comp[q];
         const AwpGeom &g = a.g;
@@ -904,8 +904,109 @@ cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st)
     return cudaSuccess;
 }
 
+/* ------------------------------------------------------------------ */
+/* kinematic source (IFAULT=5)                                         */
+/* ------------------------------------------------------------------ */
+
+/* moment tensor (xx yy zz xz yz xy) of a double couple, angles in radians */
+__device__ __forceinline__ void kin_mt(float str, float dip, float rake, float m[6])
+{
+    m[1] = -(sinf(dip) * cosf(rake) * sinf(2. * str) + sinf(2. * dip) * sinf(rake) * sinf(str) * sinf(str));
+    m[5] = sinf(dip) * cosf(rake) * cosf(2. * str) + 0.5 * (sinf(2. * dip) * sinf(rake) * sinf(2. * str));
+    m[4] = (cosf(dip) * cosf(rake) * cosf(str) + cosf(2. * dip) * sinf(rake) * sinf(str));
+    m[0] = sinf(dip) * cosf(rake) * sinf(2. * str) - sinf(2. * dip) * sinf(rake) * cosf(str) * cosf(str);
+    m[3] = (cosf(dip) * cosf(rake) * sinf(str) - cosf(2. * dip) * sinf(rake) * cosf(str));
+    m[2] = sinf(2. * dip) * sinf(rake);
+}
+
+/* slip-rate functions of unit area: Brune (1 / rise time = corner frequency),
+ * Liu et al. (2006) and its 2010 revision, t measured from rupture */
+__device__ __forceinline__ float kin_brune(float freq, float t)
+{
+    const float omega = freq * M_PI * 2.;
+    return t > 0. ? powf(omega, 2.f) * t * expf(-omega * t) : 0.f;
+}
+
+__device__ __forceinline__ float kin_liu(float tau, float t, int rev2010)
+{
+    const float tau1 = 0.13 * tau, tau2 = tau - tau1;
+    const float cn = rev2010 ? M_PI / (1.5 * M_PI * tau1 + 1.2 * tau1 + 0.2 * M_PI * tau2)
+                             : M_PI / (1.4 * M_PI * tau1 + 1.2 * tau1 + 0.3 * M_PI * tau2);
+    if (rev2010 && t < 0.) return 0.f;
+    if (t < tau1) return cn * (0.7 - 0.7 * cosf(M_PI * t / tau1) + 0.6 * sinf(0.5 * M_PI * t / tau1));
+    if (t < 2 * tau1)
+        return rev2010 ? cn * (1.0 - 0.8 * cosf(M_PI * t / tau1) + 0.2 * cosf(M_PI * (t - tau1) / tau2))
+                       : cn * (1.0 - 0.7 * cosf(M_PI * t / tau1) + 0.3 * cosf(M_PI * (t - tau1) / tau2));
+    if (t < tau)
+        return rev2010 ? cn * (0.2 + 0.2 * cosf(M_PI * (t - tau1) / tau2))
+                       : cn * (0.3 + 0.3 * cosf(M_PI * (t - tau1) / tau2));
+    return 0.f;
+}
+
+/* stress increments of every subfault at step n (= *step + 1), one thread per
+ * subfault: rows [type slip t_rupture t_rise area .] [strike dip rake . . .] */
+__global__ void k_kin_contrib(AwpPostArgs a)
+{
+    const int q = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.ncomp || j >= a.src[q].nsrc) return;
+    const float *r0 = a.src[q].stf + (size_t)j * 12, *r1 = r0 + 6;
+    const float atime = (*a.step + 1) * a.dt;
+    float out[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (atime > r0[2]) {
+        const int type = (int)r0[0];
+        float m[6];
+        kin_mt(r1[0] / 180. * M_PI, r1[1] / 180. * M_PI, r1[2] / 180. * M_PI, m);
+        float stf = 0.f;
+        if (type == 1) stf = kin_brune(1. / r0[3], atime - r0[2]);
+        else if (type == 2) stf = kin_liu(r0[3], atime - r0[2], 0);
+        else if (type == 3) stf = kin_liu(r0[3], atime - r0[2], 1);
+        const int *ijk = a.src[q].ijk + 3 * j;
+        const int c = a.g.idx(ijk[0], ijk[1], ijk[2]);
+        float mu;
+        switch (a.media_type) {
+        case 1: mu = __bfloat162float(((const __nv_bfloat16 *)a.mu)[c]); break;
+        case 2: mu = __half2float(((const __half *)a.mu)[c]) * a.mu_inv; break;
+        default: mu = ((const float *)a.mu)[c];
+        }
+        stf *= r0[1] * r0[4] / mu;
+        stf *= a.vtst;
+        for (int v = 0; v < 6; ++v) out[v] = stf * m[v];
+    }
+    float *o = a.kin[q] + (size_t)j * 6;
+    for (int v = 0; v < 6; ++v) o[v] = out[v];
+}
+
+/* applies the increments in subfault order (one thread per component), so
+ * subfaults that share a cell add up in a fixed order */
+__global__ void k_kin_apply(AwpPostArgs a)
+{
+    const int q = threadIdx.x;
+    if (q >= a.ncomp) return;
+    AwpComp &cp = a.comp[q];
+    for (int j = 0; j < a.src[q].nsrc; ++j) {
+        const int *ijk = a.src[q].ijk + 3 * j;
+        const int c = a.g.idx(ijk[0], ijk[1], ijk[2]);
+        const float *d = a.kin[q] + (size_t)j * 6;
+        cp.f[AF_XX][c] = cp.f[AF_XX][c] - d[0];
+        cp.f[AF_YY][c] = cp.f[AF_YY][c] - d[1];
+        cp.f[AF_ZZ][c] = cp.f[AF_ZZ][c] - d[2];
+        cp.f[AF_XZ][c] = cp.f[AF_XZ][c] - d[3];
+        cp.f[AF_YZ][c] = cp.f[AF_YZ][c] - d[4];
+        cp.f[AF_XY][c] = cp.f[AF_XY][c] - d[5];
+    }
+}
+
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st)
 {
+    if (a.kinematic && !initial) {
+        int nmax = 0;
+        for (int q = 0; q < a.ncomp; ++q) nmax = a.src[q].nsrc > nmax ? a.src[q].nsrc : nmax;
+        if (nmax > 0) {
+            k_kin_contrib<<<dim3((nmax + 127) / 128, a.ncomp), 128, 0, st>>>(a);
+            k_kin_apply<<<1, 32, 0, st>>>(a);
+        }
+    }
     k_post<<<1, 32, 0, st>>>(a, initial);
     return cudaGetLastError();
 }

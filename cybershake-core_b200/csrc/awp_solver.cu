@@ -76,6 +76,7 @@ struct awp_solver {
     int kchunk;                      /* z levels per fused work item        */
     int kchunk_sweep;                /* z levels per two-sweep work item    */
     int staged_on;                   /* TMA-staged velocity/stress sweeps   */
+    float *kin[AWP_MAX_COMP];        /* kinematic subfault increments       */
     size_t stagger;                  /* base-address offset step of the field arrays */
     int nstag;
     struct { void *user, *raw; } stag[128];
@@ -280,6 +281,7 @@ static void free_all(awp_solver *s)
         cudaFree(s->chkj[q]);
         cudaFree(s->src_ijk[q]);
         cudaFree(s->src_stf[q]);
+        cudaFree(s->kin[q]);
         cudaFree(s->sgt_file[q]);
     }
     free_media32(s);
@@ -346,6 +348,9 @@ static awp_status check_params(const awp_params *p)
     if (p->nst < 0) return set_err(AWP_ERR_PARAM, "NST must be >= 0");
     if (p->nvar != 3 && p->nvar != 5 && p->nvar != 8) return set_err(AWP_ERR_PARAM, "NVAR must be 3, 5 or 8");
     if (p->nve != 0 && p->nve != 1) return set_err(AWP_ERR_PARAM, "NVE must be 0 or 1");
+    if (p->kinematic != 0 && p->kinematic != 1) return set_err(AWP_ERR_PARAM, "kinematic must be 0 or 1");
+    if (p->kinematic && p->nst != 2)
+        return set_err(AWP_ERR_PARAM, "a kinematic source (IFAULT=5) needs NST = 2 (two rows per subfault)");
     if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_MIXED) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
     if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_STAGED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
     if (p->kernel == AWP_KERNEL_STAGED && store_of(p) != AWP_STORE_F32)
@@ -827,6 +832,7 @@ extern "C" awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const in
         if (s->graph[b]) { cudaGraphExecDestroy(s->graph[b]); s->graph[b] = NULL; }
     cudaFree(s->src_ijk[comp]); s->src_ijk[comp] = NULL;
     cudaFree(s->src_stf[comp]); s->src_stf[comp] = NULL;
+    cudaFree(s->kin[comp]); s->kin[comp] = NULL;
     s->nsrc[comp] = nsrc;
     if (nsrc == 0) return AWP_OK;
     int *ijk = (int *)malloc(sizeof(int) * 3 * (size_t)nsrc);
@@ -837,6 +843,7 @@ extern "C" awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const in
     }
     awp_status st = dalloc(s, (void **)&s->src_ijk[comp], sizeof(int) * 3 * (size_t)nsrc);
     if (st == AWP_OK) st = dalloc(s, (void **)&s->src_stf[comp], sizeof(float) * 6 * (size_t)nsrc * (size_t)(p->nst > 0 ? p->nst : 1));
+    if (st == AWP_OK && p->kinematic) st = dalloc(s, (void **)&s->kin[comp], sizeof(float) * 6 * (size_t)nsrc);
     if (st == AWP_OK) {
         cudaError_t e = cudaMemcpy(s->src_ijk[comp], ijk, sizeof(int) * 3 * (size_t)nsrc, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && p->nst > 0)
@@ -926,6 +933,10 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     pa.probe = (q0 <= p->nx && q0 <= p->ny && q0 <= p->nz) ? q0 : 0;
     pa.step = s->step;
     pa.d1 = s->mdt.m[AM_D1];
+    pa.kinematic = p->kinematic;
+    pa.dt = p->dt;
+    pa.mu = s->mdt.m[AM_MU];
+    pa.mu_inv = s->mdt.sc.inv[AM_MU];
     pa.media_type = s->mdt.type;
     pa.d1_inv = s->mdt.sc.inv[AM_D1];
     for (int q = 0; q < p->ncomp; q++) {
@@ -934,6 +945,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
         pa.src[q].nsrc = s->nsrc[q];
         pa.src[q].ijk = s->src_ijk[q];
         pa.src[q].stf = s->src_stf[q];
+        pa.kin[q] = s->kin[q];
         pa.comp[q] = s->comp[wr][q];
     }
 

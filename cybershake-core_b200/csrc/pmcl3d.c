@@ -157,7 +157,14 @@ int main(int argc, char **argv)
     awp_status st = awp_parse_command_line(argc, argv, &in);
     if (st != AWP_OK) return fail(st, "reading parameters");
     if (in.npc != 0) { fprintf(stderr, "pmcl3d: NPC=1 (PML) is not supported; use the Cerjan sponge (NPC=0)\n"); return 1; }
-    if (in.ifault != 0 && in.ifault != 1) { fprintf(stderr, "pmcl3d: IFAULT=%d is not supported (0 or 1)\n", in.ifault); return 1; }
+    if (in.ifault != 0 && in.ifault != 1 && in.ifault != 5) {
+        fprintf(stderr, "pmcl3d: IFAULT=%d is not supported (0, 1 or 5)\n", in.ifault);
+        return 1;
+    }
+    if (in.ifault == 5 && in.nst != 2) {   /* AWP-GPU-SGT/src/pmcl3d.c:509-515 */
+        fprintf(stderr, "pmcl3d: IFAULT=5 requires NST = READ_STEP = 2\n");
+        return 1;
+    }
 
     awp_params p;
     awp_params_from_in3d(&in, &p);

@@ -99,6 +99,14 @@ typedef struct {
     int kernel;              /* awp_kernel                                   */
     int device;              /* CUDA device ordinal                          */
     int monitor_every;       /* stability check period in steps (0 = off)    */
+    int kinematic;           /* 1: IFAULT=5 kinematic source -- each source
+                                row pair is a subfault (stf type, slip,
+                                rupture time, rise time, area | strike, dip,
+                                rake; NST = 2) whose moment rate is inserted
+                                into the stresses after every stress update
+                                (AWP-GPU-SGT kernel_kp1_fix_havg_ifault5.cu:
+                                289-376); IGREEN then only selects the SGT
+                                output                                        */
 } awp_params;
 
 typedef struct {

@@ -68,6 +68,7 @@ typedef struct {
     int ntiskp_sgt;
     int write_step;
     int igreen;
+    int kinematic;   /* 1: IFAULT=5 subfault sources (NST = 2) */
 } orc_params;
 
 enum { F_U1, F_V1, F_W1, F_XX, F_YY, F_ZZ, F_XY, F_XZ, F_YZ,
@@ -187,6 +188,7 @@ orc_t *orc_create(const orc_params *p)
 {
     if (p->nx < 4 || p->ny < 4 || p->nz < 4 || p->nd < 1 || p->dt <= 0 || p->dh <= 0) return NULL;
     if (p->ntiskp_sgt < 1 || p->write_step < 1 || p->nt < 1) return NULL;
+    if (p->kinematic && p->nst != 2) return NULL;   /* two rows per subfault */
     orc_t *h = calloc(1, sizeof(orc_t));
     h->p = *p;
     h->sx = p->nx + 4; h->sy = p->ny + 4; h->sz = p->nz + 4;
@@ -771,6 +773,82 @@ static void orc_sgt_sample(orc_t *h, int it)
     }
 }
 
+/* IFAULT=5 kinematic source, AWP-GPU-SGT/src/kernel_kp1_fix_havg_ifault5.cu:
+ * 210-376 (compmt, brune, liu, gp10, addkinsrc_cu): after the stress update of
+ * step it, every subfault whose rupture time has passed adds its moment rate
+ * (slip x area x mu x slip-rate function) times the double-couple tensor of
+ * its strike, dip and rake, in subfault order.  The FP32 build follows the
+ * float / double evaluation points of the CUDA code with the C library's
+ * sinf / cosf / expf / powf; the FP64 build evaluates everything in double. */
+#if ORC_IS_DOUBLE
+#define KSIN sin
+#define KCOS cos
+#define KEXP exp
+#define KPOW pow
+#else
+#define KSIN sinf
+#define KCOS cosf
+#define KEXP expf
+#define KPOW powf
+#endif
+static void orc_kin_mt(real str, real dip, real rake, real m[6])
+{
+    m[1] = -(KSIN(dip) * KCOS(rake) * KSIN(2. * str) + KSIN(2. * dip) * KSIN(rake) * KSIN(str) * KSIN(str));
+    m[5] = KSIN(dip) * KCOS(rake) * KCOS(2. * str) + 0.5 * (KSIN(2. * dip) * KSIN(rake) * KSIN(2. * str));
+    m[4] = (KCOS(dip) * KCOS(rake) * KCOS(str) + KCOS(2. * dip) * KSIN(rake) * KSIN(str));
+    m[0] = KSIN(dip) * KCOS(rake) * KSIN(2. * str) - KSIN(2. * dip) * KSIN(rake) * KCOS(str) * KCOS(str);
+    m[3] = (KCOS(dip) * KCOS(rake) * KSIN(str) - KCOS(2. * dip) * KSIN(rake) * KCOS(str));
+    m[2] = KSIN(2. * dip) * KSIN(rake);
+}
+
+static real orc_kin_stf(int type, real rise, real t)
+{
+    const double pi = 3.14159265358979323846;
+    if (type == 1) {
+        const real freq = 1. / rise;
+        const real omega = freq * pi * 2.;
+        return t > 0. ? KPOW(omega, (real)2.) * t * KEXP(-omega * t) : (real)0.;
+    }
+    if (type != 2 && type != 3) return 0;
+    const int rev = type == 3;
+    const real tau1 = 0.13 * rise, tau2 = rise - tau1;
+    const real cn = rev ? pi / (1.5 * pi * tau1 + 1.2 * tau1 + 0.2 * pi * tau2)
+                        : pi / (1.4 * pi * tau1 + 1.2 * tau1 + 0.3 * pi * tau2);
+    if (rev && t < 0.) return 0;
+    if (t < tau1) return cn * (0.7 - 0.7 * KCOS(pi * t / tau1) + 0.6 * KSIN(0.5 * pi * t / tau1));
+    if (t < 2 * tau1)
+        return rev ? cn * (1.0 - 0.8 * KCOS(pi * t / tau1) + 0.2 * KCOS(pi * (t - tau1) / tau2))
+                   : cn * (1.0 - 0.7 * KCOS(pi * t / tau1) + 0.3 * KCOS(pi * (t - tau1) / tau2));
+    if (t < rise)
+        return rev ? cn * (0.2 + 0.2 * KCOS(pi * (t - tau1) / tau2)) : cn * (0.3 + 0.3 * KCOS(pi * (t - tau1) / tau2));
+    return 0;
+}
+
+static void orc_addkinsrc(orc_t *h, int it)
+{
+    const orc_params *p = &h->p;
+    const double pi = 3.14159265358979323846;
+    const real dx = (real)p->dh;
+    const real vtst = (real)p->dt / (dx * dx * dx);
+    const real atime = it * (real)p->dt;
+    for (int s = 0; s < h->nsrc; s++) {
+        const float *r0 = h->stf + (size_t)s * 12, *r1 = r0 + 6;
+        if (!(atime > r0[2])) continue;
+        real m[6];
+        orc_kin_mt(r1[0] / 180. * pi, r1[1] / 180. * pi, r1[2] / 180. * pi, m);
+        real stf = orc_kin_stf((int)r0[0], r0[3], atime - r0[2]);
+        const size_t c = IDX(h, h->src[3 * s], h->src[3 * s + 1], h->src[3 * s + 2]);
+        stf *= (real)r0[1] * (real)r0[4] / h->f[F_MU][c];
+        stf *= vtst;
+        h->f[F_XX][c] = h->f[F_XX][c] - stf * m[0];
+        h->f[F_YY][c] = h->f[F_YY][c] - stf * m[1];
+        h->f[F_ZZ][c] = h->f[F_ZZ][c] - stf * m[2];
+        h->f[F_XZ][c] = h->f[F_XZ][c] - stf * m[3];
+        h->f[F_YZ][c] = h->f[F_YZ][c] - stf * m[4];
+        h->f[F_XY][c] = h->f[F_XY][c] - stf * m[5];
+    }
+}
+
 static void orc_one_step(orc_t *h, int it)
 {
     const orc_params *p = &h->p;
@@ -779,7 +857,10 @@ static void orc_one_step(orc_t *h, int it)
     orc_fvel(h);
     if (p->nve == 1) orc_dstrqc(h); else orc_dstrc(h);
     orc_addcrj(h, F_XX, F_YZ);
-    if (p->igreen >= 4 && p->igreen <= 6) {
+    if (p->kinematic) {
+        orc_fstr(h);
+        orc_addkinsrc(h, it);
+    } else if (p->igreen >= 4 && p->igreen <= 6) {
         orc_fstr(h);
         orc_addsrc(h, it + 1);
     } else {
@@ -803,7 +884,7 @@ int orc_run(orc_t *h, int nsteps)
 {
     if (!h->started) {
         orc_sgt_coeffs(h);
-        orc_addsrc(h, 1);
+        if (!h->p.kinematic) orc_addsrc(h, 1);
         h->started = 1;
     }
     for (int s = 0; s < nsteps && h->cur < h->p.nt; s++) {

@@ -86,6 +86,10 @@ def test_bad_parameters_rejected_before_any_device_call():
     with pytest.raises(awpsgt.AwpError) as e:
         awpsgt.Solver(p)
     assert e.value.status == 2
+    p = awpsgt.make_params(48, 40, 32, 200.0, 0.01, 10, nst=3, igreen=(1,), kinematic=1, ntiskp_sgt=1)
+    with pytest.raises(awpsgt.AwpError) as e:   # IFAULT=5 subfaults are two rows each
+        awpsgt.Solver(p)
+    assert e.value.status == 2 and "NST = 2" in str(e.value)
     for prec in ("bf16", "f16"):           # the staged stepper reads FP32 media only
         p = awpsgt.make_params(64, 64, 64, 100.0, 0.005, 10, ntiskp_sgt=1, precision=prec, kernel="staged")
         with pytest.raises(awpsgt.AwpError) as e:

@@ -276,3 +276,55 @@ def test_config1_full_run_bit_exact():
     assert np.abs(ref).max() > 0
     assert bits_equal(gpu, ref), rel_l2(gpu, ref)
     assert bits_equal(chkj, o.chkj())
+
+
+def kinematic_rupture(n, seed=5, dt=0.01):
+    """n subfaults: rows [type slip t_rupture t_rise area 0] [strike dip rake 0 0 0],
+    the three slip-rate functions in turn."""
+    rng = np.random.default_rng(seed)
+    t = np.zeros((n, 2, 6), np.float32)
+    t[:, 0, 0] = 1 + np.arange(n) % 3
+    t[:, 0, 1] = rng.uniform(0.5, 2.0, n)                 # slip (m)
+    t[:, 0, 2] = rng.uniform(0.0, 15 * dt, n)             # rupture time (s)
+    t[:, 0, 3] = rng.uniform(5 * dt, 20 * dt, n)          # rise time (s)
+    t[:, 0, 4] = rng.uniform(1e4, 4e4, n)                 # area (m^2)
+    t[:, 1, 0] = rng.uniform(0.0, 360.0, n)               # strike, dip, rake (degrees)
+    t[:, 1, 1] = rng.uniform(10.0, 90.0, n)
+    t[:, 1, 2] = rng.uniform(-180.0, 180.0, n)
+    return t
+
+
+@pytest.mark.parametrize("kernel", ["staged", "two_sweep"])
+def test_kinematic_source_matches_oracle(kernel):
+    """IFAULT=5: subfault moment rates inserted after every stress update.  The
+    CUDA and C-library sinf/cosf/expf/powf differ in the last bits, so the
+    bar is a tolerance (rel-L2 <= 1e-5 against the FP32 oracle, <= 1e-4
+    against FP64), not bit equality."""
+    nx, ny, nz, nt, dt = 48, 40, 32, 60, 0.01
+    xyz = [(16 + 2 * k, 20 + (k % 3), 12 + (k % 4)) for k in range(12)] + [(20, 20, 12)]   # one shared cell
+    tab = kinematic_rupture(len(xyz), dt=dt)
+    media = ai.layered_media(nx, ny, nz, 200.0, seed=3, pert_std=0.05, corr_len=1000.0)
+    pts = ai.sgt_points(nx, ny, 20, 50, seed=0)
+    kw = dict(nd=8, socalq=1, ntiskp_sgt=5, write_step=4, fl=0.01, fh=25.0, fp=0.5)
+    p = awpsgt.make_params(nx, ny, nz, 200.0, dt, nt, nst=2, igreen=(1,), kernel=kernel, kinematic=1, **kw)
+    with awpsgt.Solver(p) as s:
+        s.load_media(media)
+        s.set_source(0, xyz, tab)
+        s.set_points(pts)
+        s.run(nt)
+        g = s.sgt(0)
+        gxx = s.field("xx")
+    refs = {}
+    for prec in ("f32", "f64"):
+        o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=200.0, dt=dt, nt=nt, nst=2, igreen=1, kinematic=1,
+                          precision=prec, **kw)
+        o.load_media(media)
+        o.set_source(xyz, tab)
+        o.set_points(pts)
+        o.run(nt)
+        refs[prec] = (o.sgt(), o.field("xx"))
+    assert np.abs(g).max() > 0
+    assert rel_l2(g, refs["f32"][0]) <= 1e-5
+    assert rel_l2(gxx, refs["f32"][1]) <= 1e-5
+    assert rel_l2(g, refs["f64"][0]) <= 1e-4
+
