@@ -139,3 +139,42 @@ def test_rwg_order_output(tmp_path):
     got = np.fromfile(tmp_path / "out" / "sgt" / "awp-strain", dtype=np.float32)
     ref = oracle.reorder_rwg(oracle_sgt(media, stf, pts).sgt(), 12)
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_gpu_command_line_kinematic_source(tmp_path):
+    """IFAULT=5 with the GPU command line: a binary subfault table (two rows of
+    six per subfault, NST = READ_STEP = 2) drives the run; the SGT chunk files
+    match the oracle within the tolerance of the kinematic tests."""
+    from test_gpu_parity import kinematic_rupture, rel_l2
+    media, _, pts = write_inputs(tmp_path)
+    xyz = [(18 + k, 20, 10 + k % 3) for k in range(8)]
+    tab = kinematic_rupture(len(xyz), seed=9)
+    with open(tmp_path / "input" / "kin", "wb") as f:
+        for k, (x, y, z) in enumerate(xyz):
+            np.asarray((x, y, z), np.int32).tofile(f)
+            tab[k].astype(np.float32).tofile(f)
+    argv = [awpsgt.PMCL3D_PATH, "-T", "0.6", "--IGREEN", "1", "--DH", "200.0", "--DT", "0.01", "--NSRC", str(len(xyz)),
+            "--NST", "2", "-X", str(NX), "-Y", str(NY), "-Z", str(NZ), "-x", "1", "-y", "1", "--NPC", "0",
+            "--ARBC", "0.92", "--ND", "8", "--IFAULT", "5", "--MEDIASTART", "1", "--FL", "0.01", "--FH", "25.0",
+            "--FP", "0.5", "--READ_STEP", "2", "--WRITE_STEP", "4", "-o", "out_kin", "--INSGT", "input/cord",
+            "-c", "out_kin/CHKP", "--INSRC", "input/kin", "--INVEL", "input/media", "--NTISKP_SGT", "5",
+            "--NTISKP", "10"]
+    r = subprocess.run(argv, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    nt = int(np.float32(0.6) / np.float32(0.01)) + 1
+    o = oracle.Oracle(nx=NX, ny=NY, nz=NZ, dh=200.0, dt=0.01, nt=nt, nst=2, nd=8, fl=0.01, fh=25.0, fp=0.5,
+                      socalq=1, ntiskp_sgt=5, write_step=4, igreen=1, kinematic=1)
+    o.load_media(media)
+    o.set_source(xyz, tab)
+    o.set_points(pts)
+    o.run(nt)
+    ref = o.sgt().reshape(30, 6, -1)
+    got = np.concatenate([np.fromfile(tmp_path / "out_kin" / ("SGT%07d" % ((c + 1) * 20)), np.float32).reshape(30, 6, 4)
+                          for c in range((nt // 5) // 4)], axis=2)
+    assert np.abs(got).max() > 0
+    assert rel_l2(got, ref[:, :, :got.shape[2]]) <= 1e-5
+    bad = argv[:]
+    bad[bad.index("--NST") + 1] = "3"
+    r = subprocess.run(bad, cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "NST" in r.stderr
