@@ -30,6 +30,7 @@ struct AwpStepArgs {
     const AwpStaged *staged;     /* non-NULL: TMA-staged velocity/stress    */
     int kchunk_staged;           /* z levels per staged work item           */
     int staged_qslow;            /* staged items: one component at a time   */
+    int staged_rpt;              /* staged stress sweep: tile rows per thread */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

@@ -82,6 +82,7 @@ struct awp_solver {
     struct { void *user, *raw; } stag[128];
     int kchunk_staged;               /* z levels per staged work item       */
     int staged_qslow;                /* staged items: component slowest     */
+    int staged_rpt;                  /* staged stress sweep rows per thread */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -487,6 +488,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         const int kc = env_int("AWP_TUNE_KSTAGE", 32);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
         s->staged_qslow = env_int("AWP_TUNE_QSLOW", 1) != 0;
+        s->staged_rpt = env_int("AWP_TUNE_RPT", 1) == 2 ? 2 : 1;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -924,6 +926,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged = s->staged_on ? s->staged : NULL;
     a.kchunk_staged = s->kchunk_staged;
     a.staged_qslow = s->staged_qslow;
+    a.staged_rpt = s->staged_rpt;
     a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);

@@ -184,12 +184,12 @@ __device__ __forceinline__ float *ring_base(unsigned char *raw)
 }
 
 template <int S>
-__device__ __forceinline__ void ring_init(uint64_t *full, uint64_t *empty, volatile int *abort)
+__device__ __forceinline__ void ring_init(uint64_t *full, uint64_t *empty, volatile int *abort, int consumers = ST_CW)
 {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         for (int s = 0; s < S; ++s) {
             mb_init(&full[s], 1);
-            mb_init(&empty[s], ST_CW);
+            mb_init(&empty[s], consumers);
         }
         mb_fence_init();
         *abort = 0;
@@ -426,15 +426,18 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
     }
 }
 
-/* work items: (x tile, y tile, z chunk, component); see split_item for the order */
-template <class TR, int UNR>
-__global__ void __launch_bounds__(ST_THREADS, 3)
+/* work items: (x tile, y tile, z chunk, component); see split_item for the order.
+ * RPT rows of the tile per consumer thread (ST_Y / RPT consumer warps): with
+ * RPT = 2 a thread carries two independent cells per level. */
+template <class TR, int UNR, int RPT>
+__global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
     constexpr int S = 2 + STR_D;      /* levels k-1 and k in use, STR_D in flight */
     constexpr int RSIZE = (int)sizeof(TR);
+    constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
     float *ring = ring_base(st_smem);
     uint64_t *full = (uint64_t *)(ring + S * STR_SLOT), *empty = full + S;
@@ -444,10 +447,10 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
 #pragma unroll
         for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
-    ring_init<S>(full, empty, &abort_s);
+    ring_init<S>(full, empty, &abort_s, CW);
     const int tx = threadIdx.x, ty = threadIdx.y;
 
-    if (ty == ST_CW) {                /* producer warp */
+    if (ty == CW) {                   /* producer warp */
         if (tx != 0) return;
         uint32_t use = 0;
         bool ok = true;
@@ -470,35 +473,45 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
         return;
     }
 
-    const int sz = g.plane;
-    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
+    const int sz = g.plane, sy = g.px;
     uint32_t use0 = 0;                /* ring use of the item's first level */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
         int q, t;
-            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
+        split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
         int bx, by, k0, k1;
         work_item(g, w, t, bx, by, k0, k1);
-        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
-        const bool live = i <= g.nx && j <= g.ny;
+        const int i = bx * ST_X + 1 + tx;
         const int np = k1 - k0 + 2;   /* levels k0-1 .. k1 */
         const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
-        /* column queues: u, v at k+1, k+2 (and k+3 loaded one level ahead), w at k-2 and k+1 (k+2 ahead) */
-        float up1 = 0.f, up2 = 0.f, vp1 = 0.f, vp2 = 0.f, wm2 = 0.f, wp1 = 0.f, cxy = 0.f;
-        const int itxy = ((j & 1) << 1) | (i & 1);
-        int c = g.idx(i, j, k0);
-        if (live) {
-            up1 = U[c + sz]; up2 = U[c + 2 * sz];
-            vp1 = V[c + sz]; vp2 = V[c + 2 * sz];
-            wm2 = W[c - 2 * sz]; wp1 = W[c + sz];
-            cxy = cx[i] * cy[j];
+        /* per row: column queues u, v at k+1, k+2 (k+3 loaded one level ahead), w at k-2, k+1 (k+2 ahead) */
+        float up1[RPT], up2[RPT], vp1[RPT], vp2[RPT], wm2[RPT], wp1[RPT], cxy[RPT];
+        bool live[RPT];
+        int itxy[RPT];
+        const int c0 = g.idx(i, by * ST_Y + 1 + ty, k0);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int j = by * ST_Y + 1 + ty + r * CW, c = c0 + r * CW * sy;
+            live[r] = i <= g.nx && j <= g.ny;
+            itxy[r] = ((j & 1) << 1) | (i & 1);
+            up1[r] = up2[r] = vp1[r] = vp2[r] = wm2[r] = wp1[r] = cxy[r] = 0.f;
+            if (live[r]) {
+                up1[r] = U[c + sz]; up2[r] = U[c + 2 * sz];
+                vp1[r] = V[c + sz]; vp2[r] = V[c + 2 * sz];
+                wm2[r] = W[c - 2 * sz]; wp1[r] = W[c + sz];
+                cxy[r] = cx[i] * cy[j];
+            }
         }
+        int cc = c0;
 #pragma unroll (UNR)
-        for (int k = k0; k <= k1; ++k, c += sz) {
+        for (int k = k0; k <= k1; ++k, cc += sz) {
             const uint32_t use = use0 + (uint32_t)(k - k0 + 1), usem = use - 1;
-            float up3 = 0.f, vp3 = 0.f, wp2 = 0.f, czk = 0.f;
-            if (live) {
-                if (k < k1) { up3 = U[c + 3 * sz]; vp3 = V[c + 3 * sz]; wp2 = W[c + 2 * sz]; }
-                czk = cz[k];
+            float up3[RPT], vp3[RPT], wp2[RPT];
+            const float czk = cz[k];
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int c = cc + r * CW * sy;
+                up3[r] = vp3[r] = wp2[r] = 0.f;
+                if (live[r] && k < k1) { up3[r] = U[c + 3 * sz]; vp3[r] = V[c + 3 * sz]; wp2[r] = W[c + 2 * sz]; }
             }
             bool ok = true;
             if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s);
@@ -509,53 +522,63 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                 return;
             }
             const float *sk = ring + (use % S) * STR_SLOT, *sm = ring + (usem % S) * STR_SLOT;
-            const float wm1 = sm[2 * ST_VT + cv];
-            if (live) {
-                const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;   /* viscoop.f:93-101 */
-                const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
-                const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
-                const float *ps = sk + STR_ST + cp;
-                const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
-                const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1, up2, vp1, vp2, wm2, wp1};
-                Stress6 o;
-                if (nve == 1) {
-                    const TR *pr = (const TR *)(sk + STR_ST + 6 * ST_PT) + cp;
-                    float r[6];
+            const int ipar = ((g.nz + 1 - k) & 1) << 2;                    /* viscoop.f:93-101 */
 #pragma unroll
-                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
-                    const VelDiff dd = vel_diff(Vq);
-                    o = str_visco(kc, dd, s0, r, dth, dt, dh1);
+            for (int r = 0; r < RPT; ++r) {
+                const int row = ty + r * CW, c = cc + r * CW * sy;
+                const int cv = (row + 2) * ST_W + tx + 4, cm = (row + 1) * ST_W + tx + 4, cp = row * ST_X + tx;
+                const float wm1 = sm[2 * ST_VT + cv];
+                if (live[r]) {
+                    const int it = ipar | itxy[r];
+                    const TMed M{sk + 3 * ST_VT + cm, sm + 3 * ST_VT + cm};
+                    const StrCoef kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
+                    const float *ps = sk + STR_ST + cp;
+                    const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
+                    const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1[r], up2[r], vp1[r], vp2[r], wm2[r], wp1[r]};
+                    Stress6 o;
+                    if (nve == 1) {
+                        const TR *pr = (const TR *)(sk + STR_ST + 6 * ST_PT) + cp;
+                        float rr[6];
 #pragma unroll
-                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, r[a], 1.0f);
-                } else {
-                    o = str_elastic(kc, Vq, s0, dth);
+                        for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
+                        const VelDiff dd = vel_diff(Vq);
+                        o = str_visco(kc, dd, s0, rr, dth, dt, dh1);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, rr[a], 1.0f);
+                    } else {
+                        o = str_elastic(kc, Vq, s0, dth);
+                    }
+                    const float crj = cxy[r] * czk;
+                    tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj; tab[q].f[AF_ZZ][c] = o.zz * crj;
+                    tab[q].f[AF_XY][c] = o.xy * crj; tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
                 }
-                const float crj = cxy * czk;
-                tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj; tab[q].f[AF_ZZ][c] = o.zz * crj;
-                tab[q].f[AF_XY][c] = o.xy * crj; tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
+                up1[r] = up2[r]; up2[r] = up3[r];
+                vp1[r] = vp2[r]; vp2[r] = vp3[r];
+                wm2[r] = wm1; wp1[r] = wp2[r];
             }
-            up1 = up2; up2 = up3;
-            vp1 = vp2; vp2 = vp3;
-            wm2 = wm1; wp1 = wp2;
             __syncwarp();
             if (tx == 0) mb_arrive(&empty[usem % S]);
         }
         __syncwarp();
         if (tx == 0) mb_arrive(&empty[(use0 + np - 1) % S]);
         use0 += np;
-        if (live && k1 == g.nz) {
-            /* fstr (operator.f:594-606) on this thread's own column; the top
-             * chunk holds at least levels nz-2..nz, all written by this thread */
-            const int ct = g.idx(i, j, g.nz);
-            float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
-            ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
-            ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
-            XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
-            XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
-            YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
-            YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
-            XZ[ct] = 0.0f;
-            YZ[ct] = 0.0f;
+        if (k1 == g.nz) {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                if (!live[r]) continue;
+                /* fstr (operator.f:594-606) on this thread's own column; the top
+                 * chunk holds at least levels nz-2..nz, all written by this thread */
+                const int ct = g.idx(i, by * ST_Y + 1 + ty + r * CW, g.nz);
+                float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
+                ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+                ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+                XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+                XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+                YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+                YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+                XZ[ct] = 0.0f;
+                YZ[ct] = 0.0f;
+            }
         }
     }
 }
@@ -640,13 +663,13 @@ static AwpWork staged_work(const AwpGeom &g, int kchunk, int ncomp)
 }
 
 template <class K>
-static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid)
+static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid, int threads = ST_THREADS)
 {
     int dev = 0, nsm = 148, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, ST_THREADS, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
     if (e != cudaSuccess) return e;
     if (per < 1) return cudaErrorInvalidConfiguration;
     *grid = nsm * per < nitems ? nsm * per : nitems;
@@ -678,18 +701,25 @@ static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaS
     return cudaGetLastError();
 }
 
-template <class TR, int UNR>
-static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+template <class TR, int UNR, int RPT>
+static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
+    constexpr int CW = ST_Y / RPT;
     const size_t smem = ring_bytes(2 + STR_D, STR_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_str_tma<TR, UNR>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_str_tma<TR, UNR, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
-    k_str_tma<TR, UNR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
-                                                                     s.staged_qslow, s.cx, s.cy, s.cz, s.tau, s.dth,
-                                                                     s.dt, s.dh1, w, s.nve, s.kerr);
+    k_str_tma<TR, UNR, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
+                                                                       s.staged_qslow, s.cx, s.cy, s.cz, s.tau,
+                                                                       s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
+}
+
+template <class TR, int UNR>
+static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    return s.staged_rpt == 2 ? launch_str_rpt<TR, UNR, 2>(st, s, stream) : launch_str_rpt<TR, UNR, 1>(st, s, stream);
 }
 
 /* level loops unrolled twice unless asked otherwise: the column queues then
