@@ -488,7 +488,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         const int kc = env_int("AWP_TUNE_KSTAGE", 32);
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
         s->staged_qslow = env_int("AWP_TUNE_QSLOW", 1) != 0;
-        s->staged_rpt = env_int("AWP_TUNE_RPT", 1) == 2 ? 2 : 1;
+        /* stress sweep rows per consumer thread: two pay off once three
+         * components share the sweep with FP32 memory variables */
+        const int rpt = env_int("AWP_TUNE_RPT", 0);
+        s->staged_rpt = rpt == 1 || rpt == 2 ? rpt : (p->ncomp == 3 && s->rstore == AWP_STORE_F32 ? 2 : 1);
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;

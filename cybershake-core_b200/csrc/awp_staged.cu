@@ -716,10 +716,13 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
     return cudaGetLastError();
 }
 
-template <class TR, int UNR>
+/* two rows per thread carry twice the live state already: that variant keeps
+ * its level loop rolled (unrolled twice it needs 128 registers and runs slower) */
+template <class TR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
-    return s.staged_rpt == 2 ? launch_str_rpt<TR, UNR, 2>(st, s, stream) : launch_str_rpt<TR, UNR, 1>(st, s, stream);
+    if (s.staged_rpt == 2) return launch_str_rpt<TR, 1, 2>(st, s, stream);
+    return s.unroll == 1 ? launch_str_rpt<TR, 1, 1>(st, s, stream) : launch_str_rpt<TR, 2, 1>(st, s, stream);
 }
 
 /* level loops unrolled twice unless asked otherwise: the column queues then
@@ -733,8 +736,6 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
-    if (s.rtype == AWP_STORE_BF16)
-        return s.unroll == 1 ? launch_str_tr<__nv_bfloat16, 1>(st, s, stream)
-                             : launch_str_tr<__nv_bfloat16, 2>(st, s, stream);
-    return s.unroll == 1 ? launch_str_tr<float, 1>(st, s, stream) : launch_str_tr<float, 2>(st, s, stream);
+    if (s.rtype == AWP_STORE_BF16) return launch_str_tr<__nv_bfloat16>(st, s, stream);
+    return launch_str_tr<float>(st, s, stream);
 }
