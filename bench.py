@@ -28,7 +28,8 @@ time step of one component of the same grid per bench step.
 
 Other modes: --config N (workloads 1-4), --grid / --components (reduced
 grids for profiling captures), --serve (the 64-request serving stream:
-p50/p99 latency and throughput against serial solves).
+p50/p99 latency and throughput against serial solves), --synth (the
+reciprocity synthesis of 64 rupture variations against a resident SGT set).
 """
 import argparse
 import json
@@ -371,6 +372,95 @@ def run_serve(args):
     return 0
 
 
+def synth_workload():
+    """The synthesis benchmark case: one site, one rupture of 64 x 32 points
+    at 1 km (2048 points, 5 % of them off the SGT grid), 64 rupture
+    variations, two SGT components of 2000 samples at 0.1 s, 3000 output
+    samples, slip rates of 20-80 samples."""
+    return ai.synth_case(seed=1, nx_f=64, nz_f=32, nt=2000, nv=64, ntout=3000, ncomp=2, nstf=(20, 80),
+                         drop_frac=0.05)
+
+
+def fp32_mac_peak(sm_mhz):
+    """FP32 multiply-add pairs per second without FMA contraction: 148 SMs x
+    128 lanes, one FMUL and one FADD per multiply-add, at the sampled clock."""
+    return 148 * 128 * (sm_mhz or 1965.0) * 1e6 / 2.0
+
+
+def run_synth(args):
+    """Reciprocity synthesis (DirectSynth's worker step): rupture variations
+    per second for one site.  A step synthesises every variation of the
+    rupture against the SGT set resident in HBM (host set-up of the terms
+    included); e2e adds the SGT upload, the variation hand-over and the
+    seismogram read-back through the C ABI."""
+    import awpsgt
+    c = synth_workload()
+    nv, npts = len(c.variations), len(c.variations[0][0])
+    with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=c.ntout) as s:
+        s.set_sgt(c.master, c.index, c.headers, c.comps)
+        for i, (p, q) in enumerate(c.variations):
+            s.add_variation(i, p, q)
+        for _ in range(max(3, args.warmup)):
+            s.run()
+        dev, conv, plan, wall = [], [], [], []
+        with ClockSampler(0) as clk:
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                awpsgt._check(s.lib.awp_synth_run(s.h))
+                wall.append(time.perf_counter() - t0)
+                i = s.info()
+                dev.append(i.seconds_device)
+                conv.append(i.seconds_conv)
+                plan.append(i.seconds_plan)
+        info = s.info()
+    clocks = clk.summary()
+    t_step = statistics.median(wall)
+    macs = info.macs
+    e2e = None
+    if not args.no_e2e:
+        ts = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=c.ntout) as s2:
+                s2.set_sgt(c.master, c.index, c.headers, c.comps)
+                for i2, (p, q) in enumerate(c.variations):
+                    s2.add_variation(i2, p, q)
+                out = s2.run()
+            ts.append(time.perf_counter() - t0)
+        sgt_bytes = sum(x.nbytes for x in c.comps) + c.headers.nbytes + c.index.nbytes
+        e2e = {"value": nv / min(ts), "unit": "rupture variations/s",
+               "h2d_bytes_per_step": int(sgt_bytes + sum(p.nbytes + q.nbytes for p, q in c.variations)),
+               "d2h_bytes_per_step": int(out.nbytes)}
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        sample = c.variations[:2]
+        t0 = time.perf_counter()
+        oracle.synth(c.master, c.index, c.headers, c.comps, c.slon, c.slat, c.dtout, c.ntout, 0.0, sample)
+        dt_cpu = time.perf_counter() - t0
+        cpu = {"value": len(sample) / dt_cpu, "unit": "rupture variations/s", "cores": 1, "kind": "port",
+               "sample": "2 of the 64 variations, all 2048 points, one host thread"}
+    conv_s = statistics.median(conv)
+    peak = fp32_mac_peak(clocks.get("sm_mhz"))
+    line = {
+        "metric": "rupture variations/s", "value": nv / t_step, "unit": "rupture variations/s",
+        "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": t_step * 1e3, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded SGTs and rupture variations)",
+        "config": {"workload": "reciprocity synthesis: 1 site, %d-point rupture, %d variations, 2-component SGT "
+                               "nt=2000, ntout=3000" % (npts, nv), "terms": int(info.terms),
+                   "non_exact_points": int(info.non_exact), "sgt_points": int(info.nsgt_points)},
+        "device_ms_per_step": statistics.median(dev) * 1e3, "plan_ms_per_step": statistics.median(plan) * 1e3,
+        "roofline": {"bound": "fp32", "kernel": "k_synth_conv", "achieved": macs / conv_s * 1e-9, "peak": peak * 1e-9,
+                     "unit": "GMAC/s", "frac": macs / conv_s / peak, "traffic": None,
+                     "note": "peak = 148 SMs x 128 lanes x sampled SM clock / 2 (FMUL + FADD per multiply-add)"},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(info.gpu_launches), "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -392,9 +482,12 @@ def main():
     ap.add_argument("--serve-nst-scale", type=float, default=1.0, help="scales every request's NST")
     ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="admission order")
     ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
+    ap.add_argument("--synth", action="store_true", help="reciprocity synthesis: rupture variations per second")
     args = ap.parse_args()
     if args.serve:
         return run_serve(args)
+    if args.synth:
+        return run_synth(args)
     if args.impl == "reference":
         return run_reference(args)
 

@@ -489,3 +489,203 @@ def write_sgthead_inputs(d: str, nx: int, ny: int, nz: int, h_km: float, npts: i
     rho = (310.0 * np.power(vp.astype(np.float64), 0.25)).astype(np.float32)
     np.stack([vp, vs, rho], axis=-1).astype(np.float32).tofile(paths["media"])
     return paths
+
+
+# ---- reciprocity synthesis inputs -------------------------------------------
+
+_GEO_RPERD = 0.017453292          # DirectSynth/src/jbsim/geoproj_subs.c:6
+_GEO_ERAD = 6378.139
+
+
+def _geo_matrices(alpha: float, lon: float, lat: float) -> np.ndarray:
+    r = _GEO_RPERD
+    ca, sa = math.cos(alpha * r), math.sin(alpha * r)
+    ct, st = math.cos((90.0 - lat) * r), math.sin((90.0 - lat) * r)
+    cp, sp = math.cos(lon * r), math.sin(lon * r)
+    return np.array([ca * ct * cp + sa * sp, sa * ct * cp - ca * sp, st * cp,
+                     ca * ct * sp - sa * cp, sa * ct * sp + ca * cp, st * sp,
+                     -ca * st, -sa * st, ct])
+
+
+def model_xy_to_lonlat(master, x_km, y_km):
+    """Great-circle projection (geoproj 1) from model-frame km to degrees, the
+    forward direction of geoproj_subs.c:10-77; float64, for placing points."""
+    m = np.asarray(master).reshape(-1)[0]
+    a = _geo_matrices(float(m["modelrot"]), float(m["modellon"]), float(m["modellat"]))
+    g0 = 0.5 * (-2.0 * float(m["yshift"])) / _GEO_ERAD
+    b0 = 0.5 * (-2.0 * float(m["xshift"])) / _GEO_ERAD
+    x = np.asarray(x_km, np.float64)
+    y = np.asarray(y_km, np.float64)
+    cb, sb = np.cos(x / _GEO_ERAD - b0), np.sin(x / _GEO_ERAD - b0)
+    cg, sg = np.cos(y / _GEO_ERAD - g0), np.sin(y / _GEO_ERAD - g0)
+    arg = np.sqrt(1.0 + sb * sb * sg * sg)
+    xp, yp = sg * cb * arg, sb * cg * arg
+    zp = np.sqrt(1.0 - xp * xp - yp * yp)
+    xg = xp * a[0] + yp * a[1] + zp * a[2]
+    yg = xp * a[3] + yp * a[4] + zp * a[5]
+    zg = xp * a[6] + yp * a[7] + zp * a[8]
+    lat = 90.0 - np.arctan(np.sqrt(xg * xg + yg * yg) / zg) / _GEO_RPERD
+    lon = np.where(xg != 0.0, np.arctan(yg / np.where(xg != 0.0, xg, 1.0)) / _GEO_RPERD, 0.0)
+    lon = np.where(yg < 0.0, lon - 180.0, lon)
+    return lon, lat
+
+
+SYN_MASTER = np.dtype([("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"), ("modelrot", "<f4"),
+                       ("xshift", "<f4"), ("yshift", "<f4"), ("globnp", "<i4"), ("localnp", "<i4"), ("nt", "<i4")])
+SYN_INDEX = np.dtype([("indx", "<i8"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"), ("h", "<f4")])
+SYN_HEADER = np.dtype([("indx", "<i8"), ("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"),
+                       ("modelrot", "<f4"), ("xshift", "<f4"), ("yshift", "<f4"), ("nt", "<i4"), ("xazim", "<f4"),
+                       ("dt", "<f4"), ("tst", "<f4"), ("h", "<f4"), ("src_lat", "<f4"), ("src_lon", "<f4"),
+                       ("src_dep", "<f4"), ("xsrc", "<i4"), ("ysrc", "<i4"), ("zsrc", "<i4"), ("sgt_lat", "<f4"),
+                       ("sgt_lon", "<f4"), ("sgt_dep", "<f4"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"),
+                       ("cdist", "<f4"), ("lam", "<f4"), ("mu", "<f4"), ("rho", "<f4"), ("xmom", "<f4"),
+                       ("ymom", "<f4"), ("zmom", "<f4")])
+SYN_POINT = np.dtype([("lon", "<f4"), ("lat", "<f4"), ("dep", "<f4"), ("stk", "<f4"), ("dip", "<f4"),
+                      ("area", "<f4"), ("tinit", "<f4"), ("dt", "<f4"), ("rake", "<f4"), ("slip1", "<f4"),
+                      ("slip2", "<f4"), ("slip3", "<f4"), ("nt1", "<i4"), ("nt2", "<i4"), ("nt3", "<i4"),
+                      ("stf1", "<i8"), ("stf2", "<i8"), ("stf3", "<i8")], align=True)
+
+
+@dataclass
+class SynthCase:
+    master: np.ndarray
+    index: np.ndarray
+    headers: np.ndarray
+    comps: List[np.ndarray]
+    slon: float
+    slat: float
+    dtout: float
+    ntout: int
+    variations: List[Tuple[np.ndarray, np.ndarray]]
+    h_km: float
+
+
+def synth_case(seed: int = 0, nx_f: int = 12, nz_f: int = 6, nt: int = 300, nv: int = 3, ntout: int = 0,
+               ncomp: int = 2, h_km: float = 1.0, dt: float = 0.1, drop_frac: float = 0.15,
+               mech2_frac: float = 0.1, mech3_frac: float = 0.05, zero_frac: float = 0.05, nstf=(8, 40),
+               jitter: float = 0.3, mrot: float = -55.0) -> SynthCase:
+    """One site and one rupture in the formats DirectSynth reads: an SGT set
+    (x-component master, index sorted by indx, headers, [np][6][nt] data per
+    component) around a vertical fault of nx_f x nz_f points, and nv rupture
+    variations on that fault.  A fraction of the fault's grid points is left
+    out of the SGT set so that those rupture points take the four-point
+    bracketing path; some points slip along u2 / u3 too, some not at all."""
+    rng = np.random.default_rng(seed)
+    nxm, nym = nx_f + 40, 60
+    master = np.zeros(1, SYN_MASTER)
+    master[0] = (1, -118.2, 34.05, mrot, -0.5 * nxm * h_km, -0.5 * nym * h_km, 0, 0, nt)
+    xs, ys = 8, 10                                   # site (reciprocal source) grid location
+    x0, yf = 20, 40                                  # fault trace start, fault y
+    fault = [(x0 + i, yf, 1 + k) for i in range(nx_f) for k in range(nz_f)]
+    drop = set(tuple(fault[i]) for i in rng.choice(len(fault), int(drop_frac * len(fault)), replace=False))
+    pts = set()
+    for x in range(x0 - 1, x0 + nx_f + 1):
+        for y in (yf - 1, yf, yf + 1):
+            for z in range(1, nz_f + 2):
+                if (x, y, z) not in drop:
+                    pts.add((x, y, z))
+    pts = sorted(pts)
+    npg = len(pts)
+    master[0]["globnp"] = master[0]["localnp"] = npg
+    index = np.zeros(npg, SYN_INDEX)
+    p = np.array(pts, np.int64)
+    index["indx"] = p[:, 0] * 1000000000000 + p[:, 1] * 1000000 + p[:, 2]
+    index["xsgt"], index["ysgt"], index["zsgt"], index["h"] = p[:, 0], p[:, 1], p[:, 2], h_km
+    hd = np.zeros(npg, SYN_HEADER)
+    for f in ("geoproj", "modellon", "modellat", "modelrot", "xshift", "yshift", "nt"):
+        hd[f] = master[0][f]
+    hd["indx"], hd["xsgt"], hd["ysgt"], hd["zsgt"], hd["h"] = index["indx"], p[:, 0], p[:, 1], p[:, 2], h_km
+    hd["xazim"], hd["dt"], hd["tst"] = 90.0 + mrot, dt, -4.0
+    hd["xsrc"], hd["ysrc"], hd["zsrc"] = xs, ys, 1
+    d = np.sqrt((p[:, 0] - xs) ** 2 + (p[:, 1] - ys) ** 2 + (p[:, 2] - 1) ** 2) * h_km
+    hd["cdist"] = d
+    vs = 3.0e5 * (1.0 + 0.1 * rng.random(npg))          # cm/s
+    vp = 1.73 * vs
+    rho = 2.4 + 0.3 * rng.random(npg)
+    hd["rho"], hd["mu"], hd["lam"] = rho, rho * vs * vs, rho * (vp * vp - 2.0 * vs * vs)
+    hd["xmom"] = 1.0e20
+    t = (np.arange(nt) * dt).astype(np.float32)
+    comps = []
+    for q in range(ncomp):
+        f0 = (0.2 + 0.8 * rng.random((npg, 6, 1))).astype(np.float32)
+        td = ((d[:, None, None] / 3.0) + 2.0 * rng.random((npg, 6, 1))).astype(np.float32)
+        amp = (1.0e-9 * (0.5 + rng.random((npg, 6, 1))) * np.where(rng.random((npg, 6, 1)) < 0.5, -1.0, 1.0)
+               ).astype(np.float32)
+        out = np.empty((npg, 6, nt), np.float32)
+        for a in range(0, npg, 256):            # damped wavelets, 256 points at a time
+            b = min(npg, a + 256)
+            x = t[None, None, :] - td[a:b]
+            out[a:b] = amp[a:b] * np.exp(-(x / 3.0) ** 2) * np.sin(np.float32(2.0 * np.pi) * f0[a:b] * x)
+        comps.append(out)
+    slon, slat = model_xy_to_lonlat(master, xs * h_km, ys * h_km)
+    fx = np.array([f[0] for f in fault], np.float64) + jitter * (rng.random(len(fault)) - 0.5)
+    fz = np.array([f[2] for f in fault], np.float64) + jitter * (rng.random(len(fault)) - 0.5)
+    lon, lat = model_xy_to_lonlat(master, fx * h_km, np.full(len(fault), yf * h_km))
+    variations = []
+    nf = len(fault)
+    for v in range(nv):
+        sp = np.zeros(nf, SYN_POINT)
+        sp["lon"], sp["lat"], sp["dep"] = lon, lat, (fz - 1.0) * h_km
+        sp["stk"], sp["dip"] = 90.0 + mrot + 2.0 * (rng.random() - 0.5), 80.0 + 10.0 * rng.random()
+        sp["area"] = (h_km * 1.0e5) ** 2
+        sp["dt"] = dt
+        sp["rake"] = 180.0 * (rng.random(nf) - 0.5) + 45.0 * v
+        hyp = rng.integers(0, nf)
+        sp["tinit"] = np.hypot(fx - fx[hyp], fz - fz[hyp]) * h_km / 2.8
+        r = rng.random(nf)
+        has = np.zeros((3, nf), bool)
+        has[0] = r >= zero_frac
+        has[1] = has[0] & (r < zero_frac + mech2_frac)
+        has[2] = has[0] & (rng.random(nf) < mech3_frac)
+        k = rng.integers(nstf[0], nstf[1] + 1, size=(nf, 3))
+        slip = 20.0 + 200.0 * rng.random((nf, 3))
+        pool, n = [], 0
+        for i in range(nf):                      # samples of a point: u1, u2, u3 in order
+            for c in range(3):
+                if has[c, i]:
+                    kk = int(k[i, c])
+                    tri = np.minimum(np.arange(1, kk + 1), np.arange(kk, 0, -1)).astype(np.float64)
+                    pool.append((slip[i, c] * tri / (tri.sum() * dt)).astype(np.float32))
+                    sp[i]["slip%d" % (c + 1)], sp[i]["nt%d" % (c + 1)], sp[i]["stf%d" % (c + 1)] = slip[i, c], kk, n
+                    n += kk
+        variations.append((sp, np.concatenate(pool) if pool else np.zeros(0, np.float32)))
+    return SynthCase(master, index, hd, comps, float(slon), float(slat), dt, ntout, variations, h_km)
+
+
+def write_srf(path: str, pts: np.ndarray, pool: np.ndarray, binary: bool = False, plane: bool = True):
+    """An SRF file (version 1.0) of the points, text or binary, in the layout
+    DirectSynth/src/jbsim/srf_subs.c:521-690 reads."""
+    if binary:
+        with open(path, "wb") as f:
+            f.write(b"1.0".ljust(32, b"\0"))
+            if plane:
+                f.write(b"PLANE".ljust(32, b"\0"))
+                f.write(np.int32(1).tobytes())
+                f.write(np.zeros(13, np.float32).tobytes())
+            f.write(b"POINTS".ljust(32, b"\0"))
+            f.write(np.int32(len(pts)).tobytes())
+            for a in pts:
+                f.write(np.array([a[k] for k in ("lon", "lat", "dep", "stk", "dip", "area", "tinit", "dt", "rake")],
+                                 np.float32).tobytes())
+                for c in (1, 2, 3):
+                    f.write(np.float32(a["slip%d" % c]).tobytes() + np.int32(a["nt%d" % c]).tobytes())
+                for c in (1, 2, 3):
+                    n, o = int(a["nt%d" % c]), int(a["stf%d" % c])
+                    f.write(pool[o:o + n].astype(np.float32).tobytes())
+        return
+    with open(path, "w") as f:
+        f.write("1.0\n")
+        if plane:
+            f.write("PLANE 1\n%.5f %.5f %d %d %.2f %.2f\n%.1f %.1f %.2f %.2f %.2f\n" %
+                    (-118.0, 34.0, 10, 5, 10.0, 5.0, 0.0, 90.0, 0.0, 0.0, 5.0))
+        f.write("POINTS %d\n" % len(pts))
+        for a in pts:
+            f.write("%.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g\n" % tuple(
+                float(a[k]) for k in ("lon", "lat", "dep", "stk", "dip", "area", "tinit", "dt")))
+            f.write("%.9g %.9g %d %.9g %d %.9g %d\n" % (float(a["rake"]), float(a["slip1"]), int(a["nt1"]),
+                                                      float(a["slip2"]), int(a["nt2"]), float(a["slip3"]),
+                                                      int(a["nt3"])))
+            for c in (1, 2, 3):
+                n, o = int(a["nt%d" % c]), int(a["stf%d" % c])
+                for j in range(0, n, 6):
+                    f.write("  " + " ".join("%.9g" % float(x) for x in pool[o + j:o + min(n, j + 6)]) + "\n")

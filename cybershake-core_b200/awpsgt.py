@@ -46,6 +46,12 @@ EXPORTED = [
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
     "awp_reformat_velocity",
 ]
+# Every symbol include/awp_synth.h declares.
+EXPORTED_SYNTH = [
+    "awp_synth_create", "awp_synth_destroy", "awp_synth_set_sgt", "awp_synth_load_sgt_files",
+    "awp_synth_add_variation", "awp_synth_add_srf_file", "awp_synth_clear_variations", "awp_synth_run",
+    "awp_synth_seismograms", "awp_synth_write_grm", "awp_synth_get_info", "awp_srf_read",
+]
 
 
 class Layout(C.Structure):
@@ -166,6 +172,148 @@ def sgt_reorder_rwg(sgt: np.ndarray, nt: int, z_source: bool = False) -> np.ndar
     return out
 
 
+class SynthParams(C.Structure):
+    """awp_synth_params."""
+    _fields_ = [("device", C.c_int), ("slon", C.c_float), ("slat", C.c_float), ("dtout", C.c_float),
+                ("ntout", C.c_int), ("tstart", C.c_float), ("rv_batch", C.c_int)]
+
+
+class SynthInfo(C.Structure):
+    """awp_synth_info."""
+    _fields_ = [("ntout", C.c_int), ("ntsum", C.c_int), ("nsgt_points", C.c_int), ("non_exact", C.c_int),
+                ("nvariations", C.c_int), ("ncomp", C.c_int), ("terms", C.c_int64), ("macs", C.c_int64),
+                ("seconds_plan", C.c_double), ("seconds_device", C.c_double), ("seconds_conv", C.c_double),
+                ("gpu_launches", C.c_int)]
+
+
+# awp_srf_point (jbsim/srf_structure.h srf_apointvalues with pool offsets)
+SRFPOINT = np.dtype([("lon", "<f4"), ("lat", "<f4"), ("dep", "<f4"), ("stk", "<f4"), ("dip", "<f4"),
+                     ("area", "<f4"), ("tinit", "<f4"), ("dt", "<f4"), ("rake", "<f4"), ("slip1", "<f4"),
+                     ("slip2", "<f4"), ("slip3", "<f4"), ("nt1", "<i4"), ("nt2", "<i4"), ("nt3", "<i4"),
+                     ("stf1", "<i8"), ("stf2", "<i8"), ("stf3", "<i8")], align=True)
+# awp_seisheader (DirectSynth/src/jbsim/structure.h seisheader, 56 bytes)
+SEISHEADER = np.dtype([("version", "S8"), ("site_name", "S8"), ("padding", "S8"), ("source_id", "<i4"),
+                       ("rupture_id", "<i4"), ("rup_var_id", "<i4"), ("dt", "<f4"), ("nt", "<i4"),
+                       ("comps", "<i4"), ("det_max_freq", "<f4"), ("stoch_max_freq", "<f4")])
+
+
+def read_srf(path: str, binary: bool = False):
+    """awp_srf_read: (points as SRFPOINT records, slip-rate sample pool)."""
+    lib = load_library()
+    pts = C.c_void_p()
+    pool = C.c_void_p()
+    n = C.c_int()
+    npool = C.c_int64()
+    _check(lib.awp_srf_read(path.encode(), int(bool(binary)), C.byref(pts), C.byref(n), C.byref(pool),
+                            C.byref(npool)))
+    try:
+        a = np.frombuffer((C.c_char * (n.value * SRFPOINT.itemsize)).from_address(pts.value), SRFPOINT).copy() \
+            if n.value else np.zeros(0, SRFPOINT)
+        b = np.frombuffer((C.c_float * npool.value).from_address(pool.value), np.float32).copy() \
+            if npool.value else np.zeros(0, np.float32)
+    finally:
+        lib.awp_free(pts)
+        lib.awp_free(pool)
+    return a, b
+
+
+class Synth:
+    """Reciprocity seismogram synthesis for one site and one rupture: the
+    DirectSynth worker step (jbsim3d_synth) with the SGT set held on the GPU."""
+
+    def __init__(self, slon: float, slat: float, dtout: float, ntout: int = -1, tstart: float = 0.0,
+                 device: int = 0, rv_batch: int = 0):
+        self.lib = load_library()
+        self.p = SynthParams(device, slon, slat, dtout, ntout, tstart, rv_batch)
+        h = C.c_void_p()
+        _check(self.lib.awp_synth_create(C.byref(self.p), C.byref(h)))
+        self.h = h
+        self.nvar = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.awp_synth_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_sgt(self, master, index, headers, comps: Sequence[np.ndarray]):
+        """SGT set from host arrays: the x component's records and 1-3
+        [globnp][6][nt] float32 arrays (x, y, z)."""
+        m = np.ascontiguousarray(np.asarray(master, SGTMASTER).reshape(1))
+        ix = np.ascontiguousarray(index, SGTINDEX)
+        hd = np.ascontiguousarray(headers, SGTHEADER)
+        cs = [np.ascontiguousarray(c, np.float32) for c in comps]
+        ptrs = [_ptr(c) if i < len(cs) else None for i, c in enumerate(cs + [None] * (3 - len(cs)))]
+        _check(self.lib.awp_synth_set_sgt(self.h, _ptr(m), _ptr(ix), _ptr(hd), len(cs), *ptrs))
+
+    def load_sgt_files(self, xhead: str, xdata: str, yhead: Optional[str] = None, ydata: Optional[str] = None,
+                       zhead: Optional[str] = None, zdata: Optional[str] = None):
+        enc = lambda x: x.encode() if x else None
+        _check(self.lib.awp_synth_load_sgt_files(self.h, enc(xhead), enc(xdata), enc(yhead), enc(ydata),
+                                                 enc(zhead), enc(zdata)))
+
+    def add_variation(self, rup_var_id: int, points: np.ndarray, pool: np.ndarray):
+        pts = np.ascontiguousarray(points, SRFPOINT)
+        pl = np.ascontiguousarray(pool, np.float32)
+        _check(self.lib.awp_synth_add_variation(self.h, rup_var_id, _ptr(pts), len(pts), _ptr(pl), pl.size))
+        self.nvar += 1
+
+    def add_srf_file(self, rup_var_id: int, path: str, binary: bool = False):
+        _check(self.lib.awp_synth_add_srf_file(self.h, rup_var_id, path.encode(), int(bool(binary))))
+        self.nvar += 1
+
+    def clear_variations(self):
+        _check(self.lib.awp_synth_clear_variations(self.h))
+        self.nvar = 0
+
+    def run(self) -> np.ndarray:
+        """Synthesises every variation; returns [nvar][3][ntout] (vertical, north, east)."""
+        _check(self.lib.awp_synth_run(self.h))
+        return self.seismograms()
+
+    def info(self) -> SynthInfo:
+        i = SynthInfo()
+        _check(self.lib.awp_synth_get_info(self.h, C.byref(i)))
+        return i
+
+    def seismograms(self) -> np.ndarray:
+        i = self.info()
+        out = np.empty((i.nvariations, 3, i.ntout), np.float32)
+        _check(self.lib.awp_synth_seismograms(self.h, _ptr(out), out.size))
+        return out
+
+    def write_grm(self, path: str, site: str = "", source_id: int = 0, rupture_id: int = 0,
+                  det_max_freq: float = 0.0, stoch_max_freq: float = 0.0, version: str = "12.10"):
+        h = np.zeros(1, SEISHEADER)
+        h["version"], h["site_name"] = version.encode(), site.encode()[:7]
+        h["source_id"], h["rupture_id"] = source_id, rupture_id
+        h["det_max_freq"], h["stoch_max_freq"] = det_max_freq, stoch_max_freq
+        _check(self.lib.awp_synth_write_grm(self.h, path.encode(), _ptr(h)))
+
+
+def read_grm(path: str, ncomp_out: int, ntout: int):
+    """Records of a merged seismogram file: (headers, samples[nvar][ncomp_out][ntout])."""
+    raw = np.fromfile(path, np.uint8)
+    rec = SEISHEADER.itemsize + 4 * ncomp_out * ntout
+    n = raw.size // rec
+    hd = np.stack([raw[i * rec:i * rec + SEISHEADER.itemsize].view(SEISHEADER)[0] for i in range(n)]) \
+        if n else np.zeros(0, SEISHEADER)
+    data = np.stack([raw[i * rec + SEISHEADER.itemsize:(i + 1) * rec].view(np.float32).reshape(ncomp_out, ntout)
+                     for i in range(n)]) if n else np.zeros((0, ncomp_out, ntout), np.float32)
+    return hd, data
+
+
 def load_library(path: str = LIB_PATH):
     """Loads libawpsgt.so; raises ImportError when it has not been built."""
     global _lib
@@ -222,6 +370,19 @@ def load_library(path: str = LIB_PATH):
         "awp_load_media_rwg": (C.c_int, [C.c_void_p, C.c_char_p]),
         "awp_reformat_velocity": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
+        "awp_synth_create": (C.c_int, [P(SynthParams), P(C.c_void_p)]),
+        "awp_synth_destroy": (None, [C.c_void_p]),
+        "awp_synth_set_sgt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
+        "awp_synth_load_sgt_files": (C.c_int, [C.c_void_p] + [C.c_char_p] * 6),
+        "awp_synth_add_variation": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
+        "awp_synth_add_srf_file": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int]),
+        "awp_synth_clear_variations": (C.c_int, [C.c_void_p]),
+        "awp_synth_run": (C.c_int, [C.c_void_p]),
+        "awp_synth_seismograms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+        "awp_synth_write_grm": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p]),
+        "awp_synth_get_info": (C.c_int, [C.c_void_p, P(SynthInfo)]),
+        "awp_srf_read": (C.c_int, [C.c_char_p, C.c_int, P(C.c_void_p), P(C.c_int), P(C.c_void_p), P(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -189,3 +189,83 @@ def rwg_to_awp_media(p: np.ndarray, s: np.ndarray, d: np.ndarray, nx: int, ny: i
         a = np.asarray(a, dtype=np.float32).reshape(ny, nz, nx)
         out[..., v] = (a.transpose(1, 2, 0).astype(np.float64) * 1000.0).astype(np.float32)
     return out.reshape(-1)
+
+
+# ---- reciprocity synthesis (oracle/synth_oracle.c) -------------------------
+# Records of the RWG SGT header file and of an SRF point, as
+# DirectSynth/src/jbsim/structure.h and srf_structure.h lay them out.
+SGTMASTER = np.dtype([("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"), ("modelrot", "<f4"),
+                      ("xshift", "<f4"), ("yshift", "<f4"), ("globnp", "<i4"), ("localnp", "<i4"), ("nt", "<i4")])
+SGTINDEX = np.dtype([("indx", "<i8"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"), ("h", "<f4")])
+SGTHEADER = np.dtype([("indx", "<i8"), ("geoproj", "<i4"), ("modellon", "<f4"), ("modellat", "<f4"),
+                      ("modelrot", "<f4"), ("xshift", "<f4"), ("yshift", "<f4"), ("nt", "<i4"), ("xazim", "<f4"),
+                      ("dt", "<f4"), ("tst", "<f4"), ("h", "<f4"), ("src_lat", "<f4"), ("src_lon", "<f4"),
+                      ("src_dep", "<f4"), ("xsrc", "<i4"), ("ysrc", "<i4"), ("zsrc", "<i4"), ("sgt_lat", "<f4"),
+                      ("sgt_lon", "<f4"), ("sgt_dep", "<f4"), ("xsgt", "<i4"), ("ysgt", "<i4"), ("zsgt", "<i4"),
+                      ("cdist", "<f4"), ("lam", "<f4"), ("mu", "<f4"), ("rho", "<f4"), ("xmom", "<f4"),
+                      ("ymom", "<f4"), ("zmom", "<f4")])
+SRFPOINT = np.dtype([("lon", "<f4"), ("lat", "<f4"), ("dep", "<f4"), ("stk", "<f4"), ("dip", "<f4"),
+                     ("area", "<f4"), ("tinit", "<f4"), ("dt", "<f4"), ("rake", "<f4"), ("slip1", "<f4"),
+                     ("slip2", "<f4"), ("slip3", "<f4"), ("nt1", "<i4"), ("nt2", "<i4"), ("nt3", "<i4"),
+                     ("stf1", "<i8"), ("stf2", "<i8"), ("stf3", "<i8")], align=True)
+
+_synth_lib = None
+
+
+def _load_synth():
+    global _synth_lib
+    if _synth_lib is None:
+        path = os.path.join(_HERE, "liborc_synth.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        V = C.c_void_p
+        lib.orc_synth.restype = C.c_int
+        lib.orc_synth.argtypes = [V, V, V, C.c_int, V, V, V, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
+                                  C.c_int, C.c_int, V, V, V, V, C.POINTER(C.c_int)]
+        lib.orc_synth_get_indx.restype = None
+        lib.orc_synth_get_indx.argtypes = [V, C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_int64), V]
+        _synth_lib = lib
+    return _synth_lib
+
+
+def synth(master, index, headers, comps, slon, slat, dtout, ntout, tstart, variations):
+    """Seismograms [nvar][3][ntout] of the rupture variations [(points, pool)]
+    for one site, restating DirectSynth's jbsim3d_synth; returns (seis, ntout)."""
+    lib = _load_synth()
+    m = np.ascontiguousarray(np.asarray(master, SGTMASTER).reshape(1))
+    ix = np.ascontiguousarray(index, SGTINDEX)
+    hd = np.ascontiguousarray(headers, SGTHEADER)
+    cs = [np.ascontiguousarray(c, np.float32) for c in comps]
+    ptr = [_p(c) for c in cs] + [None] * (3 - len(cs))
+    nv = len(variations)
+    npts = len(variations[0][0])
+    pts = np.ascontiguousarray(np.concatenate([np.asarray(v[0], SRFPOINT) for v in variations]), SRFPOINT)
+    pools = [np.ascontiguousarray(v[1], np.float32) for v in variations]
+    off = np.cumsum([0] + [p.size for p in pools[:-1]]).astype(np.int64)
+    pool = np.ascontiguousarray(np.concatenate(pools + [np.zeros(1, np.float32)]))
+    maxnt, mindt = int(hd[0]["nt"]), np.float32(hd[0]["dt"])
+    if np.float32(dtout) < mindt:                     # jbsim3d.c:439-440
+        maxnt = int(np.float32(maxnt) * mindt / np.float32(dtout))
+    n = 2
+    while n < 4 * maxnt:
+        n *= 2
+    nout = ntout if ntout > 0 else n
+    seis = np.zeros((nv, 3, nout), np.float32)
+    got = C.c_int()
+    rc = lib.orc_synth(_p(m), _p(ix), _p(hd), len(cs), ptr[0], ptr[1], ptr[2], slon, slat, dtout, ntout, tstart,
+                       nv, npts, _p(pts), _p(pool), _p(off), _p(seis), C.byref(got))
+    if rc:
+        raise ValueError("oracle synthesis refused the input (code %d)" % rc)
+    assert got.value == nout, (got.value, nout)
+    return seis, nout
+
+
+def synth_get_indx(master, h, lon, lat, dep):
+    """(indx, (x, y, z)) of a point in the SGT grid (misc_subs.c:151-173)."""
+    lib = _load_synth()
+    m = np.ascontiguousarray(np.asarray(master, SGTMASTER).reshape(1))
+    indx = C.c_int64()
+    xyz = np.zeros(3, np.int32)
+    lib.orc_synth_get_indx(_p(m), h, lon, lat, dep, C.byref(indx), _p(xyz))
+    return indx.value, tuple(int(v) for v in xyz)

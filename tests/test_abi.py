@@ -12,11 +12,11 @@ import pytest
 import awpsgt
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "awp_sgt.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("awp_sgt.h", "awp_synth.h")]
 
 
 def header_functions():
-    src = open(HEADER).read()
+    src = "".join(open(h).read() for h in HEADERS)
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(awp_[a-z0-9_]+)\s*\(", src)))
 
@@ -27,7 +27,8 @@ def test_library_exports_every_declared_symbol():
     assert len(decl) >= 20
     missing = [n for n in decl if not hasattr(lib, n)]
     assert not missing, missing
-    assert sorted(awpsgt.EXPORTED) == decl
+    assert sorted(awpsgt.EXPORTED + awpsgt.EXPORTED_SYNTH) == decl
+    assert sorted(os.listdir(os.path.join(ROOT, "include"))) == sorted(os.path.basename(h) for h in HEADERS)
 
 
 def test_exports_are_c_linkage():
