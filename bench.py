@@ -402,7 +402,7 @@ def run_synth(args):
             s.add_variation(i, p, q)
         for _ in range(max(3, args.warmup)):
             s.run()
-        dev, conv, plan, wall = [], [], [], []
+        dev, conv, plan, wall, gf = [], [], [], [], []
         with ClockSampler(0) as clk:
             for _ in range(args.steps):
                 t0 = time.perf_counter()
@@ -411,6 +411,7 @@ def run_synth(args):
                 i = s.info()
                 dev.append(i.seconds_device)
                 conv.append(i.seconds_conv)
+                gf.append(i.seconds_gf)
                 plan.append(i.seconds_plan)
         info = s.info()
     clocks = clk.summary()
@@ -452,6 +453,7 @@ def run_synth(args):
                                "nt=2000, ntout=3000" % (npts, nv), "terms": int(info.terms),
                    "non_exact_points": int(info.non_exact), "sgt_points": int(info.nsgt_points)},
         "device_ms_per_step": statistics.median(dev) * 1e3, "plan_ms_per_step": statistics.median(plan) * 1e3,
+        "k_synth_gf_ms": statistics.median(gf) * 1e3, "k_synth_conv_ms": conv_s * 1e3,
         "roofline": {"bound": "fp32", "kernel": "k_synth_conv", "achieved": macs / conv_s * 1e-9, "peak": peak * 1e-9,
                      "unit": "GMAC/s", "frac": macs / conv_s / peak, "traffic": None,
                      "note": "peak = 148 SMs x 128 lanes x sampled SM clock / 2 (FMUL + FADD per multiply-add)"},

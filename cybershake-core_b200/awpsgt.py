@@ -183,7 +183,7 @@ class SynthInfo(C.Structure):
     _fields_ = [("ntout", C.c_int), ("ntsum", C.c_int), ("nsgt_points", C.c_int), ("non_exact", C.c_int),
                 ("nvariations", C.c_int), ("ncomp", C.c_int), ("terms", C.c_int64), ("macs", C.c_int64),
                 ("seconds_plan", C.c_double), ("seconds_device", C.c_double), ("seconds_conv", C.c_double),
-                ("gpu_launches", C.c_int)]
+                ("gpu_launches", C.c_int), ("seconds_gf", C.c_double)]
 
 
 # awp_srf_point (jbsim/srf_structure.h srf_apointvalues with pool offsets)

@@ -64,18 +64,28 @@ __constant__ float c_taper[SY_TAPLEN];
 
 /* ---- kernel 1: per term, the shifted sum of the bracketing SGTs --------- */
 
+/* u holds UC component traces per slot: vertical, north, east when the SGTs
+ * have three components, else north and east only -- with no z SGT the
+ * vertical trace is +0 throughout (zero rows times a zero amplitude, added
+ * to +0), and so is its convolution, which the zeroed seismogram already
+ * holds. */
+
 template <int NC>
-__device__ __forceinline__ void gf_sample(const float *__restrict__ b, int nt, const float *k, float &gv, float &gn,
-                                          float &ge)
+__device__ __forceinline__ void gf_load(const float *__restrict__ b, int nt, float *a, float *y, float *z)
 {
-    float a[6], y[6], z[6];
 #pragma unroll
     for (int r = 0; r < 6; r++) {
         a[r] = __ldg(b + (size_t)r * nt);
         y[r] = NC > 1 ? __ldg(b + (size_t)(6 + r) * nt) : 0.0f;
         z[r] = NC > 2 ? __ldg(b + (size_t)(12 + r) * nt) : 0.0f;
     }
-    /* sgt3d_subs.c:1393-1406: left-to-right sums, amplitude last */
+}
+
+/* sgt3d_subs.c:1393-1406: left-to-right sums, amplitude last, then the
+ * rotation to north / east */
+__device__ __forceinline__ void gf_combine(const float *a, const float *y, const float *z, const float *k, float &gv,
+                                           float &gn, float &ge)
+{
     const float sx = k[SY_XAMP] * (a[0] * k[SY_MXX] + a[1] * k[SY_MYY] + a[2] * k[SY_MZZ] + a[3] * k[SY_MXY] +
                                    a[4] * k[SY_MXZ] + a[5] * k[SY_MYZ]);
     const float sy = k[SY_YAMP] * (y[0] * k[SY_MXX] + y[1] * k[SY_MYY] + y[2] * k[SY_MZZ] + y[3] * k[SY_MXY] +
@@ -87,15 +97,18 @@ __device__ __forceinline__ void gf_sample(const float *__restrict__ b, int nt, c
     gv = -sz;
 }
 
-template <int NC>
+/* terms whose rupture point sits between SGT points (2-4 brackets): one
+ * block per (listed slot, 256 output samples), every output sample written */
+template <int NC, int UC>
 __global__ void __launch_bounds__(GF_THREADS) k_synth_gf(const float *__restrict__ sgt, int nt, int tapst,
                                                          const awp_synth_gterm *__restrict__ gt,
-                                                         const int *__restrict__ slot_term, long long slot0,
-                                                         int ntout, float *__restrict__ u)
+                                                         const int *__restrict__ slot_term,
+                                                         const int *__restrict__ slots, int ntout,
+                                                         float *__restrict__ u)
 {
     __shared__ awp_synth_gterm g;
-    const long long slot = blockIdx.x;
-    if (threadIdx.x == 0) g = gt[slot_term[slot0 + slot]];
+    const int slot = slots[blockIdx.x];
+    if (threadIdx.x == 0) g = gt[slot_term[slot]];
     __syncthreads();
     const int i = blockIdx.y * GF_THREADS + threadIdx.x;
     if (i >= ntout) return;
@@ -103,8 +116,9 @@ __global__ void __launch_bounds__(GF_THREADS) k_synth_gf(const float *__restrict
     for (int ig = 0; ig < g.nsgt; ig++) {
         if (i < g.lo[ig] || i >= g.hi[ig]) continue;
         const int j = i - g.shift[ig];
-        float gv, gn, ge;
-        gf_sample<NC>(sgt + (size_t)g.pt[ig] * (6 * NC) * nt + j, nt, g.c[ig], gv, gn, ge);
+        float a[6], y[6], z[6], gv, gn, ge;
+        gf_load<NC>(sgt + (size_t)g.pt[ig] * (6 * NC) * nt + j, nt, a, y, z);
+        gf_combine(a, y, z, g.c[ig], gv, gn, ge);
         if (j > tapst) {                   /* sgt3d_subs.c:1206-1212 */
             const float f = c_taper[j - tapst];
             gv = f * gv;
@@ -115,10 +129,68 @@ __global__ void __launch_bounds__(GF_THREADS) k_synth_gf(const float *__restrict
         un = un + gn;
         ue = ue + ge;
     }
-    float *o = u + (size_t)slot * 3 * ntout + i;
-    o[0] = uv;
-    o[ntout] = un;
-    o[2 * (size_t)ntout] = ue;
+    float *o = u + (size_t)slot * UC * ntout + i;
+    if (UC == 3) *o = uv, o += ntout;
+    o[0] = un;
+    o[ntout] = ue;
+}
+
+/* rupture points with an exact SGT match: one block per (point, 256 SGT
+ * samples).  Each thread loads its SGT sample once and applies every term of
+ * the point (all variations and slip components) to it, writing output
+ * sample j + shift of each term inside the term's coverage; samples outside
+ * it are +0 and the convolution supplies them.  The terms' coefficients are
+ * staged in shared memory 64 at a time. */
+constexpr int GF1_TERMS = 64;
+
+template <int NC, int UC>
+__global__ void __launch_bounds__(GF_THREADS) k_synth_gf1(const float *__restrict__ sgt, int nt, int tapst,
+                                                          const awp_synth_gterm *__restrict__ gt,
+                                                          const int *__restrict__ slot_term,
+                                                          const int4 *__restrict__ groups, int ntout,
+                                                          float *__restrict__ u)
+{
+    __shared__ float4 rec[GF1_TERMS][4];
+    const int4 grp = groups[blockIdx.y];               /* SGT point, first slot, slots */
+    const int j = blockIdx.x * GF_THREADS + threadIdx.x;
+    float a[6], y[6], z[6];
+    float f = 1.0f;
+    if (j < nt) {
+        gf_load<NC>(sgt + (size_t)grp.x * (6 * NC) * nt + j, nt, a, y, z);
+        if (j > tapst) f = c_taper[j - tapst];         /* sgt3d_subs.c:1206-1212; 1 * g is g */
+    }
+    for (int t0 = 0; t0 < grp.z; t0 += GF1_TERMS) {
+        const int nterm = grp.z - t0 < GF1_TERMS ? grp.z - t0 : GF1_TERMS;
+        __syncthreads();
+        for (int e = threadIdx.x; e < nterm * 16; e += GF_THREADS) {
+            const int tt = e >> 4, w = e & 15;
+            const awp_synth_gterm *g = gt + slot_term[grp.y + t0 + tt];
+            float v = 0.0f;
+            if (w < SY_NC) v = g->c[0][w];
+            else if (w == SY_NC) v = __int_as_float(g->shift[0]);
+            else if (w == SY_NC + 1) v = __int_as_float(g->lo[0]);
+            else if (w == SY_NC + 2) v = __int_as_float(g->hi[0]);
+            reinterpret_cast<float *>(rec[tt])[w] = v;
+        }
+        __syncthreads();
+        if (j >= nt) continue;
+        for (int tt = 0; tt < nterm; tt++) {
+            float k[16];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float4 r = rec[tt][q];
+                k[4 * q] = r.x, k[4 * q + 1] = r.y, k[4 * q + 2] = r.z, k[4 * q + 3] = r.w;
+            }
+            const int i = j + __float_as_int(k[SY_NC]);
+            if (i < __float_as_int(k[SY_NC + 1]) || i >= __float_as_int(k[SY_NC + 2])) continue;
+            float gv, gn, ge;
+            gf_combine(a, y, z, k, gv, gn, ge);
+            float *o = u + (size_t)(grp.y + t0 + tt) * UC * ntout + i;
+            if (UC == 3) *o = 0.0f + f * gv, o += ntout;    /* sgt3d_subs.c:1237-1254 */
+            o[0] = 0.0f + f * gn;
+            o[ntout] = 0.0f + f * ge;
+        }
+    }
 }
 
 /* ---- kernel 2: slip-rate convolution, terms in rupture-point order ------- */
@@ -128,61 +200,151 @@ __global__ void __launch_bounds__(GF_THREADS) k_synth_gf(const float *__restrict
  * different banks; the row stride is 4 mod 32 for the same reason on fill */
 __device__ __forceinline__ int cv_pos(int y, int stride) { return (y & (CV_Q - 1)) * stride + (y >> 3); }
 
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+struct CvTerm {
+    const float *u;       /* this term's component trace              */
+    long long stf;        /* slip-rate offset in the pool             */
+    int n8;               /* samples rounded up to 8 (zero padded)    */
+    int nstf;
+    int lo, hi;           /* trace samples written; the rest are +0   */
+};
+
+/* Each CTA owns 1024 consecutive output samples (8 per thread) of one
+ * component of one variation and walks the variation's terms in
+ * rupture-point order.  The window of term n + 1 (its trace around the block
+ * and its slip rate) is copied into the other shared buffer with cp.async
+ * while term n is convolved.
+ *
+ * Inside a term, thread samples W[j] = window[8 tid + j] feed its outputs
+ * q = 0..7 at lag k through W[q + m], m = n8 - 1 - k.  Lags go in groups of
+ * eight (m = 8g+7 .. 8g, g descending): a group needs W[8g .. 8g+14], held
+ * as lo = W[8g..8g+7] and hi = W[8g+8..8g+15]; the next group's lo is loaded
+ * while this one computes.  W[8g + j] sits in shared row j at column tid + g
+ * (rows STRIDE apart, STRIDE = 4 mod 32), so the loads of a warp hit 32
+ * banks and their offsets are immediates. */
+template <int STRIDE, int UC>
 __global__ void __launch_bounds__(CV_THREADS) k_synth_conv(const float *__restrict__ u, const int *__restrict__ tl,
-                                                           const int2 *__restrict__ range, long long slot0,
+                                                           const int2 *__restrict__ range,
                                                            const int *__restrict__ slot_term,
                                                            const awp_synth_cterm *__restrict__ ct,
-                                                           const float *__restrict__ stfpool, int ntout, int stride,
-                                                           int maxnstf, float *__restrict__ seis)
+                                                           const float *__restrict__ stfpool, int ntout, int ns8,
+                                                           float *__restrict__ seis)
 {
-    extern __shared__ float sm[];
-    float *stf = sm;                                   /* maxnstf rounded to 4 */
-    float *win = sm + ((maxnstf + 3) & ~3);
-    const int v = blockIdx.z, c = blockIdx.y, t0 = blockIdx.x * CV_BLOCK, tid = threadIdx.x;
+    extern __shared__ __align__(16) float sm[];
+    const int buf = ns8 + CV_Q * STRIDE;               /* floats per buffer: slip rate, then window */
+    const int v = blockIdx.z, cu = blockIdx.y, c = cu + 3 - UC, t0 = blockIdx.x * CV_BLOCK, tid = threadIdx.x;
     const int base = t0 + tid * CV_Q;
     float *out = seis + ((size_t)v * 3 + c) * ntout;
     float s[CV_Q];
 #pragma unroll
     for (int q = 0; q < CV_Q; q++) s[q] = base + q < ntout ? out[base + q] : 0.0f;
     const int2 rg = range[v];
-    for (int n = rg.x; n < rg.y; n++) {
+
+    auto meta = [&](int n) {
+        CvTerm t;
         const int slot = tl[n];
-        const awp_synth_cterm t = ct[slot_term[slot]];
-        const int nstf = t.nstf;
-        const float *uu = u + ((size_t)(slot - slot0) * 3 + c) * ntout;
-        const int w0 = t0 - (nstf - 1), wl = CV_BLOCK + nstf - 1;
-        __syncthreads();
-        for (int k = tid; k < nstf; k += CV_THREADS) stf[k] = stfpool[t.stf + k];
+        const awp_synth_cterm m = ct[slot_term[slot]];
+        t.u = u + ((size_t)slot * UC + cu) * ntout;
+        t.stf = m.stf;
+        t.nstf = m.nstf;
+        t.n8 = (m.nstf + 7) & ~7;
+        t.lo = m.lo;
+        t.hi = m.hi;
+        return t;
+    };
+    auto issue = [&](const CvTerm &t, float *b) {
+        for (int k = tid; k < t.n8; k += CV_THREADS) cp_async4(b + k, stfpool + t.stf + (k < t.nstf ? k : 0), k < t.nstf);
+        const int w0 = t0 - (t.n8 - 1), wl = CV_BLOCK + t.n8;
+        float *win = b + ns8;
         for (int y = tid; y < wl; y += CV_THREADS) {
             const int x = w0 + y;
-            win[cv_pos(y, stride)] = x >= 0 && x < ntout ? uu[x] : 0.0f;
+            const bool ok = x >= t.lo && x < t.hi;
+            cp_async4(win + (y & 7) * STRIDE + (y >> 3), t.u + (ok ? x : 0), ok);
         }
+    };
+
+    CvTerm cur{}, nxt{};
+    if (rg.x < rg.y) {
+        cur = meta(rg.x);
+        issue(cur, sm);
+    }
+    cp_async_commit();
+    for (int n = rg.x; n < rg.y; n++) {
+        float *b = sm + ((n - rg.x) & 1) * buf;
+        if (n + 1 < rg.y) {
+            nxt = meta(n + 1);
+            issue(nxt, sm + ((n + 1 - rg.x) & 1) * buf);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
         __syncthreads();
         /* acc_q = sum over k of stf[k] * u[base + q - k], k ascending
-         * (stf_subs.c:25-33); window samples before the trace are zero and
-         * add +-0 to an accumulator that starts at +0, which leaves it as the
-         * reference's shorter sum leaves it */
-        float acc[CV_Q], w[CV_Q];
+         * (stf_subs.c:25-33).  Slip-rate samples past nstf are zero and
+         * window samples before the trace are zero: those products add +-0
+         * to an accumulator that starts at +0 and so leave it as the
+         * reference's shorter sum leaves it. */
+        const float *stf = b;
+        int g = (cur.n8 >> 3) - 1;
+        const float *col = b + ns8 + tid + g;           /* column of group g in row 0 */
+        float acc[CV_Q], lo[8], hi[8];
 #pragma unroll
-        for (int q = 0; q < CV_Q; q++) {
-            acc[q] = 0.0f;
-            w[q] = win[cv_pos(tid * CV_Q + q + nstf - 1, stride)];
+        for (int q = 0; q < CV_Q; q++) acc[q] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            hi[j] = col[j * STRIDE + 1];
+            lo[j] = col[j * STRIDE];
         }
-        for (int k = 0; k < nstf; k++) {
-            const float f = stf[k];
+        for (; g >= 0; g--, col--) {
+            const int k0 = cur.n8 - 8 - 8 * g;               /* lags k0 .. k0 + 7 */
+            const float4 fa = *reinterpret_cast<const float4 *>(stf + k0);
+            const float4 fb = *reinterpret_cast<const float4 *>(stf + k0 + 4);
+            const float f[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
+            float nl[8];
 #pragma unroll
-            for (int q = 0; q < CV_Q; q++) acc[q] = acc[q] + f * w[q];
+            for (int j = 0; j < 8; j++) nl[j] = g > 0 ? col[j * STRIDE - 1] : 0.0f;
 #pragma unroll
-            for (int q = CV_Q - 1; q > 0; q--) w[q] = w[q - 1];
-            const int y = tid * CV_Q + nstf - 2 - k;
-            w[0] = y >= 0 ? win[cv_pos(y, stride)] : 0.0f;
+            for (int kk = 0; kk < 8; kk++) {
+                /* m = 8g + 7 - kk; W[q + m] = (q + 7 - kk < 8) ? lo[q + 7 - kk] : hi[q - 1 - kk] */
+#pragma unroll
+                for (int q = 0; q < CV_Q; q++) {
+                    const int j = q + 7 - kk;
+                    const float w = j < 8 ? lo[j] : hi[j - 8];
+                    acc[q] = acc[q] + f[kk] * w;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                hi[j] = lo[j];
+                lo[j] = nl[j];
+            }
         }
 #pragma unroll
         for (int q = 0; q < CV_Q; q++) s[q] = s[q] + acc[q];     /* stf_subs.c:34-36 */
+        __syncthreads();
+        cur = nxt;
     }
 #pragma unroll
     for (int q = 0; q < CV_Q; q++)
         if (base + q < ntout) out[base + q] = s[q];
+}
+
+/* window row strides (4 mod 32) and the longest slip rate each holds:
+ * rows of ceil((1024 + n8) / 8) + 1 samples */
+constexpr int CV_STRIDES[4] = {164, 260, 644, 1668};
+
+int cv_stride_for(int ns8)
+{
+    for (int st : CV_STRIDES)
+        if ((CV_BLOCK + ns8 + 7) / 8 + 1 <= st) return st;
+    return 0;
 }
 
 template <class T>
@@ -205,6 +367,42 @@ struct DBuf {
         p = nullptr;
         n = 0;
     }
+};
+
+template <class T>
+struct HBuf {                      /* pinned host staging, grown on demand */
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t reserve(size_t want)
+    {
+        if (want <= n) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaHostAlloc((void **)&p, want * sizeof(T) + 16, cudaHostAllocDefault);
+        if (e == cudaSuccess) n = want;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+/* the host side of one variation batch: planned terms, slot maps and chunk
+ * ranges, copied to the device asynchronously; two stages alternate so that
+ * the next batch is planned while the device works on this one */
+struct Stage {
+    HBuf<awp_synth_gterm> gt;
+    HBuf<awp_synth_cterm> ct;
+    HBuf<float> stf;
+    HBuf<int> slot_term, tl, multi;
+    HBuf<int2> range;
+    HBuf<int4> groups;
+    cudaEvent_t done = nullptr;
+    bool pending = false;
 };
 
 struct Variation {
@@ -239,8 +437,12 @@ struct awp_synth {
     DBuf<awp_synth_gterm> d_gt;
     DBuf<awp_synth_cterm> d_ct;
     DBuf<float> d_stf, d_u, d_seis;
-    DBuf<int> d_slot_term, d_tl;
+    DBuf<int> d_slot_term, d_tl, d_multi;
     DBuf<int2> d_range;
+    DBuf<int4> d_groups;
+    Stage stage[2];
+    HBuf<float> h_seis;
+    std::vector<cudaEvent_t> cev;  /* per chunk: before k_synth_gf, between, after k_synth_conv */
     size_t u_cap_bytes = (size_t)2 << 30;
 };
 
@@ -284,6 +486,7 @@ extern "C" awp_status awp_synth_create(const awp_synth_params *p, awp_synth **ou
     }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&s->stage[i].done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         awp_synth_destroy(s);
         return fail(AWP_ERR_CUDA, "awp_synth_create: %s", cudaGetErrorString(e));
@@ -306,6 +509,21 @@ extern "C" void awp_synth_destroy(awp_synth *s)
     s->d_slot_term.release();
     s->d_tl.release();
     s->d_range.release();
+    s->d_multi.release();
+    s->d_groups.release();
+    for (auto &st : s->stage) {
+        st.gt.release();
+        st.ct.release();
+        st.stf.release();
+        st.slot_term.release();
+        st.tl.release();
+        st.range.release();
+        st.multi.release();
+        st.groups.release();
+        if (st.done) cudaEventDestroy(st.done);
+    }
+    s->h_seis.release();
+    for (auto &e : s->cev) cudaEventDestroy(e);
     for (auto &e : s->ev)
         if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -456,13 +674,77 @@ static void synth_lengths(const awp_synth *s, int *ntsum, int *ntout)
     *ntout = s->p.ntout > 0 ? s->p.ntout : n;
 }
 
+template <int STRIDE, int UC>
+static cudaError_t launch_conv_uc(dim3 grid, size_t smem, cudaStream_t st, const float *u, const int *tl,
+                                  const int2 *range, const int *slot_term, const awp_synth_cterm *ct,
+                                  const float *stf, int ntout, int ns8, float *seis)
+{
+    cudaError_t e =
+        cudaFuncSetAttribute(k_synth_conv<STRIDE, UC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_synth_conv<STRIDE, UC><<<grid, CV_THREADS, smem, st>>>(u, tl, range, slot_term, ct, stf, ntout, ns8, seis);
+    return cudaGetLastError();
+}
+
+template <int STRIDE>
+static cudaError_t launch_conv(int uc, dim3 grid, size_t smem, cudaStream_t st, const float *u, const int *tl,
+                               const int2 *range, const int *slot_term, const awp_synth_cterm *ct, const float *stf,
+                               int ntout, int ns8, float *seis)
+{
+    grid.y = uc;
+    return uc == 3 ? launch_conv_uc<STRIDE, 3>(grid, smem, st, u, tl, range, slot_term, ct, stf, ntout, ns8, seis)
+                   : launch_conv_uc<STRIDE, 2>(grid, smem, st, u, tl, range, slot_term, ct, stf, ntout, ns8, seis);
+}
+
+template <int NC, int UC>
+static cudaError_t launch_gf_nc(int ngroups, int nmulti, int nt, int ntout, cudaStream_t st, const float *sgt,
+                                const awp_synth_gterm *gt, const int *slot_term, const int4 *groups,
+                                const int *multi, float *u)
+{
+    if (ngroups) {
+        const dim3 g((unsigned)((nt + GF_THREADS - 1) / GF_THREADS), (unsigned)ngroups);
+        k_synth_gf1<NC, UC><<<g, GF_THREADS, 0, st>>>(sgt, nt, nt - SY_TAPLEN, gt, slot_term, groups, ntout, u);
+    }
+    if (nmulti) {
+        const dim3 g((unsigned)nmulti, (unsigned)((ntout + GF_THREADS - 1) / GF_THREADS));
+        k_synth_gf<NC, UC><<<g, GF_THREADS, 0, st>>>(sgt, nt, nt - SY_TAPLEN, gt, slot_term, multi, ntout, u);
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_gf(int ncomp, int ngroups, int nmulti, int nt, int ntout, cudaStream_t st,
+                             const float *sgt, const awp_synth_gterm *gt, const int *slot_term, const int4 *groups,
+                             const int *multi, float *u)
+{
+    if (ncomp == 1) return launch_gf_nc<1, 2>(ngroups, nmulti, nt, ntout, st, sgt, gt, slot_term, groups, multi, u);
+    if (ncomp == 2) return launch_gf_nc<2, 2>(ngroups, nmulti, nt, ntout, st, sgt, gt, slot_term, groups, multi, u);
+    return launch_gf_nc<3, 3>(ngroups, nmulti, nt, ntout, st, sgt, gt, slot_term, groups, multi, u);
+}
+
+static cudaError_t events_for(awp_synth *s, int n)
+{
+    while ((int)s->cev.size() < n) {
+        cudaEvent_t ev;
+        cudaError_t e = cudaEventCreate(&ev);
+        if (e != cudaSuccess) return e;
+        s->cev.push_back(ev);
+    }
+    return cudaSuccess;
+}
+
+/* Work order: variations in batches (rv_batch, default all of them); inside
+ * a batch the rupture points in chunks.  A chunk is planned on the host (all
+ * its variations in parallel), copied, combined (k_synth_gf) and convolved
+ * into the batch's seismograms (k_synth_conv); the host plans chunk c + 1
+ * while the device runs chunk c.  Chunks hold whole points, at most the
+ * term buffer's capacity and about a quarter of the batch. */
 extern "C" awp_status awp_synth_run(awp_synth *s)
 {
     if (!s) return fail(AWP_ERR_PARAM, "awp_synth_run: null synth");
     if (!s->d_sgt) return fail(AWP_ERR_STATE, "awp_synth_run: no SGT set loaded");
     if (s->vars.empty()) return fail(AWP_ERR_STATE, "awp_synth_run: no rupture variation added");
     SCU(cudaSetDevice(s->p.device));
-    const double tp0 = now_s();
+    double t_plan = now_s();
     const int np = (int)s->vars[0].pts.size(), nv = (int)s->vars.size();
     int ntsum, ntout;
     synth_lengths(s, &ntsum, &ntout);
@@ -507,7 +789,96 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     cx.tstart = s->p.tstart;
     cx.taper = taper;
 
-    s->seis.assign((size_t)nv * 3 * ntout, 0.0f);
+    /* per variation and point: terms and slip-rate samples (prefix sums) */
+    std::vector<long long> tpre((size_t)nv * (np + 1)), spre((size_t)nv * (np + 1));
+    int maxnstf = 1;
+#pragma omp parallel for schedule(static) reduction(max : maxnstf)
+    for (int v = 0; v < nv; v++) {
+        long long t = 0, n = 0;
+        for (int ip = 0; ip < np; ip++) {
+            tpre[(size_t)v * (np + 1) + ip] = t;
+            spre[(size_t)v * (np + 1) + ip] = n;
+            const awp_srf_point &a = s->vars[v].pts[ip];
+            t += (a.nt1 > 0) + (a.nt2 > 0) + (a.nt3 > 0);
+            n += (a.nt1 > 0 ? a.nt1 : 0) + (a.nt2 > 0 ? a.nt2 : 0) + (a.nt3 > 0 ? a.nt3 : 0);
+            maxnstf = a.nt1 > maxnstf ? a.nt1 : maxnstf;
+            maxnstf = a.nt2 > maxnstf ? a.nt2 : maxnstf;
+            maxnstf = a.nt3 > maxnstf ? a.nt3 : maxnstf;
+        }
+        tpre[(size_t)v * (np + 1) + np] = t;
+        spre[(size_t)v * (np + 1) + np] = n;
+    }
+    maxnstf = maxnstf < ntout ? maxnstf : ntout;      /* longer ones are refused by the plan */
+    const int batch = s->p.rv_batch > 0 ? s->p.rv_batch : nv;
+
+    /* chunk boundaries per batch: whole points, terms <= cap */
+    const int uc = s->ncomp == 3 ? 3 : 2;             /* component traces kept per term */
+    const size_t slot_bytes = (size_t)uc * ntout * sizeof(float);
+    const long long ucap = (long long)(s->u_cap_bytes / slot_bytes) > 0 ? (long long)(s->u_cap_bytes / slot_bytes) : 1;
+    struct Chunk {
+        int v0, nb, p0, p1;
+        long long terms, samples;
+    };
+    std::vector<Chunk> chunks;
+    long long max_terms = 1, max_stf = 1;
+    for (int v0 = 0; v0 < nv; v0 += batch) {
+        const int nb = v0 + batch <= nv ? batch : nv - v0;
+        long long total = 0;
+        for (int v = v0; v < v0 + nb; v++) total += tpre[(size_t)v * (np + 1) + np];
+        long long target = (total + 3) / 4;
+        target = target < ucap ? target : ucap;
+        for (int p0 = 0; p0 < np;) {
+            long long t = 0, n = 0;
+            int p1 = p0;
+            while (p1 < np) {
+                long long dt = 0, dn = 0;
+                for (int v = v0; v < v0 + nb; v++) {
+                    const size_t o = (size_t)v * (np + 1) + p1;
+                    dt += tpre[o + 1] - tpre[o];
+                    dn += spre[o + 1] - spre[o];
+                }
+                if (p1 > p0 && t + dt > target) break;
+                t += dt, n += dn, p1++;
+            }
+            chunks.push_back({v0, nb, p0, p1, t, n});
+            max_terms = t > max_terms ? t : max_terms;
+            max_stf = n > max_stf ? n : max_stf;
+            p0 = p1;
+        }
+    }
+    if (max_terms >= (1LL << 31)) return fail(AWP_ERR_PARAM, "awp_synth_run: too many terms in one chunk");
+
+    cudaError_t e = cudaSuccess;
+    e = e ? e : s->d_gt.reserve((size_t)max_terms);
+    e = e ? e : s->d_ct.reserve((size_t)max_terms);
+    e = e ? e : s->d_stf.reserve((size_t)max_stf + 8);
+    e = e ? e : s->d_slot_term.reserve((size_t)max_terms);
+    e = e ? e : s->d_tl.reserve((size_t)max_terms);
+    e = e ? e : s->d_range.reserve((size_t)batch);
+    e = e ? e : s->d_multi.reserve((size_t)max_terms);
+    e = e ? e : s->d_groups.reserve((size_t)np);
+    e = e ? e : s->d_u.reserve((size_t)max_terms * uc * ntout);
+    e = e ? e : s->d_seis.reserve((size_t)nv * 3 * ntout);
+    e = e ? e : s->h_seis.reserve((size_t)nv * 3 * ntout);
+    for (auto &sg : s->stage) {
+        e = e ? e : sg.gt.reserve((size_t)max_terms);
+        e = e ? e : sg.ct.reserve((size_t)max_terms);
+        e = e ? e : sg.stf.reserve((size_t)max_stf + 8);
+        e = e ? e : sg.slot_term.reserve((size_t)max_terms);
+        e = e ? e : sg.tl.reserve((size_t)max_terms);
+        e = e ? e : sg.range.reserve((size_t)batch);
+        e = e ? e : sg.multi.reserve((size_t)max_terms);
+        e = e ? e : sg.groups.reserve((size_t)np);
+    }
+    if (e != cudaSuccess) return fail(AWP_ERR_OOM, "awp_synth_run: buffers: %s", cudaGetErrorString(e));
+    /* the range table is per chunk: one device copy per stage */
+    static_assert(sizeof(int2) == 8, "int2");
+
+    const int ns8 = (maxnstf + 7) & ~7;
+    const int stride = cv_stride_for(ns8);
+    if (!stride) return fail(AWP_ERR_PARAM, "awp_synth_run: slip-rate functions too long (%d samples)", maxnstf);
+    const size_t cv_smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)CV_Q * stride);
+
     s->nseis = 0;
     s->info = awp_synth_info{};
     s->info.ncomp = s->ncomp;
@@ -515,172 +886,160 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     s->info.ntsum = ntsum;
     s->info.nsgt_points = nm;
     s->info.non_exact = non_exact;
-    double plan_s = now_s() - tp0, dev_s = 0.0, conv_s = 0.0;
-    int launches = 0;
+    double plan_s = now_s() - t_plan;
+    int launches = 0, nk = 0;     /* chunks launched; chunk j is timed by events 3j .. 3j + 2 */
 
-    const int batch = s->p.rv_batch > 0 ? s->p.rv_batch : nv;
-    for (int v0 = 0; v0 < nv; v0 += batch) {
-        const double tb = now_s();
-        const int nb = v0 + batch <= nv ? batch : nv - v0;
-        /* per variation: terms and samples, then the plan in parallel */
-        std::vector<long long> toff(nb + 1, 0), soff(nb + 1, 0);
+    SCU(cudaEventRecord(s->ev[0], s->stream));
+    SCU(cudaMemsetAsync(s->d_seis.p, 0, (size_t)nv * 3 * ntout * sizeof(float), s->stream));
+    std::vector<long long> toff, soff, pbase;
+    std::vector<int> pslot;
+    for (size_t ic = 0; ic < chunks.size(); ic++) {
+        t_plan = now_s();
+        const Chunk &C = chunks[ic];
+        const int nb = C.nb, p0 = C.p0, p1 = C.p1, npc = p1 - p0;
+        Stage &S = s->stage[ic & 1];
+        if (S.pending) SCU(cudaEventSynchronize(S.done));   /* its copies of two chunks ago are done */
+        S.pending = false;
+        /* chunk-local term numbering: variation-major (each variation's terms
+         * contiguous, in point order); slots: point-major */
+        toff.assign(nb + 1, 0);
+        soff.assign(nb + 1, 0);
         for (int b = 0; b < nb; b++) {
-            const Variation &v = s->vars[v0 + b];
-            long long ns = 0;
-            for (auto &a : v.pts) ns += (a.nt1 > 0 ? a.nt1 : 0) + (a.nt2 > 0 ? a.nt2 : 0) + (a.nt3 > 0 ? a.nt3 : 0);
-            toff[b + 1] = toff[b] + awp_synth_count_terms(v.pts.data(), np);
-            soff[b + 1] = soff[b] + ns;
+            const size_t o = (size_t)(C.v0 + b) * (np + 1);
+            toff[b + 1] = toff[b] + tpre[o + p1] - tpre[o + p0];
+            soff[b + 1] = soff[b] + spre[o + p1] - spre[o + p0];
         }
         const long long nterm = toff[nb];
-        if (nterm >= (1LL << 31)) return fail(AWP_ERR_PARAM, "awp_synth_run: too many terms in one batch; set rv_batch");
-        std::vector<awp_synth_gterm> gt((size_t)nterm);
-        std::vector<awp_synth_cterm> ctv((size_t)nterm);
-        std::vector<float> stf((size_t)soff[nb] + 1);
         std::vector<long long> macs(nb, 0);
         std::vector<awp_status> pst(nb, AWP_OK);
 #pragma omp parallel for schedule(dynamic, 1)
         for (int b = 0; b < nb; b++) {
-            const Variation &v = s->vars[v0 + b];
+            const Variation &v = s->vars[C.v0 + b];
             long long nterms = 0, nused = 0;
-            pst[b] = awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(),
-                                              gt.data() + toff[b], ctv.data() + toff[b], stf.data() + soff[b], soff[b],
+            pst[b] = awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(), p0, p1,
+                                              S.gt.p + toff[b], S.ct.p + toff[b], S.stf.p + soff[b], soff[b],
                                               &nterms, &nused, &macs[b]);
         }
         for (int b = 0; b < nb; b++)
             if (pst[b] != AWP_OK) {
                 /* the error text is per thread: plan the variation again here */
-                const Variation &v = s->vars[v0 + b];
-                long long a, c, d;
-                return awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(),
-                                                gt.data() + toff[b], ctv.data() + toff[b], stf.data() + soff[b],
-                                                soff[b], &a, &c, &d);
+                SCU(cudaStreamSynchronize(s->stream));
+                for (auto &sg : s->stage) sg.pending = false;
+                const Variation &v = s->vars[C.v0 + b];
+                long long a1, a2, a3;
+                return awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(), p0, p1,
+                                                S.gt.p + toff[b], S.ct.p + toff[b], S.stf.p + soff[b], soff[b], &a1,
+                                                &a2, &a3);
             }
-        for (int b = 0; b < nb; b++) s->info.macs += macs[b];
+        for (int b = 0; b < nb; b++) s->info.macs += macs[b] * uc;
         s->info.terms += nterm;
-
-        /* point-major slot order: slot -> term; each variation's slots in
-         * point order (its term list for the convolution) */
-        std::vector<long long> pstart((size_t)nb * (np + 1));
-        for (int b = 0; b < nb; b++) {
-            const Variation &v = s->vars[v0 + b];
-            long long t = toff[b];
-            for (int ip = 0; ip < np; ip++) {
-                pstart[(size_t)b * (np + 1) + ip] = t;
-                const awp_srf_point &a = v.pts[ip];
-                t += (a.nt1 > 0) + (a.nt2 > 0) + (a.nt3 > 0);
-            }
-            pstart[(size_t)b * (np + 1) + np] = t;
-        }
-        std::vector<int> slot_term((size_t)nterm), tl((size_t)nterm), pslot(np + 1);
-        long long sl = 0;
-        for (int ip = 0; ip < np; ip++) {
-            pslot[ip] = (int)sl;
+        for (int k = 0; k < 8; k++) S.stf.p[soff[nb] + k] = 0.0f;
+        /* slots of point ip start at pslot[ip - p0]; a point's slots hold its
+         * variations in order */
+        pslot.assign(npc + 1, 0);
+        for (int i = 0; i < npc; i++) {
+            long long n = 0;
             for (int b = 0; b < nb; b++) {
-                const long long a0 = pstart[(size_t)b * (np + 1) + ip], a1 = pstart[(size_t)b * (np + 1) + ip + 1];
-                for (long long t = a0; t < a1; t++) {
-                    slot_term[sl] = (int)t;
-                    tl[t] = (int)sl;          /* term t of variation b sits in slot sl */
-                    sl++;
+                const size_t o = (size_t)(C.v0 + b) * (np + 1) + p0 + i;
+                n += tpre[o + 1] - tpre[o];
+            }
+            pslot[i + 1] = pslot[i] + (int)n;
+        }
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < npc; i++) {
+            long long sl = pslot[i];
+            for (int b = 0; b < nb; b++) {
+                const size_t o = (size_t)(C.v0 + b) * (np + 1);
+                const long long a0 = toff[b] + tpre[o + p0 + i] - tpre[o + p0];
+                const long long a1 = a0 + tpre[o + p0 + i + 1] - tpre[o + p0 + i];
+                for (long long t = a0; t < a1; t++, sl++) {
+                    S.slot_term.p[sl] = (int)t;
+                    S.tl.p[t] = (int)sl;
                 }
             }
         }
-        pslot[np] = (int)sl;
-        /* a variation's terms are contiguous and in point order, so tl
-         * indexed by term is each variation's slot list */
-        int maxnstf = 1;
-        for (auto &c : ctv) maxnstf = c.nstf > maxnstf ? c.nstf : maxnstf;
+        for (int b = 0; b < nb; b++) S.range.p[b] = make_int2((int)toff[b], (int)toff[b + 1]);
+        /* exactly matched points go to the per-point kernel, the others'
+         * slots to the per-term one */
+        int ngroups = 0, nmulti = 0;
+        for (int i = 0; i < npc; i++) {
+            const int n = pslot[i + 1] - pslot[i];
+            if (!n) continue;
+            const awp_synth_bracket &bk = br[p0 + i];
+            if (bk.nsgt == 1) S.groups.p[ngroups++] = make_int4(bk.pos[0], pslot[i], n, 0);
+            else
+                for (int k = pslot[i]; k < pslot[i + 1]; k++) S.multi.p[nmulti++] = k;
+        }
+        plan_s += now_s() - t_plan;
 
-        const size_t slot_bytes = (size_t)3 * ntout * sizeof(float);
-        long long cap = (long long)(s->u_cap_bytes / slot_bytes);
-        if (cap < 1) cap = 1;
-        long long maxslots = 0;
-        for (int ip = 0; ip < np; ip++)
-            maxslots = pslot[ip + 1] - pslot[ip] > maxslots ? pslot[ip + 1] - pslot[ip] : maxslots;
-        if (maxslots > cap) cap = maxslots;   /* one point's terms always fit */
-        const long long ucap = cap < nterm ? cap : (nterm > 0 ? nterm : 1);
-
-        cudaError_t e = cudaSuccess;
-        e = e ? e : s->d_gt.reserve((size_t)nterm);
-        e = e ? e : s->d_ct.reserve((size_t)nterm);
-        e = e ? e : s->d_stf.reserve(stf.size());
-        e = e ? e : s->d_slot_term.reserve((size_t)nterm);
-        e = e ? e : s->d_tl.reserve((size_t)nterm);
-        e = e ? e : s->d_range.reserve((size_t)nb);
-        e = e ? e : s->d_u.reserve((size_t)ucap * 3 * ntout);
-        e = e ? e : s->d_seis.reserve((size_t)nb * 3 * ntout);
-        if (e != cudaSuccess) return fail(AWP_ERR_OOM, "awp_synth_run: device buffers: %s", cudaGetErrorString(e));
-        plan_s += now_s() - tb;
-
-        SCU(cudaEventRecord(s->ev[0], s->stream));
         if (nterm) {
-            SCU(cudaMemcpyAsync(s->d_gt.p, gt.data(), gt.size() * sizeof(awp_synth_gterm), cudaMemcpyHostToDevice,
+            SCU(cudaMemcpyAsync(s->d_gt.p, S.gt.p, nterm * sizeof(awp_synth_gterm), cudaMemcpyHostToDevice, s->stream));
+            SCU(cudaMemcpyAsync(s->d_ct.p, S.ct.p, nterm * sizeof(awp_synth_cterm), cudaMemcpyHostToDevice, s->stream));
+            SCU(cudaMemcpyAsync(s->d_slot_term.p, S.slot_term.p, nterm * sizeof(int), cudaMemcpyHostToDevice,
                                 s->stream));
-            SCU(cudaMemcpyAsync(s->d_ct.p, ctv.data(), ctv.size() * sizeof(awp_synth_cterm), cudaMemcpyHostToDevice,
+            SCU(cudaMemcpyAsync(s->d_tl.p, S.tl.p, nterm * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+            SCU(cudaMemcpyAsync(s->d_stf.p, S.stf.p, (soff[nb] + 8) * sizeof(float), cudaMemcpyHostToDevice,
                                 s->stream));
-            SCU(cudaMemcpyAsync(s->d_slot_term.p, slot_term.data(), slot_term.size() * sizeof(int),
-                                cudaMemcpyHostToDevice, s->stream));
-            SCU(cudaMemcpyAsync(s->d_tl.p, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+            SCU(cudaMemcpyAsync(s->d_range.p, S.range.p, (size_t)nb * sizeof(int2), cudaMemcpyHostToDevice,
+                                s->stream));
+            if (ngroups)
+                SCU(cudaMemcpyAsync(s->d_groups.p, S.groups.p, (size_t)ngroups * sizeof(int4), cudaMemcpyHostToDevice,
+                                    s->stream));
+            if (nmulti)
+                SCU(cudaMemcpyAsync(s->d_multi.p, S.multi.p, (size_t)nmulti * sizeof(int), cudaMemcpyHostToDevice,
+                                    s->stream));
         }
-        SCU(cudaMemcpyAsync(s->d_stf.p, stf.data(), stf.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        SCU(cudaMemsetAsync(s->d_seis.p, 0, (size_t)nb * 3 * ntout * sizeof(float), s->stream));
-
-        /* convolution launch shape */
-        const int stride = ((((CV_BLOCK + maxnstf - 1) + CV_Q - 1) / CV_Q + 1 + 27) / 32) * 32 + 4;
-        const size_t cv_smem = sizeof(float) * (((maxnstf + 3) & ~3) + (size_t)CV_Q * stride);
-        if (cv_smem > 227 * 1024) return fail(AWP_ERR_PARAM, "awp_synth_run: slip-rate functions too long");
-        SCU(cudaFuncSetAttribute(k_synth_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cv_smem));
-        std::vector<int2> range(nb);
-        float conv_ms = 0.0f;
-        for (int p0 = 0; p0 < np;) {
-            int p1 = p0;
-            while (p1 < np && pslot[p1 + 1] - pslot[p0] <= ucap) p1++;
-            if (p1 == p0) p1 = p0 + 1;
-            const long long s0 = pslot[p0], ns = pslot[p1] - pslot[p0];
-            if (ns > 0) {
-                const dim3 g1((unsigned)ns, (unsigned)((ntout + GF_THREADS - 1) / GF_THREADS));
-                if (s->ncomp == 1)
-                    k_synth_gf<1><<<g1, GF_THREADS, 0, s->stream>>>(s->d_sgt, nt, nt - SY_TAPLEN, s->d_gt.p,
-                                                                    s->d_slot_term.p, s0, ntout, s->d_u.p);
-                else if (s->ncomp == 2)
-                    k_synth_gf<2><<<g1, GF_THREADS, 0, s->stream>>>(s->d_sgt, nt, nt - SY_TAPLEN, s->d_gt.p,
-                                                                    s->d_slot_term.p, s0, ntout, s->d_u.p);
-                else
-                    k_synth_gf<3><<<g1, GF_THREADS, 0, s->stream>>>(s->d_sgt, nt, nt - SY_TAPLEN, s->d_gt.p,
-                                                                    s->d_slot_term.p, s0, ntout, s->d_u.p);
-                SCU(cudaGetLastError());
-                for (int b = 0; b < nb; b++)
-                    range[b] = make_int2((int)pstart[(size_t)b * (np + 1) + p0], (int)pstart[(size_t)b * (np + 1) + p1]);
-                SCU(cudaMemcpyAsync(s->d_range.p, range.data(), nb * sizeof(int2), cudaMemcpyHostToDevice, s->stream));
-                SCU(cudaEventRecord(s->ev[2], s->stream));
-                const dim3 g2((unsigned)((ntout + CV_BLOCK - 1) / CV_BLOCK), 3, (unsigned)nb);
-                k_synth_conv<<<g2, CV_THREADS, cv_smem, s->stream>>>(s->d_u.p, s->d_tl.p, s->d_range.p, s0,
-                                                                      s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout,
-                                                                      stride, maxnstf, s->d_seis.p);
-                SCU(cudaGetLastError());
-                SCU(cudaEventRecord(s->ev[3], s->stream));
-                /* the range table is rewritten by the next chunk */
-                SCU(cudaEventSynchronize(s->ev[3]));
-                float ms = 0.0f;
-                SCU(cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]));
-                conv_ms += ms;
-                launches += 2;
-            }
-            p0 = p1;
-        }
-        SCU(cudaMemcpyAsync(s->seis.data() + (size_t)v0 * 3 * ntout, s->d_seis.p, (size_t)nb * 3 * ntout * sizeof(float),
-                            cudaMemcpyDeviceToHost, s->stream));
-        SCU(cudaEventRecord(s->ev[1], s->stream));
-        SCU(cudaEventSynchronize(s->ev[1]));
-        float ms = 0.0f;
-        SCU(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
-        dev_s += ms * 1e-3;
-        conv_s += conv_ms * 1e-3;
+        SCU(cudaEventRecord(S.done, s->stream));
+        S.pending = true;
+        if (!nterm) continue;
+        float *seis_b = s->d_seis.p + (size_t)C.v0 * 3 * ntout;
+        SCU(events_for(s, 3 * (nk + 1)));
+        SCU(cudaEventRecord(s->cev[3 * nk], s->stream));
+        SCU(launch_gf(s->ncomp, ngroups, nmulti, nt, ntout, s->stream, s->d_sgt, s->d_gt.p, s->d_slot_term.p,
+                      s->d_groups.p, s->d_multi.p, s->d_u.p));
+        SCU(cudaEventRecord(s->cev[3 * nk + 1], s->stream));
+        const dim3 g2((unsigned)((ntout + CV_BLOCK - 1) / CV_BLOCK), 3, (unsigned)nb);
+        if (stride == CV_STRIDES[0])
+            e = launch_conv<CV_STRIDES[0]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
+                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
+        else if (stride == CV_STRIDES[1])
+            e = launch_conv<CV_STRIDES[1]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
+                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
+        else if (stride == CV_STRIDES[2])
+            e = launch_conv<CV_STRIDES[2]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
+                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
+        else
+            e = launch_conv<CV_STRIDES[3]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
+                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
+        SCU(e);
+        SCU(cudaEventRecord(s->cev[3 * nk + 2], s->stream));
+        nk++;
+        launches += (ngroups > 0) + (nmulti > 0) + 1;
+        const bool last_of_batch = ic + 1 == chunks.size() || chunks[ic + 1].v0 != C.v0;
+        if (last_of_batch)
+            SCU(cudaMemcpyAsync(s->h_seis.p + (size_t)C.v0 * 3 * ntout, seis_b, (size_t)nb * 3 * ntout * sizeof(float),
+                                cudaMemcpyDeviceToHost, s->stream));
     }
+    SCU(cudaEventRecord(s->ev[1], s->stream));
+    SCU(cudaEventSynchronize(s->ev[1]));
+    for (auto &sg : s->stage) sg.pending = false;
+    float ms = 0.0f;
+    SCU(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
+    double gf_s = 0.0, conv_s = 0.0;
+    for (int j = 0; j < nk; j++) {
+        float a = 0.0f, c = 0.0f;
+        SCU(cudaEventElapsedTime(&a, s->cev[3 * j], s->cev[3 * j + 1]));
+        SCU(cudaEventElapsedTime(&c, s->cev[3 * j + 1], s->cev[3 * j + 2]));
+        gf_s += a * 1e-3;
+        conv_s += c * 1e-3;
+    }
+    s->seis.assign(s->h_seis.p, s->h_seis.p + (size_t)nv * 3 * ntout);
     s->nseis = nv;
     s->info.nvariations = nv;
     s->info.seconds_plan = plan_s;
-    s->info.seconds_device = dev_s;
+    s->info.seconds_device = ms * 1e-3;
     s->info.seconds_conv = conv_s;
+    s->info.seconds_gf = gf_s;
     s->info.gpu_launches = launches;
     return AWP_OK;
 }

@@ -32,6 +32,7 @@ typedef struct {
 typedef struct {
     long long stf;            /* offset in the run's sample pool                  */
     int nstf;
+    int lo, hi;               /* output samples the SGTs reach; the rest are +0   */
     int pad;
 } awp_synth_cterm;
 
@@ -61,7 +62,8 @@ typedef struct {
 void awp_synth_find_sgt(const awp_sgtindex *ix, int np, const awp_sgtindex *eq, const awp_sgtindex *stat,
                         awp_synth_bracket *out);
 
-/* One variation's terms: for each point in order, its slip components.
+/* One variation's terms for points ip0 .. ip1 - 1: for each point in order,
+ * its slip components.
  * gt/ct/stf are caller-sized with awp_synth_count_terms / pool sizes.
  * Returns AWP_OK or AWP_ERR_PARAM (text set) on an SRF the path rejects. */
 typedef struct {
@@ -75,8 +77,9 @@ typedef struct {
 
 long long awp_synth_count_terms(const awp_srf_point *pts, int np);
 awp_status awp_synth_plan_variation(const awp_synth_plan_ctx *cx, const awp_srf_point *pts, const float *pool,
-                                    long long npool, awp_synth_gterm *gt, awp_synth_cterm *ct, float *stf,
-                                    long long stf_base, long long *nterms, long long *nstf_used, long long *macs);
+                                    long long npool, int ip0, int ip1, awp_synth_gterm *gt, awp_synth_cterm *ct,
+                                    float *stf, long long stf_base, long long *nterms, long long *nstf_used,
+                                    long long *macs);
 
 void awp_synth_taper(int nt, float *fac);
 

@@ -186,19 +186,20 @@ long long awp_synth_count_terms(const awp_srf_point *pts, int np)
     return n;
 }
 
-/* One variation, every point in order: get_srfpars (srf_rupm.c:7-53), the
+/* One variation, points ip0 .. ip1 - 1 in order: get_srfpars (srf_rupm.c:7-53), the
  * scalars of mech_sgt (sgt3d_subs.c:1260-1422), the time shifts of sum_sgt /
  * timeshift_sgt (:1121-1258) and the dt-scaled slip rates of srf_stf
  * (srf_rupm.c:55-153). */
 awp_status awp_synth_plan_variation(const awp_synth_plan_ctx *cx, const awp_srf_point *pts, const float *pool,
-                                    long long npool, awp_synth_gterm *gt, awp_synth_cterm *ct, float *stf,
-                                    long long stf_base, long long *nterms, long long *nstf_used, long long *macs)
+                                    long long npool, int ip0, int ip1, awp_synth_gterm *gt, awp_synth_cterm *ct,
+                                    float *stf, long long stf_base, long long *nterms, long long *nstf_used,
+                                    long long *macs)
 {
     const float rperd = 0.017453293f, two = 2.0f;
     const float ratio_tol = 0.00001f;
     const float ptol = (float)(1.0 + ratio_tol), mtol = (float)(1.0 - ratio_tol);
     long long nt_ = 0, ns = 0, mac = 0;
-    for (int ip = 0; ip < cx->np; ip++) {
+    for (int ip = ip0; ip < ip1; ip++) {
         const awp_srf_point *a = &pts[ip];
         const awp_synth_bracket *b = &cx->br[ip];
         int flag[3], nmech = 0;
@@ -291,9 +292,13 @@ awp_status awp_synth_plan_variation(const awp_synth_plan_ctx *cx, const awp_srf_
             c->stf = stf_base + ns;
             c->nstf = nstf;
             c->pad = 0;
+            /* a single SGT point reaches [lo, hi) only; with several the
+             * combination kernel writes every sample */
+            c->lo = b->nsgt == 1 ? g->lo[0] : 0;
+            c->hi = b->nsgt == 1 ? g->hi[0] : cx->ntout;
             ns += nstf;
-            /* sum over it < ntout of min(it + 1, nstf), times three components */
-            mac += 3 * ((long long)nstf * (nstf + 1) / 2 + (long long)(cx->ntout - nstf) * nstf);
+            /* per component: sum over it < ntout of min(it + 1, nstf) */
+            mac += (long long)nstf * (nstf + 1) / 2 + (long long)(cx->ntout - nstf) * nstf;
             nt_++;
         }
     }

@@ -20,7 +20,7 @@
  *     the .sgthead point list (the "separate header" files read by
  *     DirectSynth/src/sgt_handler.c:276-333);
  *   - the x component's SGT headers are used for every component, with ymom
- *     and zmom set to its xmom (synth.c:499-514), and the components' moments
+ *     and zmom set to its xmom (synth.c:545-557), and the components' moments
  *     must agree (sgt_handler.c:226-242);
  *   - a seismogram is float32 [3][ntout] in the order vertical, north, east
  *     (sgt3d_subs.c:1190-1192); the output file keeps the components that
@@ -82,11 +82,14 @@ typedef struct {
     int nvariations;     /* variations synthesised by the last run              */
     int ncomp;           /* SGT components loaded (1..3)                        */
     long long terms;     /* (variation, point, slip component) convolutions     */
-    long long macs;      /* multiply-adds of those convolutions                 */
+    long long macs;      /* multiply-adds the convolutions performed (components
+                            with SGTs; a run without z SGTs skips the vertical,
+                            which is +0 throughout)                              */
     double seconds_plan; /* host set-up of the last run                         */
     double seconds_device; /* device time of the last run (events)              */
     double seconds_conv; /* device time of the convolution kernels              */
     int gpu_launches;    /* kernels launched by the last run                    */
+    double seconds_gf;   /* device time of the SGT combination kernels          */
 } awp_synth_info;
 
 awp_status awp_synth_create(const awp_synth_params *p, awp_synth **out);
