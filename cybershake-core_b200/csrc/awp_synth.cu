@@ -57,8 +57,6 @@ awp_status fail(awp_status st, const char *fmt, ...)
 
 constexpr int GF_THREADS = 256;
 constexpr int CV_THREADS = 128;
-constexpr int CV_Q = 8;                   /* consecutive outputs per thread  */
-constexpr int CV_BLOCK = CV_THREADS * CV_Q;
 
 __constant__ float c_taper[SY_TAPLEN];
 
@@ -195,11 +193,6 @@ __global__ void __launch_bounds__(GF_THREADS) k_synth_gf1(const float *__restric
 
 /* ---- kernel 2: slip-rate convolution, terms in rupture-point order ------- */
 
-/* shared-memory position of window sample y: Q interleaved rows, so that the
- * one new sample each thread loads per step (y = 8 * tid + const) hits 32
- * different banks; the row stride is 4 mod 32 for the same reason on fill */
-__device__ __forceinline__ int cv_pos(int y, int stride) { return (y & (CV_Q - 1)) * stride + (y >> 3); }
-
 __device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -209,141 +202,133 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-struct CvTerm {
-    const float *u;       /* this term's component trace              */
-    long long stf;        /* slip-rate offset in the pool             */
-    int n8;               /* samples rounded up to 8 (zero padded)    */
-    int nstf;
-    int lo, hi;           /* trace samples written; the rest are +0   */
-};
-
-/* Each CTA owns 1024 consecutive output samples (8 per thread) of one
- * component of one variation and walks the variation's terms in
+/* Each CTA owns CV_THREADS * Q consecutive output samples (Q per thread)
+ * of one component of one variation and walks the variation's terms in
  * rupture-point order.  The window of term n + 1 (its trace around the block
  * and its slip rate) is copied into the other shared buffer with cp.async
- * while term n is convolved.
+ * while term n is convolved; term records are read two terms ahead.
  *
- * Inside a term, thread samples W[j] = window[8 tid + j] feed its outputs
- * q = 0..7 at lag k through W[q + m], m = n8 - 1 - k.  Lags go in groups of
- * eight (m = 8g+7 .. 8g, g descending): a group needs W[8g .. 8g+14], held
- * as lo = W[8g..8g+7] and hi = W[8g+8..8g+15]; the next group's lo is loaded
- * while this one computes.  W[8g + j] sits in shared row j at column tid + g
- * (rows STRIDE apart, STRIDE = 4 mod 32), so the loads of a warp hit 32
- * banks and their offsets are immediates. */
-template <int STRIDE, int UC>
-__global__ void __launch_bounds__(CV_THREADS) k_synth_conv(const float *__restrict__ u, const int *__restrict__ tl,
+ * Inside a term, thread samples W[j] = window[Q tid + j] feed its outputs
+ * q = 0..Q-1 at lag k through W[q + m], m = n8 - 1 - k.  Lags go in groups
+ * of Q (m = Qg+Q-1 .. Qg, g descending): a group needs W[Qg .. Qg+2Q-2],
+ * held as lo = W[Qg..Qg+Q-1] and hi = W[Qg+Q..Qg+2Q-1]; the next group's lo
+ * is loaded while this one computes.  W[Qg + j] sits in shared row j at
+ * column tid + g (rows STRIDE apart, STRIDE = 32/Q mod 32), so the loads of
+ * a warp hit 32 banks and their offsets are immediates. */
+template <int Q, int STRIDE, int UC>
+__global__ void __launch_bounds__(CV_THREADS) k_synth_conv(const float *__restrict__ u,
                                                            const int2 *__restrict__ range,
-                                                           const int *__restrict__ slot_term,
                                                            const awp_synth_cterm *__restrict__ ct,
                                                            const float *__restrict__ stfpool, int ntout, int ns8,
                                                            float *__restrict__ seis)
 {
+    static_assert(Q == 4 || Q == 8, "Q");
+    static_assert(STRIDE % 32 == 32 / Q, "stride");
+    constexpr int BLOCK = CV_THREADS * Q;
     extern __shared__ __align__(16) float sm[];
-    const int buf = ns8 + CV_Q * STRIDE;               /* floats per buffer: slip rate, then window */
-    const int v = blockIdx.z, cu = blockIdx.y, c = cu + 3 - UC, t0 = blockIdx.x * CV_BLOCK, tid = threadIdx.x;
-    const int base = t0 + tid * CV_Q;
-    float *out = seis + ((size_t)v * 3 + c) * ntout;
-    float s[CV_Q];
+    const int buf = ns8 + Q * STRIDE;                  /* floats per buffer: slip rate, then window */
+    const int v = blockIdx.z, cu = blockIdx.y, t0 = blockIdx.x * BLOCK, tid = threadIdx.x;
+    const int base = t0 + tid * Q;
+    float *out = seis + ((size_t)v * 3 + cu + 3 - UC) * ntout;
+    float s[Q];
 #pragma unroll
-    for (int q = 0; q < CV_Q; q++) s[q] = base + q < ntout ? out[base + q] : 0.0f;
+    for (int q = 0; q < Q; q++) s[q] = base + q < ntout ? out[base + q] : 0.0f;
     const int2 rg = range[v];
 
-    auto meta = [&](int n) {
-        CvTerm t;
-        const int slot = tl[n];
-        const awp_synth_cterm m = ct[slot_term[slot]];
-        t.u = u + ((size_t)slot * UC + cu) * ntout;
-        t.stf = m.stf;
-        t.nstf = m.nstf;
-        t.n8 = (m.nstf + 7) & ~7;
-        t.lo = m.lo;
-        t.hi = m.hi;
-        return t;
-    };
-    auto issue = [&](const CvTerm &t, float *b) {
-        for (int k = tid; k < t.n8; k += CV_THREADS) cp_async4(b + k, stfpool + t.stf + (k < t.nstf ? k : 0), k < t.nstf);
-        const int w0 = t0 - (t.n8 - 1), wl = CV_BLOCK + t.n8;
+    auto issue = [&](const awp_synth_cterm &t, float *b) {
+        const int n8 = (t.nstf + 7) & ~7;
+        for (int k = tid; k < n8; k += CV_THREADS) cp_async4(b + k, stfpool + t.stf + (k < t.nstf ? k : 0), k < t.nstf);
+        const float *tr = u + ((size_t)t.slot * UC + cu) * ntout;
+        const int w0 = t0 - (n8 - 1), wl = BLOCK + n8;
         float *win = b + ns8;
         for (int y = tid; y < wl; y += CV_THREADS) {
             const int x = w0 + y;
             const bool ok = x >= t.lo && x < t.hi;
-            cp_async4(win + (y & 7) * STRIDE + (y >> 3), t.u + (ok ? x : 0), ok);
+            cp_async4(win + (y % Q) * STRIDE + y / Q, tr + (ok ? x : 0), ok);
         }
     };
 
-    CvTerm cur{}, nxt{};
+    awp_synth_cterm cur{}, nxt{}, nn{};
     if (rg.x < rg.y) {
-        cur = meta(rg.x);
+        cur = ct[rg.x];
         issue(cur, sm);
     }
     cp_async_commit();
+    if (rg.x + 1 < rg.y) nxt = ct[rg.x + 1];
     for (int n = rg.x; n < rg.y; n++) {
         float *b = sm + ((n - rg.x) & 1) * buf;
-        if (n + 1 < rg.y) {
-            nxt = meta(n + 1);
-            issue(nxt, sm + ((n + 1 - rg.x) & 1) * buf);
-        }
+        if (n + 2 < rg.y) nn = ct[n + 2];
+        if (n + 1 < rg.y) issue(nxt, sm + ((n + 1 - rg.x) & 1) * buf);
         cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
         /* acc_q = sum over k of stf[k] * u[base + q - k], k ascending
          * (stf_subs.c:25-33).  Slip-rate samples past nstf are zero and
-         * window samples before the trace are zero: those products add +-0
-         * to an accumulator that starts at +0 and so leave it as the
+         * window samples outside the written trace are zero: those products
+         * add +-0 to an accumulator that starts at +0 and so leave it as the
          * reference's shorter sum leaves it. */
+        const int n8 = (cur.nstf + 7) & ~7;
         const float *stf = b;
-        int g = (cur.n8 >> 3) - 1;
+        int g = n8 / Q - 1;
         const float *col = b + ns8 + tid + g;           /* column of group g in row 0 */
-        float acc[CV_Q], lo[8], hi[8];
+        float acc[Q], lo[Q], hi[Q];
 #pragma unroll
-        for (int q = 0; q < CV_Q; q++) acc[q] = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            hi[j] = col[j * STRIDE + 1];
-            lo[j] = col[j * STRIDE];
+        for (int q = 0; q < Q; q++) {
+            acc[q] = 0.0f;
+            hi[q] = col[q * STRIDE + 1];
+            lo[q] = col[q * STRIDE];
         }
         for (; g >= 0; g--, col--) {
-            const int k0 = cur.n8 - 8 - 8 * g;               /* lags k0 .. k0 + 7 */
-            const float4 fa = *reinterpret_cast<const float4 *>(stf + k0);
-            const float4 fb = *reinterpret_cast<const float4 *>(stf + k0 + 4);
-            const float f[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
-            float nl[8];
+            const int k0 = n8 - Q - Q * g;                 /* lags k0 .. k0 + Q - 1 */
+            float f[Q];
 #pragma unroll
-            for (int j = 0; j < 8; j++) nl[j] = g > 0 ? col[j * STRIDE - 1] : 0.0f;
+            for (int h = 0; h < Q / 4; h++) {
+                const float4 fv = *reinterpret_cast<const float4 *>(stf + k0 + 4 * h);
+                f[4 * h] = fv.x, f[4 * h + 1] = fv.y, f[4 * h + 2] = fv.z, f[4 * h + 3] = fv.w;
+            }
+            float nl[Q];
 #pragma unroll
-            for (int kk = 0; kk < 8; kk++) {
-                /* m = 8g + 7 - kk; W[q + m] = (q + 7 - kk < 8) ? lo[q + 7 - kk] : hi[q - 1 - kk] */
+            for (int j = 0; j < Q; j++) nl[j] = g > 0 ? col[j * STRIDE - 1] : 0.0f;
 #pragma unroll
-                for (int q = 0; q < CV_Q; q++) {
-                    const int j = q + 7 - kk;
-                    const float w = j < 8 ? lo[j] : hi[j - 8];
+            for (int kk = 0; kk < Q; kk++) {
+                /* m = Qg + Q-1 - kk: W[q + m] = lo / hi [q + Q-1 - kk] */
+#pragma unroll
+                for (int q = 0; q < Q; q++) {
+                    const int j = q + Q - 1 - kk;
+                    const float w = j < Q ? lo[j] : hi[j - Q];
                     acc[q] = acc[q] + f[kk] * w;
                 }
             }
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
+            for (int j = 0; j < Q; j++) {
                 hi[j] = lo[j];
                 lo[j] = nl[j];
             }
         }
 #pragma unroll
-        for (int q = 0; q < CV_Q; q++) s[q] = s[q] + acc[q];     /* stf_subs.c:34-36 */
+        for (int q = 0; q < Q; q++) s[q] = s[q] + acc[q];     /* stf_subs.c:34-36 */
         __syncthreads();
         cur = nxt;
+        nxt = nn;
     }
 #pragma unroll
-    for (int q = 0; q < CV_Q; q++)
+    for (int q = 0; q < Q; q++)
         if (base + q < ntout) out[base + q] = s[q];
 }
 
-/* window row strides (4 mod 32) and the longest slip rate each holds:
- * rows of ceil((1024 + n8) / 8) + 1 samples */
-constexpr int CV_STRIDES[4] = {164, 260, 644, 1668};
+/* window row strides (32/Q mod 32) by outputs per thread; a stride holds
+ * slip rates of n8 <= Q (STRIDE - 1) - CV_THREADS Q + 1 samples */
+constexpr int CV_STRIDES8[4] = {164, 260, 644, 1668};
+constexpr int CV_STRIDES4[4] = {200, 392, 1160, 3592};
 
-int cv_stride_for(int ns8)
+int cv_stride_for(int q, int ns8)
 {
-    for (int st : CV_STRIDES)
-        if ((CV_BLOCK + ns8 + 7) / 8 + 1 <= st) return st;
+    const int *tab = q == 8 ? CV_STRIDES8 : CV_STRIDES4;
+    for (int i = 0; i < 4; i++) {
+        const int st = tab[i];
+        const size_t smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)q * st);
+        if (q * (st - 1) - CV_THREADS * q + 1 >= ns8 && smem <= 227 * 1024) return st;
+    }
     return 0;
 }
 
@@ -391,9 +376,9 @@ struct HBuf {                      /* pinned host staging, grown on demand */
     }
 };
 
-/* the host side of one variation batch: planned terms, slot maps and chunk
- * ranges, copied to the device asynchronously; two stages alternate so that
- * the next batch is planned while the device works on this one */
+/* one chunk's terms on both sides: pinned host arrays the plan fills and
+ * the device copies the kernels read, with the trace buffer; two stages
+ * alternate so that chunk c + 1 is planned and copied while chunk c runs */
 struct Stage {
     HBuf<awp_synth_gterm> gt;
     HBuf<awp_synth_cterm> ct;
@@ -401,8 +386,26 @@ struct Stage {
     HBuf<int> slot_term, tl, multi;
     HBuf<int2> range;
     HBuf<int4> groups;
-    cudaEvent_t done = nullptr;
+    DBuf<awp_synth_gterm> d_gt;
+    DBuf<awp_synth_cterm> d_ct;
+    DBuf<float> d_stf, d_u;
+    DBuf<int> d_slot_term, d_multi;
+    DBuf<int2> d_range;
+    DBuf<int4> d_groups;
+    cudaEvent_t h2d = nullptr;     /* host arrays copied: the host may refill them    */
+    cudaEvent_t gf = nullptr;      /* traces written: the convolution may read them    */
+    cudaEvent_t conv = nullptr;    /* convolution done: the device arrays may be refilled */
     bool pending = false;
+    void release()
+    {
+        gt.release(), ct.release(), stf.release(), slot_term.release(), tl.release(), multi.release();
+        range.release(), groups.release();
+        d_gt.release(), d_ct.release(), d_stf.release(), d_u.release(), d_slot_term.release(), d_multi.release();
+        d_range.release(), d_groups.release();
+        for (cudaEvent_t e : {h2d, gf, conv})
+            if (e) cudaEventDestroy(e);
+        h2d = gf = conv = nullptr;
+    }
 };
 
 struct Variation {
@@ -420,7 +423,9 @@ double now_s()
 
 struct awp_synth {
     awp_synth_params p;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   /* convolutions, seismogram copies */
+    cudaStream_t cstream = nullptr;  /* host-to-device copies of chunk terms */
+    cudaStream_t gstream = nullptr;  /* SGT combination kernels */
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     /* SGT set */
     awp_sgtmaster m{};
@@ -434,16 +439,12 @@ struct awp_synth {
     int nseis = 0;
     awp_synth_info info{};
     /* run buffers */
-    DBuf<awp_synth_gterm> d_gt;
-    DBuf<awp_synth_cterm> d_ct;
-    DBuf<float> d_stf, d_u, d_seis;
-    DBuf<int> d_slot_term, d_tl, d_multi;
-    DBuf<int2> d_range;
-    DBuf<int4> d_groups;
+    DBuf<float> d_seis;
     Stage stage[2];
     HBuf<float> h_seis;
-    std::vector<cudaEvent_t> cev;  /* per chunk: before k_synth_gf, between, after k_synth_conv */
+    std::vector<cudaEvent_t> cev;  /* per chunk: around the combination, around the convolution */
     size_t u_cap_bytes = (size_t)2 << 30;
+    int conv_q = 8;                /* output samples per convolution thread (4 or 8) */
 };
 
 static awp_status synth_set_sgt_common(awp_synth *s, const awp_sgtmaster *m, const awp_sgtindex *ix,
@@ -480,13 +481,20 @@ extern "C" awp_status awp_synth_create(const awp_synth_params *p, awp_synth **ou
     SCU(cudaSetDevice(p->device));
     awp_synth *s = new awp_synth();
     s->p = *p;
+    if (const char *e = getenv("AWP_SYNTH_Q")) s->conv_q = atoi(e) == 4 ? 4 : 8;
     if (const char *e = getenv("AWP_SYNTH_UBUF_MB")) {
         const long mb = atol(e);
         if (mb > 0) s->u_cap_bytes = (size_t)mb << 20;
     }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->gstream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
-    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&s->stage[i].done, cudaEventDisableTiming);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        e = cudaEventCreateWithFlags(&s->stage[i].h2d, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->stage[i].gf, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->stage[i].conv, cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
         awp_synth_destroy(s);
         return fail(AWP_ERR_CUDA, "awp_synth_create: %s", cudaGetErrorString(e));
@@ -499,34 +507,17 @@ extern "C" void awp_synth_destroy(awp_synth *s)
 {
     if (!s) return;
     cudaSetDevice(s->p.device);
-    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaStream_t st : {s->stream, s->cstream, s->gstream})
+        if (st) cudaStreamSynchronize(st);
     if (s->d_sgt) cudaFree(s->d_sgt);
-    s->d_gt.release();
-    s->d_ct.release();
-    s->d_stf.release();
-    s->d_u.release();
     s->d_seis.release();
-    s->d_slot_term.release();
-    s->d_tl.release();
-    s->d_range.release();
-    s->d_multi.release();
-    s->d_groups.release();
-    for (auto &st : s->stage) {
-        st.gt.release();
-        st.ct.release();
-        st.stf.release();
-        st.slot_term.release();
-        st.tl.release();
-        st.range.release();
-        st.multi.release();
-        st.groups.release();
-        if (st.done) cudaEventDestroy(st.done);
-    }
+    for (auto &st : s->stage) st.release();
     s->h_seis.release();
     for (auto &e : s->cev) cudaEventDestroy(e);
     for (auto &e : s->ev)
         if (e) cudaEventDestroy(e);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    for (cudaStream_t st : {s->stream, s->cstream, s->gstream})
+        if (st) cudaStreamDestroy(st);
     delete s;
 }
 
@@ -674,26 +665,43 @@ static void synth_lengths(const awp_synth *s, int *ntsum, int *ntout)
     *ntout = s->p.ntout > 0 ? s->p.ntout : n;
 }
 
-template <int STRIDE, int UC>
-static cudaError_t launch_conv_uc(dim3 grid, size_t smem, cudaStream_t st, const float *u, const int *tl,
-                                  const int2 *range, const int *slot_term, const awp_synth_cterm *ct,
-                                  const float *stf, int ntout, int ns8, float *seis)
+template <int Q, int STRIDE, int UC>
+static cudaError_t launch_conv_t(dim3 grid, size_t smem, cudaStream_t st, const float *u, const int2 *range,
+                                 const awp_synth_cterm *ct, const float *stf, int ntout, int ns8, float *seis)
 {
     cudaError_t e =
-        cudaFuncSetAttribute(k_synth_conv<STRIDE, UC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_synth_conv<Q, STRIDE, UC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_synth_conv<STRIDE, UC><<<grid, CV_THREADS, smem, st>>>(u, tl, range, slot_term, ct, stf, ntout, ns8, seis);
+    k_synth_conv<Q, STRIDE, UC><<<grid, CV_THREADS, smem, st>>>(u, range, ct, stf, ntout, ns8, seis);
     return cudaGetLastError();
 }
 
-template <int STRIDE>
-static cudaError_t launch_conv(int uc, dim3 grid, size_t smem, cudaStream_t st, const float *u, const int *tl,
-                               const int2 *range, const int *slot_term, const awp_synth_cterm *ct, const float *stf,
-                               int ntout, int ns8, float *seis)
+template <int Q, int STRIDE>
+static cudaError_t launch_conv_s(int uc, dim3 grid, size_t smem, cudaStream_t st, const float *u, const int2 *range,
+                                 const awp_synth_cterm *ct, const float *stf, int ntout, int ns8, float *seis)
 {
-    grid.y = uc;
-    return uc == 3 ? launch_conv_uc<STRIDE, 3>(grid, smem, st, u, tl, range, slot_term, ct, stf, ntout, ns8, seis)
-                   : launch_conv_uc<STRIDE, 2>(grid, smem, st, u, tl, range, slot_term, ct, stf, ntout, ns8, seis);
+    return uc == 3 ? launch_conv_t<Q, STRIDE, 3>(grid, smem, st, u, range, ct, stf, ntout, ns8, seis)
+                   : launch_conv_t<Q, STRIDE, 2>(grid, smem, st, u, range, ct, stf, ntout, ns8, seis);
+}
+
+/* one convolution launch: nb variations, uc components */
+static cudaError_t launch_conv(int q, int stride, int uc, int nb, int ntout, int ns8, cudaStream_t st,
+                               const float *u, const int2 *range, const awp_synth_cterm *ct, const float *stf,
+                               float *seis)
+{
+    const size_t smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)q * stride);
+    const dim3 g((unsigned)((ntout + CV_THREADS * q - 1) / (CV_THREADS * q)), (unsigned)uc, (unsigned)nb);
+#define CONV_CASE(QQ, TAB)                                                                                   \
+    if (q == QQ) {                                                                                           \
+        if (stride == TAB[0]) return launch_conv_s<QQ, TAB[0]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
+        if (stride == TAB[1]) return launch_conv_s<QQ, TAB[1]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
+        if (stride == TAB[2]) return launch_conv_s<QQ, TAB[2]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
+        if (stride == TAB[3]) return launch_conv_s<QQ, TAB[3]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
+    }
+    CONV_CASE(8, CV_STRIDES8)
+    CONV_CASE(4, CV_STRIDES4)
+#undef CONV_CASE
+    return cudaErrorInvalidValue;
 }
 
 template <int NC, int UC>
@@ -825,8 +833,11 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         const int nb = v0 + batch <= nv ? batch : nv - v0;
         long long total = 0;
         for (int v = v0; v < v0 + nb; v++) total += tpre[(size_t)v * (np + 1) + np];
-        long long target = (total + 3) / 4;
-        target = target < ucap ? target : ucap;
+        /* at least four chunks (to overlap the plan with the device) of equal
+         * size, none above the term buffer */
+        long long nch = (total + ucap - 1) / ucap;
+        nch = nch < 4 ? 4 : nch;
+        const long long target = (total + nch - 1) / nch;
         for (int p0 = 0; p0 < np;) {
             long long t = 0, n = 0;
             int p1 = p0;
@@ -849,15 +860,6 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     if (max_terms >= (1LL << 31)) return fail(AWP_ERR_PARAM, "awp_synth_run: too many terms in one chunk");
 
     cudaError_t e = cudaSuccess;
-    e = e ? e : s->d_gt.reserve((size_t)max_terms);
-    e = e ? e : s->d_ct.reserve((size_t)max_terms);
-    e = e ? e : s->d_stf.reserve((size_t)max_stf + 8);
-    e = e ? e : s->d_slot_term.reserve((size_t)max_terms);
-    e = e ? e : s->d_tl.reserve((size_t)max_terms);
-    e = e ? e : s->d_range.reserve((size_t)batch);
-    e = e ? e : s->d_multi.reserve((size_t)max_terms);
-    e = e ? e : s->d_groups.reserve((size_t)np);
-    e = e ? e : s->d_u.reserve((size_t)max_terms * uc * ntout);
     e = e ? e : s->d_seis.reserve((size_t)nv * 3 * ntout);
     e = e ? e : s->h_seis.reserve((size_t)nv * 3 * ntout);
     for (auto &sg : s->stage) {
@@ -869,15 +871,21 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         e = e ? e : sg.range.reserve((size_t)batch);
         e = e ? e : sg.multi.reserve((size_t)max_terms);
         e = e ? e : sg.groups.reserve((size_t)np);
+        e = e ? e : sg.d_gt.reserve((size_t)max_terms);
+        e = e ? e : sg.d_ct.reserve((size_t)max_terms);
+        e = e ? e : sg.d_stf.reserve((size_t)max_stf + 8);
+        e = e ? e : sg.d_slot_term.reserve((size_t)max_terms);
+        e = e ? e : sg.d_range.reserve((size_t)batch);
+        e = e ? e : sg.d_multi.reserve((size_t)max_terms);
+        e = e ? e : sg.d_groups.reserve((size_t)np);
+        e = e ? e : sg.d_u.reserve((size_t)max_terms * uc * ntout);
     }
     if (e != cudaSuccess) return fail(AWP_ERR_OOM, "awp_synth_run: buffers: %s", cudaGetErrorString(e));
-    /* the range table is per chunk: one device copy per stage */
-    static_assert(sizeof(int2) == 8, "int2");
 
     const int ns8 = (maxnstf + 7) & ~7;
-    const int stride = cv_stride_for(ns8);
+    const int cvq = s->conv_q;
+    const int stride = cv_stride_for(cvq, ns8);
     if (!stride) return fail(AWP_ERR_PARAM, "awp_synth_run: slip-rate functions too long (%d samples)", maxnstf);
-    const size_t cv_smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)CV_Q * stride);
 
     s->nseis = 0;
     s->info = awp_synth_info{};
@@ -887,10 +895,18 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     s->info.nsgt_points = nm;
     s->info.non_exact = non_exact;
     double plan_s = now_s() - t_plan;
-    int launches = 0, nk = 0;     /* chunks launched; chunk j is timed by events 3j .. 3j + 2 */
+    int launches = 0, nk = 0;     /* chunks launched; chunk j is timed by events 4j .. 4j + 3 */
 
+    /* streams: copies on cstream, combination on gstream, convolution on
+     * stream.  Chunk c (stage c & 1): copy after the convolution of chunk
+     * c - 2 released the stage; combine after the copy; convolve after the
+     * combination (and, on its stream, after chunk c - 1). */
     SCU(cudaEventRecord(s->ev[0], s->stream));
     SCU(cudaMemsetAsync(s->d_seis.p, 0, (size_t)nv * 3 * ntout * sizeof(float), s->stream));
+    SCU(cudaEventRecord(s->ev[2], s->stream));
+    SCU(cudaStreamWaitEvent(s->cstream, s->ev[2], 0));
+    SCU(cudaStreamWaitEvent(s->gstream, s->ev[2], 0));
+    for (auto &sg : s->stage) sg.pending = false;
     std::vector<long long> toff, soff, pbase;
     std::vector<int> pslot;
     for (size_t ic = 0; ic < chunks.size(); ic++) {
@@ -898,7 +914,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         const Chunk &C = chunks[ic];
         const int nb = C.nb, p0 = C.p0, p1 = C.p1, npc = p1 - p0;
         Stage &S = s->stage[ic & 1];
-        if (S.pending) SCU(cudaEventSynchronize(S.done));   /* its copies of two chunks ago are done */
+        if (S.pending) SCU(cudaEventSynchronize(S.h2d));   /* its copies of two chunks ago are done */
         S.pending = false;
         /* chunk-local term numbering: variation-major (each variation's terms
          * contiguous, in point order); slots: point-major */
@@ -923,7 +939,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         for (int b = 0; b < nb; b++)
             if (pst[b] != AWP_OK) {
                 /* the error text is per thread: plan the variation again here */
-                SCU(cudaStreamSynchronize(s->stream));
+                for (cudaStream_t q : {s->stream, s->cstream, s->gstream}) SCU(cudaStreamSynchronize(q));
                 for (auto &sg : s->stage) sg.pending = false;
                 const Variation &v = s->vars[C.v0 + b];
                 long long a1, a2, a3;
@@ -958,6 +974,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
                 }
             }
         }
+        for (long long t = 0; t < nterm; t++) S.ct.p[t].slot = S.tl.p[t];
         for (int b = 0; b < nb; b++) S.range.p[b] = make_int2((int)toff[b], (int)toff[b + 1]);
         /* exactly matched points go to the per-point kernel, the others'
          * slots to the per-term one */
@@ -973,48 +990,39 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         plan_s += now_s() - t_plan;
 
         if (nterm) {
-            SCU(cudaMemcpyAsync(s->d_gt.p, S.gt.p, nterm * sizeof(awp_synth_gterm), cudaMemcpyHostToDevice, s->stream));
-            SCU(cudaMemcpyAsync(s->d_ct.p, S.ct.p, nterm * sizeof(awp_synth_cterm), cudaMemcpyHostToDevice, s->stream));
-            SCU(cudaMemcpyAsync(s->d_slot_term.p, S.slot_term.p, nterm * sizeof(int), cudaMemcpyHostToDevice,
-                                s->stream));
-            SCU(cudaMemcpyAsync(s->d_tl.p, S.tl.p, nterm * sizeof(int), cudaMemcpyHostToDevice, s->stream));
-            SCU(cudaMemcpyAsync(s->d_stf.p, S.stf.p, (soff[nb] + 8) * sizeof(float), cudaMemcpyHostToDevice,
-                                s->stream));
-            SCU(cudaMemcpyAsync(s->d_range.p, S.range.p, (size_t)nb * sizeof(int2), cudaMemcpyHostToDevice,
-                                s->stream));
+            cudaStream_t cs = s->cstream;
+            if (ic >= 2) SCU(cudaStreamWaitEvent(cs, S.conv, 0));
+            SCU(cudaMemcpyAsync(S.d_gt.p, S.gt.p, nterm * sizeof(awp_synth_gterm), cudaMemcpyHostToDevice, cs));
+            SCU(cudaMemcpyAsync(S.d_ct.p, S.ct.p, nterm * sizeof(awp_synth_cterm), cudaMemcpyHostToDevice, cs));
+            SCU(cudaMemcpyAsync(S.d_slot_term.p, S.slot_term.p, nterm * sizeof(int), cudaMemcpyHostToDevice, cs));
+            SCU(cudaMemcpyAsync(S.d_stf.p, S.stf.p, (soff[nb] + 8) * sizeof(float), cudaMemcpyHostToDevice, cs));
+            SCU(cudaMemcpyAsync(S.d_range.p, S.range.p, (size_t)nb * sizeof(int2), cudaMemcpyHostToDevice, cs));
             if (ngroups)
-                SCU(cudaMemcpyAsync(s->d_groups.p, S.groups.p, (size_t)ngroups * sizeof(int4), cudaMemcpyHostToDevice,
-                                    s->stream));
-            if (nmulti)
-                SCU(cudaMemcpyAsync(s->d_multi.p, S.multi.p, (size_t)nmulti * sizeof(int), cudaMemcpyHostToDevice,
-                                    s->stream));
+                SCU(cudaMemcpyAsync(S.d_groups.p, S.groups.p, (size_t)ngroups * sizeof(int4), cudaMemcpyHostToDevice, cs));
+            if (nmulti) SCU(cudaMemcpyAsync(S.d_multi.p, S.multi.p, (size_t)nmulti * sizeof(int), cudaMemcpyHostToDevice, cs));
         }
-        SCU(cudaEventRecord(S.done, s->stream));
+        SCU(cudaEventRecord(S.h2d, s->cstream));
         S.pending = true;
-        if (!nterm) continue;
         float *seis_b = s->d_seis.p + (size_t)C.v0 * 3 * ntout;
-        SCU(events_for(s, 3 * (nk + 1)));
-        SCU(cudaEventRecord(s->cev[3 * nk], s->stream));
-        SCU(launch_gf(s->ncomp, ngroups, nmulti, nt, ntout, s->stream, s->d_sgt, s->d_gt.p, s->d_slot_term.p,
-                      s->d_groups.p, s->d_multi.p, s->d_u.p));
-        SCU(cudaEventRecord(s->cev[3 * nk + 1], s->stream));
-        const dim3 g2((unsigned)((ntout + CV_BLOCK - 1) / CV_BLOCK), 3, (unsigned)nb);
-        if (stride == CV_STRIDES[0])
-            e = launch_conv<CV_STRIDES[0]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
-                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
-        else if (stride == CV_STRIDES[1])
-            e = launch_conv<CV_STRIDES[1]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
-                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
-        else if (stride == CV_STRIDES[2])
-            e = launch_conv<CV_STRIDES[2]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
-                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
-        else
-            e = launch_conv<CV_STRIDES[3]>(uc, g2, cv_smem, s->stream, s->d_u.p, s->d_tl.p, s->d_range.p,
-                                           s->d_slot_term.p, s->d_ct.p, s->d_stf.p, ntout, ns8, seis_b);
-        SCU(e);
-        SCU(cudaEventRecord(s->cev[3 * nk + 2], s->stream));
-        nk++;
-        launches += (ngroups > 0) + (nmulti > 0) + 1;
+        if (nterm) {
+            SCU(events_for(s, 4 * (nk + 1)));
+            SCU(cudaStreamWaitEvent(s->gstream, S.h2d, 0));
+            if (ic >= 2) SCU(cudaStreamWaitEvent(s->gstream, S.conv, 0));   /* chunk c - 2 read these traces */
+            SCU(cudaEventRecord(s->cev[4 * nk], s->gstream));
+            SCU(launch_gf(s->ncomp, ngroups, nmulti, nt, ntout, s->gstream, s->d_sgt, S.d_gt.p, S.d_slot_term.p,
+                          S.d_groups.p, S.d_multi.p, S.d_u.p));
+            SCU(cudaEventRecord(s->cev[4 * nk + 1], s->gstream));
+            SCU(cudaEventRecord(S.gf, s->gstream));
+            SCU(cudaStreamWaitEvent(s->stream, S.gf, 0));
+            SCU(cudaEventRecord(s->cev[4 * nk + 2], s->stream));
+            e = launch_conv(cvq, stride, uc, nb, ntout, ns8, s->stream, S.d_u.p, S.d_range.p, S.d_ct.p, S.d_stf.p,
+                            seis_b);
+            SCU(e);
+            SCU(cudaEventRecord(s->cev[4 * nk + 3], s->stream));
+            SCU(cudaEventRecord(S.conv, s->stream));
+            nk++;
+            launches += (ngroups > 0) + (nmulti > 0) + 1;
+        }
         const bool last_of_batch = ic + 1 == chunks.size() || chunks[ic + 1].v0 != C.v0;
         if (last_of_batch)
             SCU(cudaMemcpyAsync(s->h_seis.p + (size_t)C.v0 * 3 * ntout, seis_b, (size_t)nb * 3 * ntout * sizeof(float),
@@ -1022,14 +1030,16 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     }
     SCU(cudaEventRecord(s->ev[1], s->stream));
     SCU(cudaEventSynchronize(s->ev[1]));
+    SCU(cudaStreamSynchronize(s->cstream));
+    SCU(cudaStreamSynchronize(s->gstream));
     for (auto &sg : s->stage) sg.pending = false;
     float ms = 0.0f;
     SCU(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
     double gf_s = 0.0, conv_s = 0.0;
     for (int j = 0; j < nk; j++) {
         float a = 0.0f, c = 0.0f;
-        SCU(cudaEventElapsedTime(&a, s->cev[3 * j], s->cev[3 * j + 1]));
-        SCU(cudaEventElapsedTime(&c, s->cev[3 * j + 1], s->cev[3 * j + 2]));
+        SCU(cudaEventElapsedTime(&a, s->cev[4 * j], s->cev[4 * j + 1]));
+        SCU(cudaEventElapsedTime(&c, s->cev[4 * j + 2], s->cev[4 * j + 3]));
         gf_s += a * 1e-3;
         conv_s += c * 1e-3;
     }

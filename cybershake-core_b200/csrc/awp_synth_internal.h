@@ -33,7 +33,7 @@ typedef struct {
     long long stf;            /* offset in the run's sample pool                  */
     int nstf;
     int lo, hi;               /* output samples the SGTs reach; the rest are +0   */
-    int pad;
+    int slot;                 /* where the combination kernel put the trace       */
 } awp_synth_cterm;
 
 typedef struct {

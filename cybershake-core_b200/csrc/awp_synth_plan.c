@@ -291,7 +291,7 @@ awp_status awp_synth_plan_variation(const awp_synth_plan_ctx *cx, const awp_srf_
             for (int it = 0; it < nstf; it++) stf[ns + it] = cx->dtout * pool[off + it];
             c->stf = stf_base + ns;
             c->nstf = nstf;
-            c->pad = 0;
+            c->slot = 0;
             /* a single SGT point reaches [lo, hi) only; with several the
              * combination kernel writes every sample */
             c->lo = b->nsgt == 1 ? g->lo[0] : 0;
