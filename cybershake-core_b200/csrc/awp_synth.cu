@@ -57,6 +57,7 @@ awp_status fail(awp_status st, const char *fmt, ...)
 
 constexpr int GF_THREADS = 256;
 constexpr int CV_THREADS = 128;
+constexpr int CV_BLOCK = CV_THREADS * 8;   /* output samples of one convolution CTA */
 
 __constant__ float c_taper[SY_TAPLEN];
 
@@ -202,50 +203,70 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-/* Each CTA owns CV_THREADS * Q consecutive output samples (Q per thread)
- * of one component of one variation and walks the variation's terms in
+/* Each CTA owns CV_BLOCK consecutive output samples (8 per thread) of one
+ * component of one variation and walks the variation's terms in
  * rupture-point order.  The window of term n + 1 (its trace around the block
  * and its slip rate) is copied into the other shared buffer with cp.async
  * while term n is convolved; term records are read two terms ahead.
  *
- * Inside a term, thread samples W[j] = window[Q tid + j] feed its outputs
- * q = 0..Q-1 at lag k through W[q + m], m = n8 - 1 - k.  Lags go in groups
- * of Q (m = Qg+Q-1 .. Qg, g descending): a group needs W[Qg .. Qg+2Q-2],
- * held as lo = W[Qg..Qg+Q-1] and hi = W[Qg+Q..Qg+2Q-1]; the next group's lo
- * is loaded while this one computes.  W[Qg + j] sits in shared row j at
- * column tid + g (rows STRIDE apart, STRIDE = 32/Q mod 32), so the loads of
- * a warp hit 32 banks and their offsets are immediates. */
-template <int Q, int STRIDE, int UC>
+ * Inside a term, thread samples W[j] = window[8 tid + j] feed its outputs
+ * q = 0..7 at lag k through W[q + m], m = n8 - 1 - k.  Lags go in groups of
+ * eight (m = 8g+7 .. 8g, g descending): a group needs W[8g .. 8g+14], held
+ * as lo = W[8g..8g+7] and hi = W[8g+8..8g+15], and loads the next group's lo
+ * while it computes.  Three register sets take the lo / hi / next roles in
+ * turn (the loop is unrolled three times), so no window value is moved.
+ * W[8g + j] sits in shared row j at column tid + g (rows STRIDE apart,
+ * STRIDE = 4 mod 32), so the loads of a warp hit 32 banks and their offsets
+ * are immediates. */
+template <int STRIDE, int UC>
 __global__ void __launch_bounds__(CV_THREADS) k_synth_conv(const float *__restrict__ u,
                                                            const int2 *__restrict__ range,
                                                            const awp_synth_cterm *__restrict__ ct,
                                                            const float *__restrict__ stfpool, int ntout, int ns8,
                                                            float *__restrict__ seis)
 {
-    static_assert(Q == 4 || Q == 8, "Q");
-    static_assert(STRIDE % 32 == 32 / Q, "stride");
-    constexpr int BLOCK = CV_THREADS * Q;
+    static_assert(STRIDE % 32 == 4, "stride");
     extern __shared__ __align__(16) float sm[];
-    const int buf = ns8 + Q * STRIDE;                  /* floats per buffer: slip rate, then window */
-    const int v = blockIdx.z, cu = blockIdx.y, t0 = blockIdx.x * BLOCK, tid = threadIdx.x;
-    const int base = t0 + tid * Q;
+    const int buf = ns8 + 8 * STRIDE;                  /* floats per buffer: slip rate, then window */
+    const int v = blockIdx.z, cu = blockIdx.y, t0 = blockIdx.x * CV_BLOCK, tid = threadIdx.x;
+    const int base = t0 + tid * 8;
     float *out = seis + ((size_t)v * 3 + cu + 3 - UC) * ntout;
-    float s[Q];
+    float s[8];
 #pragma unroll
-    for (int q = 0; q < Q; q++) s[q] = base + q < ntout ? out[base + q] : 0.0f;
+    for (int q = 0; q < 8; q++) s[q] = base + q < ntout ? out[base + q] : 0.0f;
     const int2 rg = range[v];
 
     auto issue = [&](const awp_synth_cterm &t, float *b) {
         const int n8 = (t.nstf + 7) & ~7;
         for (int k = tid; k < n8; k += CV_THREADS) cp_async4(b + k, stfpool + t.stf + (k < t.nstf ? k : 0), k < t.nstf);
         const float *tr = u + ((size_t)t.slot * UC + cu) * ntout;
-        const int w0 = t0 - (n8 - 1), wl = BLOCK + n8;
-        float *win = b + ns8;
-        for (int y = tid; y < wl; y += CV_THREADS) {
+        const int w0 = t0 - (n8 - 1), wl = CV_BLOCK + n8;
+        /* window sample y = tid + 128 i: row tid & 7, column tid / 8 + 16 i */
+        float *win = b + ns8 + (tid & 7) * STRIDE + (tid >> 3);
+        for (int y = tid; y < wl; y += CV_THREADS, win += CV_THREADS / 8) {
             const int x = w0 + y;
             const bool ok = x >= t.lo && x < t.hi;
-            cp_async4(win + (y % Q) * STRIDE + y / Q, tr + (ok ? x : 0), ok);
+            cp_async4(win, tr + (ok ? x : 0), ok);
         }
+    };
+
+    /* one group of eight lags with lo = L, hi = H; loads the next lo into N.
+     * At g = 0 the load of N reads column tid - 1 (for tid = 0 the float just
+     * before the window, in this buffer's slip-rate area): in bounds, unused. */
+    auto group = [&](float(&acc)[8], const float(&L)[8], const float(&H)[8], float(&N)[8], const float *stf,
+                     const float *col, int k0) {
+        const float4 fa = *reinterpret_cast<const float4 *>(stf + k0);
+        const float4 fb = *reinterpret_cast<const float4 *>(stf + k0 + 4);
+        const float f[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
+#pragma unroll
+        for (int j = 0; j < 8; j++) N[j] = col[j * STRIDE - 1];
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++)
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int j = q + 7 - kk;                   /* W[q + m], m = 8g + 7 - kk */
+                acc[q] = acc[q] + f[kk] * (j < 8 ? L[j] : H[j - 8]);
+            }
     };
 
     awp_synth_cterm cur{}, nxt{}, nn{};
@@ -268,69 +289,47 @@ __global__ void __launch_bounds__(CV_THREADS) k_synth_conv(const float *__restri
          * add +-0 to an accumulator that starts at +0 and so leave it as the
          * reference's shorter sum leaves it. */
         const int n8 = (cur.nstf + 7) & ~7;
-        const float *stf = b;
-        int g = n8 / Q - 1;
-        const float *col = b + ns8 + tid + g;           /* column of group g in row 0 */
-        float acc[Q], lo[Q], hi[Q];
+        int g = n8 / 8 - 1;
+        const float *col = b + ns8 + tid + g;               /* column of group g in row 0 */
+        float acc[8], X[8], Y[8], Z[8];
 #pragma unroll
-        for (int q = 0; q < Q; q++) {
+        for (int q = 0; q < 8; q++) {
             acc[q] = 0.0f;
-            hi[q] = col[q * STRIDE + 1];
-            lo[q] = col[q * STRIDE];
+            Y[q] = col[q * STRIDE + 1];
+            X[q] = col[q * STRIDE];
         }
-        for (; g >= 0; g--, col--) {
-            const int k0 = n8 - Q - Q * g;                 /* lags k0 .. k0 + Q - 1 */
-            float f[Q];
-#pragma unroll
-            for (int h = 0; h < Q / 4; h++) {
-                const float4 fv = *reinterpret_cast<const float4 *>(stf + k0 + 4 * h);
-                f[4 * h] = fv.x, f[4 * h + 1] = fv.y, f[4 * h + 2] = fv.z, f[4 * h + 3] = fv.w;
-            }
-            float nl[Q];
-#pragma unroll
-            for (int j = 0; j < Q; j++) nl[j] = g > 0 ? col[j * STRIDE - 1] : 0.0f;
-#pragma unroll
-            for (int kk = 0; kk < Q; kk++) {
-                /* m = Qg + Q-1 - kk: W[q + m] = lo / hi [q + Q-1 - kk] */
-#pragma unroll
-                for (int q = 0; q < Q; q++) {
-                    const int j = q + Q - 1 - kk;
-                    const float w = j < Q ? lo[j] : hi[j - Q];
-                    acc[q] = acc[q] + f[kk] * w;
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < Q; j++) {
-                hi[j] = lo[j];
-                lo[j] = nl[j];
-            }
+        /* groups g, g - 1, g - 2 cover lags n8 - 8 - 8 g .. n8 + 15 - 8 g */
+        for (; g >= 2; g -= 3, col -= 3) {
+            group(acc, X, Y, Z, b, col, n8 - 8 - 8 * g);
+            group(acc, Z, X, Y, b, col - 1, n8 - 8 * g);
+            group(acc, Y, Z, X, b, col - 2, n8 + 8 - 8 * g);
         }
+        if (g >= 0) group(acc, X, Y, Z, b, col, n8 - 8 - 8 * g);
+        if (g >= 1) group(acc, Z, X, Y, b, col - 1, n8 - 8 * g);
 #pragma unroll
-        for (int q = 0; q < Q; q++) s[q] = s[q] + acc[q];     /* stf_subs.c:34-36 */
+        for (int q = 0; q < 8; q++) s[q] = s[q] + acc[q];     /* stf_subs.c:34-36 */
         __syncthreads();
         cur = nxt;
         nxt = nn;
     }
 #pragma unroll
-    for (int q = 0; q < Q; q++)
+    for (int q = 0; q < 8; q++)
         if (base + q < ntout) out[base + q] = s[q];
 }
 
-/* window row strides (32/Q mod 32) by outputs per thread; a stride holds
- * slip rates of n8 <= Q (STRIDE - 1) - CV_THREADS Q + 1 samples */
-constexpr int CV_STRIDES8[4] = {164, 260, 644, 1668};
-constexpr int CV_STRIDES4[4] = {200, 392, 1160, 3592};
+/* window row strides (4 mod 32); a stride holds slip rates of
+ * n8 <= 8 (STRIDE - 1) - CV_BLOCK + 1 samples */
+constexpr int CV_STRIDES[4] = {164, 260, 644, 1668};
 
-int cv_stride_for(int q, int ns8)
+size_t cv_smem_bytes(int ns8, int st) { return sizeof(float) * 2 * ((size_t)ns8 + 8 * (size_t)st); }
+
+int cv_stride_for(int ns8)
 {
-    const int *tab = q == 8 ? CV_STRIDES8 : CV_STRIDES4;
-    for (int i = 0; i < 4; i++) {
-        const int st = tab[i];
-        const size_t smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)q * st);
-        if (q * (st - 1) - CV_THREADS * q + 1 >= ns8 && smem <= 227 * 1024) return st;
-    }
+    for (int st : CV_STRIDES)
+        if (8 * (st - 1) - CV_BLOCK + 1 >= ns8 && cv_smem_bytes(ns8, st) <= 227 * 1024) return st;
     return 0;
 }
+
 
 template <class T>
 struct DBuf {
@@ -444,7 +443,6 @@ struct awp_synth {
     HBuf<float> h_seis;
     std::vector<cudaEvent_t> cev;  /* per chunk: around the combination, around the convolution */
     size_t u_cap_bytes = (size_t)2 << 30;
-    int conv_q = 8;                /* output samples per convolution thread (4 or 8) */
 };
 
 static awp_status synth_set_sgt_common(awp_synth *s, const awp_sgtmaster *m, const awp_sgtindex *ix,
@@ -481,7 +479,6 @@ extern "C" awp_status awp_synth_create(const awp_synth_params *p, awp_synth **ou
     SCU(cudaSetDevice(p->device));
     awp_synth *s = new awp_synth();
     s->p = *p;
-    if (const char *e = getenv("AWP_SYNTH_Q")) s->conv_q = atoi(e) == 4 ? 4 : 8;
     if (const char *e = getenv("AWP_SYNTH_UBUF_MB")) {
         const long mb = atol(e);
         if (mb > 0) s->u_cap_bytes = (size_t)mb << 20;
@@ -665,41 +662,31 @@ static void synth_lengths(const awp_synth *s, int *ntsum, int *ntout)
     *ntout = s->p.ntout > 0 ? s->p.ntout : n;
 }
 
-template <int Q, int STRIDE, int UC>
+template <int STRIDE, int UC>
 static cudaError_t launch_conv_t(dim3 grid, size_t smem, cudaStream_t st, const float *u, const int2 *range,
                                  const awp_synth_cterm *ct, const float *stf, int ntout, int ns8, float *seis)
 {
     cudaError_t e =
-        cudaFuncSetAttribute(k_synth_conv<Q, STRIDE, UC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_synth_conv<STRIDE, UC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_synth_conv<Q, STRIDE, UC><<<grid, CV_THREADS, smem, st>>>(u, range, ct, stf, ntout, ns8, seis);
+    k_synth_conv<STRIDE, UC><<<grid, CV_THREADS, smem, st>>>(u, range, ct, stf, ntout, ns8, seis);
     return cudaGetLastError();
 }
 
-template <int Q, int STRIDE>
-static cudaError_t launch_conv_s(int uc, dim3 grid, size_t smem, cudaStream_t st, const float *u, const int2 *range,
-                                 const awp_synth_cterm *ct, const float *stf, int ntout, int ns8, float *seis)
-{
-    return uc == 3 ? launch_conv_t<Q, STRIDE, 3>(grid, smem, st, u, range, ct, stf, ntout, ns8, seis)
-                   : launch_conv_t<Q, STRIDE, 2>(grid, smem, st, u, range, ct, stf, ntout, ns8, seis);
-}
-
 /* one convolution launch: nb variations, uc components */
-static cudaError_t launch_conv(int q, int stride, int uc, int nb, int ntout, int ns8, cudaStream_t st,
-                               const float *u, const int2 *range, const awp_synth_cterm *ct, const float *stf,
-                               float *seis)
+static cudaError_t launch_conv(int stride, int uc, int nb, int ntout, int ns8, cudaStream_t st, const float *u,
+                               const int2 *range, const awp_synth_cterm *ct, const float *stf, float *seis)
 {
-    const size_t smem = sizeof(float) * 2 * ((size_t)ns8 + (size_t)q * stride);
-    const dim3 g((unsigned)((ntout + CV_THREADS * q - 1) / (CV_THREADS * q)), (unsigned)uc, (unsigned)nb);
-#define CONV_CASE(QQ, TAB)                                                                                   \
-    if (q == QQ) {                                                                                           \
-        if (stride == TAB[0]) return launch_conv_s<QQ, TAB[0]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
-        if (stride == TAB[1]) return launch_conv_s<QQ, TAB[1]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
-        if (stride == TAB[2]) return launch_conv_s<QQ, TAB[2]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
-        if (stride == TAB[3]) return launch_conv_s<QQ, TAB[3]>(uc, g, smem, st, u, range, ct, stf, ntout, ns8, seis); \
-    }
-    CONV_CASE(8, CV_STRIDES8)
-    CONV_CASE(4, CV_STRIDES4)
+    const size_t smem = cv_smem_bytes(ns8, stride);
+    const dim3 g((unsigned)((ntout + CV_BLOCK - 1) / CV_BLOCK), (unsigned)uc, (unsigned)nb);
+#define CONV_CASE(I)                                                                                      \
+    if (stride == CV_STRIDES[I])                                                                          \
+        return uc == 3 ? launch_conv_t<CV_STRIDES[I], 3>(g, smem, st, u, range, ct, stf, ntout, ns8, seis) \
+                       : launch_conv_t<CV_STRIDES[I], 2>(g, smem, st, u, range, ct, stf, ntout, ns8, seis);
+    CONV_CASE(0)
+    CONV_CASE(1)
+    CONV_CASE(2)
+    CONV_CASE(3)
 #undef CONV_CASE
     return cudaErrorInvalidValue;
 }
@@ -883,8 +870,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     if (e != cudaSuccess) return fail(AWP_ERR_OOM, "awp_synth_run: buffers: %s", cudaGetErrorString(e));
 
     const int ns8 = (maxnstf + 7) & ~7;
-    const int cvq = s->conv_q;
-    const int stride = cv_stride_for(cvq, ns8);
+    const int stride = cv_stride_for(ns8);
     if (!stride) return fail(AWP_ERR_PARAM, "awp_synth_run: slip-rate functions too long (%d samples)", maxnstf);
 
     s->nseis = 0;
@@ -1015,8 +1001,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
             SCU(cudaEventRecord(S.gf, s->gstream));
             SCU(cudaStreamWaitEvent(s->stream, S.gf, 0));
             SCU(cudaEventRecord(s->cev[4 * nk + 2], s->stream));
-            e = launch_conv(cvq, stride, uc, nb, ntout, ns8, s->stream, S.d_u.p, S.d_range.p, S.d_ct.p, S.d_stf.p,
-                            seis_b);
+            e = launch_conv(stride, uc, nb, ntout, ns8, s->stream, S.d_u.p, S.d_range.p, S.d_ct.p, S.d_stf.p, seis_b);
             SCU(e);
             SCU(cudaEventRecord(s->cev[4 * nk + 3], s->stream));
             SCU(cudaEventRecord(S.conv, s->stream));

@@ -135,11 +135,9 @@ def test_oracle_refuses_resampling():
 
 # ---- device path ---------------------------------------------------------------
 
-def run_device(c, ntout=0, tstart=0.0, rv_batch=0, ubuf_mb=None, conv_q=None):
+def run_device(c, ntout=0, tstart=0.0, rv_batch=0, ubuf_mb=None):
     if ubuf_mb is not None:
         os.environ["AWP_SYNTH_UBUF_MB"] = str(ubuf_mb)
-    if conv_q is not None:
-        os.environ["AWP_SYNTH_Q"] = str(conv_q)
     try:
         with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=ntout, tstart=tstart, rv_batch=rv_batch) as s:
             s.set_sgt(c.master, c.index, c.headers, c.comps)
@@ -149,7 +147,6 @@ def run_device(c, ntout=0, tstart=0.0, rv_batch=0, ubuf_mb=None, conv_q=None):
             return out, s.info()
     finally:
         os.environ.pop("AWP_SYNTH_UBUF_MB", None)
-        os.environ.pop("AWP_SYNTH_Q", None)
 
 
 @pytest.mark.gpu
@@ -166,14 +163,13 @@ def test_device_matches_oracle_bitwise(ncomp, ntout, tstart):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rv_batch,ubuf_mb,conv_q", [(1, None, 8), (2, 1, 8), (0, 1, 8), (2, 1, 4), (0, None, 4)])
-def test_device_batches_and_chunks_match_oracle(rv_batch, ubuf_mb, conv_q):
+@pytest.mark.parametrize("rv_batch,ubuf_mb", [(1, None), (2, 1), (0, 1), (3, 2)])
+def test_device_batches_and_chunks_match_oracle(rv_batch, ubuf_mb):
     """Several variation batches and term-buffer chunks (1 MiB holds a few
-    points' terms) accumulate in the same order as one pass, with either
-    convolution shape (4 or 8 outputs per thread)."""
+    points' terms) accumulate in the same order as one pass."""
     c = ai.synth_case(seed=20, nx_f=20, nz_f=8, nt=400, nv=5, ntout=1200, nstf=(5, 120))
     want, _ = case_seis(c, 1200)
-    got, info = run_device(c, 1200, rv_batch=rv_batch, ubuf_mb=ubuf_mb, conv_q=conv_q)
+    got, info = run_device(c, 1200, rv_batch=rv_batch, ubuf_mb=ubuf_mb)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     if ubuf_mb:
         assert info.gpu_launches > 2 * ((5 + (rv_batch or 5) - 1) // (rv_batch or 5))
@@ -186,8 +182,6 @@ def test_device_edge_cases_match_oracle():
     c = ai.synth_case(seed=21, nv=2, zero_frac=0.3, drop_frac=1.0, nstf=(1, 100), nt=120)
     want, nout = case_seis(c, 100)
     got, info = run_device(c, 100)
-    got4, _ = run_device(c, 100, conv_q=4)
-    assert np.array_equal(got4.view(np.uint32), want.view(np.uint32))
     assert info.non_exact == len(c.variations[0][0])
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
