@@ -31,6 +31,7 @@ struct AwpStepArgs {
     int kchunk_staged;           /* z levels per staged work item           */
     int staged_qslow;            /* staged items: one component at a time   */
     int staged_rpt;              /* staged stress sweep: tile rows per thread */
+    int staged_rpt_vel;          /* staged velocity sweep: tile rows per thread */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

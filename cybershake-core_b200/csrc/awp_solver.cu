@@ -83,6 +83,7 @@ struct awp_solver {
     int kchunk_staged;               /* z levels per staged work item       */
     int staged_qslow;                /* staged items: component slowest     */
     int staged_rpt;                  /* staged stress sweep rows per thread */
+    int staged_rpt_vel;              /* staged velocity sweep rows per thread */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -492,6 +493,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
          * components share the sweep with FP32 memory variables */
         const int rpt = env_int("AWP_TUNE_RPT", 0);
         s->staged_rpt = rpt == 1 || rpt == 2 ? rpt : (p->ncomp == 3 && s->rstore == AWP_STORE_F32 ? 2 : 1);
+        s->staged_rpt_vel = env_int("AWP_TUNE_RPTV", 1) == 2 ? 2 : 1;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -930,6 +932,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.kchunk_staged = s->kchunk_staged;
     a.staged_qslow = s->staged_qslow;
     a.staged_rpt = s->staged_rpt;
+    a.staged_rpt_vel = s->staged_rpt_vel;
     a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);

@@ -256,21 +256,22 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
 }
 
 /* work items: (x tile, y tile, z chunk, component); see split_item for the order */
-template <int D, int UNR>
-__global__ void __launch_bounds__(ST_THREADS, 3)
+template <int D, int UNR, int RPT>
+__global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
           const float *__restrict__ cz, float dth, AwpWork w, int *err)
 {
     constexpr int S = 1 + D;          /* level k in use, D in flight */
+    constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
     float *ring = ring_base(st_smem);
     uint64_t *full = (uint64_t *)(ring + S * VEL_SLOT), *empty = full + S;
     __shared__ volatile int abort_s;
-    ring_init<S>(full, empty, &abort_s);
+    ring_init<S>(full, empty, &abort_s, CW);
     const int tx = threadIdx.x, ty = threadIdx.y;
 
-    if (ty == ST_CW) {                /* producer warp */
+    if (ty == CW) {                   /* producer warp */
         if (tx != 0) return;
         uint32_t use = 0;
         bool ok = true;
@@ -294,35 +295,44 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
     }
 
     const int sy = g.px, sz = g.plane;
-    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
     uint32_t use = 0;
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
         int q, t;
-            split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
+        split_item(item, ncomp, w.nitems / ncomp, qslow, q, t);
         int bx, by, k0, k1;
         work_item(g, w, t, bx, by, k0, k1);
-        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
-        const bool live = i <= g.nx && j <= g.ny;
+        const int i = bx * ST_X + 1 + tx;
         float *U = pick(cs, q, AF_U), *V = pick(cs, q, AF_V), *W = pick(cs, q, AF_W);
         const float *XZ = pick(cs, q, AF_XZ), *YZ = pick(cs, q, AF_YZ), *ZZ = pick(cs, q, AF_ZZ);
-        /* column queues, each loaded one level before it is needed */
-        float xz_m2 = 0.f, xz_m1 = 0.f, xz_p1 = 0.f, yz_m2 = 0.f, yz_m1 = 0.f, yz_p1 = 0.f;
-        float zz_m1 = 0.f, zz_0 = 0.f, zz_p1 = 0.f, zz_p2 = 0.f;
-        float dA = 0.f, dB = 0.f, dE = 0.f, cxy = 0.f;
-        int c = g.idx(i, j, k0);
-        if (live) {
-            xz_m2 = XZ[c - 2 * sz]; xz_m1 = XZ[c - sz]; xz_p1 = XZ[c + sz];
-            yz_m2 = YZ[c - 2 * sz]; yz_m1 = YZ[c - sz]; yz_p1 = YZ[c + sz];
-            zz_m1 = ZZ[c - sz]; zz_0 = ZZ[c]; zz_p1 = ZZ[c + sz]; zz_p2 = ZZ[c + 2 * sz];
-            dA = d1[c - sz]; dB = d1[c - sy - sz]; dE = d1[c + 1 - sz];
-            cxy = cx[i] * cy[j];
+        /* per row: column queues, each loaded one level before it is needed */
+        float xz_m2[RPT], xz_m1[RPT], xz_p1[RPT], yz_m2[RPT], yz_m1[RPT], yz_p1[RPT];
+        float zz_m1[RPT], zz_0[RPT], zz_p1[RPT], zz_p2[RPT], dA[RPT], dB[RPT], dE[RPT], cxy[RPT];
+        bool live[RPT];
+        const int c0 = g.idx(i, by * ST_Y + 1 + ty, k0);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int j = by * ST_Y + 1 + ty + r * CW, c = c0 + r * CW * sy;
+            live[r] = i <= g.nx && j <= g.ny;
+            xz_m2[r] = xz_m1[r] = xz_p1[r] = yz_m2[r] = yz_m1[r] = yz_p1[r] = 0.f;
+            zz_m1[r] = zz_0[r] = zz_p1[r] = zz_p2[r] = dA[r] = dB[r] = dE[r] = cxy[r] = 0.f;
+            if (live[r]) {
+                xz_m2[r] = XZ[c - 2 * sz]; xz_m1[r] = XZ[c - sz]; xz_p1[r] = XZ[c + sz];
+                yz_m2[r] = YZ[c - 2 * sz]; yz_m1[r] = YZ[c - sz]; yz_p1[r] = YZ[c + sz];
+                zz_m1[r] = ZZ[c - sz]; zz_0[r] = ZZ[c]; zz_p1[r] = ZZ[c + sz]; zz_p2[r] = ZZ[c + 2 * sz];
+                dA[r] = d1[c - sz]; dB[r] = d1[c - sy - sz]; dE[r] = d1[c + 1 - sz];
+                cxy[r] = cx[i] * cy[j];
+            }
         }
+        int cc = c0;
 #pragma unroll (UNR)
-        for (int k = k0; k <= k1; ++k, c += sz, ++use) {
-            float xz_n = 0.f, yz_n = 0.f, zz_n = 0.f, czk = 0.f;
-            if (live) {
-                if (k < k1) { xz_n = XZ[c + 2 * sz]; yz_n = YZ[c + 2 * sz]; zz_n = ZZ[c + 3 * sz]; }
-                czk = cz[k];
+        for (int k = k0; k <= k1; ++k, cc += sz, ++use) {
+            float xz_n[RPT], yz_n[RPT], zz_n[RPT];
+            const float czk = cz[k];
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int c = cc + r * CW * sy;
+                xz_n[r] = yz_n[r] = zz_n[r] = 0.f;
+                if (live[r] && k < k1) { xz_n[r] = XZ[c + 2 * sz]; yz_n[r] = YZ[c + 2 * sz]; zz_n[r] = ZZ[c + 3 * sz]; }
             }
             /* warp-uniform outcome, so a warp leaves together or not at all */
             if (!__all_sync(0xffffffffu, mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s))) {
@@ -330,25 +340,31 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
                 atomicOr(err, AWP_KERR_TMA_WAIT);
                 return;
             }
-            if (live) {
-                const float *sl = ring + (use % S) * VEL_SLOT;
-                const float u0 = sl[VEL_PT + cp], v0 = sl[VEL_PT + ST_PT + cp], w0 = sl[VEL_PT + 2 * ST_PT + cp];
-                const float *t1 = sl + 5 * ST_VT + cm;
-                const float da = t1[0], db = t1[-ST_W], de = t1[1], dg = t1[1 - ST_W];
-                float fu, fv, fw;
-                vel_factors7(da, db, dA, dB, de, dE, dg, dth, fu, fv, fw);
-                const TStr A{sl + cv, xz_m2, xz_m1, xz_p1, yz_m2, yz_m1, yz_p1, zz_m1, zz_0, zz_p1, zz_p2};
-                float u, v, w_;
-                vel_one_t(A, u0, v0, w0, fu, fv, fw, u, v, w_);
-                const float crj = cxy * czk;
-                U[c] = u * crj;
-                V[c] = v * crj;
-                W[c] = w_ * crj;
-                xz_m2 = xz_m1; xz_m1 = sl[3 * ST_VT + cv];
-                yz_m2 = yz_m1; yz_m1 = sl[4 * ST_VT + cv];
-                zz_m1 = zz_0; zz_0 = zz_p1; zz_p1 = zz_p2; zz_p2 = zz_n;
-                xz_p1 = xz_n; yz_p1 = yz_n;
-                dA = da; dB = db; dE = de;
+            const float *sl = ring + (use % S) * VEL_SLOT;
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int row = ty + r * CW, c = cc + r * CW * sy;
+                const int cv = (row + 2) * ST_W + tx + 4, cm = (row + 1) * ST_W + tx + 4, cp = row * ST_X + tx;
+                if (live[r]) {
+                    const float u0 = sl[VEL_PT + cp], v0 = sl[VEL_PT + ST_PT + cp], w0 = sl[VEL_PT + 2 * ST_PT + cp];
+                    const float *t1 = sl + 5 * ST_VT + cm;
+                    const float da = t1[0], db = t1[-ST_W], de = t1[1], dg = t1[1 - ST_W];
+                    float fu, fv, fw;
+                    vel_factors7(da, db, dA[r], dB[r], de, dE[r], dg, dth, fu, fv, fw);
+                    const TStr A{sl + cv, xz_m2[r], xz_m1[r], xz_p1[r], yz_m2[r], yz_m1[r], yz_p1[r],
+                                 zz_m1[r], zz_0[r], zz_p1[r], zz_p2[r]};
+                    float u, v, w_;
+                    vel_one_t(A, u0, v0, w0, fu, fv, fw, u, v, w_);
+                    const float crj = cxy[r] * czk;
+                    U[c] = u * crj;
+                    V[c] = v * crj;
+                    W[c] = w_ * crj;
+                    xz_m2[r] = xz_m1[r]; xz_m1[r] = sl[3 * ST_VT + cv];
+                    yz_m2[r] = yz_m1[r]; yz_m1[r] = sl[4 * ST_VT + cv];
+                    zz_m1[r] = zz_0[r]; zz_0[r] = zz_p1[r]; zz_p1[r] = zz_p2[r]; zz_p2[r] = zz_n[r];
+                    xz_p1[r] = xz_n[r]; yz_p1[r] = yz_n[r];
+                    dA[r] = da; dB[r] = db; dE[r] = de;
+                }
             }
             __syncwarp();
             if (tx == 0) mb_arrive(&empty[use % S]);
@@ -690,12 +706,15 @@ static size_t ring_bytes(int slots, int slot_floats) { return 128 + (size_t)slot
 template <int UNR>
 static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
+    constexpr int RPT = UNR < 0 ? 2 : 1;            /* UNR -1: two rows per thread, level loop rolled */
+    constexpr int U = UNR < 0 ? 1 : UNR;
+    constexpr int CW = ST_Y / RPT;
     const size_t smem = ring_bytes(1 + ST_VEL_D, VEL_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, UNR>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, U, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
-    k_vel_tma<ST_VEL_D, UNR><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
+    k_vel_tma<ST_VEL_D, U, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
         st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w,
         s.kerr);
     return cudaGetLastError();
@@ -730,6 +749,7 @@ static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cuda
 cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
+    if (s.staged_rpt_vel == 2) return launch_vel_u<-1>(st, s, stream);
     return s.unroll == 1 ? launch_vel_u<1>(st, s, stream) : launch_vel_u<2>(st, s, stream);
 }
 

@@ -142,7 +142,8 @@ def test_odd_sizes_and_boundary_points(kernel):
 
 @pytest.mark.parametrize("kernel,kstage,unroll,rpt", [("fused", None, None, None), ("staged", None, None, None),
                                                       ("staged", "8", "1", "1"), ("staged", "9", "2", "2"),
-                                                      ("staged", "16", "1", "2")])
+                                                      ("staged", "16", "1", "2"), ("staged", "9", "2", "2v"),
+                                                      ("staged", "16", "1", "1v")])
 def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, rpt, monkeypatch):
     """Several x/y tiles (partial ones at the high edges) and z chunks: halo
     recompute at the fused stepper's tile seams and redundant levels at its
@@ -152,8 +153,10 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, rpt, monkeypatch):
         monkeypatch.setenv("AWP_TUNE_KSTAGE", kstage)
     if unroll:
         monkeypatch.setenv("AWP_TUNE_UNROLL", unroll)
-    if rpt:
-        monkeypatch.setenv("AWP_TUNE_RPT", rpt)
+    if rpt:                               # "2v": two rows per thread in the velocity sweep too
+        monkeypatch.setenv("AWP_TUNE_RPT", rpt[0])
+        if rpt.endswith("v"):
+            monkeypatch.setenv("AWP_TUNE_RPTV", "2")
     c = Case(nx=100, ny=30, nz=80, nt=25, nd=6, srcs=[[(50, 15, 40)]], ntiskp=5, write_step=5)
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
@@ -161,9 +164,11 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, rpt, monkeypatch):
 @pytest.mark.parametrize("qslow", ["0", "1"])
 def test_staged_batched_components_many_items(qslow, monkeypatch):
     """Three components as neighbouring work items (or one component over
-    all tiles at a time), 8-level chunks, two tile rows per stress thread."""
+    all tiles at a time), 8-level chunks, two tile rows per thread in both
+    sweeps."""
     monkeypatch.setenv("AWP_TUNE_KSTAGE", "8")
     monkeypatch.setenv("AWP_TUNE_RPT", "2")
+    monkeypatch.setenv("AWP_TUNE_RPTV", "2")
     monkeypatch.setenv("AWP_TUNE_QSLOW", qslow)
     c = Case(nx=70, ny=20, nz=41, nt=30, igreen=(1, 2, 3),
              srcs=[[(35, 10, 20)], [(34, 9, 20)], [(36, 11, 21)]])
