@@ -486,7 +486,13 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->kchunk = choose_kchunk(s->g, 1, s->ty);
     s->kchunk_sweep = choose_kchunk(s->g, 0, s->ty == 4 ? 4 : 8);
     {
-        const int kc = env_int("AWP_TUNE_KSTAGE", 32);
+        /* z chunks of about 40 levels, split evenly: every chunk costs one
+         * prologue level, and a short last chunk leaves blocks idle */
+        int kc = env_int("AWP_TUNE_KSTAGE", 0);
+        if (kc <= 0) {
+            const int nch = (s->g.nz + 39) / 40;
+            kc = (s->g.nz + nch - 1) / nch;
+        }
         s->kchunk_staged = kc < 8 ? 8 : (kc > s->g.nz ? s->g.nz : kc);
         s->staged_qslow = env_int("AWP_TUNE_QSLOW", 1) != 0;
         /* stress sweep rows per consumer thread: two pay off once three

@@ -821,11 +821,13 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         long long total = 0;
         for (int v = v0; v < v0 + nb; v++) total += tpre[(size_t)v * (np + 1) + np];
         /* at least four chunks (to overlap the plan with the device) of equal
-         * size, none above the term buffer */
+         * size, none above the term buffer; the first one an eighth of that,
+         * so that the device starts while the host plans the rest */
         long long nch = (total + ucap - 1) / ucap;
         nch = nch < 4 ? 4 : nch;
-        const long long target = (total + nch - 1) / nch;
-        for (int p0 = 0; p0 < np;) {
+        const long long full_target = (total + nch - 1) / nch;
+        long long target = (full_target + 7) / 8;
+        for (int p0 = 0; p0 < np; target = full_target) {
             long long t = 0, n = 0;
             int p1 = p0;
             while (p1 < np) {
