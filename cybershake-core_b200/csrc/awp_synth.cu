@@ -1010,11 +1010,11 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
             nk++;
             launches += (ngroups > 0) + (nmulti > 0) + 1;
         }
-        const bool last_of_batch = ic + 1 == chunks.size() || chunks[ic + 1].v0 != C.v0;
-        if (last_of_batch)
-            SCU(cudaMemcpyAsync(s->h_seis.p + (size_t)C.v0 * 3 * ntout, seis_b, (size_t)nb * 3 * ntout * sizeof(float),
-                                cudaMemcpyDeviceToHost, s->stream));
     }
+    /* every variation's seismograms, including those of a rupture without
+     * points or without slip (zeros from the memset) */
+    SCU(cudaMemcpyAsync(s->h_seis.p, s->d_seis.p, (size_t)nv * 3 * ntout * sizeof(float), cudaMemcpyDeviceToHost,
+                        s->stream));
     SCU(cudaEventRecord(s->ev[1], s->stream));
     SCU(cudaEventSynchronize(s->ev[1]));
     SCU(cudaStreamSynchronize(s->cstream));

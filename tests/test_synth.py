@@ -269,3 +269,43 @@ def test_device_large_case_properties():
     c.variations = [(p, q * np.float32(2.0)) for p, q in c.variations[::-1]]
     d, _ = run_device(c, 1500)
     np.testing.assert_allclose(d, a * np.float32(2.0), rtol=1e-6, atol=1e-36)
+
+
+@pytest.mark.gpu
+def test_device_zero_slip_long_slip_rate_and_reuse():
+    """A rupture without slip gives zero seismograms; a slip rate longer than
+    ntout is refused; clearing the variations keeps the SGT set for the next
+    rupture, whose results equal a fresh object's."""
+    c = ai.synth_case(seed=24, nv=2)
+    with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=500) as s:
+        s.set_sgt(c.master, c.index, c.headers, c.comps)
+        p, q = c.variations[0]
+        quiet = p.copy()
+        quiet["nt1"] = quiet["nt2"] = quiet["nt3"] = 0
+        s.add_variation(0, quiet, q)
+        z = s.run()
+        assert z.shape == (1, 3, 500) and not np.any(z.view(np.uint32))
+        assert s.info().terms == 0
+        s.clear_variations()
+        longer = p.copy()
+        i = int(np.argmax(longer["nt1"]))
+        longer["nt1"][i], longer["stf1"][i] = 501, len(q)
+        s.add_variation(1, longer, np.concatenate([q, np.ones(501, np.float32)]))
+        with pytest.raises(awpsgt.AwpError, match="longer than ntout"):
+            s.run()
+        s.clear_variations()
+        for k, (pp, qq) in enumerate(c.variations):
+            s.add_variation(k, pp, qq)
+        again = s.run()
+    want, _ = case_seis(c, 500)
+    assert np.array_equal(again.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_device_empty_rupture():
+    c = ai.synth_case(seed=25, nv=1)
+    with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=300) as s:
+        s.set_sgt(c.master, c.index, c.headers, c.comps)
+        s.add_variation(0, np.zeros(0, awpsgt.SRFPOINT), np.zeros(0, np.float32))
+        out = s.run()
+    assert out.shape == (1, 3, 300) and not np.any(out)
