@@ -433,7 +433,7 @@ def run_synth(args):
             t0 = time.perf_counter()
             s2.clear_variations()
             for i2, (p, q) in enumerate(c.variations):
-                s2.add_variation(i2, p, q)
+                s2.add_variation(i2, p, q, borrow=True)
             out = s2.run()
             if it:
                 ts.append(time.perf_counter() - t0)

@@ -49,7 +49,7 @@ EXPORTED = [
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
     "awp_synth_create", "awp_synth_destroy", "awp_synth_set_sgt", "awp_synth_load_sgt_files",
-    "awp_synth_add_variation", "awp_synth_add_srf_file", "awp_synth_clear_variations", "awp_synth_run",
+    "awp_synth_add_variation", "awp_synth_add_variation_borrowed", "awp_synth_add_srf_file", "awp_synth_clear_variations", "awp_synth_run",
     "awp_synth_seismograms", "awp_synth_write_grm", "awp_synth_get_info", "awp_srf_read",
 ]
 
@@ -229,6 +229,7 @@ class Synth:
         _check(self.lib.awp_synth_create(C.byref(self.p), C.byref(h)))
         self.h = h
         self.nvar = 0
+        self._borrowed = []          # arrays the library reads in place until run / clear
 
     def close(self):
         if getattr(self, "h", None):
@@ -263,10 +264,15 @@ class Synth:
         _check(self.lib.awp_synth_load_sgt_files(self.h, enc(xhead), enc(xdata), enc(yhead), enc(ydata),
                                                  enc(zhead), enc(zdata)))
 
-    def add_variation(self, rup_var_id: int, points: np.ndarray, pool: np.ndarray):
+    def add_variation(self, rup_var_id: int, points: np.ndarray, pool: np.ndarray, borrow: bool = False):
+        """Adds a variation; with borrow the library reads the arrays in place
+        (this object keeps them alive until the next run / clear)."""
         pts = np.ascontiguousarray(points, SRFPOINT)
         pl = np.ascontiguousarray(pool, np.float32)
-        _check(self.lib.awp_synth_add_variation(self.h, rup_var_id, _ptr(pts), len(pts), _ptr(pl), pl.size))
+        fn = self.lib.awp_synth_add_variation_borrowed if borrow else self.lib.awp_synth_add_variation
+        _check(fn(self.h, rup_var_id, _ptr(pts), len(pts), _ptr(pl), pl.size))
+        if borrow:
+            self._borrowed.append((pts, pl))
         self.nvar += 1
 
     def add_srf_file(self, rup_var_id: int, path: str, binary: bool = False):
@@ -276,6 +282,7 @@ class Synth:
     def clear_variations(self):
         _check(self.lib.awp_synth_clear_variations(self.h))
         self.nvar = 0
+        self._borrowed = []
 
     def run(self) -> np.ndarray:
         """Synthesises every variation; returns [nvar][3][ntout] (vertical, north, east)."""
@@ -376,6 +383,8 @@ def load_library(path: str = LIB_PATH):
                                         C.c_void_p, C.c_void_p]),
         "awp_synth_load_sgt_files": (C.c_int, [C.c_void_p] + [C.c_char_p] * 6),
         "awp_synth_add_variation": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
+        "awp_synth_add_variation_borrowed": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                                       C.c_int64]),
         "awp_synth_add_srf_file": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int]),
         "awp_synth_clear_variations": (C.c_int, [C.c_void_p]),
         "awp_synth_run": (C.c_int, [C.c_void_p]),

@@ -407,10 +407,16 @@ struct Stage {
     }
 };
 
+/* a rupture variation: its own copy of the points and samples, or the
+ * caller's arrays (borrowed while the variation is listed) */
 struct Variation {
     int id;
-    std::vector<awp_srf_point> pts;
-    std::vector<float> pool;
+    std::vector<awp_srf_point> own_pts;
+    std::vector<float> own_pool;
+    const awp_srf_point *pts;
+    int np;
+    const float *pool;
+    long long npool;
 };
 
 double now_s()
@@ -604,14 +610,13 @@ extern "C" awp_status awp_synth_load_sgt_files(awp_synth *s, const char *xhead, 
                              ncomp > 1 ? data[1].data() : nullptr, ncomp > 2 ? data[2].data() : nullptr);
 }
 
-extern "C" awp_status awp_synth_add_variation(awp_synth *s, int rup_var_id, const awp_srf_point *pts, int np,
-                                              const float *pool, long long npool)
+static awp_status add_variation(awp_synth *s, int rup_var_id, const awp_srf_point *pts, int np, const float *pool,
+                                long long npool, bool borrow)
 {
     if (!s || (np > 0 && !pts) || (npool > 0 && !pool) || np < 0 || npool < 0)
         return fail(AWP_ERR_PARAM, "awp_synth_add_variation: bad argument");
-    if (!s->vars.empty() && (int)s->vars[0].pts.size() != np)
-        return fail(AWP_ERR_PARAM, "awp_synth_add_variation: %d points, the rupture has %d", np,
-                    (int)s->vars[0].pts.size());
+    if (!s->vars.empty() && s->vars[0].np != np)
+        return fail(AWP_ERR_PARAM, "awp_synth_add_variation: %d points, the rupture has %d", np, s->vars[0].np);
     for (int i = 0; i < np; i++) {
         const awp_srf_point &a = pts[i];
         const int n[3] = {a.nt1, a.nt2, a.nt3};
@@ -620,12 +625,33 @@ extern "C" awp_status awp_synth_add_variation(awp_synth *s, int rup_var_id, cons
             if (n[q] < 0 || (n[q] > 0 && (o[q] < 0 || o[q] + n[q] > npool)))
                 return fail(AWP_ERR_PARAM, "awp_synth_add_variation: point %d slip-rate samples outside the pool", i);
     }
-    Variation v;
+    s->vars.emplace_back();
+    Variation &v = s->vars.back();
     v.id = rup_var_id;
-    v.pts.assign(pts, pts + np);
-    v.pool.assign(pool, pool + npool);
-    s->vars.push_back(std::move(v));
+    v.np = np;
+    v.npool = npool;
+    if (borrow) {
+        v.pts = pts;
+        v.pool = pool;
+    } else {
+        v.own_pts.assign(pts, pts + np);
+        v.own_pool.assign(pool, pool + npool);
+        v.pts = v.own_pts.data();
+        v.pool = v.own_pool.data();
+    }
     return AWP_OK;
+}
+
+extern "C" awp_status awp_synth_add_variation(awp_synth *s, int rup_var_id, const awp_srf_point *pts, int np,
+                                              const float *pool, long long npool)
+{
+    return add_variation(s, rup_var_id, pts, np, pool, npool, false);
+}
+
+extern "C" awp_status awp_synth_add_variation_borrowed(awp_synth *s, int rup_var_id, const awp_srf_point *pts,
+                                                       int np, const float *pool, long long npool)
+{
+    return add_variation(s, rup_var_id, pts, np, pool, npool, true);
 }
 
 extern "C" awp_status awp_synth_add_srf_file(awp_synth *s, int rup_var_id, const char *path, int binary)
@@ -740,7 +766,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
     if (s->vars.empty()) return fail(AWP_ERR_STATE, "awp_synth_run: no rupture variation added");
     SCU(cudaSetDevice(s->p.device));
     double t_plan = now_s();
-    const int np = (int)s->vars[0].pts.size(), nv = (int)s->vars.size();
+    const int np = s->vars[0].np, nv = (int)s->vars.size();
     int ntsum, ntout;
     synth_lengths(s, &ntsum, &ntout);
     const int nt = s->m.nt;
@@ -920,7 +946,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
         for (int b = 0; b < nb; b++) {
             const Variation &v = s->vars[C.v0 + b];
             long long nterms = 0, nused = 0;
-            pst[b] = awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(), p0, p1,
+            pst[b] = awp_synth_plan_variation(&cx, v.pts, v.pool, v.npool, p0, p1,
                                               S.gt.p + toff[b], S.ct.p + toff[b], S.stf.p + soff[b], soff[b],
                                               &nterms, &nused, &macs[b]);
         }
@@ -931,7 +957,7 @@ extern "C" awp_status awp_synth_run(awp_synth *s)
                 for (auto &sg : s->stage) sg.pending = false;
                 const Variation &v = s->vars[C.v0 + b];
                 long long a1, a2, a3;
-                return awp_synth_plan_variation(&cx, v.pts.data(), v.pool.data(), (long long)v.pool.size(), p0, p1,
+                return awp_synth_plan_variation(&cx, v.pts, v.pool, v.npool, p0, p1,
                                                 S.gt.p + toff[b], S.ct.p + toff[b], S.stf.p + soff[b], soff[b], &a1,
                                                 &a2, &a3);
             }

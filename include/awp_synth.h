@@ -117,6 +117,13 @@ awp_status awp_synth_load_sgt_files(awp_synth *s, const char *xhead, const char 
 awp_status awp_synth_add_variation(awp_synth *s, int rup_var_id, const awp_srf_point *pts, int np,
                                    const float *pool, long long npool);
 
+/* The same without a copy: the library reads pts and pool in place, so they
+ * must stay valid and unchanged while the variation is listed, that is until
+ * awp_synth_clear_variations or awp_synth_destroy (no reference
+ * counterpart). */
+awp_status awp_synth_add_variation_borrowed(awp_synth *s, int rup_var_id, const awp_srf_point *pts, int np,
+                                            const float *pool, long long npool);
+
 /* Reads an SRF file (text when binary == 0; jbsim/srf_subs.c:521-690) and adds
  * it as a variation. */
 awp_status awp_synth_add_srf_file(awp_synth *s, int rup_var_id, const char *path, int binary);

@@ -309,3 +309,17 @@ def test_device_empty_rupture():
         s.add_variation(0, np.zeros(0, awpsgt.SRFPOINT), np.zeros(0, np.float32))
         out = s.run()
     assert out.shape == (1, 3, 300) and not np.any(out)
+
+
+@pytest.mark.gpu
+def test_device_borrowed_variations_equal_copied():
+    c = ai.synth_case(seed=26, nv=4)
+    a, _ = run_device(c, 600)
+    with awpsgt.Synth(c.slon, c.slat, c.dtout, ntout=600) as s:
+        s.set_sgt(c.master, c.index, c.headers, c.comps)
+        for i, (p, q) in enumerate(c.variations):
+            s.add_variation(100 + i, p, q, borrow=True)
+        b = s.run()
+        again = s.run()                      # still listed: read in place again
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(a.view(np.uint32), again.view(np.uint32))
