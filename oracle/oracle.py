@@ -269,3 +269,35 @@ def synth_get_indx(master, h, lon, lat, dep):
     xyz = np.zeros(3, np.int32)
     lib.orc_synth_get_indx(_p(m), h, lon, lat, dep, C.byref(indx), _p(xyz))
     return indx.value, tuple(int(v) for v in xyz)
+
+
+def synth_reference(master, index, headers, comps, slon, slat, dtout, ntout, tstart, variations):
+    """The same seismograms from DirectSynth's own functions, built from the
+    reference sources into oracle/_ref/libsynth_ref.so (oracle/Makefile.ref);
+    None where that library has not been built."""
+    path = os.path.join(_HERE, "_ref", "libsynth_ref.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    V = C.c_void_p
+    lib.ref_synth.restype = C.c_int
+    lib.ref_synth.argtypes = [V, V, V, C.c_int, V, V, V, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
+                              C.c_int, C.c_int, V, V, V, V, C.POINTER(C.c_int)]
+    m = np.ascontiguousarray(np.asarray(master, SGTMASTER).reshape(1))
+    ix = np.ascontiguousarray(index, SGTINDEX)
+    hd = np.ascontiguousarray(headers, SGTHEADER)
+    cs = [np.ascontiguousarray(c, np.float32) for c in comps]
+    ptr = [_p(c) for c in cs] + [None] * (3 - len(cs))
+    nv, npts = len(variations), len(variations[0][0])
+    pts = np.ascontiguousarray(np.concatenate([np.asarray(v[0], SRFPOINT) for v in variations]), SRFPOINT)
+    pools = [np.ascontiguousarray(v[1], np.float32) for v in variations]
+    off = np.cumsum([0] + [p.size for p in pools[:-1]]).astype(np.int64)
+    pool = np.ascontiguousarray(np.concatenate(pools + [np.zeros(1, np.float32)]))
+    got = C.c_int()
+    n = 1 << 22
+    seis = np.zeros(nv * 3 * (ntout if ntout > 0 else n), np.float32)
+    rc = lib.ref_synth(_p(m), _p(ix), _p(hd), len(cs), ptr[0], ptr[1], ptr[2], slon, slat, dtout, ntout, tstart, nv,
+                       npts, _p(pts), _p(pool), _p(off), _p(seis), C.byref(got))
+    if rc:
+        raise ValueError("reference synthesis failed (code %d)" % rc)
+    return seis[:nv * 3 * got.value].reshape(nv, 3, got.value)

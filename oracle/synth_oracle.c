@@ -19,9 +19,12 @@
  * point the rupture needs.  SRF resampling (srf_rupm.c:115-146) is not
  * restated; a variation whose sample interval differs from dtout is refused.
  *
- * Parity unpinned: the reference builds only against MPI, libmemcached,
- * cfuhash, getpar and the rupture generator library, none of which is
- * present, and it ships no test vectors for this path.
+ * Pinned: the reference's own functions for this path compile from their
+ * sources with declaration-only stand-ins for the libraries they do not use
+ * here (oracle/Makefile.ref, oracle/refinc, synth_ref_stubs.c), and
+ * synth_ref_driver.c runs them in jbsim3d_synth's order; this restatement
+ * equals them bit for bit on every case of tests/golden/synth (seismograms
+ * they produced) and of the live comparisons in tests/test_synth.py.
  */
 #include <math.h>
 #include <stdlib.h>

@@ -4,9 +4,13 @@ oracle's own known-answer checks and the file paths.
 
 The oracle restates jbsim3d_synth's loop (find_sgt, mech_sgt, sum_sgt /
 timeshift_sgt, srf_stf / do_cnvlv) in the reference's order; the device path
-must equal it bit for bit.  Parity with the reference itself is unpinned: the
-reference needs MPI, libmemcached, cfuhash, getpar and the rupture generator
-to build and ships no vectors for this step."""
+must equal it bit for bit.  Both are pinned to DirectSynth's own functions:
+tests/golden/synth holds seismograms those functions produced
+(tests/golden/make_synth_golden.py, via oracle/_ref/libsynth_ref.so built by
+oracle/Makefile.ref), and where that library is built the oracle is also
+compared with it live."""
+import hashlib
+import json
 import os
 
 import numpy as np
@@ -17,9 +21,54 @@ import awpsgt
 import oracle
 
 
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden", "synth")
+GOLD_CASES = json.load(open(os.path.join(GOLD, "cases.json")))
+
+
+def golden_case(g):
+    kw = dict(g["case"])
+    if "nstf" in kw:
+        kw["nstf"] = tuple(kw["nstf"])
+    c = ai.synth_case(**kw)
+    h = hashlib.sha256()
+    for a in [c.master, c.index, c.headers] + list(c.comps):
+        h.update(np.ascontiguousarray(a).tobytes())
+    for p, q in c.variations:
+        h.update(np.ascontiguousarray(p).tobytes())
+        h.update(np.ascontiguousarray(q).tobytes())
+    h.update(np.float32([c.slon, c.slat, c.dtout]).tobytes())
+    assert h.hexdigest() == g["inputs_sha256"], "synth_case no longer makes the inputs the fixture was made from"
+    return c, np.load(os.path.join(GOLD, g["name"] + ".npy"))
+
+
 def case_seis(c, ntout=0, tstart=0.0):
     return oracle.synth(c.master, c.index, c.headers, c.comps, c.slon, c.slat, c.dtout, ntout, tstart,
                         c.variations)
+
+
+# ---- pinning: the reference's own synthesis functions -----------------------
+
+@pytest.mark.parametrize("g", GOLD_CASES, ids=lambda g: g["name"])
+def test_oracle_matches_reference_fixtures(g):
+    c, want = golden_case(g)
+    got, _ = case_seis(c, g["ntout"], g["tstart"])
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsynth_ref.so")),
+                    reason="reference synthesis functions not built here")
+@pytest.mark.parametrize("seed,kw,ntout,tstart", [
+    (31, dict(nv=4, mech2_frac=0.3, mech3_frac=0.2, jitter=0.45), 900, 0.7),
+    (32, dict(ncomp=3, nv=2, drop_frac=0.5, nstf=(3, 200), nt=350), 0, -1.0),
+    (33, dict(ncomp=1, nv=3, zero_frac=0.5, nx_f=16, nz_f=10), 300, 3.0)])
+def test_oracle_matches_live_reference(seed, kw, ntout, tstart):
+    c = ai.synth_case(seed=seed, **kw)
+    got, _ = case_seis(c, ntout, tstart)
+    want = oracle.synth_reference(c.master, c.index, c.headers, c.comps, c.slon, c.slat, c.dtout, ntout, tstart,
+                                  c.variations)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
 # ---- host side: SRF reader, grid lookup, the oracle's known answers ----------
@@ -323,3 +372,12 @@ def test_device_borrowed_variations_equal_copied():
         again = s.run()                      # still listed: read in place again
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert np.array_equal(a.view(np.uint32), again.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("g", GOLD_CASES, ids=lambda g: g["name"])
+def test_device_matches_reference_fixtures(g):
+    """The device path against seismograms of DirectSynth's own functions."""
+    c, want = golden_case(g)
+    got, _ = run_device(c, g["ntout"], g["tstart"])
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
