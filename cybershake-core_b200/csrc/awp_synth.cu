@@ -464,6 +464,8 @@ static awp_status synth_set_sgt_common(awp_synth *s, const awp_sgtmaster *m, con
             return fail(AWP_ERR_PARAM, "awp_synth_set_sgt: SGT index not sorted by indx");
     }
     if (hd[0].nt != m->nt) return fail(AWP_ERR_PARAM, "awp_synth_set_sgt: header nt differs from the master nt");
+    if (!(ix[0].h > 0.0f) || !(hd[0].dt > 0.0f))
+        return fail(AWP_ERR_PARAM, "awp_synth_set_sgt: grid spacing and SGT sample interval must be > 0");
     s->m = *m;
     s->ix.assign(ix, ix + m->globnp);
     s->hd.assign(hd, hd + m->globnp);

@@ -27,6 +27,11 @@
  *     the SGT files supply (jbsim3d.c:616-660);
  *   - rupture variations are SRF point lists (jbsim/srf_subs.c:521-690).
  *
+ * Ownership and threading: a synthesis object owns its device memory (the SGT
+ * set, per-chunk term buffers, the seismograms) and its three CUDA streams;
+ * calls on one object must not overlap, separate objects may run from
+ * separate host threads.  Errors are status codes with awp_last_error().
+ *
  * Not on the path and rejected with AWP_ERR_PARAM: an SRF sample interval
  * that differs from dtout by more than the reference's 1e-5 ratio (the
  * reference resamples, srf_rupm.c:115-146; CyberShake generates the
