@@ -190,9 +190,11 @@ def solver_params(w, device, precision="f32", kernel="auto"):
                               device=device)
 
 
-def make_solver(w, media, pts, stfs, device, precision="f32", kernel="auto"):
+def make_solver(w, media, pts, stfs, device, precision="f32", kernel="auto", tuning=None):
     import awpsgt
     s = awpsgt.Solver(solver_params(w, device, precision, kernel))
+    if tuning is not None:
+        s.set_tuning(tuning)
     s.load_media(media)
     for q in range(len(w.igreen)):
         s.set_source(q, [w.src_xyz], stfs[q])
@@ -509,6 +511,9 @@ def main():
     ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="admission order")
     ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
     ap.add_argument("--synth", action="store_true", help="reciprocity synthesis: rupture variations per second")
+    ap.add_argument("--autotune", action="store_true", help="time launch shapes on this grid first (untimed)")
+    ap.add_argument("--tune-cache", default="", help="autotuner cache file")
+    ap.add_argument("--tune-steps", type=int, default=20, help="time steps per autotuner trial")
     args = ap.parse_args()
     if args.serve:
         return run_serve(args)
@@ -529,8 +534,18 @@ def main():
     steps_needed = (args.warmup + args.steps) * per_step_ts + 40
     assert steps_needed <= w.nt, "too many bench steps for one solve"
 
+    # ---------------- launch shapes (untimed) ----------------
+    tuning, tune_info = None, None
+    if args.autotune:
+        t0 = time.perf_counter()
+        tuning, trial_rate = awpsgt.autotune(solver_params(w, local, args.precision, args.kernel), media,
+                                             trial_steps=args.tune_steps, cache=args.tune_cache or None)
+        tune_info = {"trial_gcell_per_s": trial_rate, "seconds": time.perf_counter() - t0,
+                     "trial_steps": args.tune_steps}
+
     # ---------------- device-resident throughput ----------------
-    s = make_solver(w, media, pts, stfs, local, args.precision, args.kernel)
+    s = make_solver(w, media, pts, stfs, local, args.precision, args.kernel, tuning)
+    used_tuning = s.tuning().as_dict()
     s.run(args.warmup * per_step_ts)
     barrier(dist)
     with ClockSampler(local) as clk:
@@ -561,7 +576,7 @@ def main():
     for it in range(0 if args.no_e2e else 1 + args.e2e_solves):
         barrier(dist)
         t0 = time.perf_counter()
-        s = make_solver(w, media_pinned, pts, stfs, local, args.precision, args.kernel)
+        s = make_solver(w, media_pinned, pts, stfs, local, args.precision, args.kernel, tuning)
         out = s.run(w.nt, with_sgt=True)
         s.close()
         el = time.perf_counter() - t0
@@ -605,7 +620,8 @@ def main():
                    "time_steps_per_bench_step": per_step_ts, "sgt_points": int(pts.shape[0]),
                    "precision": args.precision, "l2": "inputs larger than L2 (%.1f GB state)" % (
                        s.p.nx * s.p.ny * s.p.nz * 4 * (15 * ncomp + 5) / 1e9),
-                   "parallelism": "independent SGT jobs, one per GPU" if world > 1 else "single GPU"},
+                   "parallelism": "independent SGT jobs, one per GPU" if world > 1 else "single GPU",
+                   "tuning": used_tuning, "autotune": tune_info},
         "roofline": roofline,
         "e2e": e2e,
         "gpu_launches": gpu_launches,

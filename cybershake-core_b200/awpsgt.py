@@ -44,7 +44,7 @@ EXPORTED = [
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
-    "awp_reformat_velocity",
+    "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune",
 ]
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
@@ -85,6 +85,15 @@ class Stats(C.Structure):
         ("vp_min", C.c_float), ("vp_max", C.c_float), ("vs_min", C.c_float), ("vs_max", C.c_float),
         ("rho_min", C.c_float), ("rho_max", C.c_float), ("energy", C.c_double),
     ]
+
+
+class Tuning(C.Structure):
+    """awp_tuning: launch shapes of the steppers (results do not depend on them)."""
+    _fields_ = [(n, C.c_int) for n in ("kchunk_staged", "staged_qslow", "staged_rpt", "staged_rpt_vel", "unroll",
+                                        "ty", "kchunk", "kchunk_sweep")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class KernelTimes(C.Structure):
@@ -377,6 +386,9 @@ def load_library(path: str = LIB_PATH):
         "awp_load_media_rwg": (C.c_int, [C.c_void_p, C.c_char_p]),
         "awp_reformat_velocity": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
+        "awp_get_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
+        "awp_set_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
+        "awp_autotune": (C.c_int, [P(Params), C.c_void_p, C.c_int, C.c_char_p, P(Tuning), P(C.c_double)]),
         "awp_synth_create": (C.c_int, [P(SynthParams), P(C.c_void_p)]),
         "awp_synth_destroy": (None, [C.c_void_p]),
         "awp_synth_set_sgt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
@@ -563,6 +575,31 @@ class Solver:
         s = Stats()
         _check(self.lib.awp_get_stats(self.h, C.byref(s)))
         return s
+
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        _check(self.lib.awp_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: Tuning):
+        _check(self.lib.awp_set_tuning(self.h, C.byref(t)))
+
+
+def autotune(params: Params, media: Optional[np.ndarray] = None, trial_steps: int = 20,
+             cache: Optional[str] = None):
+    """Times candidate launch shapes on the grid and settings of `params` and
+    returns (best Tuning, Gcell-updates/s).  media as for Solver.load_media, or
+    None for a homogeneous medium; with `cache` the result is read from / kept in
+    that file, keyed by grid, components, precision, stepper and GPU model."""
+    lib = load_library()
+    t = Tuning()
+    rate = C.c_double()
+    m = None
+    if media is not None:
+        m = np.ascontiguousarray(media, dtype=np.float32)
+    _check(lib.awp_autotune(C.byref(params), None if m is None else _ptr(m), trial_steps,
+                            None if cache is None else cache.encode(), C.byref(t), C.byref(rate)))
+    return t, rate.value
 
 
 class Request(C.Structure):

@@ -1485,3 +1485,216 @@ extern "C" awp_status awp_energy(awp_solver *s, double *out)
     CU(cudaStreamSynchronize(s->stream));
     return AWP_OK;
 }
+
+/* ------------------------------------------------------------------ */
+/* launch shapes and the autotuner                                     */
+/* ------------------------------------------------------------------ */
+
+static void drop_graphs(awp_solver *s)
+{
+    for (int b = 0; b < 2; b++)
+        if (s->graph[b]) {
+            cudaGraphExecDestroy(s->graph[b]);
+            s->graph[b] = NULL;
+        }
+}
+
+extern "C" awp_status awp_get_tuning(awp_solver *s, awp_tuning *t)
+{
+    if (!s || !t) return set_err(AWP_ERR_PARAM, "awp_get_tuning: null argument");
+    t->kchunk_staged = s->kchunk_staged;
+    t->staged_qslow = s->staged_qslow;
+    t->staged_rpt = s->staged_rpt;
+    t->staged_rpt_vel = s->staged_rpt_vel;
+    t->unroll = s->unroll;
+    t->ty = s->ty;
+    t->kchunk = s->kchunk;
+    t->kchunk_sweep = s->kchunk_sweep;
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
+{
+    if (!s || !t) return set_err(AWP_ERR_PARAM, "awp_set_tuning: null argument");
+    const int nz = s->g.nz, kmax = nz > 8 ? nz : 8;
+    if (t->kchunk_staged < 8 || t->kchunk_staged > kmax || t->kchunk < 8 || t->kchunk > kmax ||
+        t->kchunk_sweep < 8 || t->kchunk_sweep > kmax)
+        return set_err(AWP_ERR_PARAM, "awp_set_tuning: z levels per work item must be 8..%d", kmax);
+    if ((t->staged_qslow != 0 && t->staged_qslow != 1) || (t->staged_rpt != 1 && t->staged_rpt != 2) ||
+        (t->staged_rpt_vel != 1 && t->staged_rpt_vel != 2) || (t->unroll != 1 && t->unroll != 2) ||
+        (t->ty != 4 && t->ty != 8 && t->ty != 16))
+        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16");
+    CU(cudaSetDevice(s->p.device));
+    CU(cudaStreamSynchronize(s->stream));   /* no captured step in flight when its graph goes */
+    s->kchunk_staged = t->kchunk_staged;
+    s->staged_qslow = t->staged_qslow;
+    s->staged_rpt = t->staged_rpt;
+    s->staged_rpt_vel = t->staged_rpt_vel;
+    s->unroll = t->unroll;
+    s->ty = t->ty;
+    s->kchunk = t->kchunk;
+    s->kchunk_sweep = t->kchunk_sweep;
+    drop_graphs(s);
+    return AWP_OK;
+}
+
+/* "nx ny nz ncomp precision nve stepper gpu-model" */
+static void tune_key(const awp_params *p, int stepper, char *key, size_t n)
+{
+    cudaDeviceProp prop;
+    char model[256] = "unknown";
+    if (cudaGetDeviceProperties(&prop, p->device) == cudaSuccess) {
+        snprintf(model, sizeof model, "%s", prop.name);
+        for (char *c = model; *c; ++c)
+            if (*c == ' ') *c = '_';
+    }
+    snprintf(key, n, "%d %d %d %d %d %d %d %s", p->nx, p->ny, p->nz, p->ncomp, (int)p->precision, p->nve, stepper,
+             model);
+}
+
+static int tune_cache_get(const char *path, const char *key, awp_tuning *t, double *rate)
+{
+    FILE *f = path ? fopen(path, "r") : NULL;
+    if (!f) return 0;
+    char line[512];
+    int found = 0;
+    const size_t kl = strlen(key);
+    while (fgets(line, sizeof line, f)) {
+        if (strncmp(line, key, kl) != 0 || line[kl] != ' ') continue;
+        awp_tuning u;
+        double r = 0.0;
+        if (sscanf(line + kl, "%d %d %d %d %d %d %d %d %lf", &u.kchunk_staged, &u.staged_qslow, &u.staged_rpt,
+                   &u.staged_rpt_vel, &u.unroll, &u.ty, &u.kchunk, &u.kchunk_sweep, &r) == 9) {
+            *t = u;
+            *rate = r;
+            found = 1;                        /* the last entry for a key wins */
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void tune_cache_put(const char *path, const char *key, const awp_tuning *t, double rate)
+{
+    FILE *f = path ? fopen(path, "a") : NULL;
+    if (!f) return;
+    fprintf(f, "%s %d %d %d %d %d %d %d %d %.6g\n", key, t->kchunk_staged, t->staged_qslow, t->staged_rpt,
+            t->staged_rpt_vel, t->unroll, t->ty, t->kchunk, t->kchunk_sweep, rate);
+    fclose(f);
+}
+
+/* Gcell-updates/s of trial_steps steps with tuning t (after one warm-up
+ * step that rebuilds the captured graph) */
+static awp_status tune_trial(awp_solver *s, const awp_tuning *t, int trial_steps, double *rate)
+{
+    awp_status st = awp_set_tuning(s, t);
+    if (st != AWP_OK) return st;
+    if ((st = awp_run(s, s->p.ntiskp_sgt, NULL)) != AWP_OK) return st;
+    awp_stats a, b;
+    if ((st = awp_get_stats(s, &a)) != AWP_OK) return st;
+    if ((st = awp_run(s, trial_steps, NULL)) != AWP_OK) return st;
+    if ((st = awp_get_stats(s, &b)) != AWP_OK) return st;
+    const double sec = b.seconds_loop - a.seconds_loop;
+    const double upd = (double)s->g.nx * s->g.ny * s->g.nz * s->p.ncomp * (double)(b.steps_done - a.steps_done);
+    *rate = sec > 0 ? upd / sec * 1e-9 : 0.0;
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, int trial_steps, const char *cache_path,
+                                   awp_tuning *best, double *gcell_updates_per_s)
+{
+    if (!pin || !best) return set_err(AWP_ERR_PARAM, "awp_autotune: null argument");
+    if (trial_steps < 1) return set_err(AWP_ERR_PARAM, "awp_autotune: trial_steps must be >= 1");
+    awp_params p = *pin;
+    const int max_trials = 24;
+    p.nt = max_trials * (trial_steps + p.ntiskp_sgt) + p.ntiskp_sgt + 1;
+    p.nst = 1;
+    p.monitor_every = 0;
+    if (!media) p.mediastart = 0;
+    awp_solver *s = NULL;
+    awp_status st = awp_create(&p, &s);
+    if (st != AWP_OK) return st;
+    const int stepper = s->staged_on ? AWP_KERNEL_STAGED : (fused_of(&s->p) ? AWP_KERNEL_FUSED : AWP_KERNEL_TWO_SWEEP);
+    char key[320];
+    tune_key(&p, stepper, key, sizeof key);
+    double rate = 0.0;
+    awp_tuning t;
+    if (tune_cache_get(cache_path, key, &t, &rate)) {
+        awp_destroy(s);
+        *best = t;
+        if (gcell_updates_per_s) *gcell_updates_per_s = rate;
+        return AWP_OK;
+    }
+    /* without media the trial solve uses the homogeneous medium (inihomo):
+     * the speed of a step does not depend on the values */
+    st = awp_load_media(s, media);
+    awp_tuning cur;
+    if (st == AWP_OK) st = awp_get_tuning(s, &cur);
+    double cur_rate = 0.0;
+    if (st == AWP_OK) st = tune_trial(s, &cur, trial_steps, &cur_rate);
+    /* coordinate descent over the fields the stepper uses */
+    enum { F_KSTAGE, F_RPT, F_UNROLL, F_QSLOW, F_RPTV, F_TY, F_KFUSED, F_KSWEEP };
+    int fields[8], nf = 0;
+    if (stepper == AWP_KERNEL_STAGED) {
+        fields[nf++] = F_KSTAGE, fields[nf++] = F_RPT, fields[nf++] = F_UNROLL, fields[nf++] = F_QSLOW;
+        fields[nf++] = F_RPTV;
+    } else if (stepper == AWP_KERNEL_FUSED) {
+        fields[nf++] = F_TY, fields[nf++] = F_KFUSED;
+    } else {
+        fields[nf++] = F_TY, fields[nf++] = F_UNROLL, fields[nf++] = F_KSWEEP;
+    }
+    int trials = 1;
+    for (int fi = 0; fi < nf && st == AWP_OK; fi++) {
+        int vals[6], nv = 0;
+        switch (fields[fi]) {
+        case F_KSTAGE:
+            for (int target : {24, 32, 40, 48, 64}) {
+                const int nch = (p.nz + target - 1) / target;
+                int kc = (p.nz + nch - 1) / nch;
+                kc = kc < 8 ? 8 : kc;
+                bool dup = kc == cur.kchunk_staged;
+                for (int i = 0; i < nv; i++) dup = dup || vals[i] == kc;
+                if (!dup) vals[nv++] = kc;
+            }
+            break;
+        case F_RPT: vals[nv++] = 3 - cur.staged_rpt; break;
+        case F_RPTV: vals[nv++] = 3 - cur.staged_rpt_vel; break;
+        case F_UNROLL: vals[nv++] = 3 - cur.unroll; break;
+        case F_QSLOW: vals[nv++] = 1 - cur.staged_qslow; break;
+        case F_TY:
+            for (int ty : {4, 8, 16})
+                if (ty != cur.ty && (stepper == AWP_KERNEL_FUSED || ty != 16)) vals[nv++] = ty;
+            break;
+        case F_KFUSED:
+            for (int kc : {16, 32, 64})
+                if (kc != cur.kchunk && kc <= (p.nz > 8 ? p.nz : 8)) vals[nv++] = kc;
+            break;
+        case F_KSWEEP:
+            for (int kc : {16, 32})
+                if (kc != cur.kchunk_sweep && kc <= (p.nz > 8 ? p.nz : 8)) vals[nv++] = kc;
+            break;
+        }
+        for (int vi = 0; vi < nv && st == AWP_OK && trials < max_trials; vi++, trials++) {
+            awp_tuning cand = cur;
+            switch (fields[fi]) {
+            case F_KSTAGE: cand.kchunk_staged = vals[vi]; break;
+            case F_RPT: cand.staged_rpt = vals[vi]; break;
+            case F_RPTV: cand.staged_rpt_vel = vals[vi]; break;
+            case F_UNROLL: cand.unroll = vals[vi]; break;
+            case F_QSLOW: cand.staged_qslow = vals[vi]; break;
+            case F_TY: cand.ty = vals[vi]; break;
+            case F_KFUSED: cand.kchunk = vals[vi]; break;
+            case F_KSWEEP: cand.kchunk_sweep = vals[vi]; break;
+            }
+            double r = 0.0;
+            st = tune_trial(s, &cand, trial_steps, &r);
+            if (st == AWP_OK && r > cur_rate) cur = cand, cur_rate = r;
+        }
+    }
+    awp_destroy(s);
+    if (st != AWP_OK) return st;
+    *best = cur;
+    if (gcell_updates_per_s) *gcell_updates_per_s = cur_rate;
+    tune_cache_put(cache_path, key, &cur, cur_rate);
+    return AWP_OK;
+}

@@ -257,6 +257,36 @@ typedef struct {
 
 awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_times *out);
 
+/* Launch shapes of the steppers (no reference counterpart).  Every shape
+ * gives bit-identical results; they differ only in speed.  awp_create fills
+ * them from measured defaults (and the AWP_TUNE_* environment variables);
+ * awp_set_tuning replaces them at any point of a solve (a captured time-loop
+ * graph is rebuilt on the next step). */
+typedef struct {
+    int kchunk_staged;       /* staged sweeps: z levels per work item (8..nz)          */
+    int staged_qslow;        /* staged sweeps: 1 = one component over all tiles first  */
+    int staged_rpt;          /* staged stress sweep: tile rows per thread (1, 2)       */
+    int staged_rpt_vel;      /* staged velocity sweep: tile rows per thread (1, 2)     */
+    int unroll;              /* z-loop unroll of the sweeps (1, 2)                     */
+    int ty;                  /* two-sweep / fused steppers: block rows (4, 8, 16)      */
+    int kchunk;              /* fused stepper: z levels per work item (8..nz)          */
+    int kchunk_sweep;        /* two-sweep stepper: z levels per work item (8..nz)      */
+} awp_tuning;
+
+awp_status awp_get_tuning(awp_solver *s, awp_tuning *t);
+awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t);
+
+/* Autotuner: times candidate launch shapes on a solver of these parameters
+ * (the caller's media, or a homogeneous medium when media is NULL) for
+ * trial_steps time steps each, by coordinate descent over the fields of
+ * awp_tuning that the chosen stepper uses, and returns the fastest with its
+ * Gcell-updates/s.  With a cache path, a result stored there for the same
+ * grid, components, precision, stepper and GPU model is returned without
+ * timing, and a new result is appended.  Allocates one solver's device
+ * memory for the duration of the call. */
+awp_status awp_autotune(const awp_params *p, const float *media, int trial_steps, const char *cache_path,
+                        awp_tuning *best, double *gcell_updates_per_s);
+
 /* Device memory one solver of these parameters would hold (admission). */
 int64_t awp_footprint_bytes(const awp_params *p, int npts);
 
