@@ -44,7 +44,7 @@ EXPORTED = [
     "awp_server_create", "awp_submit", "awp_poll", "awp_cancel", "awp_wait", "awp_server_time",
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
-    "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune",
+    "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune", "awp_release_cached_memory",
 ]
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
@@ -386,6 +386,7 @@ def load_library(path: str = LIB_PATH):
         "awp_load_media_rwg": (C.c_int, [C.c_void_p, C.c_char_p]),
         "awp_reformat_velocity": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p]),
         "awp_sgt_floats_for": (C.c_int64, [P(Params), C.c_int]),
+        "awp_release_cached_memory": (None, []),
         "awp_get_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
         "awp_set_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
         "awp_autotune": (C.c_int, [P(Params), C.c_void_p, C.c_int, C.c_char_p, P(Tuning), P(C.c_double)]),
@@ -583,6 +584,11 @@ class Solver:
 
     def set_tuning(self, t: Tuning):
         _check(self.lib.awp_set_tuning(self.h, C.byref(t)))
+
+
+def release_cached_memory():
+    """Returns the device blocks kept from destroyed solvers to the driver."""
+    load_library().awp_release_cached_memory()
 
 
 def autotune(params: Params, media: Optional[np.ndarray] = None, trial_steps: int = 20,

@@ -722,6 +722,29 @@ cudaError_t awp_launch_media_ghosts(const AwpGeom &g, const AwpMedia &md, int nv
     return cudaGetLastError();
 }
 
+/* integer hash of the index (murmur3 finaliser), top 24 bits to [-amp, amp) */
+__global__ void k_fill_noise(float *p, int64_t n, unsigned seed, float amp)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 0x9E3779B1u ^ (unsigned)(i >> 32) ^ seed;
+        h ^= h >> 16;
+        h *= 0x85EBCA6Bu;
+        h ^= h >> 13;
+        h *= 0xC2B2AE35u;
+        h ^= h >> 16;
+        p[i] = amp * ((float)(h >> 8) * (1.0f / 8388608.0f) - 1.0f);
+    }
+}
+
+cudaError_t awp_launch_fill_noise(float *p, int64_t n, unsigned seed, float amp, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_fill_noise<<<(int)blocks, 256, 0, st>>>(p, n, seed, amp);
+    return cudaGetLastError();
+}
+
 cudaError_t awp_launch_media_homo(const AwpGeom &g, const AwpMedia &md, float lam, float mu, float d1, cudaStream_t st)
 {
     dim3 b(32, 8);

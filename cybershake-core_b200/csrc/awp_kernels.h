@@ -75,5 +75,7 @@ struct AwpEnergyArgs {
 };
 cudaError_t awp_launch_energy(const AwpEnergyArgs &a, double *partial, int nblocks, double *out, int *flag,
                               cudaStream_t st);
+/* n floats of bounded pseudo-random values in [-amp, amp) (autotuner trials) */
+cudaError_t awp_launch_fill_noise(float *p, int64_t n, unsigned seed, float amp, cudaStream_t st);
 
 #endif

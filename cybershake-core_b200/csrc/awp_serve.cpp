@@ -264,6 +264,7 @@ extern "C" awp_status awp_server_create(int device, int64_t hbm_budget, int max_
     if (max_active < 1 || chunk_steps < 1) return fail(AWP_ERR_PARAM, "max_active and chunk_steps must be >= 1");
     if (cudaSetDevice(device) != cudaSuccess) return fail(AWP_ERR_CUDA, "cannot select the device");
     size_t fr = 0, tot = 0;
+    awp_release_cached_memory();       /* the budget counts idle cached blocks as free */
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return fail(AWP_ERR_CUDA, "cudaMemGetInfo failed");
     awp_server *sv = new awp_server();
     sv->device = device;

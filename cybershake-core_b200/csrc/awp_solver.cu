@@ -18,8 +18,12 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <map>
 #include <mutex>
 #include <new>
+#include <unordered_map>
+#include <utility>
+#include <vector>
 
 #include "awp_internal.h"
 #include "awp_kernels.h"
@@ -258,6 +262,7 @@ static float crj_high(float alpha, int nd, int n, int g)
 }
 
 static void dfree_field(awp_solver *s, void *p);
+static void dfree(awp_solver *s, void *p);
 
 static void free_media32(awp_solver *s)
 {
@@ -280,27 +285,138 @@ static void free_all(awp_solver *s)
             dfree_field(s, s->comp[0][q].f[f]);
             if (f < AF_R1 && s->comp[1][q].f[f] != s->comp[0][q].f[f]) dfree_field(s, s->comp[1][q].f[f]);
         }
-        cudaFree(s->chkj[q]);
-        cudaFree(s->src_ijk[q]);
-        cudaFree(s->src_stf[q]);
-        cudaFree(s->kin[q]);
-        cudaFree(s->sgt_file[q]);
+        dfree(s, s->chkj[q]);
+        dfree(s, s->src_ijk[q]);
+        dfree(s, s->src_stf[q]);
+        dfree(s, s->kin[q]);
+        dfree(s, s->sgt_file[q]);
     }
     free_media32(s);
     awp_staged_destroy(s->staged);
     for (int m = 0; m < AM_N; m++) dfree_field(s, s->mdt.m[m]);
-    cudaFree(s->cx); cudaFree(s->cy); cudaFree(s->cz);
-    cudaFree(s->tau); cudaFree(s->step); cudaFree(s->ext); cudaFree(s->rng);
-    cudaFree(s->pt_idx); cudaFree(s->sg);
-    cudaFree(s->en_partial); cudaFree(s->en_out); cudaFree(s->flag);
+    dfree(s, s->cx); dfree(s, s->cy); dfree(s, s->cz);
+    dfree(s, s->tau); dfree(s, s->step); dfree(s, s->ext); dfree(s, s->rng);
+    dfree(s, s->pt_idx); dfree(s, s->sg);
+    dfree(s, s->en_partial); dfree(s, s->en_out); dfree(s, s->flag);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
 }
 
+/* ------------------------------------------------------------------ */
+/* device block cache                                                  */
+/* ------------------------------------------------------------------ */
+
+/* Blocks a solver frees stay on the device for the next solver of the
+ * process: the next job on the same grid asks for the same sizes, so its
+ * create skips cudaMalloc and its destroy skips cudaFree, whose device-wide
+ * synchronisation would also stall the other solvers of a server.  Only exact
+ * sizes are reused.  A failed cudaMalloc returns the device's idle blocks and
+ * tries again.  AWP_DEVICE_CACHE_MB bounds the idle bytes per device
+ * (default: half the device memory; 0 turns the cache off).  Callers hand a
+ * block back only when no queued work uses it. */
+namespace {
+struct BlkInfo {
+    int dev;
+    size_t bytes;
+};
+std::mutex g_blk_mu;
+std::unordered_map<void *, BlkInfo> g_blk_live;
+std::multimap<std::pair<int, size_t>, void *> g_blk_idle;
+std::map<int, size_t> g_blk_idle_bytes, g_blk_limit;
+}
+
+static size_t blk_limit_locked(int dev)
+{
+    auto it = g_blk_limit.find(dev);
+    if (it != g_blk_limit.end()) return it->second;
+    size_t lim = 0;
+    if (const char *e = getenv("AWP_DEVICE_CACHE_MB")) {
+        lim = (size_t)strtoull(e, NULL, 10) << 20;
+    } else {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) lim = prop.totalGlobalMem / 2;
+    }
+    g_blk_limit[dev] = lim;
+    return lim;
+}
+
+/* frees idle blocks of `dev` (all of them when dev < 0) */
+static void blk_trim(int dev)
+{
+    std::vector<void *> out;
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        for (auto it = g_blk_idle.begin(); it != g_blk_idle.end();) {
+            if (dev < 0 || it->first.first == dev) {
+                g_blk_idle_bytes[it->first.first] -= it->first.second;
+                out.push_back(it->second);
+                it = g_blk_idle.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    for (void *p : out) cudaFree(p);
+}
+
+static cudaError_t blk_alloc(int dev, void **ptr, size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        auto it = g_blk_idle.find(std::make_pair(dev, bytes));
+        if (it != g_blk_idle.end()) {
+            *ptr = it->second;
+            g_blk_idle.erase(it);
+            g_blk_idle_bytes[dev] -= bytes;
+            g_blk_live[*ptr] = BlkInfo{dev, bytes};
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        blk_trim(dev);
+        e = cudaMalloc(ptr, bytes);
+    }
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    g_blk_live[*ptr] = BlkInfo{dev, bytes};
+    return cudaSuccess;
+}
+
+static void blk_free(void *p)
+{
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        auto it = g_blk_live.find(p);
+        if (it != g_blk_live.end()) {
+            const BlkInfo b = it->second;
+            g_blk_live.erase(it);
+            if (g_blk_idle_bytes[b.dev] + b.bytes <= blk_limit_locked(b.dev)) {
+                g_blk_idle.emplace(std::make_pair(b.dev, b.bytes), p);
+                g_blk_idle_bytes[b.dev] += b.bytes;
+                return;
+            }
+        }
+    }
+    cudaFree(p);
+}
+
+/* a solver's block back to the cache, once the solver's queued work is done */
+static void dfree(awp_solver *s, void *p)
+{
+    if (!p) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    blk_free(p);
+}
+
+extern "C" void awp_release_cached_memory(void) { blk_trim(-1); }
+
 static awp_status dalloc(awp_solver *s, void **ptr, size_t bytes)
 {
-    cudaError_t e = cudaMalloc(ptr, bytes);
+    cudaError_t e = blk_alloc(s->p.device, ptr, bytes);
     if (e != cudaSuccess) {
         *ptr = NULL;
         return set_err(AWP_ERR_OOM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
@@ -332,11 +448,11 @@ static void dfree_field(awp_solver *s, void *p)
     if (!p) return;
     for (int n = 0; n < s->nstag && n < 128; n++)
         if (s->stag[n].user == p && s->stag[n].raw) {
-            cudaFree(s->stag[n].raw);
+            dfree(s, s->stag[n].raw);
             s->stag[n].raw = NULL;
             return;
         }
-    cudaFree(p);
+    dfree(s, p);
 }
 
 static awp_status check_params(const awp_params *p)
@@ -606,7 +722,56 @@ typedef int (*slab_reader)(void *ctx, float *dst, int zf0, int nzs, size_t float
 /* rwg_nx > 0: the reader delivers z-slabs of RWG p/s/d volumes ([3][ny][n][nx],
  * rwg_nx x rwg_ny = ny x nx of the AWP grid), turned into AWP media order on
  * the device before the transform */
-static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, int rwg_nx = 0, int rwg_ny = 0)
+/* Two pinned staging slabs kept for the process (the read of slab n+1
+ * overlaps the copy and transform of slab n); a second loader running at the
+ * same time takes slabs of its own. */
+namespace {
+std::mutex g_stage_mu;
+float *g_stage[2] = {NULL, NULL};
+size_t g_stage_bytes = 0;
+}
+
+struct StageLease {
+    float *h[2] = {NULL, NULL};
+    bool shared = false;
+    ~StageLease()
+    {
+        if (shared) {
+            g_stage_mu.unlock();
+        } else {
+            if (h[0]) cudaFreeHost(h[0]);
+            if (h[1]) cudaFreeHost(h[1]);
+        }
+    }
+    cudaError_t take(size_t bytes)
+    {
+        if (g_stage_mu.try_lock()) {
+            shared = true;
+            if (g_stage_bytes < bytes) {
+                for (int b = 0; b < 2; b++) {
+                    if (g_stage[b]) cudaFreeHost(g_stage[b]);
+                    g_stage[b] = NULL;
+                }
+                g_stage_bytes = 0;
+                for (int b = 0; b < 2; b++) {
+                    const cudaError_t e = cudaMallocHost((void **)&g_stage[b], bytes);
+                    if (e != cudaSuccess) return e;
+                }
+                g_stage_bytes = bytes;
+            }
+            h[0] = g_stage[0], h[1] = g_stage[1];
+            return cudaSuccess;
+        }
+        cudaError_t e = cudaMallocHost((void **)&h[0], bytes);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&h[1], bytes);
+        return e;
+    }
+};
+
+/* direct != NULL: the media are already in page-locked host memory and are
+ * copied from there slab by slab, without staging */
+static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, int rwg_nx = 0, int rwg_ny = 0,
+                                    const float *direct = NULL)
 {
     const awp_params *p = &s->p;
     CU(cudaSetDevice(p->device));
@@ -653,11 +818,14 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, in
      * transform of slab n */
     float *hbuf[2] = {NULL, NULL}, *dbuf = NULL;
     cudaEvent_t done[2];
-    CU(cudaMallocHost((void **)&hbuf[0], per_level * nzs * sizeof(float)));
-    CU(cudaMallocHost((void **)&hbuf[1], per_level * nzs * sizeof(float)));
+    StageLease lease;
+    if (!direct) {
+        CU(lease.take(per_level * nzs * sizeof(float)));
+        hbuf[0] = lease.h[0], hbuf[1] = lease.h[1];
+    }
     CU(cudaEventCreate(&done[0]));
     CU(cudaEventCreate(&done[1]));
-    cudaError_t e = cudaMalloc((void **)&dbuf, per_level * nzs * sizeof(float) * (rwg_nx > 0 ? 3 : 2));
+    cudaError_t e = blk_alloc(p->device, (void **)&dbuf, per_level * nzs * sizeof(float) * (rwg_nx > 0 ? 3 : 2));
     awp_status st = AWP_OK;
     if (e != cudaSuccess) st = set_err(AWP_ERR_OOM, "media staging: %s", cudaGetErrorString(e));
     float *draw = rwg_nx > 0 && dbuf ? dbuf + 2 * per_level * nzs : NULL;
@@ -665,13 +833,14 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, in
     for (int z0 = 0; z0 < p->nz && st == AWP_OK; z0 += nzs, slab ^= 1) {
         const int n = (z0 + nzs <= p->nz) ? nzs : p->nz - z0;
         if (z0 >= 2 * nzs && cudaEventSynchronize(done[slab]) != cudaSuccess) { st = set_err(AWP_ERR_CUDA, "media stream"); break; }
-        if (rd(ctx, hbuf[slab], z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "media: short read at level %d", z0); break; }
+        const float *src = direct ? direct + per_level * (size_t)z0 : hbuf[slab];
+        if (!direct && rd(ctx, hbuf[slab], z0, n, per_level) != 0) { st = set_err(AWP_ERR_IO, "media: short read at level %d", z0); break; }
         float *d = dbuf + (size_t)slab * per_level * nzs;
         if (draw) {
-            e = cudaMemcpyAsync(draw, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+            e = cudaMemcpyAsync(draw, src, per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
             if (e == cudaSuccess) e = awp_launch_rwg_slab(draw, d, rwg_nx, rwg_ny, n, s->stream);
         } else {
-            e = cudaMemcpyAsync(d, hbuf[slab], per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+            e = cudaMemcpyAsync(d, src, per_level * n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
         }
         if (e == cudaSuccess)
             e = awp_launch_media_interior(s->g, s->md, d, z0, n, p->nvar, var_offset, p->socalq, p->nve,
@@ -684,9 +853,7 @@ static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, in
         if (e != cudaSuccess) st = set_err(AWP_ERR_CUDA, "media ghosts: %s", cudaGetErrorString(e));
     }
     cudaStreamSynchronize(s->stream);
-    cudaFree(dbuf);
-    cudaFreeHost(hbuf[0]);
-    cudaFreeHost(hbuf[1]);
+    blk_free(dbuf);
     cudaEventDestroy(done[0]);
     cudaEventDestroy(done[1]);
     if (st != AWP_OK) return st;
@@ -718,7 +885,10 @@ extern "C" awp_status awp_load_media(awp_solver *s, const float *media)
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
     if (s->p.mediastart != 0 && !media) return set_err(AWP_ERR_PARAM, "media array required when MEDIARESTART != 0");
     mem_ctx m = {media};
-    return load_media_common(s, mem_reader, &m);
+    cudaPointerAttributes attr;
+    const bool pinned = media && cudaPointerGetAttributes(&attr, media) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    if (media && !pinned) cudaGetLastError();
+    return load_media_common(s, mem_reader, &m, 0, 0, pinned ? media : NULL);
 }
 
 extern "C" awp_status awp_load_media_file(awp_solver *s, const char *path)
@@ -843,9 +1013,9 @@ extern "C" awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const in
     CU(cudaSetDevice(p->device));
     for (int b = 0; b < 2; b++)
         if (s->graph[b]) { cudaGraphExecDestroy(s->graph[b]); s->graph[b] = NULL; }
-    cudaFree(s->src_ijk[comp]); s->src_ijk[comp] = NULL;
-    cudaFree(s->src_stf[comp]); s->src_stf[comp] = NULL;
-    cudaFree(s->kin[comp]); s->kin[comp] = NULL;
+    dfree(s, s->src_ijk[comp]); s->src_ijk[comp] = NULL;
+    dfree(s, s->src_stf[comp]); s->src_stf[comp] = NULL;
+    dfree(s, s->kin[comp]); s->kin[comp] = NULL;
     s->nsrc[comp] = nsrc;
     if (nsrc == 0) return AWP_OK;
     int *ijk = (int *)malloc(sizeof(int) * 3 * (size_t)nsrc);
@@ -881,9 +1051,9 @@ extern "C" awp_status awp_set_points(awp_solver *s, int npts, const int *xyz)
     CU(cudaSetDevice(p->device));
     for (int b = 0; b < 2; b++)
         if (s->graph[b]) { cudaGraphExecDestroy(s->graph[b]); s->graph[b] = NULL; }
-    cudaFree(s->pt_idx); s->pt_idx = NULL;
-    cudaFree(s->sg); s->sg = NULL;
-    for (int q = 0; q < AWP_MAX_COMP; q++) { cudaFree(s->sgt_file[q]); s->sgt_file[q] = NULL; }
+    dfree(s, s->pt_idx); s->pt_idx = NULL;
+    dfree(s, s->sg); s->sg = NULL;
+    for (int q = 0; q < AWP_MAX_COMP; q++) { dfree(s, s->sgt_file[q]); s->sgt_file[q] = NULL; }
     s->npts = npts;
     s->sgt_file_floats = file_floats_of(p, npts);
     if (npts == 0) return AWP_OK;
@@ -1628,6 +1798,17 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
     /* without media the trial solve uses the homogeneous medium (inihomo):
      * the speed of a step does not depend on the values */
     st = awp_load_media(s, media);
+    /* a developed wavefield: under the power cap a zero wavefield runs at
+     * higher clocks than a real solve, so the trials start from bounded noise
+     * in u v w and the stresses (the memory variables follow within a step) */
+    for (int q = 0; q < p.ncomp && st == AWP_OK; q++)
+        for (int b = 0; b < 2 && st == AWP_OK; b++)
+            for (int f = 0; f < 9 && st == AWP_OK; f++) {
+                if (b == 1 && s->comp[1][q].f[f] == s->comp[0][q].f[f]) continue;
+                const cudaError_t e = awp_launch_fill_noise(s->comp[b][q].f[f], s->g.vol,
+                                                            0x5EED0000u + 64u * q + 16u * b + f, 1e-3f, s->stream);
+                if (e != cudaSuccess) st = set_err(AWP_ERR_CUDA, "awp_autotune: %s", cudaGetErrorString(e));
+            }
     awp_tuning cur;
     if (st == AWP_OK) st = awp_get_tuning(s, &cur);
     double cur_rate = 0.0;

@@ -410,6 +410,15 @@ typedef struct {
     int64_t footprint;         /* device bytes reserved for the request      */
 } awp_request_info;
 
+/* Device blocks freed by awp_destroy stay on the device for the next solver of
+ * the process (exact sizes are reused; a failed allocation returns them first;
+ * AWP_DEVICE_CACHE_MB bounds the idle bytes per device, default half the device
+ * memory, 0 = off).  This returns every idle block to the driver.  Work that
+ * uses a solver's device pointers (awp_device_field) must be complete before
+ * awp_destroy.  No reference counterpart (the reference runs one solve per
+ * process). */
+void awp_release_cached_memory(void);
+
 /* hbm_budget <= 0: 90 % of the device's free memory at creation.
  * chunk_steps: fewest steps a resident solve advances per chunk. */
 awp_status awp_server_create(int device, int64_t hbm_budget, int max_active, int chunk_steps, awp_server **out);
