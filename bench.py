@@ -113,6 +113,16 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
+    def power_w(self):
+        w = []
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                w.append(float(f[3]))
+            except (IndexError, ValueError):
+                pass
+        return statistics.median(w) if w else None
+
 
 def dist_setup(n_gpus):
     if n_gpus <= 1 or "RANK" not in os.environ:
@@ -222,6 +232,37 @@ def cpu_oracle_rate(w, media, stf, nsteps, warm=1):
     threads = oracle.threads()
     o.close()
     return cells / statistics.median(times), threads, times
+
+
+def run_job_profile(args):
+    """Step time, median SM clock and board power over one complete job, chunk by
+    chunk; then the same solver with its wavefield zeroed, for comparison."""
+    w = workload(args)
+    media, pts = w.media(), w.points()
+    stfs = [w.stf(q) for q in range(len(w.igreen))]
+    s = make_solver(w, media, pts, stfs, 0, args.precision, args.kernel)
+
+    def chunk(n, tag):
+        with ClockSampler(0) as clk:
+            a = s.stats()
+            s.run(n)
+            b = s.stats()
+        c = clk.summary()
+        line = {"workload": w.name, "chunk": tag, "steps": [int(a.steps_done), int(b.steps_done)],
+                "ms_per_step": (b.seconds_loop - a.seconds_loop) / n * 1e3, "sm_mhz": c["sm_mhz"],
+                "power_w": clk.power_w(), "reasons": c["reasons"]}
+        print(json.dumps(line), flush=True)
+
+    n = args.job_profile
+    done = 0
+    while done < w.nt:
+        k = min(n, w.nt - done)
+        chunk(k, "job")
+        done += k
+    s.reset()
+    chunk(n, "zeroed wavefield")
+    s.close()
+    return 0
 
 
 def run_reference(args):
@@ -512,6 +553,8 @@ def main():
     ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
     ap.add_argument("--synth", action="store_true", help="reciprocity synthesis: rupture variations per second")
     ap.add_argument("--autotune", action="store_true", help="time launch shapes on this grid first (untimed)")
+    ap.add_argument("--job-profile", type=int, default=0, metavar="STEPS",
+                    help="one complete job in chunks of STEPS time steps: step time, SM clock and power per chunk")
     ap.add_argument("--tune-cache", default="", help="autotuner cache file")
     ap.add_argument("--tune-steps", type=int, default=20, help="time steps per autotuner trial")
     args = ap.parse_args()
@@ -521,6 +564,8 @@ def main():
         return run_synth(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.job_profile:
+        return run_job_profile(args)
 
     dist, rank, world, local = dist_setup(args.gpus)
     import awpsgt
