@@ -553,6 +553,8 @@ def main():
     ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
     ap.add_argument("--synth", action="store_true", help="reciprocity synthesis: rupture variations per second")
     ap.add_argument("--autotune", action="store_true", help="time launch shapes on this grid first (untimed)")
+    ap.add_argument("--prefill", type=int, default=-1, metavar="STEPS",
+                    help="untimed time steps before the warm-up (default: half the job; 0 for short profiling runs)")
     ap.add_argument("--job-profile", type=int, default=0, metavar="STEPS",
                     help="one complete job in chunks of STEPS time steps: step time, SM clock and power per chunk")
     ap.add_argument("--tune-cache", default="", help="autotuner cache file")
@@ -583,6 +585,8 @@ def main():
     # under the 1 kW cap its clocks (and step rate) run about 13 % above the
     # rest of the job.
     prefill = min(w.nt // 2, w.nt - steps_needed) // per_step_ts * per_step_ts
+    if args.prefill >= 0:
+        prefill = min(args.prefill, w.nt - steps_needed) // per_step_ts * per_step_ts
 
     # ---------------- launch shapes (untimed) ----------------
     tuning, tune_info = None, None
