@@ -32,6 +32,7 @@ struct AwpStepArgs {
     int staged_qslow;            /* staged items: one component at a time   */
     int staged_rpt;              /* staged stress sweep: tile rows per thread */
     int staged_rpt_vel;          /* staged velocity sweep: tile rows per thread */
+    int staged_batch;            /* staged stress sweep: components side by side in one item */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

@@ -88,6 +88,7 @@ struct awp_solver {
     int staged_qslow;                /* staged items: component slowest     */
     int staged_rpt;                  /* staged stress sweep rows per thread */
     int staged_rpt_vel;              /* staged velocity sweep rows per thread */
+    int staged_batch;                /* staged stress: components in one item */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -616,6 +617,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         const int rpt = env_int("AWP_TUNE_RPT", 0);
         s->staged_rpt = rpt == 1 || rpt == 2 ? rpt : (p->ncomp == 3 && s->rstore == AWP_STORE_F32 ? 2 : 1);
         s->staged_rpt_vel = env_int("AWP_TUNE_RPTV", 1) == 2 ? 2 : 1;
+        /* two or three components share one stress work item (media tiles
+         * and cell coefficients once per level): 14 % faster for fx+fy on
+         * 640 x 640 x 256, 3-4 % for fx+fy+fz on 400 x 400 x 200 */
+        s->staged_batch = env_int("AWP_TUNE_BATCH", 1) != 0;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -1109,6 +1114,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_qslow = s->staged_qslow;
     a.staged_rpt = s->staged_rpt;
     a.staged_rpt_vel = s->staged_rpt_vel;
+    a.staged_batch = s->staged_batch;
     a.kerr = s->flag + 1;
 
     memset(&pa, 0, sizeof pa);
@@ -1343,7 +1349,8 @@ extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_ti
     const int nk = np + 2;
     o->nkernels = nk;
     for (int k = 0; k < np; k++) {
-        snprintf(o->name[k], sizeof o->name[k], "%s", (s->staged_on ? pname_staged : pname)[parts[k]]);
+        const bool batched = s->staged_on && parts[k] == AWP_PART_STR && s->staged_batch && p->ncomp >= 2;
+        snprintf(o->name[k], sizeof o->name[k], "%s", batched ? "k_str_tmab" : (s->staged_on ? pname_staged : pname)[parts[k]]);
         o->bytes_per_launch[k] = part_bytes(s, parts[k]);
     }
     snprintf(o->name[np], sizeof o->name[np], "k_post");
@@ -1680,6 +1687,7 @@ extern "C" awp_status awp_get_tuning(awp_solver *s, awp_tuning *t)
     t->ty = s->ty;
     t->kchunk = s->kchunk;
     t->kchunk_sweep = s->kchunk_sweep;
+    t->staged_batch = s->staged_batch;
     return AWP_OK;
 }
 
@@ -1692,8 +1700,8 @@ extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
         return set_err(AWP_ERR_PARAM, "awp_set_tuning: z levels per work item must be 8..%d", kmax);
     if ((t->staged_qslow != 0 && t->staged_qslow != 1) || (t->staged_rpt != 1 && t->staged_rpt != 2) ||
         (t->staged_rpt_vel != 1 && t->staged_rpt_vel != 2) || (t->unroll != 1 && t->unroll != 2) ||
-        (t->ty != 4 && t->ty != 8 && t->ty != 16))
-        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16");
+        (t->ty != 4 && t->ty != 8 && t->ty != 16) || (t->staged_batch != 0 && t->staged_batch != 1))
+        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16, batch 0/1");
     CU(cudaSetDevice(s->p.device));
     CU(cudaStreamSynchronize(s->stream));   /* no captured step in flight when its graph goes */
     s->kchunk_staged = t->kchunk_staged;
@@ -1704,6 +1712,7 @@ extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
     s->ty = t->ty;
     s->kchunk = t->kchunk;
     s->kchunk_sweep = t->kchunk_sweep;
+    s->staged_batch = t->staged_batch;
     drop_graphs(s);
     return AWP_OK;
 }
@@ -1733,8 +1742,8 @@ static int tune_cache_get(const char *path, const char *key, awp_tuning *t, doub
         if (strncmp(line, key, kl) != 0 || line[kl] != ' ') continue;
         awp_tuning u;
         double r = 0.0;
-        if (sscanf(line + kl, "%d %d %d %d %d %d %d %d %lf", &u.kchunk_staged, &u.staged_qslow, &u.staged_rpt,
-                   &u.staged_rpt_vel, &u.unroll, &u.ty, &u.kchunk, &u.kchunk_sweep, &r) == 9) {
+        if (sscanf(line + kl, "%d %d %d %d %d %d %d %d %d %lf", &u.kchunk_staged, &u.staged_qslow, &u.staged_rpt,
+                   &u.staged_rpt_vel, &u.unroll, &u.ty, &u.kchunk, &u.kchunk_sweep, &u.staged_batch, &r) == 10) {
             *t = u;
             *rate = r;
             found = 1;                        /* the last entry for a key wins */
@@ -1748,8 +1757,8 @@ static void tune_cache_put(const char *path, const char *key, const awp_tuning *
 {
     FILE *f = path ? fopen(path, "a") : NULL;
     if (!f) return;
-    fprintf(f, "%s %d %d %d %d %d %d %d %d %.6g\n", key, t->kchunk_staged, t->staged_qslow, t->staged_rpt,
-            t->staged_rpt_vel, t->unroll, t->ty, t->kchunk, t->kchunk_sweep, rate);
+    fprintf(f, "%s %d %d %d %d %d %d %d %d %d %.6g\n", key, t->kchunk_staged, t->staged_qslow, t->staged_rpt,
+            t->staged_rpt_vel, t->unroll, t->ty, t->kchunk, t->kchunk_sweep, t->staged_batch, rate);
     fclose(f);
 }
 
@@ -1814,9 +1823,10 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
     double cur_rate = 0.0;
     if (st == AWP_OK) st = tune_trial(s, &cur, trial_steps, &cur_rate);
     /* coordinate descent over the fields the stepper uses */
-    enum { F_KSTAGE, F_RPT, F_UNROLL, F_QSLOW, F_RPTV, F_TY, F_KFUSED, F_KSWEEP };
-    int fields[8], nf = 0;
+    enum { F_KSTAGE, F_RPT, F_UNROLL, F_QSLOW, F_RPTV, F_TY, F_KFUSED, F_KSWEEP, F_BATCH };
+    int fields[9], nf = 0;
     if (stepper == AWP_KERNEL_STAGED) {
+        if (p.ncomp >= 2) fields[nf++] = F_BATCH;
         fields[nf++] = F_KSTAGE, fields[nf++] = F_RPT, fields[nf++] = F_UNROLL, fields[nf++] = F_QSLOW;
         fields[nf++] = F_RPTV;
     } else if (stepper == AWP_KERNEL_FUSED) {
@@ -1842,6 +1852,7 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
         case F_RPTV: vals[nv++] = 3 - cur.staged_rpt_vel; break;
         case F_UNROLL: vals[nv++] = 3 - cur.unroll; break;
         case F_QSLOW: vals[nv++] = 1 - cur.staged_qslow; break;
+        case F_BATCH: vals[nv++] = 1 - cur.staged_batch; break;
         case F_TY:
             for (int ty : {4, 8, 16})
                 if (ty != cur.ty && (stepper == AWP_KERNEL_FUSED || ty != 16)) vals[nv++] = ty;
@@ -1863,6 +1874,7 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
             case F_RPTV: cand.staged_rpt_vel = vals[vi]; break;
             case F_UNROLL: cand.unroll = vals[vi]; break;
             case F_QSLOW: cand.staged_qslow = vals[vi]; break;
+            case F_BATCH: cand.staged_batch = vals[vi]; break;
             case F_TY: cand.ty = vals[vi]; break;
             case F_KFUSED: cand.kchunk = vals[vi]; break;
             case F_KSWEEP: cand.kchunk_sweep = vals[vi]; break;

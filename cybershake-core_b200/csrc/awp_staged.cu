@@ -599,6 +599,221 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     }
 }
 
+/* ---- components side by side in one work item -------------------------- */
+
+/* A work item is (x tile, y tile, z chunk) with every component.  The media
+ * tiles of a level, and the cell coefficients computed from them (the 8-cell
+ * sums and the five divisions), serve all components: the media ring (levels
+ * k-1 and k in use, k+1 in flight) is filled once per level.  The components'
+ * tiles follow in a ring of their own, one sub-slot per (level, component);
+ * a component's plane k-1 values at the cell (u, v, w) travel in registers,
+ * so a sub-slot is released as soon as its level is done. */
+#define STB_MS 3                                  /* media slots              */
+#define STB_MSLOT (4 * ST_MP)
+#define STB_CST (3 * ST_VT)                       /* first stress tile        */
+#define STB_CSLOT (STB_CST + 12 * ST_PT)          /* r tiles fit in 6 x 256   */
+
+__host__ __device__ __forceinline__ uint32_t strb_med_txb(int nve) { return (uint32_t)((nve == 1 ? 4 : 2) * ST_MT * 4); }
+__host__ __device__ __forceinline__ uint32_t strb_comp_txb(int nve, int rsize)
+{
+    return (uint32_t)((3 * ST_VT + 6 * ST_PT) * 4 + (nve == 1 ? 6 * ST_PT * rsize : 0));
+}
+
+template <class TR, int NCB, int STB_CS>
+__global__ void __launch_bounds__(ST_THREADS, 2)
+k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
+           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
+           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
+{
+    constexpr int RSIZE = (int)sizeof(TR);
+    extern __shared__ unsigned char st_smem[];
+    float *mring = ring_base(st_smem);
+    float *cring = mring + STB_MS * STB_MSLOT;
+    uint64_t *mfull = (uint64_t *)(cring + STB_CS * STB_CSLOT), *mempty = mfull + STB_MS;
+    uint64_t *cfull = mempty + STB_MS, *cempty = cfull + STB_CS;
+    __shared__ volatile int abort_s;
+    __shared__ AwpComp tab[AWP_MAX_COMP];
+    if (threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
+#pragma unroll
+        for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
+    }
+    ring_init<STB_MS>(mfull, mempty, &abort_s, ST_CW);
+    ring_init<STB_CS>(cfull, cempty, &abort_s, ST_CW);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+
+    if (ty == ST_CW) {                /* producer warp */
+        if (tx != 0) return;
+        uint32_t um = 0, uc = 0;
+        bool ok = true;
+        const int nmed = nve == 1 ? 4 : 2;
+        for (int item = blockIdx.x; ok && item < w.nitems; item += gridDim.x) {
+            int bx, by, k0, k1;
+            work_item(g, w, item, bx, by, k0, k1);
+            const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1;
+            const int x = tile_x(i0), xp = i0 + AWP_XO - 1;
+            for (int k = k0 - 1; ok && k <= k1; ++k) {
+                ok = ring_acquire<STB_MS>(mempty, um, &abort_s);
+                if (!ok) break;
+                {
+                    float *sl = mring + (um % STB_MS) * STB_MSLOT;
+                    uint64_t *b = &mfull[um % STB_MS];
+                    fence_async_smem();
+                    mb_expect(b, strb_med_txb(nve));
+                    for (int a = 0; a < nmed; ++a) tma_3d(sl + a * ST_MP, &maps.med[a], b, x, j0, k + 1);
+                }
+                ++um;
+                if (k < k0) continue;
+#pragma unroll
+                for (int q = 0; q < NCB; ++q) {
+                    ok = ring_acquire<STB_CS>(cempty, uc, &abort_s);
+                    if (!ok) break;
+                    float *sl = cring + (uc % STB_CS) * STB_CSLOT;
+                    uint64_t *b = &cfull[uc % STB_CS];
+                    fence_async_smem();
+                    mb_expect(b, strb_comp_txb(nve, RSIZE));
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) tma_3d(sl + STB_CST + a * ST_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
+                    if (nve == 1) {
+                        unsigned char *rb = (unsigned char *)(sl + STB_CST + 6 * ST_PT);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a)
+                            tma_3d(rb + a * ST_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
+                    }
+                    ++uc;
+                }
+            }
+        }
+        if (!ok) {
+            abort_s = 1;
+            atomicOr(err, AWP_KERR_TMA_WAIT);
+        }
+        ring_drain<STB_MS>(mfull, um);
+        ring_drain<STB_CS>(cfull, uc);
+        return;
+    }
+
+    const int sz = g.plane;
+    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
+    uint32_t um0 = 0, uc = 0;         /* media use of the item's level k0 - 1; next component use */
+    for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
+        int bx, by, k0, k1;
+        work_item(g, w, item, bx, by, k0, k1);
+        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
+        const bool live = i <= g.nx && j <= g.ny;
+        const int itxy = ((j & 1) << 1) | (i & 1);
+        const int c0 = g.idx(i, j, k0);
+        /* per component: column queues u, v at k+1, k+2 and w at k+1, fed by
+         * loads one level ahead (pu, pv, pw) that rotate in when the component
+         * comes up at the next level, a full level after their issue; w at
+         * k-2, k-1 and u, v at k-1 come from the tiles of earlier levels */
+        float up1[NCB], up2[NCB], pu[NCB], vp1[NCB], vp2[NCB], pv[NCB], wp1[NCB], pw[NCB];
+        float wm2[NCB], wm1[NCB], um1[NCB], vm1[NCB];
+#pragma unroll
+        for (int q = 0; q < NCB; ++q) {
+            up1[q] = up2[q] = pu[q] = vp1[q] = vp2[q] = pv[q] = wp1[q] = pw[q] = 0.f;
+            wm2[q] = wm1[q] = um1[q] = vm1[q] = 0.f;
+            if (live) {
+                const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
+                up2[q] = U[c0 + sz]; pu[q] = U[c0 + 2 * sz];
+                vp2[q] = V[c0 + sz]; pv[q] = V[c0 + 2 * sz];
+                pw[q] = W[c0 + sz];
+                wm2[q] = W[c0 - 2 * sz]; wm1[q] = W[c0 - sz];
+                um1[q] = U[c0 - sz]; vm1[q] = V[c0 - sz];
+            }
+        }
+        const float cxy = live ? cx[i] * cy[j] : 0.f;
+        int cc = c0;
+#pragma unroll 1
+        for (int k = k0; k <= k1; ++k, cc += sz) {
+            const uint32_t mk = um0 + (uint32_t)(k - k0 + 1), mm = mk - 1;
+            const float czk = cz[k];
+            bool ok = true;
+            if (k == k0) ok = mb_wait_or_abort(&mfull[mm % STB_MS], (mm / STB_MS) & 1, &abort_s);
+            if (ok) ok = mb_wait_or_abort(&mfull[mk % STB_MS], (mk / STB_MS) & 1, &abort_s);
+            if (!__all_sync(0xffffffffu, ok)) {   /* warp-uniform outcome */
+                abort_s = 1;
+                atomicOr(err, AWP_KERR_TMA_WAIT);
+                return;
+            }
+            const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;                 /* viscoop.f:93-101 */
+            StrCoef kc;
+            {
+                const TMed M{mring + (mk % STB_MS) * STB_MSLOT + cm, mring + (mm % STB_MS) * STB_MSLOT + cm};
+                kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
+            }
+            __syncwarp();
+            if (tx == 0) mb_arrive(&mempty[mm % STB_MS]);
+#pragma unroll
+            for (int q = 0; q < NCB; ++q, ++uc) {
+                ok = mb_wait_or_abort(&cfull[uc % STB_CS], (uc / STB_CS) & 1, &abort_s);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    abort_s = 1;
+                    atomicOr(err, AWP_KERR_TMA_WAIT);
+                    return;
+                }
+                /* rotate this component's queues, then load one level ahead */
+                up1[q] = up2[q]; up2[q] = pu[q];
+                vp1[q] = vp2[q]; vp2[q] = pv[q];
+                wp1[q] = pw[q];
+                pu[q] = pv[q] = pw[q] = 0.f;
+                if (live && k < k1) {
+                    pu[q] = tab[q].f[AF_U][cc + 3 * sz];
+                    pv[q] = tab[q].f[AF_V][cc + 3 * sz];
+                    pw[q] = tab[q].f[AF_W][cc + 2 * sz];
+                }
+                const float *sk = cring + (uc % STB_CS) * STB_CSLOT;
+                const float nu = sk[cv], nv = sk[ST_VT + cv], nw = sk[2 * ST_VT + cv];
+                if (live) {
+                    const float *ps = sk + STB_CST + cp;
+                    const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
+                    const TVel Vq{sk + cv, um1[q], vm1[q], wm1[q], up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
+                    Stress6 o;
+                    if (nve == 1) {
+                        const TR *pr = (const TR *)(sk + STB_CST + 6 * ST_PT) + cp;
+                        float rr[6];
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
+                        const VelDiff dd = vel_diff(Vq);
+                        o = str_visco(kc, dd, s0, rr, dth, dt, dh1);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], cc, rr[a], 1.0f);
+                    } else {
+                        o = str_elastic(kc, Vq, s0, dth);
+                    }
+                    const float crj = cxy * czk;
+                    tab[q].f[AF_XX][cc] = o.xx * crj; tab[q].f[AF_YY][cc] = o.yy * crj; tab[q].f[AF_ZZ][cc] = o.zz * crj;
+                    tab[q].f[AF_XY][cc] = o.xy * crj; tab[q].f[AF_XZ][cc] = o.xz * crj; tab[q].f[AF_YZ][cc] = o.yz * crj;
+                }
+                __syncwarp();
+                if (tx == 0) mb_arrive(&cempty[uc % STB_CS]);
+                wm2[q] = wm1[q];
+                um1[q] = nu; vm1[q] = nv; wm1[q] = nw;
+            }
+        }
+        __syncwarp();
+        if (tx == 0) mb_arrive(&mempty[(um0 + (uint32_t)(k1 - k0 + 1)) % STB_MS]);
+        um0 += (uint32_t)(k1 - k0 + 2);
+        if (k1 == g.nz && live) {
+#pragma unroll
+            for (int q = 0; q < NCB; ++q) {
+                /* fstr (operator.f:594-606) on this thread's own column */
+                const int ct = g.idx(i, j, g.nz);
+                float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
+                ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+                ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+                XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+                XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+                YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+                YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+                XZ[ct] = 0.0f;
+                YZ[ct] = 0.0f;
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* host side                                                           */
 /* ------------------------------------------------------------------ */
@@ -735,11 +950,35 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
     return cudaGetLastError();
 }
 
+/* CS component sub-slots: CS - 1 (level, component) tiles in flight */
+template <class TR, int NCB, int CS>
+static cudaError_t launch_str_bc(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    const size_t smem = 128 + (size_t)(STB_MS * STB_MSLOT + CS * STB_CSLOT) * 4 + 2 * 8 * (STB_MS + CS);
+    const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
+    int grid = 0;
+    cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS>, smem, w.nitems, &grid);
+    if (e != cudaSuccess) return e;
+    k_str_tmab<TR, NCB, CS><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
+        st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+    return cudaGetLastError();
+}
+
+/* five sub-slots (109 KB with the media ring, two blocks per SM) measured
+ * slightly ahead of four on the 400 x 400 x 200 three-component grid */
+template <class TR, int NCB>
+static cudaError_t launch_str_b(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+{
+    return launch_str_bc<TR, NCB, 5>(st, s, stream);
+}
+
 /* two rows per thread carry twice the live state already: that variant keeps
  * its level loop rolled (unrolled twice it needs 128 registers and runs slower) */
 template <class TR>
 static cudaError_t launch_str_tr(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
+    if (s.staged_batch && s.ncomp == 3) return launch_str_b<TR, 3>(st, s, stream);
+    if (s.staged_batch && s.ncomp == 2) return launch_str_b<TR, 2>(st, s, stream);
     if (s.staged_rpt == 2) return launch_str_rpt<TR, 1, 2>(st, s, stream);
     return s.unroll == 1 ? launch_str_rpt<TR, 1, 1>(st, s, stream) : launch_str_rpt<TR, 2, 1>(st, s, stream);
 }

@@ -161,11 +161,12 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, rpt, monkeypatch):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-@pytest.mark.parametrize("qslow", ["0", "1"])
-def test_staged_batched_components_many_items(qslow, monkeypatch):
+@pytest.mark.parametrize("qslow,batch", [("0", "0"), ("1", "0"), ("1", "1")])
+def test_staged_batched_components_many_items(qslow, batch, monkeypatch):
     """Three components as neighbouring work items (or one component over
-    all tiles at a time), 8-level chunks, two tile rows per thread in both
-    sweeps."""
+    all tiles at a time, or side by side in one item of the stress sweep),
+    8-level chunks, two tile rows per thread in both sweeps."""
+    monkeypatch.setenv("AWP_TUNE_BATCH", batch)
     monkeypatch.setenv("AWP_TUNE_KSTAGE", "8")
     monkeypatch.setenv("AWP_TUNE_RPT", "2")
     monkeypatch.setenv("AWP_TUNE_RPTV", "2")

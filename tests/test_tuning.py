@@ -38,7 +38,7 @@ def variant(t, **kw):
 # shape 2 is one work item over the whole depth (nz = 30)
 SHAPES = {
     "staged": [dict(kchunk_staged=9, staged_rpt=2, staged_rpt_vel=2, unroll=1, staged_qslow=0),
-               dict(kchunk_staged=16, staged_rpt=1, staged_rpt_vel=1, unroll=2, staged_qslow=1),
+               dict(kchunk_staged=16, staged_rpt=1, staged_rpt_vel=1, unroll=2, staged_qslow=1, staged_batch=1),
                dict(kchunk_staged=30)],
     "fused": [dict(ty=4, kchunk=16), dict(ty=16, kchunk=8), dict(ty=8, kchunk=30)],
     "two_sweep": [dict(ty=4, kchunk_sweep=8, unroll=2), dict(ty=16, kchunk_sweep=12, unroll=1),
@@ -119,3 +119,38 @@ def test_autotune_rejects_bad_arguments():
     p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, **c.kw())
     with pytest.raises(awpsgt.AwpError):
         awpsgt.autotune(p, c.media, trial_steps=0)
+
+
+STATE = awpsgt.FIELDS[:15]
+
+
+@pytest.mark.parametrize("igreen", [(1, 2), (1, 2, 3), (-2, 4, 6)])
+@pytest.mark.parametrize("precision", ["f32", "mixed"])
+@pytest.mark.parametrize("nve", [1, 0])
+def test_batched_stress_sweep_matches_per_component(igreen, precision, nve):
+    """Components side by side in one work item (shared media tiles and cell
+    coefficients) against one component per work item: every state field, the
+    CHKJ series and the SGTs bit for bit; FP32 also against the oracle."""
+    n = len(igreen)
+    c = Case(nx=45, ny=37, nz=29, nt=30, igreen=igreen, srcs=[[(20, 18, 6)]] * n, nve=nve)
+    runs = []
+    for batch in (0, 1):
+        p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, igreen=c.igreen, kernel="staged",
+                               precision=precision, **c.kw())
+        s = awpsgt.Solver(p)
+        s.set_tuning(variant(s.tuning(), staged_batch=batch, kchunk_staged=11))
+        s.load_media(c.media)
+        for q in range(n):
+            s.set_source(q, c.srcs[q], c.stfs[q])
+        s.set_points(c.pts)
+        s.run(c.nt)
+        assert s.tuning().staged_batch == batch
+        runs.append(s)
+    a, b = runs
+    for q in range(n):
+        for f in STATE[:9] + (STATE[9:] if nve == 1 else []):
+            assert bits_equal(a.field(f, q), b.field(f, q)), (q, f)
+        assert bits_equal(a.chkj(q), b.chkj(q))
+        assert bits_equal(a.sgt(q), b.sgt(q))
+    if precision == "f32" and igreen[0] > 0:
+        assert_same_state(b, c.oracle(0), 0, fields=STATE if nve == 1 else STATE[:9])
