@@ -32,7 +32,8 @@ struct AwpStepArgs {
     int staged_qslow;            /* staged items: one component at a time   */
     int staged_rpt;              /* staged stress sweep: tile rows per thread */
     int staged_rpt_vel;          /* staged velocity sweep: tile rows per thread */
-    int staged_batch;            /* staged stress sweep: components side by side in one item */
+    int staged_batch;            /* staged sweeps with the components side by side in one item:
+                                    bit 0 stress, bit 1 velocity */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
 };
 

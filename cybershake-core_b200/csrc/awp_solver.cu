@@ -620,7 +620,7 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         /* two or three components share one stress work item (media tiles
          * and cell coefficients once per level): 14 % faster for fx+fy on
          * 640 x 640 x 256, 3-4 % for fx+fy+fz on 400 x 400 x 200 */
-        s->staged_batch = env_int("AWP_TUNE_BATCH", 1) != 0;
+        s->staged_batch = env_int("AWP_TUNE_BATCH", 1) & 3;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -1349,8 +1349,10 @@ extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_ti
     const int nk = np + 2;
     o->nkernels = nk;
     for (int k = 0; k < np; k++) {
-        const bool batched = s->staged_on && parts[k] == AWP_PART_STR && s->staged_batch && p->ncomp >= 2;
-        snprintf(o->name[k], sizeof o->name[k], "%s", batched ? "k_str_tmab" : (s->staged_on ? pname_staged : pname)[parts[k]]);
+        const bool bstr = s->staged_on && parts[k] == AWP_PART_STR && (s->staged_batch & 1) && p->ncomp >= 2;
+        const bool bvel = s->staged_on && parts[k] == AWP_PART_VEL && (s->staged_batch & 2) && p->ncomp >= 2;
+        snprintf(o->name[k], sizeof o->name[k], "%s",
+                 bstr ? "k_str_tmab" : (bvel ? "k_vel_tmab" : (s->staged_on ? pname_staged : pname)[parts[k]]));
         o->bytes_per_launch[k] = part_bytes(s, parts[k]);
     }
     snprintf(o->name[np], sizeof o->name[np], "k_post");
@@ -1700,8 +1702,8 @@ extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
         return set_err(AWP_ERR_PARAM, "awp_set_tuning: z levels per work item must be 8..%d", kmax);
     if ((t->staged_qslow != 0 && t->staged_qslow != 1) || (t->staged_rpt != 1 && t->staged_rpt != 2) ||
         (t->staged_rpt_vel != 1 && t->staged_rpt_vel != 2) || (t->unroll != 1 && t->unroll != 2) ||
-        (t->ty != 4 && t->ty != 8 && t->ty != 16) || (t->staged_batch != 0 && t->staged_batch != 1))
-        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16, batch 0/1");
+        (t->ty != 4 && t->ty != 8 && t->ty != 16) || t->staged_batch < 0 || t->staged_batch > 3)
+        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16, batch 0-3");
     CU(cudaSetDevice(s->p.device));
     CU(cudaStreamSynchronize(s->stream));   /* no captured step in flight when its graph goes */
     s->kchunk_staged = t->kchunk_staged;
@@ -1852,7 +1854,10 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
         case F_RPTV: vals[nv++] = 3 - cur.staged_rpt_vel; break;
         case F_UNROLL: vals[nv++] = 3 - cur.unroll; break;
         case F_QSLOW: vals[nv++] = 1 - cur.staged_qslow; break;
-        case F_BATCH: vals[nv++] = 1 - cur.staged_batch; break;
+        case F_BATCH:
+            for (int b = 0; b < 4; b++)
+                if (b != cur.staged_batch) vals[nv++] = b;
+            break;
         case F_TY:
             for (int ty : {4, 8, 16})
                 if (ty != cur.ty && (stepper == AWP_KERNEL_FUSED || ty != 16)) vals[nv++] = ty;

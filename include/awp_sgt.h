@@ -271,8 +271,9 @@ typedef struct {
     int ty;                  /* two-sweep / fused steppers: block rows (4, 8, 16)      */
     int kchunk;              /* fused stepper: z levels per work item (8..nz)          */
     int kchunk_sweep;        /* two-sweep stepper: z levels per work item (8..nz)      */
-    int staged_batch;        /* staged stress sweep: 1 = all components of a tile in one
-                                work item, sharing media tiles and cell coefficients */
+    int staged_batch;        /* staged sweeps with all components of a tile in one work
+                                item, sharing media tiles and cell coefficients:
+                                bit 0 the stress sweep, bit 1 the velocity sweep */
 } awp_tuning;
 
 awp_status awp_get_tuning(awp_solver *s, awp_tuning *t);

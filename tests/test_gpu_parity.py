@@ -161,7 +161,7 @@ def test_multi_tile_multi_chunk_grid(kernel, kstage, unroll, rpt, monkeypatch):
     assert_same_state(c.gpu(kernel=kernel), c.oracle())
 
 
-@pytest.mark.parametrize("qslow,batch", [("0", "0"), ("1", "0"), ("1", "1")])
+@pytest.mark.parametrize("qslow,batch", [("0", "0"), ("1", "0"), ("1", "1"), ("1", "3")])
 def test_staged_batched_components_many_items(qslow, batch, monkeypatch):
     """Three components as neighbouring work items (or one component over
     all tiles at a time, or side by side in one item of the stress sweep),

@@ -38,7 +38,7 @@ def variant(t, **kw):
 # shape 2 is one work item over the whole depth (nz = 30)
 SHAPES = {
     "staged": [dict(kchunk_staged=9, staged_rpt=2, staged_rpt_vel=2, unroll=1, staged_qslow=0),
-               dict(kchunk_staged=16, staged_rpt=1, staged_rpt_vel=1, unroll=2, staged_qslow=1, staged_batch=1),
+               dict(kchunk_staged=16, staged_rpt=1, staged_rpt_vel=1, unroll=2, staged_qslow=1, staged_batch=3),
                dict(kchunk_staged=30)],
     "fused": [dict(ty=4, kchunk=16), dict(ty=16, kchunk=8), dict(ty=8, kchunk=30)],
     "two_sweep": [dict(ty=4, kchunk_sweep=8, unroll=2), dict(ty=16, kchunk_sweep=12, unroll=1),
@@ -124,17 +124,19 @@ def test_autotune_rejects_bad_arguments():
 STATE = awpsgt.FIELDS[:15]
 
 
+@pytest.mark.parametrize("batch", [1, 2, 3])
 @pytest.mark.parametrize("igreen", [(1, 2), (1, 2, 3), (-2, 4, 6)])
 @pytest.mark.parametrize("precision", ["f32", "mixed"])
 @pytest.mark.parametrize("nve", [1, 0])
-def test_batched_stress_sweep_matches_per_component(igreen, precision, nve):
+def test_batched_sweeps_match_per_component(igreen, precision, nve, batch):
     """Components side by side in one work item (shared media tiles and cell
-    coefficients) against one component per work item: every state field, the
-    CHKJ series and the SGTs bit for bit; FP32 also against the oracle."""
+    coefficients; batch bit 0 the stress sweep, bit 1 the velocity sweep)
+    against one component per work item: every state field, the CHKJ series
+    and the SGTs bit for bit; FP32 also against the oracle."""
     n = len(igreen)
     c = Case(nx=45, ny=37, nz=29, nt=30, igreen=igreen, srcs=[[(20, 18, 6)]] * n, nve=nve)
     runs = []
-    for batch in (0, 1):
+    for batch in (0, batch):
         p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, igreen=c.igreen, kernel="staged",
                                precision=precision, **c.kw())
         s = awpsgt.Solver(p)
