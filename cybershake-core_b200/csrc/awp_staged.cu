@@ -785,13 +785,15 @@ __host__ __device__ __forceinline__ uint32_t strb_comp_txb(int nve, int rsize)
     return (uint32_t)((3 * ST_VT + 6 * ST_PT) * 4 + (nve == 1 ? 6 * ST_PT * rsize : 0));
 }
 
-template <class TR, int NCB, int STB_CS>
-__global__ void __launch_bounds__(ST_THREADS, 2)
+/* RPT tile rows per consumer thread (ST_Y / RPT consumer warps) */
+template <class TR, int NCB, int STB_CS, int RPT>
+__global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 2)
 k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
            const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
            const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
     constexpr int RSIZE = (int)sizeof(TR);
+    constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
     float *mring = ring_base(st_smem);
     float *cring = mring + STB_MS * STB_MSLOT;
@@ -803,11 +805,11 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
 #pragma unroll
         for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
-    ring_init<STB_MS>(mfull, mempty, &abort_s, ST_CW);
-    ring_init<STB_CS>(cfull, cempty, &abort_s, ST_CW);
+    ring_init<STB_MS>(mfull, mempty, &abort_s, CW);
+    ring_init<STB_CS>(cfull, cempty, &abort_s, CW);
     const int tx = threadIdx.x, ty = threadIdx.y;
 
-    if (ty == ST_CW) {                /* producer warp */
+    if (ty == CW) {                   /* producer warp */
         if (tx != 0) return;
         uint32_t um = 0, uc = 0;
         bool ok = true;
@@ -860,36 +862,42 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
         return;
     }
 
-    const int sz = g.plane;
-    const int cv = (ty + 2) * ST_W + tx + 4, cm = (ty + 1) * ST_W + tx + 4, cp = ty * ST_X + tx;
+    const int sz = g.plane, sy = g.px;
     uint32_t um0 = 0, uc = 0;         /* media use of the item's level k0 - 1; next component use */
     for (int item = blockIdx.x; item < w.nitems; item += gridDim.x) {
         int bx, by, k0, k1;
         work_item(g, w, item, bx, by, k0, k1);
-        const int i = bx * ST_X + 1 + tx, j = by * ST_Y + 1 + ty;
-        const bool live = i <= g.nx && j <= g.ny;
-        const int itxy = ((j & 1) << 1) | (i & 1);
-        const int c0 = g.idx(i, j, k0);
-        /* per component: column queues u, v at k+1, k+2 and w at k+1, fed by
-         * loads one level ahead (pu, pv, pw) that rotate in when the component
-         * comes up at the next level, a full level after their issue; w at
-         * k-2, k-1 and u, v at k-1 come from the tiles of earlier levels */
-        float up1[NCB], up2[NCB], pu[NCB], vp1[NCB], vp2[NCB], pv[NCB], wp1[NCB], pw[NCB];
-        float wm2[NCB], wm1[NCB], um1[NCB], vm1[NCB];
+        const int i = bx * ST_X + 1 + tx;
+        const int c0 = g.idx(i, by * ST_Y + 1 + ty, k0);
+        /* per row and component: column queues u, v at k+1, k+2 and w at k+1,
+         * fed by loads one level ahead (pu, pv, pw) that rotate in when the
+         * component comes up at the next level, a full level after their
+         * issue; w at k-2, k-1 and u, v at k-1 come from earlier tiles */
+        float up1[RPT][NCB], up2[RPT][NCB], pu[RPT][NCB], vp1[RPT][NCB], vp2[RPT][NCB], pv[RPT][NCB];
+        float wp1[RPT][NCB], pw[RPT][NCB], wm2[RPT][NCB], wm1[RPT][NCB], um1[RPT][NCB], vm1[RPT][NCB];
+        bool live[RPT];
+        int itxy[RPT];
+        float cxy[RPT];
 #pragma unroll
-        for (int q = 0; q < NCB; ++q) {
-            up1[q] = up2[q] = pu[q] = vp1[q] = vp2[q] = pv[q] = wp1[q] = pw[q] = 0.f;
-            wm2[q] = wm1[q] = um1[q] = vm1[q] = 0.f;
-            if (live) {
-                const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
-                up2[q] = U[c0 + sz]; pu[q] = U[c0 + 2 * sz];
-                vp2[q] = V[c0 + sz]; pv[q] = V[c0 + 2 * sz];
-                pw[q] = W[c0 + sz];
-                wm2[q] = W[c0 - 2 * sz]; wm1[q] = W[c0 - sz];
-                um1[q] = U[c0 - sz]; vm1[q] = V[c0 - sz];
+        for (int r = 0; r < RPT; ++r) {
+            const int j = by * ST_Y + 1 + ty + r * CW, c = c0 + r * CW * sy;
+            live[r] = i <= g.nx && j <= g.ny;
+            itxy[r] = ((j & 1) << 1) | (i & 1);
+            cxy[r] = live[r] ? cx[i] * cy[j] : 0.f;
+#pragma unroll
+            for (int q = 0; q < NCB; ++q) {
+                up1[r][q] = up2[r][q] = pu[r][q] = vp1[r][q] = vp2[r][q] = pv[r][q] = wp1[r][q] = pw[r][q] = 0.f;
+                wm2[r][q] = wm1[r][q] = um1[r][q] = vm1[r][q] = 0.f;
+                if (live[r]) {
+                    const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
+                    up2[r][q] = U[c + sz]; pu[r][q] = U[c + 2 * sz];
+                    vp2[r][q] = V[c + sz]; pv[r][q] = V[c + 2 * sz];
+                    pw[r][q] = W[c + sz];
+                    wm2[r][q] = W[c - 2 * sz]; wm1[r][q] = W[c - sz];
+                    um1[r][q] = U[c - sz]; vm1[r][q] = V[c - sz];
+                }
             }
         }
-        const float cxy = live ? cx[i] * cy[j] : 0.f;
         int cc = c0;
 #pragma unroll 1
         for (int k = k0; k <= k1; ++k, cc += sz) {
@@ -903,78 +911,96 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                 atomicOr(err, AWP_KERR_TMA_WAIT);
                 return;
             }
-            const int it = (((g.nz + 1 - k) & 1) << 2) | itxy;                 /* viscoop.f:93-101 */
-            StrCoef kc;
-            {
+            const int ipar = ((g.nz + 1 - k) & 1) << 2;                        /* viscoop.f:93-101 */
+            StrCoef kc[RPT];
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int cm = (ty + r * CW + 1) * ST_W + tx + 4;
+                const int it = ipar | itxy[r];
                 const TMed M{mring + (mk % STB_MS) * STB_MSLOT + cm, mring + (mm % STB_MS) * STB_MSLOT + cm};
-                kc = str_coef_t(M, nve, tau[it], tau[8 + it]);
+                kc[r] = str_coef_t(M, nve, tau[it], tau[8 + it]);
             }
             __syncwarp();
             if (tx == 0) mb_arrive(&mempty[mm % STB_MS]);
 #pragma unroll
             for (int q = 0; q < NCB; ++q, ++uc) {
+#pragma unroll
+                for (int r = 0; r < RPT; ++r) {
+                    /* rotate this component's queues, then load one level ahead */
+                    const int c = cc + r * CW * sy;
+                    up1[r][q] = up2[r][q]; up2[r][q] = pu[r][q];
+                    vp1[r][q] = vp2[r][q]; vp2[r][q] = pv[r][q];
+                    wp1[r][q] = pw[r][q];
+                    pu[r][q] = pv[r][q] = pw[r][q] = 0.f;
+                    if (live[r] && k < k1) {
+                        pu[r][q] = tab[q].f[AF_U][c + 3 * sz];
+                        pv[r][q] = tab[q].f[AF_V][c + 3 * sz];
+                        pw[r][q] = tab[q].f[AF_W][c + 2 * sz];
+                    }
+                }
                 ok = mb_wait_or_abort(&cfull[uc % STB_CS], (uc / STB_CS) & 1, &abort_s);
                 if (!__all_sync(0xffffffffu, ok)) {
                     abort_s = 1;
                     atomicOr(err, AWP_KERR_TMA_WAIT);
                     return;
                 }
-                /* rotate this component's queues, then load one level ahead */
-                up1[q] = up2[q]; up2[q] = pu[q];
-                vp1[q] = vp2[q]; vp2[q] = pv[q];
-                wp1[q] = pw[q];
-                pu[q] = pv[q] = pw[q] = 0.f;
-                if (live && k < k1) {
-                    pu[q] = tab[q].f[AF_U][cc + 3 * sz];
-                    pv[q] = tab[q].f[AF_V][cc + 3 * sz];
-                    pw[q] = tab[q].f[AF_W][cc + 2 * sz];
-                }
                 const float *sk = cring + (uc % STB_CS) * STB_CSLOT;
-                const float nu = sk[cv], nv = sk[ST_VT + cv], nw = sk[2 * ST_VT + cv];
-                if (live) {
-                    const float *ps = sk + STB_CST + cp;
-                    const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
-                    const TVel Vq{sk + cv, um1[q], vm1[q], wm1[q], up1[q], up2[q], vp1[q], vp2[q], wm2[q], wp1[q]};
-                    Stress6 o;
-                    if (nve == 1) {
-                        const TR *pr = (const TR *)(sk + STB_CST + 6 * ST_PT) + cp;
-                        float rr[6];
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
-                        const VelDiff dd = vel_diff(Vq);
-                        o = str_visco(kc, dd, s0, rr, dth, dt, dh1);
+                for (int r = 0; r < RPT; ++r) {
+                    const int row = ty + r * CW, c = cc + r * CW * sy;
+                    const int cv = (row + 2) * ST_W + tx + 4, cp = row * ST_X + tx;
+                    const float nu = sk[cv], nv = sk[ST_VT + cv], nw = sk[2 * ST_VT + cv];
+                    if (live[r]) {
+                        const float *ps = sk + STB_CST + cp;
+                        const Stress6 s0{ps[0], ps[ST_PT], ps[2 * ST_PT], ps[3 * ST_PT], ps[4 * ST_PT], ps[5 * ST_PT]};
+                        const TVel Vq{sk + cv, um1[r][q], vm1[r][q], wm1[r][q], up1[r][q], up2[r][q], vp1[r][q],
+                                      vp2[r][q], wm2[r][q], wp1[r][q]};
+                        Stress6 o;
+                        if (nve == 1) {
+                            const TR *pr = (const TR *)(sk + STB_CST + 6 * ST_PT) + cp;
+                            float rr[6];
 #pragma unroll
-                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], cc, rr[a], 1.0f);
-                    } else {
-                        o = str_elastic(kc, Vq, s0, dth);
+                            for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
+                            const VelDiff dd = vel_diff(Vq);
+                            o = str_visco(kc[r], dd, s0, rr, dth, dt, dh1);
+#pragma unroll
+                            for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, rr[a], 1.0f);
+                        } else {
+                            o = str_elastic(kc[r], Vq, s0, dth);
+                        }
+                        const float crj = cxy[r] * czk;
+                        tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj;
+                        tab[q].f[AF_ZZ][c] = o.zz * crj; tab[q].f[AF_XY][c] = o.xy * crj;
+                        tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
                     }
-                    const float crj = cxy * czk;
-                    tab[q].f[AF_XX][cc] = o.xx * crj; tab[q].f[AF_YY][cc] = o.yy * crj; tab[q].f[AF_ZZ][cc] = o.zz * crj;
-                    tab[q].f[AF_XY][cc] = o.xy * crj; tab[q].f[AF_XZ][cc] = o.xz * crj; tab[q].f[AF_YZ][cc] = o.yz * crj;
+                    wm2[r][q] = wm1[r][q];
+                    um1[r][q] = nu; vm1[r][q] = nv; wm1[r][q] = nw;
                 }
                 __syncwarp();
                 if (tx == 0) mb_arrive(&cempty[uc % STB_CS]);
-                wm2[q] = wm1[q];
-                um1[q] = nu; vm1[q] = nv; wm1[q] = nw;
             }
         }
         __syncwarp();
         if (tx == 0) mb_arrive(&mempty[(um0 + (uint32_t)(k1 - k0 + 1)) % STB_MS]);
         um0 += (uint32_t)(k1 - k0 + 2);
-        if (k1 == g.nz && live) {
+        if (k1 == g.nz) {
 #pragma unroll
-            for (int q = 0; q < NCB; ++q) {
-                /* fstr (operator.f:594-606) on this thread's own column */
-                const int ct = g.idx(i, j, g.nz);
-                float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
-                ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
-                ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
-                XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
-                XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
-                YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
-                YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
-                XZ[ct] = 0.0f;
-                YZ[ct] = 0.0f;
+            for (int r = 0; r < RPT; ++r) {
+                if (!live[r]) continue;
+#pragma unroll
+                for (int q = 0; q < NCB; ++q) {
+                    /* fstr (operator.f:594-606) on this thread's own column */
+                    const int ct = g.idx(i, by * ST_Y + 1 + ty + r * CW, g.nz);
+                    float *ZZ = tab[q].f[AF_ZZ], *XZ = tab[q].f[AF_XZ], *YZ = tab[q].f[AF_YZ];
+                    ZZ[ct + sz] = -__ldcg(&ZZ[ct]);
+                    ZZ[ct + 2 * sz] = -__ldcg(&ZZ[ct - sz]);
+                    XZ[ct + sz] = -__ldcg(&XZ[ct - sz]);
+                    XZ[ct + 2 * sz] = -__ldcg(&XZ[ct - 2 * sz]);
+                    YZ[ct + sz] = -__ldcg(&YZ[ct - sz]);
+                    YZ[ct + 2 * sz] = -__ldcg(&YZ[ct - 2 * sz]);
+                    XZ[ct] = 0.0f;
+                    YZ[ct] = 0.0f;
+                }
             }
         }
     }
@@ -1117,25 +1143,28 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
 }
 
 /* CS component sub-slots: CS - 1 (level, component) tiles in flight */
-template <class TR, int NCB, int CS>
+template <class TR, int NCB, int CS, int RPT>
 static cudaError_t launch_str_bc(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
+    constexpr int CW = ST_Y / RPT;
     const size_t smem = 128 + (size_t)(STB_MS * STB_MSLOT + CS * STB_CSLOT) * 4 + 2 * 8 * (STB_MS + CS);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
     int grid = 0;
-    cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
-    k_str_tmab<TR, NCB, CS><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
+    k_str_tmab<TR, NCB, CS, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
         st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
     return cudaGetLastError();
 }
 
 /* five sub-slots (109 KB with the media ring, two blocks per SM) measured
- * slightly ahead of four on the 400 x 400 x 200 three-component grid */
+ * slightly ahead of four on the 400 x 400 x 200 three-component grid; one
+ * row per thread: with two (161 registers) a launch took 3.00 ms against
+ * 2.39 ms there, so staged_rpt applies to the one-component-per-item form only */
 template <class TR, int NCB>
 static cudaError_t launch_str_b(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
-    return launch_str_bc<TR, NCB, 5>(st, s, stream);
+    return launch_str_bc<TR, NCB, 5, 1>(st, s, stream);
 }
 
 /* two rows per thread carry twice the live state already: that variant keeps

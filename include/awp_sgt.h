@@ -265,7 +265,8 @@ awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_times *out);
 typedef struct {
     int kchunk_staged;       /* staged sweeps: z levels per work item (8..nz)          */
     int staged_qslow;        /* staged sweeps: 1 = one component over all tiles first  */
-    int staged_rpt;          /* staged stress sweep: tile rows per thread (1, 2)       */
+    int staged_rpt;          /* staged stress sweep, one component per item: tile rows
+                                per thread (1, 2)                                      */
     int staged_rpt_vel;      /* staged velocity sweep: tile rows per thread (1, 2)     */
     int unroll;              /* z-loop unroll of the sweeps (1, 2)                     */
     int ty;                  /* two-sweep / fused steppers: block rows (4, 8, 16)      */
