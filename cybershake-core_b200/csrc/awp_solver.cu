@@ -1850,10 +1850,17 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
                 if (!dup) vals[nv++] = kc;
             }
             break;
-        case F_RPT: vals[nv++] = 3 - cur.staged_rpt; break;
-        case F_RPTV: vals[nv++] = 3 - cur.staged_rpt_vel; break;
+        /* the side-by-side sweeps ignore rows per thread and component order */
+        case F_RPT:
+            if (!((cur.staged_batch & 1) && p.ncomp >= 2)) vals[nv++] = 3 - cur.staged_rpt;
+            break;
+        case F_RPTV:
+            if (!((cur.staged_batch & 2) && p.ncomp >= 2)) vals[nv++] = 3 - cur.staged_rpt_vel;
+            break;
         case F_UNROLL: vals[nv++] = 3 - cur.unroll; break;
-        case F_QSLOW: vals[nv++] = 1 - cur.staged_qslow; break;
+        case F_QSLOW:
+            if (!(cur.staged_batch == 3 && p.ncomp >= 2)) vals[nv++] = 1 - cur.staged_qslow;
+            break;
         case F_BATCH:
             for (int b = 0; b < 4; b++)
                 if (b != cur.staged_batch) vals[nv++] = b;
