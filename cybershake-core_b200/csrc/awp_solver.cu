@@ -311,9 +311,10 @@ static void free_all(awp_solver *s)
 /* Blocks a solver frees stay on the device for the next solver of the
  * process: the next job on the same grid asks for the same sizes, so its
  * create skips cudaMalloc and its destroy skips cudaFree, whose device-wide
- * synchronisation would also stall the other solvers of a server.  Only exact
- * sizes are reused.  A failed cudaMalloc returns the device's idle blocks and
- * tries again.  AWP_DEVICE_CACHE_MB bounds the idle bytes per device
+ * synchronisation would also stall the other solvers of a server.  An idle
+ * block is reused for a request of its size or up to 1/8 smaller (the
+ * smallest such block).  A failed cudaMalloc returns the device's idle blocks
+ * and tries again.  AWP_DEVICE_CACHE_MB bounds the idle bytes per device
  * (default: half the device memory; 0 turns the cache off).  Callers hand a
  * block back only when no queued work uses it. */
 namespace {
@@ -365,12 +366,13 @@ static cudaError_t blk_alloc(int dev, void **ptr, size_t bytes)
 {
     {
         std::lock_guard<std::mutex> lk(g_blk_mu);
-        auto it = g_blk_idle.find(std::make_pair(dev, bytes));
-        if (it != g_blk_idle.end()) {
+        auto it = g_blk_idle.lower_bound(std::make_pair(dev, bytes));
+        if (it != g_blk_idle.end() && it->first.first == dev && it->first.second - bytes <= bytes / 8) {
+            const size_t have = it->first.second;
             *ptr = it->second;
             g_blk_idle.erase(it);
-            g_blk_idle_bytes[dev] -= bytes;
-            g_blk_live[*ptr] = BlkInfo{dev, bytes};
+            g_blk_idle_bytes[dev] -= have;
+            g_blk_live[*ptr] = BlkInfo{dev, have};
             return cudaSuccess;
         }
     }

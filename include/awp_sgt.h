@@ -415,7 +415,8 @@ typedef struct {
 } awp_request_info;
 
 /* Device blocks freed by awp_destroy stay on the device for the next solver of
- * the process (exact sizes are reused; a failed allocation returns them first;
+ * the process (a block serves a request of its size or up to 1/8 smaller; a
+ * failed allocation returns them first;
  * AWP_DEVICE_CACHE_MB bounds the idle bytes per device, default half the device
  * memory, 0 = off).  This returns every idle block to the driver.  Work that
  * uses a solver's device pointers (awp_device_field) must be complete before

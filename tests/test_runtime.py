@@ -57,3 +57,16 @@ def test_pinned_media_upload_matches_pageable():
     ref = solve(c)
     assert all(bits_equal(x, y) for x, y in zip(got, ref))
     assert np.abs(ref[0]).max() > 0
+
+
+def test_slightly_smaller_grid_reuses_blocks_and_matches():
+    """A grid a few percent smaller takes the idle blocks of a larger one
+    (their tails hold stale data) and still matches a fresh solve."""
+    awpsgt.release_cached_memory()
+    big = Case(nx=50, ny=40, nz=32, nt=20)
+    small = Case(nx=48, ny=40, nz=31, nt=20, seed=5)
+    fresh = solve(small)
+    awpsgt.release_cached_memory()
+    solve(big)
+    reused = solve(small)
+    assert all(bits_equal(x, y) for x, y in zip(fresh, reused))
