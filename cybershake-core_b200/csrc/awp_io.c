@@ -124,7 +124,8 @@ awp_status awp_read_in3d(const char *path, awp_in3d *o)
         } else if (fd->t == T_REAL) {
             *(float *)dst = (float)fortran_real(item, &ok);
         } else {
-            snprintf(dst, 512, "%s", item);
+            /* string fields are 512 bytes: longer names are cut there */
+            snprintf(dst, 512, "%.511s", item);
         }
         if (!ok) { fclose(f); return ioerr(AWP_ERR_IO, "IN3D: bad value for %s", fd->name); }
         k++;
