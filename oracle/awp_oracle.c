@@ -81,6 +81,7 @@ typedef struct {
     size_t nvol;
     real *f[F_NFIELDS];
     real tau1[2][2][2], tau2[2][2][2];   /* [itz][ity][itx], 0-based parity */
+    real tau[2][2][2];                   /* relaxation times before viscoop.f:80-88 */
     real *cx, *cy, *cz;                  /* 1-D sponge factors, index 1..n */
     float vpe[2], vse[2], dde[2];
     /* source */
@@ -122,6 +123,7 @@ static void orc_tausub(orc_t *h, real taumin, real taumax)
                 tmp = (tmp - (real)0.5) / (real)8;
                 tmp = (real)2.0 * tmp - (real)1.0;
                 real tau = r_exp((real)0.5 * (r_log(taumax * taumin) + r_log(taumax / taumin) * tmp));
+                h->tau[z][y][x] = tau;
                 /* viscoop.f:80-88 */
                 h->tau1[z][y][x] = (real)1 / ((tau * dt1) + ((real)1. / (real)2.));
                 h->tau2[z][y][x] = (tau * dt1) - ((real)1. / (real)2.);
@@ -921,6 +923,22 @@ int orc_set_field(orc_t *h, int fid, const real *in)
 }
 
 int orc_real_bytes(void) { return (int)sizeof(real); }
+
+/* relaxation times [itz][ity][itx] (relax.f:15-36), as float */
+void orc_get_tau(const orc_t *h, float *out8)
+{
+    for (int z = 0; z < 2; z++)
+        for (int y = 0; y < 2; y++)
+            for (int x = 0; x < 2; x++) out8[(z * 2 + y) * 2 + x] = (float)h->tau[z][y][x];
+}
+
+/* Cerjan factors cx[1..nx], cy[1..ny], cz[1..nz] (cerjan.f), as float */
+void orc_get_sponge(const orc_t *h, float *cx, float *cy, float *cz)
+{
+    for (int i = 0; i < h->p.nx; i++) cx[i] = (float)h->cx[i + 1];
+    for (int j = 0; j < h->p.ny; j++) cy[j] = (float)h->cy[j + 1];
+    for (int k = 0; k < h->p.nz; k++) cz[k] = (float)h->cz[k + 1];
+}
 
 int orc_num_threads(void)
 {

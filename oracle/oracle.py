@@ -71,6 +71,8 @@ def load(precision: str = "f32"):
     lib.orc_real_bytes.restype = C.c_int
     lib.orc_num_threads.restype = C.c_int
     lib.orc_set_num_threads.argtypes = [C.c_int]
+    lib.orc_get_tau.argtypes = [V, V]
+    lib.orc_get_sponge.argtypes = [V, V, V, V]
     _libs[precision] = lib
     return lib
 
@@ -161,6 +163,20 @@ class Oracle:
         out = np.zeros(6, dtype=np.float32)
         self.lib.orc_get_extremes(self.h, _p(out))
         return out
+
+    def tau(self):
+        """Relaxation times [itz][ity][itx] (relax.f:15-36), set by load_media."""
+        out = np.zeros((2, 2, 2), dtype=np.float32)
+        self.lib.orc_get_tau(self.h, _p(out))
+        return out
+
+    def sponge(self):
+        """Cerjan factors (cx[nx], cy[ny], cz[nz]), index 0 at the low x / y face
+        and at the bottom."""
+        p = self.p
+        cx, cy, cz = (np.zeros(n, np.float32) for n in (p.nx, p.ny, p.nz))
+        self.lib.orc_get_sponge(self.h, _p(cx), _p(cy), _p(cz))
+        return cx, cy, cz
 
 
 def threads():
@@ -301,3 +317,40 @@ def synth_reference(master, index, headers, comps, slon, slat, dtout, ntout, tst
     if rc:
         raise ValueError("reference synthesis failed (code %d)" % rc)
     return seis[:nv * 3 * got.value].reshape(nv, 3, got.value)
+
+
+def setup_reference(media, *, nvar=3, nve=1, socalq=0, fp=0.5, fl=0.01, fh=25.0, arbc=0.92, nd=20):
+    """The reference CUDA stepper's own host set-up on one rank (AWP-GPU-SGT
+    mesh.c inimesh and tausub, cerjan.c inicrj), built from the reference
+    sources into oracle/_ref/libsetup_ref.so (oracle/Makefile.ref): media
+    [nz][ny][nx][nvar] (z = 0 at the surface) in, a dict of lam mu d1 qp qs in
+    the same [z][y][x] order, the extremes (vs, vp, rho min/max), taumin /
+    taumax, tau [idx][idy][idz] and the sponge factors out.  None where that
+    library has not been built."""
+    import tempfile
+    path = os.path.join(_HERE, "_ref", "libsetup_ref.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    V, I, F = C.c_void_p, C.c_int, C.c_float
+    lib.ref_inimesh.argtypes = [I, I, I, I, I, I, F, F, F, C.c_char_p, V, V, V, V, V, V, V]
+    lib.ref_tausub.argtypes = [F, F, V]
+    lib.ref_inicrj.argtypes = [F, I, I, I, I, V, V, V]
+    m = np.ascontiguousarray(media, np.float32)
+    nz, ny, nx = m.shape[:3]
+    out = {k: np.zeros((nz, ny, nx), np.float32) for k in ("lam", "mu", "d1", "qp", "qs")}
+    ext, tmm, tau8 = np.zeros(6, np.float32), np.zeros(2, np.float32), np.zeros(8, np.float32)
+    # mesh.c copies the path into a 40-byte buffer: a short name under /tmp
+    fd, fname = tempfile.mkstemp(prefix="m", suffix=".b", dir="/tmp")
+    try:
+        with os.fdopen(fd, "wb") as f:
+            f.write(m.tobytes())
+        lib.ref_inimesh(nx, ny, nz, nvar, nve, socalq, fp, fl, fh, fname.encode(), _p(out["lam"]), _p(out["mu"]),
+                        _p(out["d1"]), _p(out["qp"]), _p(out["qs"]), _p(ext), _p(tmm))
+    finally:
+        os.unlink(fname)
+    lib.ref_tausub(tmm[0], tmm[1], _p(tau8))
+    cx, cy, cz = np.zeros(nx, np.float32), np.zeros(ny, np.float32), np.zeros(nz, np.float32)
+    lib.ref_inicrj(arbc, nx, ny, nz, nd, _p(cx), _p(cy), _p(cz))
+    out.update(extremes=ext, taumin=tmm[0], taumax=tmm[1], tau=tau8.reshape(2, 2, 2), cx=cx, cy=cy, cz=cz)
+    return out
