@@ -382,7 +382,7 @@ class In3d:
 
 
 # ---------------------------------------------------------------------------
-# benchmark configurations (sizes of the north-star configs)
+# benchmark configurations: the four CyberShake-style SGT workloads
 # ---------------------------------------------------------------------------
 
 @dataclass
@@ -426,7 +426,9 @@ class Workload:
 
 
 def config(n: int) -> Workload:
-    """North-star workload n (1..4) with its grid, steps and point count."""
+    """Workload n (1..4) with its grid, steps and point count: 1 a 160x160x80
+    homogeneous fx run, 2 a 400x400x200 layered fx+fy+fz run, 3 a 640x640x256
+    layered fx+fy run, 4 a 1400x1000x400 basin fx+fy run."""
     if n == 1:
         return Workload("cfg1_homog_160x160x80_fx", 160, 160, 80, 200.0, 0.01, 1000, (1,), 1000,
                         media_kind="homogeneous", src_xyz=(80, 80, 11))

@@ -3,15 +3,19 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / --impl reference legs of bench.py load this code, and only as
- * the checker or the timed CPU baseline.  The product path (the CUDA library
- * under cybershake-core_b200/) never links, loads or calls it.
+ * the oracle the device results are compared with or as the timed CPU
+ * baseline.  The product path (the CUDA library under cybershake-core_b200/)
+ * never links, loads or calls it.
  *
- * PARITY UNPINNED: the reference ships no solver tests, no golden SGT output
- * and no fixtures for this path, and its own implementations cannot be built
- * in this image (no Fortran compiler, no MPI; the CUDA variant uses texture
- * references removed in CUDA 12).  This file restates the Fortran semantics
- * statement by statement, with the same evaluation order, and is checked by
- * self-made known-answer tests (analytic travel times, linearity, symmetry).
+ * TIME LOOP PARITY UNPINNED: the reference ships no solver tests, no golden
+ * SGT output and no fixtures for this path, and its time-loop implementations
+ * cannot be built in this image (no Fortran compiler, no MPI; the CUDA variant
+ * uses texture references removed in CUDA 12).  This file restates the Fortran
+ * semantics statement by statement, with the same evaluation order, and is
+ * checked by known-answer tests (analytic travel times, linearity, symmetry).
+ * The set-up stage (media transform, relaxation times, Cerjan factors) is
+ * pinned to the reference CUDA variant's own host code (mesh.c, cerjan.c),
+ * built from its sources: tests/test_oracle_pin.py.
  *
  * Compiled twice: -DORC_REAL=float (FP32, operation order of the Fortran) and
  * -DORC_REAL=double (FP64 reference for rounding error).  Inputs are always

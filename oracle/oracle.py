@@ -1,12 +1,16 @@
 """ctypes binding of the CPU oracle (oracle/awp_oracle.c) -- TEST INFRASTRUCTURE.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use this
-module, as the checker or as the timed CPU restatement of the reference.  The
-product path (cybershake-core_b200/) never imports it.
+module, as the oracle the device results are compared with or as the timed CPU
+restatement of the reference.  The product path (cybershake-core_b200/) never
+imports it.
 
-PARITY UNPINNED: the reference ships no solver tests or golden outputs and
-cannot be built here; the oracle is a statement-by-statement restatement of the
-Fortran (see the header of awp_oracle.c), checked by known-answer tests.
+TIME LOOP PARITY UNPINNED: the reference ships no solver tests or golden
+outputs and its time loop cannot be built here; the oracle is a
+statement-by-statement restatement of the Fortran (see the header of
+awp_oracle.c), checked by known-answer tests.  Its set-up stage is pinned to
+the reference CUDA variant's host code (setup_reference below), and the
+synthesis oracle to DirectSynth's own functions (synth_reference).
 """
 from __future__ import annotations
 

@@ -261,7 +261,7 @@ def test_mixed_precision_same_result_both_kernels():
 
 
 def test_config1_full_run_bit_exact():
-    """North-star config 1 (160x160x80, h=200 m, dt=0.01 s, 1000 steps,
+    """Workload 1 (160x160x80, h=200 m, dt=0.01 s, 1000 steps,
     homogeneous half-space, fx at the centre 2 km deep, 1000 SGT points,
     every 10 steps) against the FP32 oracle, and its FP64 error."""
     w = ai.config(1)
