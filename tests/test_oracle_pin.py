@@ -89,3 +89,27 @@ def test_oracle_setup_matches_live_reference():
     if ref is None:
         pytest.skip("oracle/_ref/libsetup_ref.so not built (reference sources absent)")
     check(oracle_setup(grid, m, nvar, nd, arbc, 0.5, 0.01, 25.0), ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_device_media_match_reference_fixtures(case):
+    """The media the device holds (awp_get_field) against the same fixtures,
+    and bit for bit against the oracle."""
+    import awpsgt
+    name, grid, seed, nvar, nd, arbc, fp, fl, fh = case
+    nx, ny, nz = grid
+    m = media_for(grid, seed, nvar)
+    p = awpsgt.make_params(nx, ny, nz, 200.0, 0.01, 20, nd=nd, arbc=arbc, fp=fp, fl=fl, fh=fh, socalq=1, nvar=nvar,
+                           nve=1, ntiskp_sgt=10, write_step=2)
+    with awpsgt.Solver(p) as s:
+        s.load_media(m)
+        dev = {f: np.stack([s.field(f, 0)[nz + 1 - k, 2:ny + 2, 2:nx + 2] for k in range(nz)])
+               for f in ("lam", "mu", "d1", "qp", "qs")}
+    orc = oracle_setup(grid, m, nvar, nd, arbc, fp, fl, fh)
+    for f in dev:
+        assert np.array_equal(dev[f].view(np.uint32), orc[f].view(np.uint32)), f
+    ref = dict(np.load(os.path.join(OUT, name + ".npz")))
+    assert np.array_equal(dev["d1"].view(np.uint32), ref["d1"].view(np.uint32))
+    for f in ("lam", "mu", "qp", "qs"):
+        assert ulps(dev[f], ref[f]).max() <= MAX_ULP, f
