@@ -108,3 +108,53 @@ def test_create_without_gpu_fails_loudly():
     with pytest.raises(awpsgt.AwpError) as e:
         awpsgt.Solver(p)
     assert e.value.status in (3, 4)
+
+
+# ctypes mirror -> C type, for the layout check below
+MIRRORS = [("Layout", "awp_layout"), ("Params", "awp_params"), ("Stats", "awp_stats"), ("Tuning", "awp_tuning"),
+           ("KernelTimes", "awp_kernel_times"), ("In3dC", "awp_in3d"), ("SgtHeadArgs", "awp_sgthead_args"),
+           ("Request", "awp_request"), ("RequestInfo", "awp_request_info"), ("SynthParams", "awp_synth_params"),
+           ("SynthInfo", "awp_synth_info")]
+# numpy record dtype -> C type
+RECORDS = [("SRFPOINT", "awp_srf_point"), ("SEISHEADER", "awp_seisheader")]
+
+
+def test_ctypes_mirrors_match_the_header_layouts(tmp_path):
+    """Size and every field offset of each Python mirror (ctypes structures and
+    numpy record dtypes) equal the C compiler's for the header's struct (gcc on
+    this host)."""
+    import ctypes
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "awp_sgt.h"', '#include "awp_synth.h"',
+             'int main(void) {']
+    for py, c in MIRRORS:
+        cls = getattr(awpsgt, py)
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (py, c))
+        for name, _ in cls._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (py, name, c, name))
+    for py, c in RECORDS:
+        dt = getattr(awpsgt, py)
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (py, c))
+        for name in dt.names:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (py, name, c, name))
+    lines.append('return 0; }')
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(tuple(l.rsplit(" ", 1)) for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                                 text=True).stdout.splitlines())
+    for py, _ in MIRRORS:
+        cls = getattr(awpsgt, py)
+        assert int(got["%s size" % py]) == ctypes.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert int(got["%s %s" % (py, name)]) == getattr(cls, name).offset, (py, name)
+    for py, _ in RECORDS:
+        dt = getattr(awpsgt, py)
+        assert int(got["%s size" % py]) == dt.itemsize, py
+        for name in dt.names:
+            assert int(got["%s %s" % (py, name)]) == dt.fields[name][1], (py, name)

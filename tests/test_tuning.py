@@ -156,3 +156,23 @@ def test_batched_sweeps_match_per_component(igreen, precision, nve, batch):
         assert bits_equal(a.sgt(q), b.sgt(q))
     if precision == "f32" and igreen[0] > 0:
         assert_same_state(b, c.oracle(0), 0, fields=STATE if nve == 1 else STATE[:9])
+
+
+@pytest.mark.parametrize("batch", [0, 1, 3])
+def test_single_level_chunk_all_batch_masks(batch):
+    """nz = 33 in 8-level chunks leaves a one-level chunk at the bottom: the
+    queues of the side-by-side sweeps are set up and rotated on the same
+    level there."""
+    c = Case(nx=40, ny=20, nz=33, nt=20, igreen=(1, 2, 3), srcs=[[(20, 10, 5)], [(21, 9, 6)], [(19, 11, 4)]])
+    s = solver_for(c, "staged", None)
+    s.close()
+    p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, igreen=c.igreen, kernel="staged", **c.kw())
+    s = awpsgt.Solver(p)
+    s.set_tuning(variant(s.tuning(), staged_batch=batch, kchunk_staged=8))
+    s.load_media(c.media)
+    for q in range(3):
+        s.set_source(q, c.srcs[q], c.stfs[q])
+    s.set_points(c.pts)
+    s.run(c.nt)
+    for q in range(3):
+        assert_same_state(s, c.oracle(q), q)
