@@ -1787,7 +1787,8 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
                                    awp_tuning *best, double *gcell_updates_per_s)
 {
     if (!pin || !best) return set_err(AWP_ERR_PARAM, "awp_autotune: null argument");
-    if (trial_steps < 1) return set_err(AWP_ERR_PARAM, "awp_autotune: trial_steps must be >= 1");
+    if (trial_steps < 1 || trial_steps > 100000)
+        return set_err(AWP_ERR_PARAM, "awp_autotune: trial_steps must be 1..100000");
     awp_params p = *pin;
     const int max_trials = 24;
     p.nt = max_trials * (trial_steps + p.ntiskp_sgt) + p.ntiskp_sgt + 1;

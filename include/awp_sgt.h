@@ -281,13 +281,15 @@ awp_status awp_get_tuning(awp_solver *s, awp_tuning *t);
 awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t);
 
 /* Autotuner: times candidate launch shapes on a solver of these parameters
- * (the caller's media, or a homogeneous medium when media is NULL) for
- * trial_steps time steps each, by coordinate descent over the fields of
- * awp_tuning that the chosen stepper uses, and returns the fastest with its
- * Gcell-updates/s.  With a cache path, a result stored there for the same
- * grid, components, precision, stepper and GPU model is returned without
- * timing, and a new result is appended.  Allocates one solver's device
- * memory for the duration of the call. */
+ * (the caller's media, or a homogeneous medium when media is NULL; the
+ * wavefield filled with bounded noise, since a zero wavefield runs at higher
+ * clocks under the power cap) for trial_steps (1..100000) time steps each, by
+ * coordinate descent over the fields of awp_tuning that the chosen stepper
+ * uses, and returns the fastest with its Gcell-updates/s.  With a cache path,
+ * a result stored there for the same grid, components, precision, NVE,
+ * stepper and GPU model is returned without timing, and a new result is
+ * appended.  Allocates one solver's device memory for the duration of the
+ * call. */
 awp_status awp_autotune(const awp_params *p, const float *media, int trial_steps, const char *cache_path,
                         awp_tuning *best, double *gcell_updates_per_s);
 

@@ -117,8 +117,9 @@ def test_autotune_and_cache(kernel, tmp_path):
 def test_autotune_rejects_bad_arguments():
     c = Case(nx=32, ny=24, nz=20, nt=10)
     p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, **c.kw())
-    with pytest.raises(awpsgt.AwpError):
-        awpsgt.autotune(p, c.media, trial_steps=0)
+    for bad in (0, -3, 100001):
+        with pytest.raises(awpsgt.AwpError):
+            awpsgt.autotune(p, c.media, trial_steps=bad)
 
 
 STATE = awpsgt.FIELDS[:15]
