@@ -13,7 +13,9 @@
  * Everything runs on one GPU; NPX/NPY/NPZ are read and ignored.  With
  * AWP_RWG_SGT=x|y|z in the environment the SGTs are written in RWG component
  * order (SgtHead/src/reformat_awp_mpi.c:104-122), so no separate reformat
- * pass is needed.
+ * pass is needed.  With AWP_AUTOTUNE_CACHE=<file> the launch shapes are tuned
+ * for the job's grid before the solve (awp_autotune on the homogeneous
+ * medium, a few seconds once per grid and GPU model) and kept in that file.
  */
 #include <math.h>
 #include <stdio.h>
@@ -189,8 +191,17 @@ int main(int argc, char **argv)
         }
     }
 
+    awp_tuning tuned;
+    const char *tune_cache = getenv("AWP_AUTOTUNE_CACHE");
+    if (tune_cache && *tune_cache) {
+        double rate = 0.0;
+        if ((st = awp_autotune(&p, NULL, 20, tune_cache, &tuned, &rate)) != AWP_OK) return fail(st, "tuning");
+        printf("Launch shapes tuned: %.2f Gcell-updates/s in trial (cache %s)\n", rate, tune_cache);
+    }
+
     awp_solver *s = NULL;
     if ((st = awp_create(&p, &s)) != AWP_OK) return fail(st, "creating the solver");
+    if (tune_cache && *tune_cache && (st = awp_set_tuning(s, &tuned)) != AWP_OK) return fail(st, "applying the tuning");
     /* MEDIASTART 1 and 2 read INVEL; 3 reads the rank's partition file, which
      * on one GPU is the whole domain (AWP-GPU-SGT/src/mesh.c:97-118) */
     const char *media_path = p.mediastart == 3 ? "input_rst/mediapart/media0000000.bin" : in.invel;

@@ -178,3 +178,23 @@ def test_gpu_command_line_kinematic_source(tmp_path):
     bad[bad.index("--NST") + 1] = "3"
     r = subprocess.run(bad, cwd=tmp_path, capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "NST" in r.stderr
+
+
+@pytest.mark.gpu
+def test_autotuned_drop_in_run(tmp_path):
+    """AWP_AUTOTUNE_CACHE: the driver tunes the launch shapes for the grid
+    first, keeps them in the file, reuses them on the next run, and the SGT
+    file stays bit-identical to the oracle's."""
+    media, stf, pts = write_inputs(tmp_path)
+    in3d(tmp_path)
+    cache = tmp_path / "tune.txt"
+    env = dict(os.environ, AWP_AUTOTUNE_CACHE=str(cache))
+    ref = oracle_sgt(media, stf, pts).sgt()
+    for run in range(2):
+        r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=300,
+                           env=env)
+        assert r.returncode == 0, r.stderr + r.stdout
+        assert "Launch shapes tuned" in r.stdout
+        got = np.fromfile(tmp_path / "out" / "sgt" / "awp-strain", dtype=np.float32)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+        assert len(cache.read_text().splitlines()) == 1      # the second run reads it back
