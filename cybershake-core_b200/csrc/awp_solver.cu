@@ -621,8 +621,12 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
         s->staged_rpt_vel = env_int("AWP_TUNE_RPTV", 1) == 2 ? 2 : 1;
         /* two or three components share one stress work item (media tiles
          * and cell coefficients once per level): 14 % faster for fx+fy on
-         * 640 x 640 x 256, 3-4 % for fx+fy+fz on 400 x 400 x 200 */
-        s->staged_batch = env_int("AWP_TUNE_BATCH", 1) & 3;
+         * 640 x 640 x 256 (14.7 GB), 3-4 % for fx+fy+fz on 400 x 400 x 200
+         * (6.4 GB), but 10 % slower for fx+fy on 1400 x 1000 x 400 (78 GB),
+         * where one component at a time touches half as many pages at once;
+         * so by default up to 32 GiB of solver state */
+        const int batch_default = (double)awp_footprint_bytes(p, 0) <= 32.0 * (double)(1ull << 30) ? 1 : 0;
+        s->staged_batch = env_int("AWP_TUNE_BATCH", batch_default) & 3;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
