@@ -274,7 +274,8 @@ typedef struct {
     int kchunk_sweep;        /* two-sweep stepper: z levels per work item (8..nz)      */
     int staged_batch;        /* staged sweeps with all components of a tile in one work
                                 item, sharing media tiles and cell coefficients:
-                                bit 0 the stress sweep, bit 1 the velocity sweep */
+                                bit 0 the stress sweep, bit 1 the velocity sweep
+                                (default 1 up to 32 GiB of solver state, else 0) */
 } awp_tuning;
 
 awp_status awp_get_tuning(awp_solver *s, awp_tuning *t);
