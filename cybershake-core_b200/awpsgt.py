@@ -45,6 +45,7 @@ EXPORTED = [
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
     "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune", "awp_release_cached_memory",
+    "awp_set_field", "awp_checkpoint_write", "awp_checkpoint_read",
 ]
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
@@ -351,6 +352,9 @@ def load_library(path: str = LIB_PATH):
         "awp_get_sgt": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
         "awp_get_chkj": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
         "awp_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_checkpoint_write": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "awp_checkpoint_read": (C.c_int, [C.c_void_p, C.c_char_p, P(C.c_int)]),
         "awp_get_stats": (C.c_int, [C.c_void_p, P(Stats)]),
         "awp_reset": (C.c_int, [C.c_void_p]),
         "awp_destroy": (C.c_int, [C.c_void_p]),
@@ -542,6 +546,26 @@ class Solver:
         _check(self.lib.awp_get_field(self.h, comp, FIELDS.index(name), _ptr(out)))
         return out
 
+    def set_field(self, name: str, arr, comp: int = 0) -> None:
+        """awp_set_field: one state field from the padded host layout
+        [nz+4][ny+4][nx+4] float32."""
+        p = self.p
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        if a.shape != (p.nz + 4, p.ny + 4, p.nx + 4):
+            raise ValueError("set_field: shape %s, expected %s" % (a.shape, (p.nz + 4, p.ny + 4, p.nx + 4)))
+        _check(self.lib.awp_set_field(self.h, comp, FIELDS.index(name), _ptr(a)))
+
+    def checkpoint_write(self, directory: str) -> None:
+        """awp_checkpoint_write: the reference's checkpoint files in `directory`."""
+        _check(self.lib.awp_checkpoint_write(self.h, directory.encode()))
+
+    def checkpoint_read(self, directory: str) -> int:
+        """awp_checkpoint_read: restores the newest checkpoint; returns its step
+        (0 when none was found)."""
+        t = C.c_int(0)
+        _check(self.lib.awp_checkpoint_read(self.h, directory.encode(), C.byref(t)))
+        return t.value
+
     def run_async(self, nsteps: int):
         _check(self.lib.awp_run_async(self.h, nsteps))
 
@@ -709,7 +733,18 @@ def field_energy(ptrs: Sequence[int], layout: Layout, ncomp: int) -> np.ndarray:
 def field_energy_noalloc(ptrs: Sequence[int], layout: Layout, ncomp: int, out, stream: int = 0) -> None:
     """awp_field_energy_noalloc: enqueues the energy of the device arrays into
     the caller's device buffer `out` (a torch float64 tensor of >= ncomp
-    elements) on `stream` (a raw cudaStream_t handle) and returns at once."""
+    elements) on `stream` (a raw cudaStream_t handle) and returns at once.
+    The library looks up its scratch on the current device, so `out` must
+    live there."""
+    import torch
+    if not (isinstance(out, torch.Tensor) and out.is_cuda and out.dtype == torch.float64):
+        raise ValueError("field_energy_noalloc: out must be a CUDA float64 tensor")
+    if out.device.index != torch.cuda.current_device():
+        raise ValueError("field_energy_noalloc: out is on cuda:%d, the current device is cuda:%d"
+                         % (out.device.index, torch.cuda.current_device()))
+    if ncomp < 1 or out.numel() < ncomp or len(ptrs) < 3 * ncomp:
+        raise ValueError("field_energy_noalloc: %d components need 3*%d field pointers and %d outputs "
+                         "(got %d and %d)" % (ncomp, ncomp, ncomp, len(ptrs), out.numel()))
     arr = (C.c_void_p * len(ptrs))(*ptrs)
     _check(load_library().awp_field_energy_noalloc(arr, ncomp, C.byref(layout), C.c_void_p(out.data_ptr()),
                                                    C.c_void_p(stream)))

@@ -691,6 +691,8 @@ cudaError_t awp_launch_energy(const AwpEnergyArgs &a, double *partial, int nbloc
                               cudaStream_t st)
 {
     k_energy_partial<<<nblocks, AWP_EN_BLOCK, 0, st>>>(a, partial);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     k_energy_final<<<1, 32, 0, st>>>(partial, nblocks, a.ncomp, out, flag);
     return cudaGetLastError();
 }
@@ -931,39 +933,59 @@ cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st)
 /* kinematic source (IFAULT=5)                                         */
 /* ------------------------------------------------------------------ */
 
-/* moment tensor (xx yy zz xz yz xy) of a double couple, angles in radians */
+/* Unit double-couple moment tensor M = n d^T + d n^T from the fault normal n
+ * and the slip direction d of a fault with strike `str`, dip and rake
+ * (radians), after Aki & Richards, Quantitative Seismology (2002), section
+ * 4.5.  The vectors are written in the AWP axes (x east, y north, z up):
+ *   n = ( sin(dip) cos(str), -sin(dip) sin(str), cos(dip) )
+ *   d = ( cos(rake) sin(str) - cos(dip) sin(rake) cos(str),
+ *         cos(rake) cos(str) + cos(dip) sin(rake) sin(str),  sin(rake) sin(dip) )
+ * Output order: xx yy zz xz yz xy. */
 __device__ __forceinline__ void kin_mt(float str, float dip, float rake, float m[6])
 {
-    m[1] = -(sinf(dip) * cosf(rake) * sinf(2. * str) + sinf(2. * dip) * sinf(rake) * sinf(str) * sinf(str));
-    m[5] = sinf(dip) * cosf(rake) * cosf(2. * str) + 0.5 * (sinf(2. * dip) * sinf(rake) * sinf(2. * str));
-    m[4] = (cosf(dip) * cosf(rake) * cosf(str) + cosf(2. * dip) * sinf(rake) * sinf(str));
-    m[0] = sinf(dip) * cosf(rake) * sinf(2. * str) - sinf(2. * dip) * sinf(rake) * cosf(str) * cosf(str);
-    m[3] = (cosf(dip) * cosf(rake) * sinf(str) - cosf(2. * dip) * sinf(rake) * cosf(str));
-    m[2] = sinf(2. * dip) * sinf(rake);
+    float ss, cs, sd, cd, sr, cr;
+    sincosf(str, &ss, &cs);
+    sincosf(dip, &sd, &cd);
+    sincosf(rake, &sr, &cr);
+    const float n[3] = {sd * cs, -(sd * ss), cd};
+    const float d[3] = {cr * ss - cd * sr * cs, cr * cs + cd * sr * ss, sr * sd};
+    m[0] = 2.f * n[0] * d[0];
+    m[1] = 2.f * n[1] * d[1];
+    m[2] = 2.f * n[2] * d[2];
+    m[3] = n[0] * d[2] + n[2] * d[0];
+    m[4] = n[1] * d[2] + n[2] * d[1];
+    m[5] = n[0] * d[1] + n[1] * d[0];
 }
 
-/* slip-rate functions of unit area: Brune (1 / rise time = corner frequency),
- * Liu et al. (2006) and its 2010 revision, t measured from rupture */
-__device__ __forceinline__ float kin_brune(float freq, float t)
+/* Brune (1970) slip rate of unit slip for a rise time `rise`: with
+ * w = 2 pi / rise and x = w t, rate(t) = w x exp(-x) for t > 0. */
+__device__ __forceinline__ float kin_brune(float rise, float t)
 {
-    const float omega = freq * M_PI * 2.;
-    return t > 0. ? powf(omega, 2.f) * t * expf(-omega * t) : 0.f;
+    if (!(t > 0.f)) return 0.f;
+    const float w = 6.28318530717958647692f / rise, x = w * t;
+    return w * x * expf(-x);
 }
 
-__device__ __forceinline__ float kin_liu(float tau, float t, int rev2010)
+/* Slip rate of unit slip of Liu, Archuleta & Hartzell (2006, BSSA 96) and of
+ * its revision in Graves & Pitarka (2010, BSSA 100), both of one family set by
+ * the tail weight c (0.3 and 0.2).  With t1 = 0.13 rise, t2 = rise - t1,
+ * s = t / t1 and u = (t - t1) / t2 the shape is
+ *   0.7 (1 - cos(pi s)) + 0.6 sin(pi s / 2)     0    <= t < t1
+ *   1 - (1 - c) cos(pi s) + c cos(pi u)         t1   <= t < 2 t1
+ *   c (1 + cos(pi u))                           2 t1 <= t < rise
+ * and its integral over the rise time, (1.7 - c) t1 + 1.2 t1 / pi + c t2,
+ * normalises it to unit area. */
+__device__ __forceinline__ float kin_liu(float rise, float t, float c)
 {
-    const float tau1 = 0.13 * tau, tau2 = tau - tau1;
-    const float cn = rev2010 ? M_PI / (1.5 * M_PI * tau1 + 1.2 * tau1 + 0.2 * M_PI * tau2)
-                             : M_PI / (1.4 * M_PI * tau1 + 1.2 * tau1 + 0.3 * M_PI * tau2);
-    if (rev2010 && t < 0.) return 0.f;
-    if (t < tau1) return cn * (0.7 - 0.7 * cosf(M_PI * t / tau1) + 0.6 * sinf(0.5 * M_PI * t / tau1));
-    if (t < 2 * tau1)
-        return rev2010 ? cn * (1.0 - 0.8 * cosf(M_PI * t / tau1) + 0.2 * cosf(M_PI * (t - tau1) / tau2))
-                       : cn * (1.0 - 0.7 * cosf(M_PI * t / tau1) + 0.3 * cosf(M_PI * (t - tau1) / tau2));
-    if (t < tau)
-        return rev2010 ? cn * (0.2 + 0.2 * cosf(M_PI * (t - tau1) / tau2))
-                       : cn * (0.3 + 0.3 * cosf(M_PI * (t - tau1) / tau2));
-    return 0.f;
+    if (!(t > 0.f) || !(t < rise)) return 0.f;
+    const float t1 = 0.13f * rise, t2 = rise - t1;
+    const float area = (1.7f - c) * t1 + 1.2f * t1 / 3.14159265358979323846f + c * t2;
+    const float s = t / t1, u = (t - t1) / t2;
+    float f;
+    if (t < t1) f = 0.7f * (1.f - cospif(s)) + 0.6f * sinpif(0.5f * s);
+    else if (t < 2.f * t1) f = 1.f - (1.f - c) * cospif(s) + c * cospif(u);
+    else f = c * (1.f + cospif(u));
+    return f / area;
 }
 
 /* stress increments of every subfault at step n (= *step + 1), one thread per
@@ -979,11 +1001,12 @@ __global__ void k_kin_contrib(AwpPostArgs a)
     if (atime > r0[2]) {
         const int type = (int)r0[0];
         float m[6];
-        kin_mt(r1[0] / 180. * M_PI, r1[1] / 180. * M_PI, r1[2] / 180. * M_PI, m);
+        const float deg = 3.14159265358979323846f / 180.f;
+        kin_mt(r1[0] * deg, r1[1] * deg, r1[2] * deg, m);
         float stf = 0.f;
-        if (type == 1) stf = kin_brune(1. / r0[3], atime - r0[2]);
-        else if (type == 2) stf = kin_liu(r0[3], atime - r0[2], 0);
-        else if (type == 3) stf = kin_liu(r0[3], atime - r0[2], 1);
+        if (type == 1) stf = kin_brune(r0[3], atime - r0[2]);
+        else if (type == 2) stf = kin_liu(r0[3], atime - r0[2], 0.3f);
+        else if (type == 3) stf = kin_liu(r0[3], atime - r0[2], 0.2f);
         const int *ijk = a.src[q].ijk + 3 * j;
         const int c = a.g.idx(ijk[0], ijk[1], ijk[2]);
         float mu;

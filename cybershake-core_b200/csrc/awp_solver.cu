@@ -1498,6 +1498,223 @@ extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *o
     return AWP_OK;
 }
 
+/* float32 -> bfloat16, round to nearest even (the device's __float2bfloat16_rn;
+ * NaN stays a quiet NaN) */
+static uint16_t bf16_rn(float v)
+{
+    uint32_t b;
+    memcpy(&b, &v, 4);
+    if ((b & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((b >> 16) | 0x40);
+    b += 0x7fffu + ((b >> 16) & 1u);
+    return (uint16_t)(b >> 16);
+}
+
+extern "C" awp_status awp_set_field(awp_solver *s, int comp, int field, const float *in)
+{
+    if (!s || !in) return set_err(AWP_ERR_PARAM, "null argument");
+    if (field < 0 || field >= AWP_NF_STATE)
+        return set_err(AWP_ERR_PARAM, "awp_set_field: field %d is not a state field (0..%d)", field, AWP_NF_STATE - 1);
+    if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
+    if (!s->comp[0][comp].f[field]) return set_err(AWP_ERR_PARAM, "field %d not held by this solver", field);
+    if (s->pending) {
+        awp_status st = awp_sync(s);
+        if (st != AWP_OK) return st;
+    }
+    CU(cudaSetDevice(s->p.device));
+    CU(cudaStreamSynchronize(s->stream));
+    const AwpGeom &g = s->g;
+    const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4);
+    const int type = field >= AF_R1 ? s->rstore : AWP_STORE_F32;
+    uint16_t *tmp = NULL;
+    if (type != AWP_STORE_F32) {
+        tmp = (uint16_t *)malloc(w * rows * 2);
+        if (!tmp) return set_err(AWP_ERR_OOM, "host buffer");
+        for (size_t n = 0; n < w * rows; n++) tmp[n] = bf16_rn(in[n]);
+    }
+    /* both wavefield buffers of the fused stepper get the values, so the next
+     * step reads them whatever its buffer parity */
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+        void *dst = s->comp[b][comp].f[field];
+        if (!dst || (b == 1 && dst == s->comp[0][comp].f[field])) continue;
+        if (type == AWP_STORE_F32)
+            e = cudaMemcpy2D((float *)dst + (AWP_XO - 2), (size_t)g.px * sizeof(float), in, w * sizeof(float),
+                             w * sizeof(float), rows, cudaMemcpyHostToDevice);
+        else
+            e = cudaMemcpy2D((uint16_t *)dst + (AWP_XO - 2), (size_t)g.px * 2, tmp, w * 2, w * 2, rows,
+                             cudaMemcpyHostToDevice);
+    }
+    free(tmp);
+    if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "awp_set_field: %s", cudaGetErrorString(e));
+    return AWP_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* checkpoint / restart (pmcl3d.f:1018-1097 read, 1967-2045 write)     */
+/* ------------------------------------------------------------------ */
+
+#define AWP_CKP_MAGIC "AWPSGTCK"
+#define AWP_CKP_VERSION 1
+
+/* header of the ckpsgt file: what the reference's checkpoint does not hold
+ * (it writes SGT chunks as it goes), so that a resumed solve ends with the
+ * same SGT file image and CHKJ series as an uninterrupted one */
+struct CkpSgtHeader {
+    char magic[8];
+    int32_t version, step, nt, npts;
+    int64_t nt_file, sgt_floats;
+};
+
+static awp_status write_all(FILE *f, const void *p, size_t bytes, const char *path)
+{
+    if (bytes && fwrite(p, 1, bytes, f) != bytes) return set_err(AWP_ERR_IO, "cannot write %s", path);
+    return AWP_OK;
+}
+
+static awp_status read_all(FILE *f, void *p, size_t bytes, const char *path)
+{
+    if (bytes && fread(p, 1, bytes, f) != bytes) return set_err(AWP_ERR_IO, "%s is short", path);
+    return AWP_OK;
+}
+
+extern "C" awp_status awp_checkpoint_write(awp_solver *s, const char *dir)
+{
+    if (!s || !dir) return set_err(AWP_ERR_PARAM, "null argument");
+    awp_status st = awp_sync(s);
+    if (st != AWP_OK) return st;
+    const awp_params *p = &s->p;
+    const size_t nvol = (size_t)(p->nx + 4) * (p->ny + 4) * (p->nz + 4);
+    float *buf = (float *)malloc(nvol * sizeof(float));
+    float *aux = (float *)malloc(sizeof(float) * ((size_t)3 * p->nt + (size_t)s->sgt_file_floats + 1));
+    if (!buf || !aux) { free(buf); free(aux); return set_err(AWP_ERR_OOM, "host buffer"); }
+    char path[1200], tmpp[1300];
+    const int step = s->steps_done;
+    for (int q = 0; q < p->ncomp && st == AWP_OK; q++) {
+        /* ckp<rank><step>.bin: five records [u1 v1 w1] [xx yy zz] [xy xz yz] [r1 r2 r3] [r4 r5 r6],
+         * each array (nx+4)(ny+4)(nz+4) float32 with its ghost cells, x fastest */
+        snprintf(path, sizeof path, "%s/ckp%07d%07d.bin", dir, q, step);
+        FILE *f = fopen(path, "wb");
+        if (!f) { st = set_err(AWP_ERR_IO, "cannot create %s", path); break; }
+        for (int fld = 0; fld < AWP_NF_STATE && st == AWP_OK; fld++) {
+            if (s->comp[0][q].f[fld]) st = awp_get_field(s, q, fld, buf);
+            else memset(buf, 0, nvol * sizeof(float));      /* elastic scheme: no memory variables */
+            if (st == AWP_OK) st = write_all(f, buf, nvol * sizeof(float), path);
+        }
+        if (fclose(f) != 0 && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", path);
+        if (st != AWP_OK) break;
+        /* ckpdy<rank><step>.bin: u2, broken (dynamic-rupture arrays, zero here), mu */
+        snprintf(path, sizeof path, "%s/ckpdy%07d%07d.bin", dir, q, step);
+        f = fopen(path, "wb");
+        if (!f) { st = set_err(AWP_ERR_IO, "cannot create %s", path); break; }
+        memset(buf, 0, nvol * sizeof(float));
+        st = write_all(f, buf, nvol * sizeof(float), path);
+        if (st == AWP_OK) st = write_all(f, buf, nvol * sizeof(float), path);
+        if (st == AWP_OK) st = awp_get_field(s, q, AWP_NF_STATE + AM_MU, buf);
+        if (st == AWP_OK) st = write_all(f, buf, nvol * sizeof(float), path);
+        if (fclose(f) != 0 && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", path);
+        if (st != AWP_OK) break;
+        /* ckpsgt<rank><step>.bin: the SGT file image and CHKJ series so far */
+        snprintf(path, sizeof path, "%s/ckpsgt%07d%07d.bin", dir, q, step);
+        f = fopen(path, "wb");
+        if (!f) { st = set_err(AWP_ERR_IO, "cannot create %s", path); break; }
+        CkpSgtHeader h;
+        memset(&h, 0, sizeof h);
+        memcpy(h.magic, AWP_CKP_MAGIC, 8);
+        h.version = AWP_CKP_VERSION; h.step = step; h.nt = p->nt; h.npts = s->npts;
+        h.nt_file = s->nt_file; h.sgt_floats = s->sgt_file_floats;
+        st = write_all(f, &h, sizeof h, path);
+        if (st == AWP_OK) st = awp_get_chkj(s, q, aux);
+        if (st == AWP_OK && s->sgt_file_floats > 0) st = awp_get_sgt(s, q, aux + (size_t)3 * p->nt);
+        if (st == AWP_OK)
+            st = write_all(f, aux, sizeof(float) * ((size_t)3 * p->nt + (size_t)s->sgt_file_floats), path);
+        if (fclose(f) != 0 && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", path);
+        if (st != AWP_OK) break;
+        /* ckp<rank>.hdr names the step last, once the data files are complete
+         * (written to a temporary name and renamed into place) */
+        snprintf(path, sizeof path, "%s/ckp%07d.hdr", dir, q);
+        snprintf(tmpp, sizeof tmpp, "%s.tmp", path);
+        f = fopen(tmpp, "w");
+        if (!f) { st = set_err(AWP_ERR_IO, "cannot create %s", tmpp); break; }
+        fprintf(f, "%12d\n", step);
+        if (fclose(f) != 0 || rename(tmpp, path) != 0) st = set_err(AWP_ERR_IO, "cannot write %s", path);
+    }
+    free(buf);
+    free(aux);
+    return st;
+}
+
+extern "C" awp_status awp_checkpoint_read(awp_solver *s, const char *dir, int *step_out)
+{
+    if (!s || !dir) return set_err(AWP_ERR_PARAM, "null argument");
+    if (step_out) *step_out = 0;
+    const awp_params *p = &s->p;
+    /* the step to resume from: the smallest over the components' headers; a
+     * missing header counts as 0 (pmcl3d.f:1019-1036, MPI_MIN over ranks) */
+    char path[1200];
+    int t0 = INT32_MAX;
+    for (int q = 0; q < p->ncomp; q++) {
+        snprintf(path, sizeof path, "%s/ckp%07d.hdr", dir, q);
+        FILE *f = fopen(path, "r");
+        int t = 0;
+        if (f) {
+            if (fscanf(f, "%d", &t) != 1) t = 0;
+            fclose(f);
+        }
+        if (t < t0) t0 = t;
+    }
+    if (t0 <= 0) return AWP_OK;
+    if (t0 > p->nt) return set_err(AWP_ERR_PARAM, "checkpoint step %d beyond the %d steps of the solve", t0, p->nt);
+    if (!s->media_loaded) return set_err(AWP_ERR_STATE, "media must be loaded before restoring a checkpoint");
+    awp_status st = awp_sync(s);
+    if (st != AWP_OK) return st;
+    const size_t nvol = (size_t)(p->nx + 4) * (p->ny + 4) * (p->nz + 4);
+    float *buf = (float *)malloc(nvol * sizeof(float));
+    float *aux = (float *)malloc(sizeof(float) * ((size_t)3 * p->nt + (size_t)s->sgt_file_floats + 1));
+    if (!buf || !aux) { free(buf); free(aux); return set_err(AWP_ERR_OOM, "host buffer"); }
+    /* the first step of the restored solve must not insert addsrc(1) again */
+    if (!s->started) st = start_if_needed(s);
+    for (int q = 0; q < p->ncomp && st == AWP_OK; q++) {
+        snprintf(path, sizeof path, "%s/ckp%07d%07d.bin", dir, q, t0);
+        FILE *f = fopen(path, "rb");
+        if (!f) { st = set_err(AWP_ERR_IO, "checkpoint %s missing", path); break; }
+        for (int fld = 0; fld < AWP_NF_STATE && st == AWP_OK; fld++) {
+            st = read_all(f, buf, nvol * sizeof(float), path);
+            if (st == AWP_OK && s->comp[0][q].f[fld]) st = awp_set_field(s, q, fld, buf);
+        }
+        fclose(f);
+        if (st != AWP_OK) break;
+        CU(cudaSetDevice(p->device));
+        snprintf(path, sizeof path, "%s/ckpsgt%07d%07d.bin", dir, q, t0);
+        f = fopen(path, "rb");
+        /* a checkpoint without it (written by the reference) restores the
+         * wavefield only: SGT samples and CHKJ before the step stay zero */
+        if (!f) continue;
+        CkpSgtHeader h;
+        st = read_all(f, &h, sizeof h, path);
+        if (st == AWP_OK && (memcmp(h.magic, AWP_CKP_MAGIC, 8) != 0 || h.version != AWP_CKP_VERSION || h.step != t0 ||
+                             h.nt != p->nt || h.npts != s->npts || h.nt_file != s->nt_file ||
+                             h.sgt_floats != s->sgt_file_floats))
+            st = set_err(AWP_ERR_IO, "%s does not match this solve (step, nt, points or SGT size)", path);
+        if (st == AWP_OK)
+            st = read_all(f, aux, sizeof(float) * ((size_t)3 * p->nt + (size_t)s->sgt_file_floats), path);
+        fclose(f);
+        if (st != AWP_OK) break;
+        CU(cudaMemcpy(s->chkj[q], aux, sizeof(float) * 3 * (size_t)p->nt, cudaMemcpyHostToDevice));
+        if (s->sgt_file_floats > 0)
+            CU(cudaMemcpy(s->sgt_file[q], aux + (size_t)3 * p->nt, sizeof(float) * (size_t)s->sgt_file_floats,
+                          cudaMemcpyHostToDevice));
+    }
+    free(buf);
+    free(aux);
+    if (st != AWP_OK) return st;
+    /* the device step counter drives the source, CHKJ and SGT kernels */
+    CU(cudaMemcpy(s->step, &t0, sizeof(int), cudaMemcpyHostToDevice));
+    s->steps_done = t0;
+    if (p->monitor_every > 0) s->next_check = (t0 / p->monitor_every + 1) * p->monitor_every;
+    if (step_out) *step_out = t0;
+    return AWP_OK;
+}
+
 extern "C" awp_status awp_get_stats(awp_solver *s, awp_stats *o)
 {
     if (!s || !o) return set_err(AWP_ERR_PARAM, "null argument");
@@ -1619,7 +1836,9 @@ static std::mutex g_energy_scratch_mu;
 
 /* Device address of the scratch on the current device: looked up once per
  * device (cudaGetSymbolAddress, which may load this module onto the device --
- * the reason the first call on a device is the set-up call), then cached. */
+ * the reason the first call on a device is the set-up call), then cached for
+ * the life of the process.  A device reset (cudaDeviceReset) between calls
+ * would leave the cached address stale; the header rules that out. */
 static awp_status energy_scratch(double **addr)
 {
     int dev = 0;
@@ -1649,6 +1868,12 @@ extern "C" awp_status awp_field_energy_noalloc(const float *const *fields, int n
     awp_status st = check_layout(fields, ncomp, L);
     if (st != AWP_OK) return st;
     if (!out) return set_err(AWP_ERR_PARAM, "null output");
+    /* an error left pending by earlier work of this thread is not this call's
+     * failure: report it without clearing it, and launch nothing */
+    const cudaError_t pend = cudaPeekAtLastError();
+    if (pend != cudaSuccess)
+        return set_err(AWP_ERR_CUDA, "awp_field_energy_noalloc: a CUDA error from earlier work is pending: %s",
+                       cudaGetErrorString(pend));
     double *partial = NULL;
     st = energy_scratch(&partial);
     if (st != AWP_OK) return st;

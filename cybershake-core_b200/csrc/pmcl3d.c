@@ -16,6 +16,8 @@
  * pass is needed.  With AWP_AUTOTUNE_CACHE=<file> the launch shapes are tuned
  * for the job's grid before the solve (awp_autotune on the homogeneous
  * medium, a few seconds once per grid and GPU model) and kept in that file.
+ * CHECKPOINT > 0 in IN3D resumes from output_ckp/ when a checkpoint is there
+ * and writes one every CHECKPOINT steps (pmcl3d.f:1018-1097, 1967-2045).
  */
 #include <math.h>
 #include <stdio.h>
@@ -214,7 +216,27 @@ int main(int argc, char **argv)
     if (in.gpu_cli) write_chkp_gpu(&in, &stats);
     else write_chkp_fortran(&in, &stats);
 
-    if ((st = awp_run(s, p.nt, NULL)) != AWP_OK) return fail(st, "time stepping");
+    if (in.checkpoint > 0) {
+        /* pmcl3d.f:1018-1097: resume from output_ckp/ when a checkpoint is
+         * there; pmcl3d.f:1967-2045: a checkpoint after every step i with
+         * mod(i, CHECKPOINT) == 0 */
+        mkdir("output_ckp", 0755);
+        int t0 = 0;
+        if ((st = awp_checkpoint_read(s, "output_ckp", &t0)) != AWP_OK) return fail(st, "reading the checkpoint");
+        if (t0 > 0) printf("Checkpoint found, starting from step %d\n", t0);
+        for (int done = t0; done < p.nt;) {
+            int n = in.checkpoint - done % in.checkpoint;
+            if (n > p.nt - done) n = p.nt - done;
+            if ((st = awp_run(s, n, NULL)) != AWP_OK) return fail(st, "time stepping");
+            done += n;
+            if (done % in.checkpoint == 0) {
+                printf("Writing checkpoint file\n");
+                if ((st = awp_checkpoint_write(s, "output_ckp")) != AWP_OK) return fail(st, "writing the checkpoint");
+            }
+        }
+    } else if ((st = awp_run(s, p.nt, NULL)) != AWP_OK) {
+        return fail(st, "time stepping");
+    }
     awp_get_stats(s, &stats);
     printf("time loop: %d steps in %.3f s, %.3f Gcell-updates/s\n", (int)stats.steps_done, stats.seconds_loop,
            stats.gcell_updates_per_s);

@@ -178,6 +178,35 @@ awp_status awp_get_chkj(awp_solver *s, int comp, float *out);
  * 15..19 = lam mu d1 qp qs (compliances as stored by structure.f:488-519). */
 awp_status awp_get_field(awp_solver *s, int comp, int field, float *out);
 
+/* Sets one state field (0..14, numbering as awp_get_field) of one component
+ * from the padded host layout in[(k+1)][(j+1)][(i+1)], extents (nz+4, ny+4,
+ * nx+4), float32; memory variables stored in 16 bits are rounded to nearest.
+ * Used by the checkpoint restart below and to start a solve from a given
+ * state.  Replaces the state part of the checkpoint read
+ * (AWP-ODC-SGT/src/pmcl3d.f:1044-1056). */
+awp_status awp_set_field(awp_solver *s, int comp, int field, const float *in);
+
+/* Checkpoint of the state after the steps done so far, in the reference's
+ * files (AWP-ODC-SGT/src/pmcl3d.f:1967-2045; the component index stands for
+ * the MPI rank):
+ *   dir/ckp<rank:7><step:7>.bin    records [u1 v1 w1] [xx yy zz] [xy xz yz]
+ *                                  [r1 r2 r3] [r4 r5 r6], each array
+ *                                  (nx+4)(ny+4)(nz+4) float32 with ghosts;
+ *   dir/ckpdy<rank:7><step:7>.bin  u2, broken (zero: no dynamic rupture), mu;
+ *   dir/ckp<rank:7>.hdr            the step, written last;
+ * plus dir/ckpsgt<rank:7><step:7>.bin (this library's addition: the SGT file
+ * image and CHKJ series so far, which the reference writes out as it goes)
+ * so that a resumed solve ends with the files of an uninterrupted one. */
+awp_status awp_checkpoint_write(awp_solver *s, const char *dir);
+
+/* Restores the newest checkpoint in `dir` (the smallest step over the
+ * components' .hdr files, as pmcl3d.f:1019-1036 takes the minimum over
+ * ranks); *step receives it, 0 when there is none (then nothing changes).
+ * Media, sources and points must be set first, as for a new solve.  Without
+ * the ckpsgt file only the wavefield is restored.  The next awp_run continues
+ * with step *step + 1 (pmcl3d.f:1103). */
+awp_status awp_checkpoint_read(awp_solver *s, const char *dir, int *step);
+
 /* Statistics of the solver (timers, throughput, media extremes for CHKP). */
 awp_status awp_get_stats(awp_solver *s, awp_stats *st);
 
@@ -231,9 +260,13 @@ awp_status awp_field_energy(const float *const *fields, int ncomp, const awp_lay
  * device array of the library (592 x 3 doubles), so ncomp is at most 3 and a
  * larger count is rejected with AWP_ERR_PARAM.  The first call on a device
  * does a one-time set-up (looks up that array's device address) and should
- * come before any stream capture.  Calls on one device share the array: calls
- * that overlap in time, from other streams or threads, race and must be
- * serialized by the caller. */
+ * come before any stream capture; its address is kept for the life of the
+ * process, so the device must not be reset (cudaDeviceReset, or anything else
+ * that destroys its primary context) between calls.  Calls on one device
+ * share the array: calls that overlap in time, from other streams or threads,
+ * race and must be serialized by the caller.  A CUDA error left pending by
+ * earlier work of the calling thread is reported (AWP_ERR_CUDA) without being
+ * cleared, and nothing is launched. */
 awp_status awp_field_energy_noalloc(const float *const *fields, int ncomp, const awp_layout *L, double *out,
                                     void *stream);
 

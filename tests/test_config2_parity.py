@@ -1,0 +1,70 @@
+"""Parity on the bench's own workload: 400x400x200, h = 100 m, dt = 5 ms,
+fx+fy+fz stepped together by the default stepper (the staged sweeps, the
+stress sweep with the three components side by side), 5000 SGT points, the
+layered + 5 % perturbed medium.
+
+The solve starts from a state filled with bounded noise (every wavefield and
+memory-variable cell of the interior; ghosts zero, as a solve keeps them), so
+that every cell of every component is active from the first step on, and runs
+60 steps with an SGT sample every 10.  Every field of every component, the
+CHKJ series and the SGT file image must equal the FP32 oracle's bit for bit.
+"""
+import numpy as np
+import pytest
+
+import awp_inputs as ai
+import awpsgt
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+NT = 60
+# magnitudes of the noise per state field: velocities, stresses, memory variables
+SCALE = [1e-2] * 3 + [1e6] * 6 + [1e3] * 6
+
+
+def noise(w, q, f):
+    a = np.zeros((w.nz + 4, w.ny + 4, w.nx + 4), np.float32)
+    rng = np.random.default_rng(1000 * (q + 1) + f)
+    a[2:-2, 2:-2, 2:-2] = (rng.uniform(-1.0, 1.0, (w.nz, w.ny, w.nx)) * SCALE[f]).astype(np.float32)
+    return a
+
+
+def test_config2_workload_bit_exact_from_a_noise_state():
+    w = ai.config(2)
+    media = w.media()
+    pts = w.points()
+    assert (w.nx, w.ny, w.nz, len(pts), w.igreen) == (400, 400, 200, 5000, (1, 2, 3))
+    kw = dict(nd=20, arbc=0.92, fl=w.fl, fh=w.fh, fp=w.fp, socalq=w.socalq, ntiskp_sgt=10, write_step=6)
+    stfs = [w.stf(q)[:NT] for q in range(3)]
+    p = awpsgt.make_params(w.nx, w.ny, w.nz, w.dh, w.dt, NT, igreen=w.igreen, nst=NT, **kw)
+    with awpsgt.Solver(p) as s:
+        tune = s.tuning()
+        assert tune.staged_batch & 1                        # components side by side in the stress sweep
+        s.load_media(media)
+        for q in range(3):
+            s.set_source(q, [w.src_xyz], stfs[q])
+        s.set_points(pts)
+        for q in range(3):
+            for f in range(15):
+                s.set_field(awpsgt.FIELDS[f], noise(w, q, f), q)
+        s.run(NT)
+        for q in range(3):
+            o = oracle.Oracle(nx=w.nx, ny=w.ny, nz=w.nz, dh=w.dh, dt=w.dt, nt=NT, nst=NT, igreen=w.igreen[q], **kw)
+            o.load_media(media)
+            o.set_source([w.src_xyz], stfs[q])
+            o.set_points(pts)
+            for f in range(15):
+                o.set_field(oracle.FIELDS[f], noise(w, q, f))
+            o.run(NT)
+            bad = []
+            for f in oracle.FIELDS[:15]:
+                a, b = s.field(f, q), o.field(f)
+                if not np.array_equal(a.view(np.uint32), b.view(np.uint32)):
+                    bad.append((q, f, np.argwhere(a.view(np.uint32) != b.view(np.uint32))[0].tolist()))
+            assert not bad, bad
+            sg = s.sgt(q)
+            assert sg.size == 5000 * 6 * 6 and np.abs(sg).max() > 0
+            assert np.array_equal(sg.view(np.uint32), o.sgt().view(np.uint32))
+            assert np.array_equal(s.chkj(q).view(np.uint32), o.chkj().view(np.uint32))
+            o.close()
