@@ -28,7 +28,7 @@ AWP_OK = 0
 STATUS = {0: "AWP_OK", 1: "AWP_ERR_IO", 2: "AWP_ERR_PARAM", 3: "AWP_ERR_OOM", 4: "AWP_ERR_CUDA",
           5: "AWP_ERR_UNSTABLE", 6: "AWP_ERR_TIMEOUT", 7: "AWP_ERR_STATE", 8: "AWP_ERR_BUSY",
           9: "AWP_ERR_CANCELLED"}
-PREC = {"f32": 0, "bf16": 1, "f16": 2, "mixed": 3}
+PREC = {"f32": 0, "bf16": 1, "f16": 2, "mixed": 3, "bfp": 4}
 KERNEL = {"auto": 0, "two_sweep": 1, "fused": 2, "staged": 3}
 FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3", "r4", "r5", "r6",
           "lam", "mu", "d1", "qp", "qs"]

@@ -17,10 +17,12 @@
 
 #define AWP_XO 8
 #define AWP_NF_STATE 15   /* u v w xx yy zz xy xz yz r1..r6 */
+#define AWP_NF_ARRAYS 16  /* the state plus the exponent words of 16-bit block floating point r1..r6 */
 
 enum {
     AF_U = 0, AF_V, AF_W, AF_XX, AF_YY, AF_ZZ, AF_XY, AF_XZ, AF_YZ,
-    AF_R1, AF_R2, AF_R3, AF_R4, AF_R5, AF_R6
+    AF_R1, AF_R2, AF_R3, AF_R4, AF_R5, AF_R6,
+    AF_RX   /* AWP_STORE_BFP only: per cell, the exponents of (r1 r2 r3) and (r4 r5 r6) */
 };
 enum { AM_LAM = 0, AM_MU, AM_D1, AM_QP, AM_QS, AM_N };
 
@@ -37,7 +39,7 @@ struct AwpGeom {
 };
 
 struct AwpComp {
-    float *f[AWP_NF_STATE];
+    float *f[AWP_NF_ARRAYS];
 };
 
 template <int NC>
@@ -49,8 +51,24 @@ struct AwpMedia {
     float *m[AM_N];
 };
 
-/* storage type of the media arrays and of r1..r6 */
-enum { AWP_STORE_F32 = 0, AWP_STORE_BF16 = 1, AWP_STORE_F16 = 2 };
+/* storage type of the media arrays and of r1..r6.  AWP_STORE_BFP (r1..r6
+ * only): 16-bit block floating point -- each memory variable an int16
+ * mantissa, the three normal (r1 r2 r3) and the three shear (r4 r5 r6)
+ * memory variables of a cell sharing one exponent each, both exponents in
+ * one uint16 word per cell (AF_RX: low byte r1..r3, high byte r4..r6). */
+enum { AWP_STORE_F32 = 0, AWP_STORE_BF16 = 1, AWP_STORE_F16 = 2, AWP_STORE_BFP = 3 };
+
+/* bytes of the six memory variables of one cell in a storage type */
+static inline int awp_r_bytes(int rstore) { return rstore == AWP_STORE_F32 ? 24 : (rstore == AWP_STORE_BFP ? 14 : 12); }
+
+/* Block floating point of three values sharing an exponent, the host and
+ * device rule: e = the float exponent field of the largest magnitude; with
+ * e >= 15 each value v is stored as the integer nearest (ties to even) to
+ * v * 2^(141 - e) clamped to [-32767, 32767] (|v| * 2^(141 - e) < 2^15), and
+ * read back as m * 2^(max(e, 15) - 141); e < 15 stores zero mantissas and a
+ * zero exponent.  Both scalings are powers of two (exact), and decoding then
+ * encoding again returns the same mantissas and exponent. */
+#define AWP_BFP_EMIN 15u
 
 /* binary16 arrays hold value * scale (a power of two); inv = 1/scale */
 struct AwpMediaScale {

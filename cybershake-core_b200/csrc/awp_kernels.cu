@@ -301,12 +301,10 @@ k_str(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> cs, const float *__restrict__ cx,
                 Stress6 o;
                 if (nve == 1) {
                     float r[6];
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)cp.f[AF_R1 + a], c, 1.0f);
+                    RVars<TR>::ld(cp, c, r);
                     const VelDiff d = vel_diff(V);
                     o = str_visco(kc, d, s, r, dth, dt, dh1);
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)cp.f[AF_R1 + a], c, r[a], 1.0f);
+                    RVars<TR>::st(cp, c, r);
                 } else {
                     o = str_elastic(kc, V, s, dth);
                 }
@@ -468,12 +466,10 @@ k_fused(AwpGeom g, MediaT<TM> md, AwpCompSet<NC> old, AwpCompSet<NC> nw, const f
                 Stress6 ns;
                 if (nve == 1) {
                     float r[6];
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)o.f[AF_R1 + a], c, 1.0f);
+                    RVars<TR>::ld(o, c, r);
                     const VelDiff d = vel_diff(V);
                     ns = str_visco(kc, d, s, r, dth, dt, dh1);
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)o.f[AF_R1 + a], c, r[a], 1.0f);
+                    RVars<TR>::st(o, c, r);
                 } else {
                     ns = str_elastic(kc, V, s, dth);
                 }
@@ -906,6 +902,7 @@ static cudaError_t launch_part_nc(const AwpStepArgs &s, int part, cudaStream_t s
     if (s.md.type == AWP_STORE_BF16) return launch_part_t<NC, __nv_bfloat16, __nv_bfloat16>(s, part, st);
     if (s.md.type == AWP_STORE_F16) return launch_part_t<NC, __half, __nv_bfloat16>(s, part, st);
     if (s.rtype == AWP_STORE_BF16) return launch_part_t<NC, float, __nv_bfloat16>(s, part, st);
+    if (s.rtype == AWP_STORE_BFP) return launch_part_t<NC, float, RBfp>(s, part, st);
     return launch_part_t<NC, float, float>(s, part, st);
 }
 

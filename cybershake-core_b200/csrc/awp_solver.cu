@@ -185,7 +185,10 @@ static int store_of(const awp_params *p)
     return p->precision == AWP_PREC_BF16 ? AWP_STORE_BF16 : p->precision == AWP_PREC_F16 ? AWP_STORE_F16 : AWP_STORE_F32;
 }
 /* storage of r1..r6 */
-static int rstore_of(const awp_params *p) { return p->precision == AWP_PREC_F32 ? AWP_STORE_F32 : AWP_STORE_BF16; }
+static int rstore_of(const awp_params *p)
+{
+    return p->precision == AWP_PREC_F32 ? AWP_STORE_F32 : (p->precision == AWP_PREC_BFP ? AWP_STORE_BFP : AWP_STORE_BF16);
+}
 static int fused_of(const awp_params *p) { return p->kernel == AWP_KERNEL_FUSED; }
 static double media_word(int store) { return store == AWP_STORE_F32 ? 4.0 : 2.0; }
 
@@ -194,14 +197,13 @@ extern "C" double awp_bytes_per_cell_update(const awp_params *p)
     const int nc = p->ncomp < 1 ? 1 : p->ncomp;
     const int st = store_of(p);
     const double mb = media_word(st);
-    const double rb = media_word(rstore_of(p));        /* r1..r6 word       */
+    const double rcell = (p->nve == 1) ? 2.0 * awp_r_bytes(rstore_of(p)) : 0.0;   /* r1..r6 read+write */
     const int nmedia = (p->nve == 1) ? 5 : 3;
-    const int nr = (p->nve == 1) ? 12 : 0;             /* r1..r6 read+write */
     double state;
     if (fused_of(p))
-        state = 18 * 4.0 + nr * rb;                    /* u v w + 6 stresses R+W */
+        state = 18 * 4.0 + rcell;                      /* u v w + 6 stresses R+W */
     else
-        state = 12 * 4.0 + 15 * 4.0 + nr * rb;         /* vel R9 W3; stress R9 W6 */
+        state = 12 * 4.0 + 15 * 4.0 + rcell;           /* vel R9 W3; stress R9 W6 */
     return (nc * state + nmedia * mb) / nc;
 }
 
@@ -239,8 +241,8 @@ extern "C" int64_t awp_footprint_bytes(const awp_params *p, int npts)
     const int st = store_of(p);
     const double mb = media_word(st);
     const int nbuf = fused_of(p) ? 2 : 1;
-    const double rb = media_word(rstore_of(p));
-    int64_t b = (int64_t)g.vol * (int64_t)(nc * (9 * 4 * nbuf + (p->nve == 1 ? 6 * rb : 0)));
+    const double rcell = p->nve == 1 ? awp_r_bytes(rstore_of(p)) : 0;
+    int64_t b = (int64_t)g.vol * (int64_t)(nc * (9 * 4 * nbuf + rcell));
     b += (int64_t)g.vol * (int64_t)(AM_N * 4);                        /* FP32 media during ingest */
     if (st != AWP_STORE_F32) b += (int64_t)g.vol * (int64_t)(AM_N * mb);
     b += file_floats_of(p, npts) * 4 * nc;
@@ -282,7 +284,7 @@ static void free_all(awp_solver *s)
     for (int b = 0; b < 2; b++)
         if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
     for (int q = 0; q < AWP_MAX_COMP; q++) {
-        for (int f = 0; f < AWP_NF_STATE; f++) {
+        for (int f = 0; f < AWP_NF_ARRAYS; f++) {
             dfree_field(s, s->comp[0][q].f[f]);
             if (f < AF_R1 && s->comp[1][q].f[f] != s->comp[0][q].f[f]) dfree_field(s, s->comp[1][q].f[f]);
         }
@@ -472,10 +474,10 @@ static awp_status check_params(const awp_params *p)
     if (p->kinematic != 0 && p->kinematic != 1) return set_err(AWP_ERR_PARAM, "kinematic must be 0 or 1");
     if (p->kinematic && p->nst != 2)
         return set_err(AWP_ERR_PARAM, "a kinematic source (IFAULT=5) needs NST = 2 (two rows per subfault)");
-    if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_MIXED) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
+    if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_BFP) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
     if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_STAGED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
     if (p->kernel == AWP_KERNEL_STAGED && store_of(p) != AWP_STORE_F32)
-        return set_err(AWP_ERR_PARAM, "the staged stepper reads FP32 media (precision f32 or mixed)");
+        return set_err(AWP_ERR_PARAM, "the staged stepper reads FP32 media (precision f32, mixed or bfp)");
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
         int ig = p->igreen[q];
@@ -531,9 +533,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     TRYCU(cudaEventCreate(&s->ev0));
     TRYCU(cudaEventCreate(&s->ev1));
     for (int q = 0; q < p->ncomp; q++) {
-        for (int f = 0; f < AWP_NF_STATE; f++) {
+        for (int f = 0; f < AWP_NF_ARRAYS; f++) {
             if (f >= AF_R1) {
-                if (p->nve == 0) continue;
+                if (p->nve == 0 || (f == AF_RX && s->rstore != AWP_STORE_BFP)) continue;
                 TRY(dalloc_field(s, (void **)&s->comp[0][q].f[f], rb));
                 TRYCU(cudaMemsetAsync(s->comp[0][q].f[f], 0, rb, s->stream));
                 s->comp[1][q].f[f] = s->comp[0][q].f[f];
@@ -1324,14 +1326,13 @@ static double part_bytes(const awp_solver *s, int part)
     const double cells = (double)p->nx * p->ny * p->nz;
     const double nc = p->ncomp;
     const double mb = media_word(s->store);
-    const double rb = media_word(s->rstore);
-    const int nr = p->nve == 1 ? 12 : 0;
+    const double rcell = p->nve == 1 ? 2.0 * awp_r_bytes(s->rstore) : 0.0;   /* r1..r6 read+write */
     const int nmed = p->nve == 1 ? 5 : 3;
     switch (part) {
     case AWP_PART_VEL: return cells * (nc * 12 * 4.0 + mb);                          /* R 9 W 3 + d1 */
     case AWP_PART_FSVEL: return (double)p->nx * p->ny * (nc * (8 * 4.0) + 2 * mb);
-    case AWP_PART_STR: return cells * (nc * (15 * 4.0 + nr * rb) + (nmed - 1) * mb);
-    case AWP_PART_FUSED: return cells * (nc * (18 * 4.0 + nr * rb) + nmed * mb);
+    case AWP_PART_STR: return cells * (nc * (15 * 4.0 + rcell) + (nmed - 1) * mb);
+    case AWP_PART_FUSED: return cells * (nc * (18 * 4.0 + rcell) + nmed * mb);
     }
     return 0.0;
 }
@@ -1447,6 +1448,89 @@ extern "C" awp_status awp_get_chkj(awp_solver *s, int comp, float *out)
     return AWP_OK;
 }
 
+/* 16-bit block floating point of r1..r6 on the host (the rule of
+ * awp_internal.h, as the device kernels apply it) */
+static float f_of_bits(uint32_t b) { float v; memcpy(&v, &b, 4); return v; }
+static uint32_t bits_of_f(float v) { uint32_t b; memcpy(&b, &v, 4); return b; }
+
+static float bfp_down(uint32_t e) { return f_of_bits(((e < AWP_BFP_EMIN ? AWP_BFP_EMIN : e) - 14u) << 23); }
+
+static uint32_t bfp_enc3_host(const float v[3], int16_t m[3])
+{
+    const float mx = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
+    const uint32_t e = bits_of_f(mx) >> 23;
+    if (e < AWP_BFP_EMIN) {
+        m[0] = m[1] = m[2] = 0;
+        return 0u;
+    }
+    const float up = f_of_bits((268u - e) << 23);
+    for (int a = 0; a < 3; a++) m[a] = (int16_t)lrintf(fminf(fmaxf(v[a] * up, -32767.f), 32767.f));
+    return e;
+}
+
+/* the three mantissa arrays of r group g (0: r1..r3, 1: r4..r6) and the
+ * exponent words of component q, in the padded host layout */
+static awp_status bfp_fetch(awp_solver *s, int q, int grp, int16_t *m[3], uint16_t *x)
+{
+    const AwpGeom &g = s->g;
+    const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4);
+    const AwpComp &c = s->comp[0][q];
+    for (int a = 0; a < 3; a++)
+        CU(cudaMemcpy2D(m[a], w * 2, (const int16_t *)c.f[AF_R1 + 3 * grp + a] + (AWP_XO - 2), (size_t)g.px * 2,
+                        w * 2, rows, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy2D(x, w * 2, (const uint16_t *)c.f[AF_RX] + (AWP_XO - 2), (size_t)g.px * 2, w * 2, rows,
+                    cudaMemcpyDeviceToHost));
+    return AWP_OK;
+}
+
+static awp_status bfp_get(awp_solver *s, int q, int field, float *out)
+{
+    const AwpGeom &g = s->g;
+    const size_t n = (size_t)(g.nx + 4) * (g.ny + 4) * (g.nz + 4);
+    const int a = field - AF_R1, grp = a / 3;
+    std::vector<int16_t> mm(3 * n);
+    std::vector<uint16_t> xx(n);
+    int16_t *m[3] = {&mm[0], &mm[n], &mm[2 * n]};
+    awp_status st = bfp_fetch(s, q, grp, m, xx.data());
+    if (st != AWP_OK) return st;
+    for (size_t c = 0; c < n; c++) {
+        const uint32_t e = grp ? (uint32_t)(xx[c] >> 8) : (uint32_t)(xx[c] & 0xffu);
+        out[c] = (float)m[a % 3][c] * bfp_down(e);
+    }
+    return AWP_OK;
+}
+
+/* replaces one memory variable: its group is decoded, the field replaced and
+ * the group encoded again (the other group's exponent byte is kept) */
+static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
+{
+    const AwpGeom &g = s->g;
+    const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4), n = w * rows;
+    const int a = field - AF_R1, grp = a / 3;
+    std::vector<int16_t> mm(3 * n);
+    std::vector<uint16_t> xx(n);
+    int16_t *m[3] = {&mm[0], &mm[n], &mm[2 * n]};
+    awp_status st = bfp_fetch(s, q, grp, m, xx.data());
+    if (st != AWP_OK) return st;
+    for (size_t c = 0; c < n; c++) {
+        const uint32_t e = grp ? (uint32_t)(xx[c] >> 8) : (uint32_t)(xx[c] & 0xffu);
+        const float down = bfp_down(e);
+        float v[3] = {(float)m[0][c] * down, (float)m[1][c] * down, (float)m[2][c] * down};
+        v[a % 3] = in[c];
+        int16_t nm[3];
+        const uint32_t ne = bfp_enc3_host(v, nm);
+        for (int b = 0; b < 3; b++) m[b][c] = nm[b];
+        xx[c] = grp ? (uint16_t)((xx[c] & 0x00ffu) | (ne << 8)) : (uint16_t)((xx[c] & 0xff00u) | ne);
+    }
+    const AwpComp &cp = s->comp[0][q];
+    for (int b = 0; b < 3; b++)
+        CU(cudaMemcpy2D((int16_t *)cp.f[AF_R1 + 3 * grp + b] + (AWP_XO - 2), (size_t)g.px * 2, m[b], w * 2, w * 2,
+                        rows, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy2D((uint16_t *)cp.f[AF_RX] + (AWP_XO - 2), (size_t)g.px * 2, xx.data(), w * 2, w * 2, rows,
+                    cudaMemcpyHostToDevice));
+    return AWP_OK;
+}
+
 extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *out)
 {
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
@@ -1461,6 +1545,7 @@ extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *o
         if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
         src = s->comp[cur_buf(s, s->steps_done)][comp].f[field];
         if (field >= AF_R1) type = s->rstore;
+        if (src && type == AWP_STORE_BFP) return bfp_get(s, comp, field, out);
     } else if (field >= AWP_NF_STATE && field < AWP_NF_STATE + AM_N) {
         src = s->mdt.m[field - AWP_NF_STATE];
         type = s->mdt.type;
@@ -1525,6 +1610,7 @@ extern "C" awp_status awp_set_field(awp_solver *s, int comp, int field, const fl
     const AwpGeom &g = s->g;
     const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4);
     const int type = field >= AF_R1 ? s->rstore : AWP_STORE_F32;
+    if (type == AWP_STORE_BFP) return bfp_set(s, comp, field, in);
     uint16_t *tmp = NULL;
     if (type != AWP_STORE_F32) {
         tmp = (uint16_t *)malloc(w * rows * 2);
@@ -1741,7 +1827,7 @@ extern "C" awp_status awp_reset(awp_solver *s)
     const size_t rb = (size_t)s->g.vol * (s->rstore == AWP_STORE_F32 ? 4 : 2);
     for (int q = 0; q < p->ncomp; q++) {
         for (int b = 0; b < 2; b++)
-            for (int f = 0; f < AWP_NF_STATE; f++) {
+            for (int f = 0; f < AWP_NF_ARRAYS; f++) {
                 if (!s->comp[b][q].f[f] || (b == 1 && s->comp[1][q].f[f] == s->comp[0][q].f[f])) continue;
                 CU(cudaMemsetAsync(s->comp[b][q].f[f], 0, f >= AF_R1 ? rb : vb, s->stream));
             }

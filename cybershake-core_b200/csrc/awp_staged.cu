@@ -57,7 +57,8 @@ struct AwpStagedStrMaps {
     CUtensorMap v[AWP_MAX_COMP][3];  /* u v w, box 40 x 12                     */
     CUtensorMap med[4];              /* lam mu qp qs, box 40 x 9               */
     CUtensorMap s[AWP_MAX_COMP][6];  /* xx yy zz xy xz yz, box 32 x 8          */
-    CUtensorMap r[AWP_MAX_COMP][6];  /* r1..r6 (FP32 or bf16), box 32 x 8      */
+    CUtensorMap r[AWP_MAX_COMP][6];  /* r1..r6 (FP32, bf16 or int16), box 32 x 8 */
+    CUtensorMap rx[AWP_MAX_COMP];    /* exponent words of block floating point r */
 };
 struct AwpStaged {
     AwpStagedVelMaps vm;
@@ -578,20 +579,51 @@ struct TVel {
     }
 };
 
-/* bytes one level brings in */
-__host__ __device__ __forceinline__ uint32_t str_txb(int nve, int rsize)
+/* the memory-variable tiles of a slot by storage type: element size, tile
+ * count (block floating point adds the tile of exponent words) and the six
+ * values of the cell at point-tile offset cp */
+template <class TR>
+struct RTile {
+    static constexpr int size = (int)sizeof(TR), ntiles = 6;
+    static __device__ __forceinline__ void ld(const unsigned char *base, int cp, float r[6])
+    {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)base + cp, a * ST_PT, 1.0f);
+    }
+};
+template <>
+struct RTile<RBfp> {
+    static constexpr int size = 2, ntiles = 7;
+    static __device__ __forceinline__ void ld(const unsigned char *base, int cp, float r[6])
+    {
+        bfp_load6((const short *)base + cp, ST_PT, ((const unsigned short *)base)[6 * ST_PT + cp], r);
+    }
+};
+
+/* bytes one level brings in (rbytes: the r tiles of one cell row set) */
+__host__ __device__ __forceinline__ uint32_t str_txb(int nve, int rtile_bytes)
 {
-    return (uint32_t)((3 * ST_VT + (nve == 1 ? 4 : 2) * ST_MT + 6 * ST_PT) * 4 + (nve == 1 ? 6 * ST_PT * rsize : 0));
+    return (uint32_t)((3 * ST_VT + (nve == 1 ? 4 : 2) * ST_MT + 6 * ST_PT) * 4 + (nve == 1 ? rtile_bytes : 0));
 }
 
-template <int S, int RSIZE>
+/* issues the r tiles of component q at a point-tile position */
+template <class TR>
+__device__ __forceinline__ void r_issue(const AwpStagedStrMaps &maps, int q, unsigned char *rb, uint64_t *b, int xp,
+                                        int y, int z)
+{
+#pragma unroll
+    for (int a = 0; a < 6; ++a) tma_3d(rb + a * ST_PT * RTile<TR>::size, &maps.r[q][a], b, xp, y, z);
+    if (RTile<TR>::ntiles == 7) tma_3d(rb + 6 * ST_PT * RTile<TR>::size, &maps.rx[q], b, xp, y, z);
+}
+
+template <int S, class TR>
 __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, int nve, float *ring, uint64_t *full,
                                           uint32_t use, int i0, int j0, int k)
 {
     float *sl = ring + (use % S) * STR_SLOT;
     uint64_t *b = &full[use % S];
     fence_async_smem();
-    mb_expect(b, str_txb(nve, RSIZE));
+    mb_expect(b, str_txb(nve, RTile<TR>::ntiles * ST_PT * RTile<TR>::size));
     const int x = tile_x(i0);
 #pragma unroll
     for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
@@ -601,11 +633,7 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
     const int xp = i0 + AWP_XO - 1;
 #pragma unroll
     for (int a = 0; a < 6; ++a) tma_3d(sl + STR_ST + a * ST_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
-    if (nve == 1) {
-        unsigned char *rb = (unsigned char *)(sl + STR_ST + 6 * ST_PT);
-#pragma unroll
-        for (int a = 0; a < 6; ++a) tma_3d(rb + a * ST_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
-    }
+    if (nve == 1) r_issue<TR>(maps, q, (unsigned char *)(sl + STR_ST + 6 * ST_PT), b, xp, j0 + 1, k + 1);
 }
 
 /* work items: (x tile, y tile, z chunk, component); see split_item for the order.
@@ -618,7 +646,6 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
     constexpr int S = 2 + STR_D;      /* levels k-1 and k in use, STR_D in flight */
-    constexpr int RSIZE = (int)sizeof(TR);
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
     float *ring = ring_base(st_smem);
@@ -644,7 +671,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             for (int k = k0 - 1; k <= k1; ++k, ++use) {
                 ok = ring_acquire<S>(empty, use, &abort_s);
                 if (!ok) break;
-                str_issue<S, RSIZE>(maps, q, nve, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
+                str_issue<S, TR>(maps, q, nve, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
         }
         if (!ok) {
@@ -719,14 +746,11 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                     const TVel Vq{sk + cv, sm[cv], sm[ST_VT + cv], wm1, up1[r], up2[r], vp1[r], vp2[r], wm2[r], wp1[r]};
                     Stress6 o;
                     if (nve == 1) {
-                        const TR *pr = (const TR *)(sk + STR_ST + 6 * ST_PT) + cp;
                         float rr[6];
-#pragma unroll
-                        for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
+                        RTile<TR>::ld((const unsigned char *)(sk + STR_ST + 6 * ST_PT), cp, rr);
                         const VelDiff dd = vel_diff(Vq);
                         o = str_visco(kc, dd, s0, rr, dth, dt, dh1);
-#pragma unroll
-                        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, rr[a], 1.0f);
+                        RVars<TR>::st(tab[q], c, rr);
                     } else {
                         o = str_elastic(kc, Vq, s0, dth);
                     }
@@ -780,9 +804,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
 #define STB_CSLOT (STB_CST + 12 * ST_PT)          /* r tiles fit in 6 x 256   */
 
 __host__ __device__ __forceinline__ uint32_t strb_med_txb(int nve) { return (uint32_t)((nve == 1 ? 4 : 2) * ST_MT * 4); }
-__host__ __device__ __forceinline__ uint32_t strb_comp_txb(int nve, int rsize)
+__host__ __device__ __forceinline__ uint32_t strb_comp_txb(int nve, int rtile_bytes)
 {
-    return (uint32_t)((3 * ST_VT + 6 * ST_PT) * 4 + (nve == 1 ? 6 * ST_PT * rsize : 0));
+    return (uint32_t)((3 * ST_VT + 6 * ST_PT) * 4 + (nve == 1 ? rtile_bytes : 0));
 }
 
 /* RPT tile rows per consumer thread (ST_Y / RPT consumer warps) */
@@ -792,7 +816,6 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
            const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
            const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
 {
-    constexpr int RSIZE = (int)sizeof(TR);
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
     float *mring = ring_base(st_smem);
@@ -838,17 +861,12 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                     float *sl = cring + (uc % STB_CS) * STB_CSLOT;
                     uint64_t *b = &cfull[uc % STB_CS];
                     fence_async_smem();
-                    mb_expect(b, strb_comp_txb(nve, RSIZE));
+                    mb_expect(b, strb_comp_txb(nve, RTile<TR>::ntiles * ST_PT * RTile<TR>::size));
 #pragma unroll
                     for (int a = 0; a < 3; ++a) tma_3d(sl + a * ST_VT, &maps.v[q][a], b, x, j0 - 1, k + 1);
 #pragma unroll
                     for (int a = 0; a < 6; ++a) tma_3d(sl + STB_CST + a * ST_PT, &maps.s[q][a], b, xp, j0 + 1, k + 1);
-                    if (nve == 1) {
-                        unsigned char *rb = (unsigned char *)(sl + STB_CST + 6 * ST_PT);
-#pragma unroll
-                        for (int a = 0; a < 6; ++a)
-                            tma_3d(rb + a * ST_PT * RSIZE, &maps.r[q][a], b, xp, j0 + 1, k + 1);
-                    }
+                    if (nve == 1) r_issue<TR>(maps, q, (unsigned char *)(sl + STB_CST + 6 * ST_PT), b, xp, j0 + 1, k + 1);
                     ++uc;
                 }
             }
@@ -957,14 +975,11 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                                       vp2[r][q], wm2[r][q], wp1[r][q]};
                         Stress6 o;
                         if (nve == 1) {
-                            const TR *pr = (const TR *)(sk + STB_CST + 6 * ST_PT) + cp;
                             float rr[6];
-#pragma unroll
-                            for (int a = 0; a < 6; ++a) rr[a] = Store<TR>::ld(pr, a * ST_PT, 1.0f);
+                            RTile<TR>::ld((const unsigned char *)(sk + STB_CST + 6 * ST_PT), cp, rr);
                             const VelDiff dd = vel_diff(Vq);
                             o = str_visco(kc[r], dd, s0, rr, dth, dt, dh1);
-#pragma unroll
-                            for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)tab[q].f[AF_R1 + a], c, rr[a], 1.0f);
+                            RVars<TR>::st(tab[q], c, rr);
                         } else {
                             o = str_elastic(kc[r], Vq, s0, dth);
                         }
@@ -1053,7 +1068,7 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
     memset(s, 0, sizeof *s);
     static const int vel_f[5] = {AF_XX, AF_YY, AF_XY, AF_XZ, AF_YZ};
     static const int med_f[4] = {AM_LAM, AM_MU, AM_QP, AM_QS};
-    const int rsize = rtype == AWP_STORE_BF16 ? 2 : 4;
+    const int rsize = rtype == AWP_STORE_F32 ? 4 : 2;
     bool ok = make_map(&s->vm.d1, g, md.m[AM_D1], ST_W, ST_MR);
     for (int q = 0; q < ncomp; ++q) {
         for (int a = 0; a < 5; ++a) ok = ok && make_map(&s->vm.st[q][a], g, comp[q].f[vel_f[a]], ST_W, ST_HR);
@@ -1062,6 +1077,8 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
         for (int a = 0; a < 6; ++a) ok = ok && make_map(&s->sm.s[q][a], g, comp[q].f[AF_XX + a], ST_X, ST_Y);
         for (int a = 0; a < 6; ++a)     /* absent in the elastic scheme, which never loads them */
             if (comp[q].f[AF_R1 + a]) ok = ok && make_map(&s->sm.r[q][a], g, comp[q].f[AF_R1 + a], ST_X, ST_Y, rsize);
+        if (rtype == AWP_STORE_BFP && comp[q].f[AF_R1])
+            ok = ok && comp[q].f[AF_RX] && make_map(&s->sm.rx[q], g, comp[q].f[AF_RX], ST_X, ST_Y, 2);
     }
     for (int a = 0; a < 4; ++a) ok = ok && make_map(&s->sm.med[a], g, md.m[med_f[a]], ST_W, ST_MR);
     if (!ok) {
@@ -1215,5 +1232,6 @@ cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cud
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
     if (s.rtype == AWP_STORE_BF16) return launch_str_tr<__nv_bfloat16>(st, s, stream);
+    if (s.rtype == AWP_STORE_BFP) return launch_str_tr<RBfp>(st, s, stream);
     return launch_str_tr<float>(st, s, stream);
 }

@@ -53,6 +53,78 @@ template <> struct Store<__half> {
     static __device__ __forceinline__ void st(__half *p, int c, float v, float scale) { p[c] = __float2half_rn(v * scale); }
 };
 
+/* 16-bit block floating point of r1..r6 (AWP_STORE_BFP; the rule is stated
+ * in awp_internal.h).  RBfp is the storage tag of the steppers' templates. */
+struct RBfp {};
+
+/* encodes three values; returns the exponent byte */
+__device__ __forceinline__ uint32_t bfp_enc3(float a, float b, float c, short &ma, short &mb, short &mc)
+{
+    const float mx = fmaxf(fabsf(a), fmaxf(fabsf(b), fabsf(c)));
+    const uint32_t e = __float_as_uint(mx) >> 23;
+    if (e < AWP_BFP_EMIN) {
+        ma = mb = mc = 0;
+        return 0u;
+    }
+    const float up = __uint_as_float((268u - e) << 23);
+    ma = (short)__float2int_rn(fminf(fmaxf(a * up, -32767.f), 32767.f));
+    mb = (short)__float2int_rn(fminf(fmaxf(b * up, -32767.f), 32767.f));
+    mc = (short)__float2int_rn(fminf(fmaxf(c * up, -32767.f), 32767.f));
+    return e;
+}
+
+/* decodes three values of exponent byte e */
+__device__ __forceinline__ void bfp_dec3(uint32_t e, short ma, short mb, short mc, float &a, float &b, float &c)
+{
+    const float down = __uint_as_float((max(e, AWP_BFP_EMIN) - 14u) << 23);
+    a = (float)ma * down;
+    b = (float)mb * down;
+    c = (float)mc * down;
+}
+
+/* the six memory variables of a cell from their storage (m: the mantissa
+ * arrays at the cell, stride apart; x: the exponent word) */
+__device__ __forceinline__ void bfp_load6(const short *m, int stride, uint32_t x, float r[6])
+{
+    bfp_dec3(x & 0xffu, m[0], m[stride], m[2 * stride], r[0], r[1], r[2]);
+    bfp_dec3(x >> 8, m[3 * stride], m[4 * stride], m[5 * stride], r[3], r[4], r[5]);
+}
+
+/* memory variables r1..r6 of one cell in global memory, by storage type */
+template <class TR>
+struct RVars {
+    static __device__ __forceinline__ void ld(const AwpComp &o, int c, float r[6])
+    {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) r[a] = Store<TR>::ld((const TR *)o.f[AF_R1 + a], c, 1.0f);
+    }
+    static __device__ __forceinline__ void st(const AwpComp &o, int c, const float r[6])
+    {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) Store<TR>::st((TR *)o.f[AF_R1 + a], c, r[a], 1.0f);
+    }
+};
+template <>
+struct RVars<RBfp> {
+    static __device__ __forceinline__ void ld(const AwpComp &o, int c, float r[6])
+    {
+        const uint32_t x = ((const unsigned short *)o.f[AF_RX])[c];
+        bfp_dec3(x & 0xffu, ((const short *)o.f[AF_R1])[c], ((const short *)o.f[AF_R2])[c],
+                 ((const short *)o.f[AF_R3])[c], r[0], r[1], r[2]);
+        bfp_dec3(x >> 8, ((const short *)o.f[AF_R4])[c], ((const short *)o.f[AF_R5])[c],
+                 ((const short *)o.f[AF_R6])[c], r[3], r[4], r[5]);
+    }
+    static __device__ __forceinline__ void st(const AwpComp &o, int c, const float r[6])
+    {
+        short m[6];
+        const uint32_t e0 = bfp_enc3(r[0], r[1], r[2], m[0], m[1], m[2]);
+        const uint32_t e1 = bfp_enc3(r[3], r[4], r[5], m[3], m[4], m[5]);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) ((short *)o.f[AF_R1 + a])[c] = m[a];
+        ((unsigned short *)o.f[AF_RX])[c] = (unsigned short)(e0 | (e1 << 8));
+    }
+};
+
 /* typed view of the media arrays */
 template <class TM>
 struct MediaT {

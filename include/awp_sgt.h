@@ -60,7 +60,12 @@ typedef enum {
                            array, r1..r6 as bfloat16 (binary16 lacks the
                            exponent range for memory variables, whose size
                            follows the source amplitude)                     */
-    AWP_PREC_MIXED = 3  /* media FP32, r1..r6 bfloat16                       */
+    AWP_PREC_MIXED = 3, /* media FP32, r1..r6 bfloat16                       */
+    AWP_PREC_BFP = 4    /* media FP32, r1..r6 in 16-bit block floating point:
+                           an int16 mantissa each, the normal (r1..r3) and
+                           the shear (r4..r6) memory variables of a cell
+                           sharing one exponent each (one 16-bit word per
+                           cell); 14 bytes per cell instead of 24           */
 } awp_precision;
 
 /* Stepper implementation. */

@@ -73,7 +73,16 @@ typedef struct {
     int write_step;
     int igreen;
     int kinematic;   /* 1: IFAULT=5 subfault sources (NST = 2) */
+    int rstore;      /* storage of r1..r6 (FP32 build only): ORC_RS_* */
 } orc_params;
+
+/* Storage formats of the memory variables r1..r6 emulated by the FP32 build:
+ * the new value of a memory variable feeds the stress update as computed and
+ * is stored rounded to the format (the device steppers' order).  Stochastic
+ * rounding takes its bits from orc_sr_bits, a counter-based hash of the cell,
+ * the step and the variable, which the device kernels compute the same way. */
+enum { ORC_RS_F32 = 0, ORC_RS_BF16_RN = 1, ORC_RS_BF16_SR = 2, ORC_RS_F16M_RN = 3, ORC_RS_F16M_SR = 4,
+       ORC_RS_BFP6 = 5, ORC_RS_BFP33 = 6 };
 
 enum { F_U1, F_V1, F_W1, F_XX, F_YY, F_ZZ, F_XY, F_XZ, F_YZ,
        F_R1, F_R2, F_R3, F_R4, F_R5, F_R6,
@@ -534,6 +543,78 @@ static void orc_fvel(orc_t *h)
         }
 }
 
+/* 32 random bits for stochastic rounding of memory variable pair `pair`
+ * (0: r1 r2, 1: r3 r4, 2: r5 r6; low half for the first) of cell (i,j,k) at
+ * step `step`: an integer mix of the three counters (multiply-xorshift
+ * rounds), the same on the host and the device. */
+static inline uint32_t orc_sr_bits(int i, int j, int k, int nx, int ny, int step, int pair)
+{
+    uint32_t h = (((uint32_t)k * (uint32_t)ny + (uint32_t)j) * (uint32_t)nx + (uint32_t)i) * 0x9E3779B1u;
+    h += (uint32_t)step * 0x85EBCA77u + (uint32_t)pair * 0xC2B2AE3Du;
+    h ^= h >> 15; h *= 0x2C1B3C6Du;
+    h ^= h >> 12; h *= 0x297A2D39u;
+    h ^= h >> 15;
+    return h;
+}
+
+static inline float orc_bits_f(uint32_t b) { float v; memcpy(&v, &b, 4); return v; }
+static inline uint32_t orc_f_bits(float v) { uint32_t b; memcpy(&b, &v, 4); return b; }
+
+/* float rounded to `keep` mantissa bits (bf16 keeps 7, binary16 10; the
+ * exponent range of float is kept): nearest even, or stochastic with the
+ * low bits of `rnd` (adding a uniform integer below one unit of the kept
+ * last place to the magnitude, then truncating, rounds away from zero with
+ * the probability of the dropped fraction) */
+static inline float orc_round_mant(float v, int keep, int stochastic, uint32_t rnd)
+{
+    const int drop = 23 - keep;
+    const uint32_t mask = (1u << drop) - 1u;
+    uint32_t b = orc_f_bits(v);
+    if ((b & 0x7fffffffu) >= 0x7f800000u) return v;
+    if (stochastic) b += rnd & mask;
+    else b += (mask >> 1) + ((b >> drop) & 1u);
+    return orc_bits_f(b & ~mask);
+}
+
+/* Block floating point of n values sharing one exponent (the storage
+ * AWP_PREC_BFP of the device steppers; ORC_RS_BFP33 is that mode, two groups
+ * of three): E = the float exponent field of the largest magnitude; with
+ * E >= 15 each value is stored as the integer nearest (ties to even) to
+ * v * 2^(141 - E) clamped to [-32767, 32767] (the magnitude is below 2^15),
+ * read back as m * 2^(E - 141); E < 15 stores zeros.  Both scalings are
+ * exact; the integer conversion makes a value that rounds to 0 a +0. */
+static inline void orc_bfp(float *v, int n)
+{
+    float mx = 0.f;
+    for (int a = 0; a < n; a++) mx = fmaxf(fabsf(v[a]), mx);
+    const uint32_t e = orc_f_bits(mx) >> 23;
+    if (e < 15u) {
+        for (int a = 0; a < n; a++) v[a] = 0.f;
+        return;
+    }
+    const float up = orc_bits_f((268u - e) << 23), down = orc_bits_f((e - 14u) << 23);
+    for (int a = 0; a < n; a++) {
+        const long m = lrintf(fminf(fmaxf(v[a] * up, -32767.f), 32767.f));
+        v[a] = (float)m * down;
+    }
+}
+
+static inline real orc_rstore(int mode, real v, uint32_t rnd)
+{
+#if ORC_IS_DOUBLE
+    (void)mode; (void)rnd;
+    return v;
+#else
+    switch (mode) {
+    case ORC_RS_BF16_RN: return orc_round_mant(v, 7, 0, 0);
+    case ORC_RS_BF16_SR: return orc_round_mant(v, 7, 1, rnd);
+    case ORC_RS_F16M_RN: return orc_round_mant(v, 10, 0, 0);
+    case ORC_RS_F16M_SR: return orc_round_mant(v, 10, 1, rnd);
+    default: return v;
+    }
+#endif
+}
+
 static void orc_dstrqc(orc_t *h)
 {
     /* viscoop.f:49-191 (allq over the whole subdomain) */
@@ -551,6 +632,7 @@ static void orc_dstrqc(orc_t *h)
     const real *lam = h->f[F_LAM], *mu = h->f[F_MU], *qp = h->f[F_QP], *qs = h->f[F_QS];
     const long sx = 1, sy = h->sx, sz = (long)h->sx * h->sy;
     const int nz = p->nz;
+    const int rs = p->rstore, step = h->cur;
     #pragma omp parallel for schedule(static)
     for (int k = 1; k <= p->nz; k++) {
         const int itz = ((nz + 1) - k) % 2;          /* mod(...,2)+1, 0-based */
@@ -602,19 +684,38 @@ static void orc_dstrqc(orc_t *h)
                 real vh2_r6 = -(vaas * vxmu / (real)2.);
                 yz[c] = yz[c] + vxmu * (dth * vt6 + dth * vt7) + dt * r6[c];
 
-                r1[c] = (vx2 * r1[c] - vh1 * (vt2 + vt3) * dh1 + va1) * vx1;
-                r2[c] = (vx2 * r2[c] - vh1 * (vt1 + vt3) * dh1 + va1) * vx1;
-                r3[c] = (vx2 * r3[c] - vh1 * (vt1 + vt2) * dh1 + va1) * vx1;
-                r4[c] = (vx2 * r4[c] + vh2_r4 * dh1 * vt4) * vx1;
-                r5[c] = (vx2 * r5[c] + vh2_r5 * dh1 * vt5) * vx1;
-                r6[c] = (vx2 * r6[c] + vh2_r6 * dh1 * (vt6 + vt7)) * vx1;
+                const real n1 = (vx2 * r1[c] - vh1 * (vt2 + vt3) * dh1 + va1) * vx1;
+                const real n2 = (vx2 * r2[c] - vh1 * (vt1 + vt3) * dh1 + va1) * vx1;
+                const real n3 = (vx2 * r3[c] - vh1 * (vt1 + vt2) * dh1 + va1) * vx1;
+                const real n4 = (vx2 * r4[c] + vh2_r4 * dh1 * vt4) * vx1;
+                const real n5 = (vx2 * r5[c] + vh2_r5 * dh1 * vt5) * vx1;
+                const real n6 = (vx2 * r6[c] + vh2_r6 * dh1 * (vt6 + vt7)) * vx1;
 
-                xx[c] = xx[c] + dt * r1[c];
-                yy[c] = yy[c] + dt * r2[c];
-                zz[c] = zz[c] + dt * r3[c];
-                xy[c] = xy[c] + dt * r4[c];
-                xz[c] = xz[c] + dt * r5[c];
-                yz[c] = yz[c] + dt * r6[c];
+                xx[c] = xx[c] + dt * n1;
+                yy[c] = yy[c] + dt * n2;
+                zz[c] = zz[c] + dt * n3;
+                xy[c] = xy[c] + dt * n4;
+                xz[c] = xz[c] + dt * n5;
+                yz[c] = yz[c] + dt * n6;
+                if (rs == ORC_RS_F32) {
+                    r1[c] = n1; r2[c] = n2; r3[c] = n3; r4[c] = n4; r5[c] = n5; r6[c] = n6;
+                } else if (rs == ORC_RS_BFP6 || rs == ORC_RS_BFP33) {
+#if ORC_IS_DOUBLE
+                    r1[c] = n1; r2[c] = n2; r3[c] = n3; r4[c] = n4; r5[c] = n5; r6[c] = n6;
+#else
+                    float v[6] = {n1, n2, n3, n4, n5, n6};
+                    if (rs == ORC_RS_BFP6) orc_bfp(v, 6);
+                    else { orc_bfp(v, 3); orc_bfp(v + 3, 3); }
+                    r1[c] = v[0]; r2[c] = v[1]; r3[c] = v[2]; r4[c] = v[3]; r5[c] = v[4]; r6[c] = v[5];
+#endif
+                } else {
+                    const uint32_t b0 = orc_sr_bits(i, j, k, p->nx, p->ny, step, 0);
+                    const uint32_t b1 = orc_sr_bits(i, j, k, p->nx, p->ny, step, 1);
+                    const uint32_t b2 = orc_sr_bits(i, j, k, p->nx, p->ny, step, 2);
+                    r1[c] = orc_rstore(rs, n1, b0); r2[c] = orc_rstore(rs, n2, b0 >> 16);
+                    r3[c] = orc_rstore(rs, n3, b1); r4[c] = orc_rstore(rs, n4, b1 >> 16);
+                    r5[c] = orc_rstore(rs, n5, b2); r6[c] = orc_rstore(rs, n6, b2 >> 16);
+                }
             }
         }
     }

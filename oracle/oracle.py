@@ -33,8 +33,12 @@ class OrcParams(C.Structure):
         ("fl", C.c_float), ("fh", C.c_float), ("fp", C.c_float),
         ("socalq", C.c_int), ("nve", C.c_int), ("mediastart", C.c_int), ("nvar", C.c_int),
         ("idyna", C.c_int), ("nst", C.c_int), ("nt", C.c_int), ("ntiskp_sgt", C.c_int),
-        ("write_step", C.c_int), ("igreen", C.c_int), ("kinematic", C.c_int),
+        ("write_step", C.c_int), ("igreen", C.c_int), ("kinematic", C.c_int), ("rstore", C.c_int),
     ]
+
+
+# storage formats of r1..r6 the FP32 build emulates (awp_oracle.c ORC_RS_*)
+RSTORE = {"f32": 0, "bf16": 1, "bf16_sr": 2, "f16m": 3, "f16m_sr": 4, "bfp6": 5, "bfp33": 6}
 
 
 _libs = {}
@@ -90,7 +94,7 @@ class Oracle:
 
     def __init__(self, *, nx, ny, nz, dh, dt, nt, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5,
                  socalq=0, nve=1, mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10,
-                 write_step=None, igreen=1, precision="f32", threads=0, kinematic=0):
+                 write_step=None, igreen=1, precision="f32", threads=0, kinematic=0, rstore="f32"):
         self.lib = load(precision)
         if threads:
             self.lib.orc_set_num_threads(threads)
@@ -104,6 +108,9 @@ class Oracle:
         p.write_step = (nt // ntiskp_sgt) if write_step is None else write_step
         p.igreen = igreen
         p.kinematic = kinematic
+        if rstore != "f32" and precision != "f32":
+            raise ValueError("r storage formats are emulated by the FP32 build only")
+        p.rstore = RSTORE[rstore]
         self.p = p
         self.h = self.lib.orc_create(C.byref(p))
         if not self.h:

@@ -52,7 +52,7 @@ def state(s, ncomp):
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel,precision,ncomp,stop", [
     ("staged", "f32", 3, 23), ("staged", "f32", 1, 10), ("fused", "f32", 2, 23), ("two_sweep", "f32", 1, 17),
-    ("staged", "mixed", 2, 19), ("two_sweep", "bf16", 1, 31)])
+    ("staged", "mixed", 2, 19), ("two_sweep", "bf16", 1, 31), ("staged", "bfp", 3, 29), ("fused", "bfp", 1, 13)])
 def test_resume_is_bitwise_equal(tmp_path, kernel, precision, ncomp, stop):
     with make_solver(kernel, precision, ncomp) as s:
         s.run(NT)
@@ -153,3 +153,28 @@ def test_set_field_round_trip():
         assert np.array_equal(s.field("r4"), bf16_rn(a))
         with pytest.raises(awpsgt.AwpError):
             s.set_field("mu", a)                     # media are not state
+
+
+@pytest.mark.gpu
+def test_set_field_block_floating_point():
+    """Memory variables in block floating point: a value set comes back within
+    2^-14 of its group's largest magnitude; setting what was read back leaves
+    the stored words unchanged (checkpoint restore is exact)."""
+    with make_solver("staged", "bfp", 1) as s:
+        rng = np.random.default_rng(4)
+        shape = (NZ + 4, NY + 4, NX + 4)
+        vals = []
+        for n, f in enumerate(("r1", "r2", "r3", "r4", "r5", "r6")):
+            a = np.zeros(shape, np.float32)
+            a[2:-2, 2:-2, 2:-2] = (rng.standard_normal((NZ, NY, NX)) * 10.0 ** (n - 2)).astype(np.float32)
+            s.set_field(f, a)
+            vals.append(a)
+        got = [s.field(f) for f in ("r1", "r2", "r3", "r4", "r5", "r6")]
+        for g0 in (0, 3):
+            mx = np.maximum.reduce([np.abs(vals[g0 + a]) for a in range(3)])
+            for a in range(3):
+                assert np.all(np.abs(got[g0 + a] - vals[g0 + a]) <= mx * 2.0 ** -14)
+        for f, a in zip(("r1", "r2", "r3", "r4", "r5", "r6"), got):
+            s.set_field(f, a)
+        for f, a in zip(("r1", "r2", "r3", "r4", "r5", "r6"), got):
+            assert np.array_equal(s.field(f).view(np.uint32), a.view(np.uint32))

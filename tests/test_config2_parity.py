@@ -7,7 +7,9 @@ The solve starts from a state filled with bounded noise (every wavefield and
 memory-variable cell of the interior; ghosts zero, as a solve keeps them), so
 that every cell of every component is active from the first step on, and runs
 60 steps with an SGT sample every 10.  Every field of every component, the
-CHKJ series and the SGT file image must equal the FP32 oracle's bit for bit.
+CHKJ series and the SGT file image must equal the FP32 oracle's bit for bit;
+with the memory variables in block floating point ("bfp"), the FP32 oracle's
+emulation of that storage.
 """
 import numpy as np
 import pytest
@@ -30,14 +32,15 @@ def noise(w, q, f):
     return a
 
 
-def test_config2_workload_bit_exact_from_a_noise_state():
+@pytest.mark.parametrize("precision,rstore", [("f32", "f32"), ("bfp", "bfp33")])
+def test_config2_workload_bit_exact_from_a_noise_state(precision, rstore):
     w = ai.config(2)
     media = w.media()
     pts = w.points()
     assert (w.nx, w.ny, w.nz, len(pts), w.igreen) == (400, 400, 200, 5000, (1, 2, 3))
     kw = dict(nd=20, arbc=0.92, fl=w.fl, fh=w.fh, fp=w.fp, socalq=w.socalq, ntiskp_sgt=10, write_step=6)
     stfs = [w.stf(q)[:NT] for q in range(3)]
-    p = awpsgt.make_params(w.nx, w.ny, w.nz, w.dh, w.dt, NT, igreen=w.igreen, nst=NT, **kw)
+    p = awpsgt.make_params(w.nx, w.ny, w.nz, w.dh, w.dt, NT, igreen=w.igreen, nst=NT, precision=precision, **kw)
     with awpsgt.Solver(p) as s:
         tune = s.tuning()
         assert tune.staged_batch & 1                        # components side by side in the stress sweep
@@ -45,17 +48,22 @@ def test_config2_workload_bit_exact_from_a_noise_state():
         for q in range(3):
             s.set_source(q, [w.src_xyz], stfs[q])
         s.set_points(pts)
+        start_r = []
         for q in range(3):
             for f in range(15):
                 s.set_field(awpsgt.FIELDS[f], noise(w, q, f), q)
+            # the memory variables as stored (block floating point rounds them)
+            start_r.append([s.field(awpsgt.FIELDS[f], q) for f in range(9, 15)])
         s.run(NT)
         for q in range(3):
-            o = oracle.Oracle(nx=w.nx, ny=w.ny, nz=w.nz, dh=w.dh, dt=w.dt, nt=NT, nst=NT, igreen=w.igreen[q], **kw)
+            o = oracle.Oracle(nx=w.nx, ny=w.ny, nz=w.nz, dh=w.dh, dt=w.dt, nt=NT, nst=NT, igreen=w.igreen[q],
+                              rstore=rstore, **kw)
             o.load_media(media)
             o.set_source([w.src_xyz], stfs[q])
             o.set_points(pts)
             for f in range(15):
-                o.set_field(oracle.FIELDS[f], noise(w, q, f))
+                o.set_field(oracle.FIELDS[f], noise(w, q, f) if f < 9 else start_r[q][f - 9])
+            start_r[q] = None
             o.run(NT)
             bad = []
             for f in oracle.FIELDS[:15]:

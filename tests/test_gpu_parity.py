@@ -83,9 +83,9 @@ class Case:
             s.run(n)
         return s
 
-    def oracle(self, q=0, steps=None, precision="f32"):
+    def oracle(self, q=0, steps=None, precision="f32", rstore="f32"):
         o = oracle.Oracle(nx=self.nx, ny=self.ny, nz=self.nz, dh=self.dh, dt=self.dt, nt=self.nt,
-                          igreen=self.igreen[q], precision=precision, **self.kw())
+                          igreen=self.igreen[q], precision=precision, rstore=rstore, **self.kw())
         o.load_media(self.media if self.mediastart else None)
         o.set_source(self.srcs[q], self.stfs[q])
         o.set_points(self.pts)
@@ -249,6 +249,42 @@ def test_mixed_precision_runs_close_to_fp64(precision, kernel):
     assert np.isfinite(g).all()
     err = rel_l2(g, o64.sgt())
     assert err <= 2e-2, err
+
+
+# storage of r1..r6 in the device modes with FP32 media -> the oracle's emulation of it
+RSTORE = {"mixed": "bf16", "bfp": "bfp33"}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "bfp"])
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_16bit_memory_variables_bit_exact(precision, kernel):
+    """FP32 media with r1..r6 in 16 bits (bf16, or block floating point) are
+    bit-exact with the FP32 oracle storing r1..r6 in the same format: every
+    field (memory variables decoded), CHKJ and the SGT image."""
+    c = Case(nx=44, ny=36, nz=30, nt=40, igreen=(1, 2, 3), srcs=[[(22, 18, 8)], [(22, 18, 8)], [(22, 18, 8)]])
+    s = c.gpu(kernel=kernel, precision=precision)
+    for q in range(3):
+        assert_same_state(s, c.oracle(q, rstore=RSTORE[precision]), q)
+
+
+@pytest.mark.parametrize("qslow,batch,rpt", [("0", "0", "1"), ("1", "0", "2"), ("1", "1", "1")])
+def test_bfp_staged_shapes_bit_exact(qslow, batch, rpt, monkeypatch):
+    monkeypatch.setenv("AWP_TUNE_QSLOW", qslow)
+    monkeypatch.setenv("AWP_TUNE_BATCH", batch)
+    monkeypatch.setenv("AWP_TUNE_RPT", rpt)
+    monkeypatch.setenv("AWP_TUNE_KSTAGE", "9")
+    c = Case(nx=70, ny=20, nz=41, nt=30, igreen=(1, 2), srcs=[[(35, 10, 20)], [(30, 12, 33)]], ntiskp=3,
+             write_step=5)
+    s = c.gpu(kernel="staged", precision="bfp")
+    for q in range(2):
+        assert_same_state(s, c.oracle(q, rstore="bfp33"), q)
+
+
+def test_bfp_error_budget():
+    """Block floating point r1..r6 stays within the 1e-4 SGT budget of FP64."""
+    c = Case(nt=80, stf_seed=11)
+    err = rel_l2(c.gpu(precision="bfp").sgt(), c.oracle(precision="f64").sgt())
+    assert err <= 1e-4, err
 
 
 def test_mixed_mode_same_result_staged_and_two_sweep():
