@@ -401,7 +401,7 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
     __shared__ AwpComp tab[AWP_MAX_COMP];
     if (threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
 #pragma unroll
-        for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
+        for (int f = 0; f < AWP_NF_ARRAYS; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
     ring_init<VB_MS>(mfull, mempty, &abort_s, ST_CW);
     ring_init<CS>(cfull, cempty, &abort_s, ST_CW);
@@ -654,7 +654,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     __shared__ AwpComp tab[AWP_MAX_COMP];
     if (threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
 #pragma unroll
-        for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
+        for (int f = 0; f < AWP_NF_ARRAYS; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
     ring_init<S>(full, empty, &abort_s, CW);
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -826,7 +826,7 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
     __shared__ AwpComp tab[AWP_MAX_COMP];
     if (threadIdx.y == 0 && threadIdx.x < AWP_MAX_COMP) {
 #pragma unroll
-        for (int f = 0; f < AWP_NF_STATE; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
+        for (int f = 0; f < AWP_NF_ARRAYS; ++f) tab[threadIdx.x].f[f] = pick(cs, threadIdx.x, f);
     }
     ring_init<STB_MS>(mfull, mempty, &abort_s, CW);
     ring_init<STB_CS>(cfull, cempty, &abort_s, CW);

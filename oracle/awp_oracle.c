@@ -1037,6 +1037,18 @@ void orc_get_tau(const orc_t *h, float *out8)
             for (int x = 0; x < 2; x++) out8[(z * 2 + y) * 2 + x] = (float)h->tau[z][y][x];
 }
 
+/* relaxation coefficients tau1 then tau2 of viscoop.f:79-88, each [itz][ity][itx]
+ * with the 0-based parities itx = i mod 2, ity = j mod 2, itz = (nz+1-k) mod 2 */
+void orc_get_tau12(const orc_t *h, float *out16)
+{
+    for (int z = 0; z < 2; z++)
+        for (int y = 0; y < 2; y++)
+            for (int x = 0; x < 2; x++) {
+                out16[(z * 2 + y) * 2 + x] = (float)h->tau1[z][y][x];
+                out16[8 + (z * 2 + y) * 2 + x] = (float)h->tau2[z][y][x];
+            }
+}
+
 /* Cerjan factors cx[1..nx], cy[1..ny], cz[1..nz] (cerjan.f), as float */
 void orc_get_sponge(const orc_t *h, float *cx, float *cy, float *cz)
 {

@@ -81,6 +81,7 @@ def load(precision: str = "f32"):
     lib.orc_set_num_threads.argtypes = [C.c_int]
     lib.orc_get_tau.argtypes = [V, V]
     lib.orc_get_sponge.argtypes = [V, V, V, V]
+    lib.orc_get_tau12.argtypes = [V, V]
     _libs[precision] = lib
     return lib
 
@@ -180,6 +181,12 @@ class Oracle:
         out = np.zeros((2, 2, 2), dtype=np.float32)
         self.lib.orc_get_tau(self.h, _p(out))
         return out
+
+    def tau12(self):
+        """tau1 and tau2 of viscoop.f:79-88, each [itz][ity][itx] (0-based parities)."""
+        out = np.zeros(16, dtype=np.float32)
+        self.lib.orc_get_tau12(self.h, _p(out))
+        return out[:8].copy(), out[8:].copy()
 
     def sponge(self):
         """Cerjan factors (cx[nx], cy[ny], cz[nz]), index 0 at the low x / y face

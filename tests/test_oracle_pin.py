@@ -113,3 +113,78 @@ def test_device_media_match_reference_fixtures(case):
     assert np.array_equal(dev["d1"].view(np.uint32), ref["d1"].view(np.uint32))
     for f in ("lam", "mu", "qp", "qs"):
         assert ulps(dev[f], ref[f]).max() <= MAX_ULP, f
+
+
+# ---------------------------------------------------------------------------
+# The time loop pinned to the reference's own stencil kernels.
+#
+# The reference CUDA stepper's dvelcx and dstrqc (AWP-GPU-SGT/src/
+# kernel_kp1_fix_havg_ifault5.cu:420-504, 726-973), run on the host from the
+# reference sources (oracle/Makefile.ref, oracle/gpusgt_step_driver.cpp), made
+# the fixtures in tests/golden/timeloop (tests/golden/make_timeloop_golden.py).
+# Their dstrqc is an algebraic regrouping of the Fortran allq (the two
+# dt * r terms folded into one coefficient, double-precision literals, other
+# association orders), so the bar is a relative L2 difference per field of
+# at most 2e-6 (measured: 1.6e-7 to 2.1e-7, the FP32 rounding level; the FP32
+# oracle lies as far from its FP64 build).  Every state field is compared,
+# the memory variables included, in the cells below the free surface's reach.
+# ---------------------------------------------------------------------------
+
+from tests.golden import make_timeloop_golden as tl
+
+TL_TOL = 2e-6
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("case", tl.CASES, ids=[c[0] for c in tl.CASES])
+def test_timeloop_oracle_matches_reference_kernels_fixture(case):
+    got = np.load(os.path.join(tl.OUT, case[0] + ".npz"))
+    for precision in ("f32", "f64"):
+        o = tl.make_oracle(case, precision)
+        o.run(case[2])
+        for f in oracle.FIELDS[:15]:
+            want = got[f]
+            assert want.shape == (tl.kmax(case), case[1][1], case[1][0])
+            assert np.abs(want).max() > 0
+            err = rel_l2(tl.region(case, o.field(f)), want)
+            assert err <= TL_TOL, (case[0], precision, f, err)
+        o.close()
+
+
+needs_ref = pytest.mark.skipif(not os.path.exists(tl.REF_LIB), reason="reference kernels not built here")
+
+
+@needs_ref
+@pytest.mark.parametrize("case", tl.CASES + tl.LIVE_CASES, ids=[c[0] for c in tl.CASES + tl.LIVE_CASES])
+def test_timeloop_oracle_matches_reference_kernels_live(case):
+    ref = tl.run_reference(tl.load_ref(), case)
+    o = tl.make_oracle(case)
+    o.run(case[2])
+    for f in range(15):
+        err = rel_l2(tl.region(case, o.field(oracle.FIELDS[f])), tl.region(case, ref[f]))
+        assert err <= TL_TOL, (case[0], oracle.FIELDS[f], err)
+    o.close()
+
+
+@needs_ref
+def test_timeloop_comparison_detects_a_misplaced_coefficient():
+    """The comparison has the power to see a wrong coefficient: the reference
+    kernels given the relaxation coefficients with the x parity swapped (the
+    kind of divergence the reference's own texture set-up has, by starting
+    its parity from ghost indices) disagree with the oracle by orders of
+    magnitude more than the bar, in the memory variables and the stresses."""
+    case = tl.CASES[0]
+    o = tl.make_oracle(case)
+    t1, t2 = o.tau12()
+    swap = lambda t: t.reshape(2, 2, 2)[:, :, ::-1].ravel().copy()   # noqa: E731
+    ref = tl.run_reference(tl.load_ref(), case, tau_override=(swap(t1), swap(t2)))
+    o.run(case[2])
+    for f in ("r1", "r4", "xx"):
+        err = rel_l2(tl.region(case, o.field(f)), tl.region(case, ref[oracle.FIELDS.index(f)]))
+        assert err > 100 * TL_TOL, (f, err)
+    o.close()
