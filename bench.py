@@ -333,14 +333,20 @@ def pct(x, q):
 
 
 def run_serve(args):
+    print(json.dumps(serve_stream(args.serve_requests, args.serve_nst_scale, args.serve_load, args.serve_active,
+                                  args.serve_policy, args.serve_fill)))
+    return 0
+
+
+def serve_stream(n_requests, nst_scale, load, active, policy, fill):
     """Serial solves (one at a time) give the service times; the same requests
-    then arrive as a Poisson stream at `--serve-load` times the serial service
-    rate and go through the continuous-batching server.  Latency = completion
+    then arrive as a Poisson stream at `load` times the serial service rate
+    and go through the continuous-batching server.  Latency = completion
     minus arrival.  The serial latencies are those of a FIFO single server fed
     the same arrival times with the measured service times."""
     import queue
     import awpsgt
-    specs = serve_requests(args.serve_requests, 1, args.serve_nst_scale)
+    specs = serve_requests(n_requests, 1, nst_scale)
     work = [sp["nx"] * sp["ny"] * sp["nz"] * len(sp["igreen"]) * (sp["nst"] + 1) for sp in specs]
 
     def producer(out_q):
@@ -364,7 +370,7 @@ def run_serve(args):
         service.append(time.perf_counter() - t0)
     th.join()
     total_serial = float(sum(service))
-    rate = args.serve_load * len(specs) / total_serial
+    rate = load * len(specs) / total_serial
     arr = np.cumsum(np.random.default_rng(1).exponential(1.0 / rate, size=len(specs)))
     arr -= arr[0]
     free_at, serial_lat = 0.0, []
@@ -379,8 +385,8 @@ def run_serve(args):
     # submitter fall behind the arrival schedule
     reqs = [build_request(sp) for sp in specs]
     lat, ids, late = [], [], []
-    with awpsgt.Server(device=0, max_active=args.serve_active, chunk_steps=10) as sv:
-        sv.configure(args.serve_policy, args.serve_fill, 0.0)
+    with awpsgt.Server(device=0, max_active=active, chunk_steps=10) as sv:
+        sv.configure(policy, fill, 0.0)
         t_start = sv.time()
         for k, sp in enumerate(specs):
             req = reqs[k]
@@ -406,14 +412,13 @@ def run_serve(args):
         "serial": {"p50_s": pct(serial_lat, 50), "p99_s": pct(serial_lat, 99),
                    "throughput": {"value": sum(work) / total_serial * 1e-9, "unit": METRIC,
                                   "busy_s": total_serial}},
-        "offered_load": args.serve_load, "arrival_rate_per_s": rate, "requests": len(specs),
+        "offered_load": load, "arrival_rate_per_s": rate, "requests": len(specs),
         "max_submit_lateness_s": float(max(late)),
-        "max_active": args.serve_active, "policy": args.serve_policy, "dtype": "f32", "data": "synthetic (seeded layered media, seeded arrivals)",
+        "max_active": active, "policy": policy, "dtype": "f32", "data": "synthetic (seeded layered media, seeded arrivals)",
         "config": {"workload": "serving stream: %d requests, sizes 100x100x50..500x500x250, NST 1000-4000 x %g"
-                               % (len(specs), args.serve_nst_scale), "cell_updates": int(sum(work))},
+                               % (len(specs), nst_scale), "cell_updates": int(sum(work))},
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def synth_workload():
@@ -531,6 +536,60 @@ def run_synth(args):
     return 0
 
 
+def window_rate(w, media, pts, stfs, device, precision, kernel, tuning, prefill, warm_ts, timed_ts):
+    """Device-resident rate of one stepper / storage mode over the same window
+    of the job as the headline measurement: Gcell-updates/s, the dominant
+    kernel's roofline fraction and the clocks seen."""
+    import awpsgt
+    s = make_solver(w, media, pts, stfs, device, precision, kernel, tuning if kernel == "auto" else None)
+    s.run(prefill + warm_ts)
+    with ClockSampler(device) as clk:
+        st0 = s.stats()
+        s.run(timed_ts)
+        st1 = s.stats()
+    prof = s.profile(w.ntiskp_sgt)
+    bpcu = awpsgt.bytes_per_cell_update(s.p)
+    s.close()
+    peak, _ = peaks()
+    dom = max((k for k in prof if prof[k]["launches"] and prof[k]["bytes"] > 0),
+              key=lambda k: prof[k]["ms"] * prof[k]["launches"])
+    cells = w.nx * w.ny * w.nz * len(w.igreen)
+    return {"value": cells * timed_ts / (st1.seconds_loop - st0.seconds_loop) * 1e-9, "unit": METRIC,
+            "precision": precision, "kernel": kernel, "bytes_per_cell_update": bpcu,
+            "dominant_kernel": dom, "frac": prof[dom]["bytes"] / (prof[dom]["ms"] * 1e-3) / 1e9 / peak,
+            "clocks": clk.summary()}
+
+
+def small_case_error(precision, nx=64, ny=64, nz=48, nst=600):
+    """SGT relative-L2 error of a storage mode against the FP64 oracle on a
+    reduced layered case (fx, h = 100 m, dt = 5 ms, nst steps, 200 points),
+    measured in the same run: the GPU solve against the FP64 restatement on
+    the host cores."""
+    import awpsgt
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    dh, dt = 100.0, 0.005
+    media = ai.layered_media(nx, ny, nz, dh, seed=5)
+    pts = ai.sgt_points(nx, ny, min(nz, 101), 200, seed=0)
+    stf = ai.gaussian_derivative_stf(nst, dt, f0=0.5)
+    src = (nx // 2, ny // 2, 21)
+    kw = dict(nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5, socalq=1, ntiskp_sgt=10, write_step=nst // 10)
+    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=dh, dt=dt, nt=nst + 1, nst=nst, igreen=1, precision="f64", **kw)
+    o.load_media(media)
+    o.set_source([src], stf)
+    o.set_points(pts)
+    o.run(nst + 1)
+    ref = o.sgt().astype(np.float64)
+    o.close()
+    p = awpsgt.make_params(nx, ny, nz, dh, dt, nst + 1, nst=nst, igreen=(1,), precision=precision, **kw)
+    with awpsgt.Solver(p) as s:
+        s.load_media(media)
+        s.set_source(0, [src], stf)
+        s.set_points(pts)
+        g = s.run(nst + 1, with_sgt=True)[0].astype(np.float64)
+    return float(np.linalg.norm(g - ref) / np.linalg.norm(ref))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -542,6 +601,9 @@ def main():
     ap.add_argument("--e2e-solves", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the plain-FP32 and block-floating-point windows, the error check and the short "
+                         "serving stream of the 1-GPU line")
     ap.add_argument("--config", type=int, default=0, help="workload 1..4 (default 2: 400x400x200 fx+fy+fz)")
     ap.add_argument("--grid", default="", help="nx,ny,nz: reduced grid for profiling captures")
     ap.add_argument("--components", type=int, default=0, help="first n of the fx, fy, fz components")
@@ -573,8 +635,14 @@ def main():
     dist, rank, world, local = dist_setup(args.gpus)
     import awpsgt
     w = workload(args)
+    # one complete SGT job per site; the sites are dealt to the ranks (one
+    # each here: weak scaling, no data-path collective).  Site k differs from
+    # the others by its seeded SGT points.
+    sites = shard_jobs(list(range(world)), rank, world)
+    site = sites[0]
     media = w.media()
-    pts = w.points()
+    zmax = min(w.nz, max(1, int(round(10000.0 / w.dh)) + 1))
+    pts = ai.sgt_points(w.nx, w.ny, zmax, w.npts, seed=site)
     stfs = [w.stf(q) for q in range(len(w.igreen))]
     ncomp = len(w.igreen)
     cells = w.nx * w.ny * w.nz
@@ -681,13 +749,28 @@ def main():
                        w.nt),
                    "precision": args.precision, "l2": "inputs larger than L2 (%.1f GB state)" % (
                        s.p.nx * s.p.ny * s.p.nz * 4 * (15 * ncomp + 5) / 1e9),
-                   "parallelism": "independent SGT jobs, one per GPU" if world > 1 else "single GPU",
+                   "parallelism": "independent SGT jobs (sites) dealt to the GPUs" if world > 1 else "single GPU",
+                   "site": site,
                    "tuning": used_tuning, "autotune": tune_info},
         "roofline": roofline,
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "kernels": prof,
     }
+    if world == 1 and not args.no_extras and not args.grid:
+        # the plain FP32 two-sweep stepper (the comparison point of the north-star
+        # ratio) and block floating point memory variables on the same window
+        warm_ts, timed_ts = args.warmup * per_step_ts, min(args.steps, 10) * per_step_ts
+        plain = window_rate(w, media, pts, stfs, local, "f32", "two_sweep", None, prefill, warm_ts, timed_ts)
+        line["plain_fp32"] = plain
+        line["vs_plain_fp32"] = value / plain["value"]
+        if args.precision != "bfp":
+            b = window_rate(w, media, pts, stfs, local, "bfp", "auto", None, prefill, warm_ts, timed_ts)
+            b["vs_plain_fp32"] = b["value"] / plain["value"]
+            b["sgt_rel_l2_vs_fp64"] = small_case_error("bfp")
+            b["error_case"] = "64x64x48 layered, fx, 600 steps, 200 points (FP64 oracle on the host, same run)"
+            line["bfp"] = b
+        line["serving"] = serve_stream(16, 0.1, 1.2, 4, "fifo", 0.0)
     if rank == 0:
         line["clocks"] = clk.summary()
         if not args.no_cpu and world == 1:

@@ -35,6 +35,10 @@ struct AwpStepArgs {
     int staged_batch;            /* staged sweeps with the components side by side in one item:
                                     bit 0 stress, bit 1 velocity */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
+    unsigned long long wait_ns;  /* bound of one barrier wait of the staged sweeps */
+    int withhold;                /* test injection, -1 = off: block 0's producer of the
+                                    staged stress sweep issues no copies for ring use
+                                    `withhold`, so its consumers' wait runs out */
 };
 
 cudaError_t awp_launch_media_interior(const AwpGeom &g, const AwpMedia &md, const float *raw, int zf0, int nzs,

@@ -106,6 +106,11 @@ struct awp_solver {
     int next_check;
     int pending;                     /* asynchronous steps not yet synced  */
     int pending_steps;
+    /* failure injection for tests (environment, read by awp_create) */
+    unsigned long long wait_ns;      /* bound of a staged barrier wait (AWP_TEST_WAIT_US) */
+    int withhold;                    /* AWP_TEST_TMA_WITHHOLD: ring use block 0 withholds, -1 off */
+    int fail_alloc;                  /* AWP_TEST_FAIL_ALLOC: that device allocation fails, 0 off */
+    int nalloc;                      /* device allocations so far          */
 };
 
 /* ------------------------------------------------------------------ */
@@ -421,6 +426,11 @@ extern "C" void awp_release_cached_memory(void) { blk_trim(-1); }
 
 static awp_status dalloc(awp_solver *s, void **ptr, size_t bytes)
 {
+    if (s->fail_alloc > 0 && ++s->nalloc == s->fail_alloc) {
+        *ptr = NULL;
+        return set_err(AWP_ERR_OOM, "device allocation %d of %zu bytes failed (injected by AWP_TEST_FAIL_ALLOC)",
+                       s->fail_alloc, bytes);
+    }
     cudaError_t e = blk_alloc(s->p.device, ptr, bytes);
     if (e != cudaSuccess) {
         *ptr = NULL;
@@ -516,6 +526,12 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     memset(s, 0, sizeof *s);
     s->p = *pin;
     s->g = make_geom(pin);
+    s->withhold = env_int("AWP_TEST_TMA_WITHHOLD", -1);
+    {
+        const int us = env_int("AWP_TEST_WAIT_US", 0);
+        s->wait_ns = us > 0 ? (unsigned long long)us * 1000ull : 2000000000ull;
+    }
+    s->fail_alloc = env_int("AWP_TEST_FAIL_ALLOC", 0);
     s->fused = fused_of(pin);
     s->store = store_of(pin);
     s->rstore = rstore_of(pin);
@@ -1124,6 +1140,8 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_rpt_vel = s->staged_rpt_vel;
     a.staged_batch = s->staged_batch;
     a.kerr = s->flag + 1;
+    a.wait_ns = s->wait_ns;
+    a.withhold = s->withhold;
 
     memset(&pa, 0, sizeof pa);
     pa.g = s->g; pa.ncomp = p->ncomp; pa.nst = p->nst; pa.nt = p->nt;
@@ -1293,8 +1311,8 @@ extern "C" awp_status awp_sync(awp_solver *s)
         int flag[2] = {0, 0};
         CU(cudaMemcpyAsync(flag, s->flag, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
         CU(cudaStreamSynchronize(s->stream));
-        if (flag[1]) return set_err(AWP_ERR_CUDA, "staged stepper: a tile barrier wait ran out (error word %d)",
-                                    flag[1]);
+        if (flag[1]) return set_err(AWP_ERR_TIMEOUT, "staged stepper: a tile barrier wait ran out after %.3f s "
+                                    "(error word %d); the solve's state is not valid", s->wait_ns * 1e-9, flag[1]);
         if (flag[0]) return set_err(AWP_ERR_UNSTABLE, "stability monitor: non-finite wavefield energy by step %d",
                                     s->steps_done);
     }
@@ -1500,13 +1518,16 @@ static awp_status bfp_get(awp_solver *s, int q, int field, float *out)
     return AWP_OK;
 }
 
-/* replaces one memory variable: its group is decoded, the field replaced and
- * the group encoded again (the other group's exponent byte is kept) */
-static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
+/* stores one group of memory variables (grp 0: r1..r3, 1: r4..r6) of
+ * component q: v[b] is the new value of member b, or NULL to keep the group's
+ * current (decoded) value; the group is encoded once from the three values
+ * (the other group's exponent byte is kept).  Setting all three members at
+ * once restores decoded values exactly; setting them one at a time need not,
+ * since each encode flushes to zero what lies below its exponent's range. */
+static awp_status bfp_set_group(awp_solver *s, int q, int grp, const float *const v[3])
 {
     const AwpGeom &g = s->g;
     const size_t w = (size_t)(g.nx + 4), rows = (size_t)(g.ny + 4) * (size_t)(g.nz + 4), n = w * rows;
-    const int a = field - AF_R1, grp = a / 3;
     std::vector<int16_t> mm(3 * n);
     std::vector<uint16_t> xx(n);
     int16_t *m[3] = {&mm[0], &mm[n], &mm[2 * n]};
@@ -1515,10 +1536,10 @@ static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
     for (size_t c = 0; c < n; c++) {
         const uint32_t e = grp ? (uint32_t)(xx[c] >> 8) : (uint32_t)(xx[c] & 0xffu);
         const float down = bfp_down(e);
-        float v[3] = {(float)m[0][c] * down, (float)m[1][c] * down, (float)m[2][c] * down};
-        v[a % 3] = in[c];
+        float val[3];
+        for (int b = 0; b < 3; b++) val[b] = v[b] ? v[b][c] : (float)m[b][c] * down;
         int16_t nm[3];
-        const uint32_t ne = bfp_enc3_host(v, nm);
+        const uint32_t ne = bfp_enc3_host(val, nm);
         for (int b = 0; b < 3; b++) m[b][c] = nm[b];
         xx[c] = grp ? (uint16_t)((xx[c] & 0x00ffu) | (ne << 8)) : (uint16_t)((xx[c] & 0xff00u) | ne);
     }
@@ -1529,6 +1550,14 @@ static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
     CU(cudaMemcpy2D((uint16_t *)cp.f[AF_RX] + (AWP_XO - 2), (size_t)g.px * 2, xx.data(), w * 2, w * 2, rows,
                     cudaMemcpyHostToDevice));
     return AWP_OK;
+}
+
+static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
+{
+    const int a = field - AF_R1;
+    const float *v[3] = {NULL, NULL, NULL};
+    v[a % 3] = in;
+    return bfp_set_group(s, q, a / 3, v);
 }
 
 extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *out)
@@ -1764,6 +1793,16 @@ extern "C" awp_status awp_checkpoint_read(awp_solver *s, const char *dir, int *s
         FILE *f = fopen(path, "rb");
         if (!f) { st = set_err(AWP_ERR_IO, "checkpoint %s missing", path); break; }
         for (int fld = 0; fld < AWP_NF_STATE && st == AWP_OK; fld++) {
+            if (fld >= AF_R1 && s->rstore == AWP_STORE_BFP && s->comp[0][q].f[fld]) {
+                /* block floating point: each group of three encoded at once */
+                if ((fld - AF_R1) % 3 == 0) {
+                    std::vector<float> grp(3 * nvol);
+                    st = read_all(f, grp.data(), 3 * nvol * sizeof(float), path);
+                    const float *v[3] = {&grp[0], &grp[nvol], &grp[2 * nvol]};
+                    if (st == AWP_OK) st = bfp_set_group(s, q, (fld - AF_R1) / 3, v);
+                }
+                continue;
+            }
             st = read_all(f, buf, nvol * sizeof(float), path);
             if (st == AWP_OK && s->comp[0][q].f[fld]) st = awp_set_field(s, q, fld, buf);
         }

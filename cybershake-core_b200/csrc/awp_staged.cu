@@ -45,7 +45,13 @@
 #define ST_MT (ST_W * ST_MR)         /* floats a media tile receives (1440 B)   */
 #define ST_MP 384                    /* floats reserved per media tile (1536 B) */
 #define ST_PT (ST_X * ST_Y)          /* floats of a point tile (no halo)        */
-#define ST_WAIT_NS 2000000000ull     /* bound of one barrier wait               */
+
+/* bound of every barrier wait (the solver's setting, 2 s by default) and the
+ * test-only injection of AwpStepArgs::withhold */
+struct AwpWait {
+    unsigned long long ns;
+    int withhold;
+};
 #define ST_VEL_D 3                   /* levels in flight, velocity sweep        */
 
 struct AwpStagedVelMaps {
@@ -103,13 +109,13 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 /* true once the phase of the given parity has completed; false after the bound */
-__device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity)
+__device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity, uint64_t limit_ns)
 {
     if (mb_try(b, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t n = 0; n < (1u << 26); ++n) {
         if (mb_try(b, parity)) return true;
-        if ((n & 63) == 63 && global_ns() - t0 > ST_WAIT_NS) return false;
+        if ((n & 63) == 63 && global_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
@@ -168,13 +174,14 @@ __device__ __forceinline__ void mb_arrive(uint64_t *b)
 }
 
 /* bounded wait that also gives up once another thread has flagged an abort */
-__device__ __forceinline__ bool mb_wait_or_abort(uint64_t *b, uint32_t parity, const volatile int *abort)
+__device__ __forceinline__ bool mb_wait_or_abort(uint64_t *b, uint32_t parity, const volatile int *abort,
+                                                 uint64_t limit_ns)
 {
     if (mb_try(b, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t n = 0; n < (1u << 26); ++n) {
         if (mb_try(b, parity)) return true;
-        if ((n & 63) == 63 && (*abort || global_ns() - t0 > ST_WAIT_NS)) return false;
+        if ((n & 63) == 63 && (*abort || global_ns() - t0 > limit_ns)) return false;
     }
     return false;
 }
@@ -199,19 +206,27 @@ __device__ __forceinline__ void ring_init(uint64_t *full, uint64_t *empty, volat
 }
 
 /* the producer's last act: the most recent use of every slot has landed, so
- * no copy into this block's shared memory is still in flight when it exits */
+ * no copy into this block's shared memory is still in flight when it exits
+ * (`skip`: a use it issued nothing for) */
 template <int S>
-__device__ __forceinline__ void ring_drain(uint64_t *full, uint32_t uses)
+__device__ __forceinline__ void ring_drain(uint64_t *full, uint32_t uses, uint64_t limit_ns, uint32_t skip = 0xffffffffu)
 {
     for (uint32_t u = uses > (uint32_t)S ? uses - S : 0; u < uses; ++u)
-        if (!mb_wait(&full[u % S], (u / S) & 1)) return;
+        if (u != skip && !mb_wait(&full[u % S], (u / S) & 1, limit_ns)) return;
+}
+
+/* the ring use block 0's producer withholds under the test injection */
+__device__ __forceinline__ uint32_t withheld_use(const AwpWait &wt)
+{
+    return blockIdx.x == 0 && wt.withhold >= 0 ? (uint32_t)wt.withhold : 0xffffffffu;
 }
 
 /* producer: wait until use `use` of its slot may be refilled */
 template <int S>
-__device__ __forceinline__ bool ring_acquire(uint64_t *empty, uint32_t use, const volatile int *abort)
+__device__ __forceinline__ bool ring_acquire(uint64_t *empty, uint32_t use, const volatile int *abort,
+                                             uint64_t limit_ns)
 {
-    return use < (uint32_t)S || mb_wait_or_abort(&empty[use % S], ((use / S) - 1) & 1, abort);
+    return use < (uint32_t)S || mb_wait_or_abort(&empty[use % S], ((use / S) - 1) & 1, abort, limit_ns);
 }
 
 /* ------------------------------------------------------------------ */
@@ -261,7 +276,7 @@ template <int D, int UNR, int RPT>
 __global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
-          const float *__restrict__ cz, float dth, AwpWork w, int *err)
+          const float *__restrict__ cz, float dth, AwpWork w, int *err, AwpWait wt)
 {
     constexpr int S = 1 + D;          /* level k in use, D in flight */
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
@@ -282,7 +297,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             int bx, by, k0, k1;
             work_item(g, w, t, bx, by, k0, k1);
             for (int k = k0; k <= k1; ++k, ++use) {
-                ok = ring_acquire<S>(empty, use, &abort_s);
+                ok = ring_acquire<S>(empty, use, &abort_s, wt.ns);
                 if (!ok) break;
                 vel_issue<S>(maps.st[q], &maps.d1, maps.p[q], ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
@@ -291,7 +306,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
             abort_s = 1;
             atomicOr(err, AWP_KERR_TMA_WAIT);
         }
-        ring_drain<S>(full, use);
+        ring_drain<S>(full, use, wt.ns);
         return;
     }
 
@@ -336,7 +351,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
                 if (live[r] && k < k1) { xz_n[r] = XZ[c + 2 * sz]; yz_n[r] = YZ[c + 2 * sz]; zz_n[r] = ZZ[c + 3 * sz]; }
             }
             /* warp-uniform outcome, so a warp leaves together or not at all */
-            if (!__all_sync(0xffffffffu, mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s))) {
+            if (!__all_sync(0xffffffffu, mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s, wt.ns))) {
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
                 return;
@@ -390,7 +405,7 @@ template <int NCB, int CS>
 __global__ void __launch_bounds__(ST_THREADS, 2)
 k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
            const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
-           const float *__restrict__ cz, float dth, AwpWork w, int *err)
+           const float *__restrict__ cz, float dth, AwpWork w, int *err, AwpWait wt)
 {
     extern __shared__ unsigned char st_smem[];
     float *mring = ring_base(st_smem);
@@ -417,7 +432,7 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
             const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1;
             const int x = tile_x(i0), xp = i0 + AWP_XO - 1;
             for (int k = k0; ok && k <= k1; ++k) {
-                ok = ring_acquire<VB_MS>(mempty, um, &abort_s);
+                ok = ring_acquire<VB_MS>(mempty, um, &abort_s, wt.ns);
                 if (!ok) break;
                 {
                     float *sl = mring + (um % VB_MS) * ST_MP;
@@ -429,7 +444,7 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
                 ++um;
 #pragma unroll
                 for (int q = 0; q < NCB; ++q) {
-                    ok = ring_acquire<CS>(cempty, uc, &abort_s);
+                    ok = ring_acquire<CS>(cempty, uc, &abort_s, wt.ns);
                     if (!ok) break;
                     float *sl = cring + (uc % CS) * VB_CSLOT;
                     uint64_t *b = &cfull[uc % CS];
@@ -447,8 +462,8 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
             abort_s = 1;
             atomicOr(err, AWP_KERR_TMA_WAIT);
         }
-        ring_drain<VB_MS>(mfull, um);
-        ring_drain<CS>(cfull, uc);
+        ring_drain<VB_MS>(mfull, um, wt.ns);
+        ring_drain<CS>(cfull, uc, wt.ns);
         return;
     }
 
@@ -488,7 +503,7 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
 #pragma unroll 1
         for (int k = k0; k <= k1; ++k, cc += sz, ++um) {
             const float czk = cz[k];
-            if (!__all_sync(0xffffffffu, mb_wait_or_abort(&mfull[um % VB_MS], (um / VB_MS) & 1, &abort_s))) {
+            if (!__all_sync(0xffffffffu, mb_wait_or_abort(&mfull[um % VB_MS], (um / VB_MS) & 1, &abort_s, wt.ns))) {
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
                 return;
@@ -512,7 +527,7 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
                     pyz[q] = tab[q].f[AF_YZ][cc + 2 * sz];
                     pzz[q] = tab[q].f[AF_ZZ][cc + 3 * sz];
                 }
-                if (!__all_sync(0xffffffffu, mb_wait_or_abort(&cfull[uc % CS], (uc / CS) & 1, &abort_s))) {
+                if (!__all_sync(0xffffffffu, mb_wait_or_abort(&cfull[uc % CS], (uc / CS) & 1, &abort_s, wt.ns))) {
                     abort_s = 1;
                     atomicOr(err, AWP_KERR_TMA_WAIT);
                     return;
@@ -643,7 +658,7 @@ template <class TR, int UNR, int RPT>
 __global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
-          const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
+          const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err, AwpWait wt)
 {
     constexpr int S = 2 + STR_D;      /* levels k-1 and k in use, STR_D in flight */
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
@@ -669,8 +684,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             int bx, by, k0, k1;
             work_item(g, w, t, bx, by, k0, k1);
             for (int k = k0 - 1; k <= k1; ++k, ++use) {
-                ok = ring_acquire<S>(empty, use, &abort_s);
+                ok = ring_acquire<S>(empty, use, &abort_s, wt.ns);
                 if (!ok) break;
+                if (use == withheld_use(wt)) continue;   /* test injection: nothing issued, no arrival */
                 str_issue<S, TR>(maps, q, nve, ring, full, use, bx * ST_X + 1, by * ST_Y + 1, k);
             }
         }
@@ -678,7 +694,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             abort_s = 1;
             atomicOr(err, AWP_KERR_TMA_WAIT);
         }
-        ring_drain<S>(full, use);
+        ring_drain<S>(full, use, wt.ns, withheld_use(wt));
         return;
     }
 
@@ -723,8 +739,8 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                 if (live[r] && k < k1) { up3[r] = U[c + 3 * sz]; vp3[r] = V[c + 3 * sz]; wp2[r] = W[c + 2 * sz]; }
             }
             bool ok = true;
-            if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s);
-            if (ok) ok = mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s);
+            if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s, wt.ns);
+            if (ok) ok = mb_wait_or_abort(&full[use % S], (use / S) & 1, &abort_s, wt.ns);
             if (!__all_sync(0xffffffffu, ok)) {   /* warp-uniform outcome */
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
@@ -814,7 +830,7 @@ template <class TR, int NCB, int STB_CS, int RPT>
 __global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 2)
 k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs,
            const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
-           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err)
+           const float *__restrict__ tau, float dth, float dt, float dh1, AwpWork w, int nve, int *err, AwpWait wt)
 {
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
@@ -843,9 +859,9 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
             const int i0 = bx * ST_X + 1, j0 = by * ST_Y + 1;
             const int x = tile_x(i0), xp = i0 + AWP_XO - 1;
             for (int k = k0 - 1; ok && k <= k1; ++k) {
-                ok = ring_acquire<STB_MS>(mempty, um, &abort_s);
+                ok = ring_acquire<STB_MS>(mempty, um, &abort_s, wt.ns);
                 if (!ok) break;
-                {
+                if (um != withheld_use(wt)) {                 /* test injection: nothing issued, no arrival */
                     float *sl = mring + (um % STB_MS) * STB_MSLOT;
                     uint64_t *b = &mfull[um % STB_MS];
                     fence_async_smem();
@@ -856,7 +872,7 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                 if (k < k0) continue;
 #pragma unroll
                 for (int q = 0; q < NCB; ++q) {
-                    ok = ring_acquire<STB_CS>(cempty, uc, &abort_s);
+                    ok = ring_acquire<STB_CS>(cempty, uc, &abort_s, wt.ns);
                     if (!ok) break;
                     float *sl = cring + (uc % STB_CS) * STB_CSLOT;
                     uint64_t *b = &cfull[uc % STB_CS];
@@ -875,8 +891,8 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
             abort_s = 1;
             atomicOr(err, AWP_KERR_TMA_WAIT);
         }
-        ring_drain<STB_MS>(mfull, um);
-        ring_drain<STB_CS>(cfull, uc);
+        ring_drain<STB_MS>(mfull, um, wt.ns, withheld_use(wt));
+        ring_drain<STB_CS>(cfull, uc, wt.ns);
         return;
     }
 
@@ -922,8 +938,8 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
             const uint32_t mk = um0 + (uint32_t)(k - k0 + 1), mm = mk - 1;
             const float czk = cz[k];
             bool ok = true;
-            if (k == k0) ok = mb_wait_or_abort(&mfull[mm % STB_MS], (mm / STB_MS) & 1, &abort_s);
-            if (ok) ok = mb_wait_or_abort(&mfull[mk % STB_MS], (mk / STB_MS) & 1, &abort_s);
+            if (k == k0) ok = mb_wait_or_abort(&mfull[mm % STB_MS], (mm / STB_MS) & 1, &abort_s, wt.ns);
+            if (ok) ok = mb_wait_or_abort(&mfull[mk % STB_MS], (mk / STB_MS) & 1, &abort_s, wt.ns);
             if (!__all_sync(0xffffffffu, ok)) {   /* warp-uniform outcome */
                 abort_s = 1;
                 atomicOr(err, AWP_KERR_TMA_WAIT);
@@ -956,7 +972,7 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                         pw[r][q] = tab[q].f[AF_W][c + 2 * sz];
                     }
                 }
-                ok = mb_wait_or_abort(&cfull[uc % STB_CS], (uc / STB_CS) & 1, &abort_s);
+                ok = mb_wait_or_abort(&cfull[uc % STB_CS], (uc / STB_CS) & 1, &abort_s, wt.ns);
                 if (!__all_sync(0xffffffffu, ok)) {
                     abort_s = 1;
                     atomicOr(err, AWP_KERR_TMA_WAIT);
@@ -1091,6 +1107,14 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
 
 void awp_staged_destroy(AwpStaged *s) { free(s); }
 
+static AwpWait awp_wait_of(const AwpStepArgs &s)
+{
+    AwpWait w;
+    w.ns = s.wait_ns ? s.wait_ns : 2000000000ull;
+    w.withhold = s.withhold;
+    return w;
+}
+
 static AwpWork staged_work(const AwpGeom &g, int kchunk, int ncomp)
 {
     AwpWork w;
@@ -1140,7 +1164,7 @@ static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaS
     if (e != cudaSuccess) return e;
     k_vel_tma<ST_VEL_D, U, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
         st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w,
-        s.kerr);
+        s.kerr, awp_wait_of(s));
     return cudaGetLastError();
 }
 
@@ -1155,7 +1179,7 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
     if (e != cudaSuccess) return e;
     k_str_tma<TR, UNR, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
                                                                        s.staged_qslow, s.cx, s.cy, s.cz, s.tau,
-                                                                       s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+                                                                       s.dth, s.dt, s.dh1, w, s.nve, s.kerr, awp_wait_of(s));
     return cudaGetLastError();
 }
 
@@ -1170,7 +1194,7 @@ static cudaError_t launch_str_bc(const AwpStaged *st, const AwpStepArgs &s, cuda
     cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_str_tmab<TR, NCB, CS, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
-        st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr);
+        st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr, awp_wait_of(s));
     return cudaGetLastError();
 }
 
@@ -1204,7 +1228,7 @@ static cudaError_t launch_vel_b(const AwpStaged *st, const AwpStepArgs &s, cudaS
     cudaError_t e = staged_grid(k_vel_tmab<NCB, CS>, smem, w.nitems, &grid);
     if (e != cudaSuccess) return e;
     k_vel_tmab<NCB, CS><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
-        st->vm, s.g, comp_set3(s), (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w, s.kerr);
+        st->vm, s.g, comp_set3(s), (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w, s.kerr, awp_wait_of(s));
     return cudaGetLastError();
 }
 

@@ -185,7 +185,11 @@ awp_status awp_get_field(awp_solver *s, int comp, int field, float *out);
 
 /* Sets one state field (0..14, numbering as awp_get_field) of one component
  * from the padded host layout in[(k+1)][(j+1)][(i+1)], extents (nz+4, ny+4,
- * nx+4), float32; memory variables stored in 16 bits are rounded to nearest.
+ * nx+4), float32; memory variables stored in 16 bits are rounded to nearest
+ * (bf16), or, in block floating point, their group of three (r1..r3 or
+ * r4..r6) is encoded again with the new member -- values below the group
+ * exponent's range become zero, so restoring decoded values needs all three
+ * members, as awp_checkpoint_read sets them.
  * Used by the checkpoint restart below and to start a solve from a given
  * state.  Replaces the state part of the checkpoint read
  * (AWP-ODC-SGT/src/pmcl3d.f:1044-1056). */

@@ -5,11 +5,12 @@ module, as the oracle the device results are compared with or as the timed CPU
 restatement of the reference.  The product path (cybershake-core_b200/) never
 imports it.
 
-TIME LOOP PARITY UNPINNED: the reference ships no solver tests or golden
-outputs and its time loop cannot be built here; the oracle is a
-statement-by-statement restatement of the Fortran (see the header of
-awp_oracle.c), checked by known-answer tests.  Its set-up stage is pinned to
-the reference CUDA variant's host code (setup_reference below), and the
+PINNING: the reference ships no solver tests or golden outputs and its
+Fortran cannot be built here; the oracle is a statement-by-statement
+restatement of the Fortran (see the header of awp_oracle.c).  Its set-up stage
+is pinned to the reference CUDA variant's host code (setup_reference below),
+its time loop to that variant's own velocity and stress kernels run on the
+host (tests/golden/make_timeloop_golden.py, within 2e-6 relative L2), and the
 synthesis oracle to DirectSynth's own functions (synth_reference).
 """
 from __future__ import annotations
