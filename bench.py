@@ -560,34 +560,14 @@ def window_rate(w, media, pts, stfs, device, precision, kernel, tuning, prefill,
             "clocks": clk.summary()}
 
 
-def small_case_error(precision, nx=64, ny=64, nz=48, nst=600):
-    """SGT relative-L2 error of a storage mode against the FP64 oracle on a
-    reduced layered case (fx, h = 100 m, dt = 5 ms, nst steps, 200 points),
-    measured in the same run: the GPU solve against the FP64 restatement on
-    the host cores."""
-    import awpsgt
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    dh, dt = 100.0, 0.005
-    media = ai.layered_media(nx, ny, nz, dh, seed=5)
-    pts = ai.sgt_points(nx, ny, min(nz, 101), 200, seed=0)
-    stf = ai.gaussian_derivative_stf(nst, dt, f0=0.5)
-    src = (nx // 2, ny // 2, 21)
-    kw = dict(nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5, socalq=1, ntiskp_sgt=10, write_step=nst // 10)
-    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=dh, dt=dt, nt=nst + 1, nst=nst, igreen=1, precision="f64", **kw)
-    o.load_media(media)
-    o.set_source([src], stf)
-    o.set_points(pts)
-    o.run(nst + 1)
-    ref = o.sgt().astype(np.float64)
-    o.close()
-    p = awpsgt.make_params(nx, ny, nz, dh, dt, nst + 1, nst=nst, igreen=(1,), precision=precision, **kw)
-    with awpsgt.Solver(p) as s:
-        s.load_media(media)
-        s.set_source(0, [src], stf)
-        s.set_points(pts)
-        g = s.run(nst + 1, with_sgt=True)[0].astype(np.float64)
-    return float(np.linalg.norm(g - ref) / np.linalg.norm(ref))
+def precision_study():
+    """Measured SGT errors of the storage modes against the FP64 oracle
+    (profiles/precision.json, written by tests/test_precision_study.py)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "precision.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
 
 
 def main():
@@ -767,8 +747,10 @@ def main():
         if args.precision != "bfp":
             b = window_rate(w, media, pts, stfs, local, "bfp", "auto", None, prefill, warm_ts, timed_ts)
             b["vs_plain_fp32"] = b["value"] / plain["value"]
-            b["sgt_rel_l2_vs_fp64"] = small_case_error("bfp")
-            b["error_case"] = "64x64x48 layered, fx, 600 steps, 200 points (FP64 oracle on the host, same run)"
+            study = precision_study()
+            if study:
+                b["sgt_rel_l2_vs_fp64"] = {k: v.get("bfp") for k, v in study.get("cases", {}).items()}
+                b["error_source"] = study.get("source")
             line["bfp"] = b
         line["serving"] = serve_stream(16, 0.1, 1.2, 4, "fifo", 0.0)
     if rank == 0:

@@ -91,7 +91,7 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     """awp_tuning: launch shapes of the steppers (results do not depend on them)."""
     _fields_ = [(n, C.c_int) for n in ("kchunk_staged", "staged_qslow", "staged_rpt", "staged_rpt_vel", "unroll",
-                                        "ty", "kchunk", "kchunk_sweep", "staged_batch")]
+                                        "ty", "kchunk", "kchunk_sweep", "staged_batch", "sm_limit")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

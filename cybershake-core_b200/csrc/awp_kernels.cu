@@ -815,11 +815,12 @@ static AwpWork make_work(const AwpGeom &g, int ty, int kchunk)
 
 /* persistent grid: every SM filled to its occupancy, capped by the items */
 template <class K>
-static int persistent_grid(K kernel, int threads, size_t smem, int nitems)
+static int persistent_grid(K kernel, int threads, size_t smem, int nitems, int sm_limit)
 {
     int dev = 0, nsm = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (sm_limit > 0 && sm_limit < nsm) nsm = sm_limit;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) per = 1;
     const int grid = nsm * per;
     return grid < nitems ? grid : nitems;
@@ -841,7 +842,7 @@ static cudaError_t launch_fused(const AwpStepArgs &s, const MediaT<TM> &md, cons
         if (dev < 64) attr_done |= 1ull << dev;
     }
     const AwpWork w = make_work(s.g, TY, s.kchunk);
-    const int grid = persistent_grid(k_fused<NC, TM, TR, TY>, FX * TY, smem, w.nitems);
+    const int grid = persistent_grid(k_fused<NC, TM, TR, TY>, FX * TY, smem, w.nitems, s.sm_limit);
     k_fused<NC, TM, TR, TY><<<grid, b, smem, st>>>(s.g, md, cs, cn, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w,
                                                    s.nve);
     return cudaGetLastError();
@@ -852,7 +853,7 @@ static cudaError_t launch_vel(const AwpStepArgs &s, const MediaT<TM> &md, const 
                               cudaStream_t st)
 {
     const AwpWork w = make_work(s.g, ty, s.kchunk_sweep);
-    const int grid = persistent_grid(k_vel<NC, TM, UNR>, 32 * ty, 0, w.nitems);
+    const int grid = persistent_grid(k_vel<NC, TM, UNR>, 32 * ty, 0, w.nitems, s.sm_limit);
     k_vel<NC, TM, UNR><<<grid, dim3(32, ty), 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.dth, w);
     return cudaGetLastError();
 }
@@ -862,7 +863,7 @@ static cudaError_t launch_str(const AwpStepArgs &s, const MediaT<TM> &md, const 
                               cudaStream_t st)
 {
     const AwpWork w = make_work(s.g, ty, s.kchunk_sweep);
-    const int grid = persistent_grid(k_str<NC, TM, TR, UNR>, 32 * ty, 0, w.nitems);
+    const int grid = persistent_grid(k_str<NC, TM, TR, UNR>, 32 * ty, 0, w.nitems, s.sm_limit);
     k_str<NC, TM, TR, UNR><<<grid, dim3(32, ty), 0, st>>>(s.g, md, cs, s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1,
                                                           w, s.nve);
     return cudaGetLastError();

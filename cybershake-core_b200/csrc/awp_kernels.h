@@ -35,6 +35,7 @@ struct AwpStepArgs {
     int staged_batch;            /* staged sweeps with the components side by side in one item:
                                     bit 0 stress, bit 1 velocity */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
+    int sm_limit;                /* persistent grids sized for this many SMs (0 = all) */
     unsigned long long wait_ns;  /* bound of one barrier wait of the staged sweeps */
     int withhold;                /* test injection, -1 = off: block 0's producer of the
                                     staged stress sweep issues no copies for ring use

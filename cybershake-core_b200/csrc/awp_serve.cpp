@@ -42,6 +42,7 @@ struct Req {
     bool in_flight = false;
     double cells = 0;      /* cells x components: work of one step */
     double work = 0;       /* cells x components x steps           */
+    int sm_share = 0;      /* SMs its grids are sized for (0 = all)  */
 };
 
 awp_status fail(awp_status st, const char *msg)
@@ -54,6 +55,7 @@ awp_status fail(awp_status st, const char *msg)
 
 struct awp_server {
     int device;
+    int nsm = 148;                   /* SMs of the device                */
     int64_t budget;
     int64_t reserved = 0;
     int max_active;
@@ -82,6 +84,7 @@ struct awp_server {
     void sched_loop();
     void admit_loop();
     void reap_loop();
+    awp_status share_sms(Req *r, int resident);
     void end(Req *r, int state, awp_status st);
     awp_status build(Req *r);
     double resident_cells() const
@@ -127,6 +130,24 @@ awp_status awp_server::build(Req *r)
     }
     r->s = s;
     return AWP_OK;
+}
+
+/* Each resident solve's persistent grids span its share of the SMs (all of
+ * them when it is alone), so that solves sharing the GPU run side by side
+ * instead of taking turns with grids that each fill the device.  The share is
+ * set between chunks, when nothing of the solve is in flight; launch shapes
+ * do not change results. */
+awp_status awp_server::share_sms(Req *r, int resident)
+{
+    const int want = resident <= 1 ? 0 : (nsm + resident - 1) / resident;
+    if (want == r->sm_share) return AWP_OK;
+    awp_tuning t;
+    awp_status st = awp_get_tuning(r->s, &t);
+    if (st != AWP_OK) return st;
+    t.sm_limit = want;
+    st = awp_set_tuning(r->s, &t);
+    if (st == AWP_OK) r->sm_share = want;
+    return st;
 }
 
 /* steps of the next chunk: about chunk_cells cell-updates, at least `chunk`,
@@ -202,7 +223,8 @@ void awp_server::sched_loop()
             }
             if (q < 0 && st == AWP_OK) st = AWP_ERR_CUDA;
             if (st == AWP_OK && !r->cancel && steps < r->rq.params.nt) {
-                st = awp_run_async(r->s, chunk_steps_for(this, r));
+                st = share_sms(r, (int)snap.size());
+                if (st == AWP_OK) st = awp_run_async(r->s, chunk_steps_for(this, r));
                 r->in_flight = st == AWP_OK;
             }
             lk.lock();
@@ -268,6 +290,7 @@ extern "C" awp_status awp_server_create(int device, int64_t hbm_budget, int max_
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return fail(AWP_ERR_CUDA, "cudaMemGetInfo failed");
     awp_server *sv = new awp_server();
     sv->device = device;
+    cudaDeviceGetAttribute(&sv->nsm, cudaDevAttrMultiProcessorCount, device);
     sv->budget = hbm_budget > 0 ? hbm_budget : (int64_t)(0.9 * (double)fr);
     sv->max_active = max_active;
     sv->chunk = chunk_steps;

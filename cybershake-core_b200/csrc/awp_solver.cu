@@ -89,6 +89,7 @@ struct awp_solver {
     int staged_rpt;                  /* staged stress sweep rows per thread */
     int staged_rpt_vel;              /* staged velocity sweep rows per thread */
     int staged_batch;                /* staged stress: components in one item */
+    int sm_limit;                    /* persistent grids for this many SMs (0 = all) */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -1139,6 +1140,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_rpt = s->staged_rpt;
     a.staged_rpt_vel = s->staged_rpt_vel;
     a.staged_batch = s->staged_batch;
+    a.sm_limit = s->sm_limit;
     a.kerr = s->flag + 1;
     a.wait_ns = s->wait_ns;
     a.withhold = s->withhold;
@@ -2046,6 +2048,7 @@ extern "C" awp_status awp_get_tuning(awp_solver *s, awp_tuning *t)
     t->kchunk = s->kchunk;
     t->kchunk_sweep = s->kchunk_sweep;
     t->staged_batch = s->staged_batch;
+    t->sm_limit = s->sm_limit;
     return AWP_OK;
 }
 
@@ -2058,8 +2061,9 @@ extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
         return set_err(AWP_ERR_PARAM, "awp_set_tuning: z levels per work item must be 8..%d", kmax);
     if ((t->staged_qslow != 0 && t->staged_qslow != 1) || (t->staged_rpt != 1 && t->staged_rpt != 2) ||
         (t->staged_rpt_vel != 1 && t->staged_rpt_vel != 2) || (t->unroll != 1 && t->unroll != 2) ||
-        (t->ty != 4 && t->ty != 8 && t->ty != 16) || t->staged_batch < 0 || t->staged_batch > 3)
-        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16, batch 0-3");
+        (t->ty != 4 && t->ty != 8 && t->ty != 16) || t->staged_batch < 0 || t->staged_batch > 3 || t->sm_limit < 0)
+        return set_err(AWP_ERR_PARAM, "awp_set_tuning: qslow 0/1, rows per thread 1/2, unroll 1/2, ty 4/8/16, batch "
+                       "0-3, sm_limit >= 0");
     CU(cudaSetDevice(s->p.device));
     CU(cudaStreamSynchronize(s->stream));   /* no captured step in flight when its graph goes */
     s->kchunk_staged = t->kchunk_staged;
@@ -2071,6 +2075,7 @@ extern "C" awp_status awp_set_tuning(awp_solver *s, const awp_tuning *t)
     s->kchunk = t->kchunk;
     s->kchunk_sweep = t->kchunk_sweep;
     s->staged_batch = t->staged_batch;
+    s->sm_limit = t->sm_limit;
     drop_graphs(s);
     return AWP_OK;
 }

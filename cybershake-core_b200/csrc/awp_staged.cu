@@ -1127,11 +1127,12 @@ static AwpWork staged_work(const AwpGeom &g, int kchunk, int ncomp)
 }
 
 template <class K>
-static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid, int threads = ST_THREADS)
+static cudaError_t staged_grid(K kernel, size_t smem, int nitems, int *grid, int sm_limit, int threads = ST_THREADS)
 {
     int dev = 0, nsm = 148, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (sm_limit > 0 && sm_limit < nsm) nsm = sm_limit;
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
     if (e != cudaSuccess) return e;
@@ -1160,7 +1161,7 @@ static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaS
     const size_t smem = ring_bytes(1 + ST_VEL_D, VEL_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, U, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
+    cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, U, RPT>, smem, w.nitems, &grid, s.sm_limit, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_vel_tma<ST_VEL_D, U, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
         st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w,
@@ -1175,7 +1176,7 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
     const size_t smem = ring_bytes(2 + STR_D, STR_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
-    cudaError_t e = staged_grid(k_str_tma<TR, UNR, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
+    cudaError_t e = staged_grid(k_str_tma<TR, UNR, RPT>, smem, w.nitems, &grid, s.sm_limit, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_str_tma<TR, UNR, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
                                                                        s.staged_qslow, s.cx, s.cy, s.cz, s.tau,
@@ -1191,7 +1192,7 @@ static cudaError_t launch_str_bc(const AwpStaged *st, const AwpStepArgs &s, cuda
     const size_t smem = 128 + (size_t)(STB_MS * STB_MSLOT + CS * STB_CSLOT) * 4 + 2 * 8 * (STB_MS + CS);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
     int grid = 0;
-    cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS, RPT>, smem, w.nitems, &grid, 32 * (CW + 1));
+    cudaError_t e = staged_grid(k_str_tmab<TR, NCB, CS, RPT>, smem, w.nitems, &grid, s.sm_limit, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_str_tmab<TR, NCB, CS, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
         st->sm, s.g, comp_set3(s), s.cx, s.cy, s.cz, s.tau, s.dth, s.dt, s.dh1, w, s.nve, s.kerr, awp_wait_of(s));
@@ -1225,7 +1226,7 @@ static cudaError_t launch_vel_b(const AwpStaged *st, const AwpStepArgs &s, cudaS
     const size_t smem = 128 + (size_t)(VB_MS * ST_MP + CS * VB_CSLOT) * 4 + 2 * 8 * (VB_MS + CS);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, 1);
     int grid = 0;
-    cudaError_t e = staged_grid(k_vel_tmab<NCB, CS>, smem, w.nitems, &grid);
+    cudaError_t e = staged_grid(k_vel_tmab<NCB, CS>, smem, w.nitems, &grid, s.sm_limit);
     if (e != cudaSuccess) return e;
     k_vel_tmab<NCB, CS><<<grid, dim3(32, ST_CW + 1), smem, stream>>>(
         st->vm, s.g, comp_set3(s), (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth, w, s.kerr, awp_wait_of(s));

@@ -318,6 +318,9 @@ typedef struct {
                                 item, sharing media tiles and cell coefficients:
                                 bit 0 the stress sweep, bit 1 the velocity sweep
                                 (default 1 up to 32 GiB of solver state, else 0) */
+    int sm_limit;            /* persistent grids sized for this many SMs (0 = every
+                                SM of the device): solves that share a GPU each take
+                                their share instead of time-slicing the whole device */
 } awp_tuning;
 
 awp_status awp_get_tuning(awp_solver *s, awp_tuning *t);

@@ -49,6 +49,7 @@ def free_device_bytes():
 @pytest.mark.parametrize("nth", [1, 7, 30])
 def test_failed_allocation_is_oom_and_releases_everything(monkeypatch, nth):
     c = Case(nt=20)
+    c.gpu(steps=1).close()               # the library's one-time module and context costs first
     awpsgt.release_cached_memory()
     before = free_device_bytes()
     monkeypatch.setenv("AWP_TEST_FAIL_ALLOC", str(nth))
