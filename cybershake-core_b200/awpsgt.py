@@ -29,7 +29,7 @@ STATUS = {0: "AWP_OK", 1: "AWP_ERR_IO", 2: "AWP_ERR_PARAM", 3: "AWP_ERR_OOM", 4:
           5: "AWP_ERR_UNSTABLE", 6: "AWP_ERR_TIMEOUT", 7: "AWP_ERR_STATE", 8: "AWP_ERR_BUSY",
           9: "AWP_ERR_CANCELLED"}
 PREC = {"f32": 0, "bf16": 1, "f16": 2, "mixed": 3, "bfp": 4}
-KERNEL = {"auto": 0, "two_sweep": 1, "fused": 2, "staged": 3}
+KERNEL = {"auto": 0, "two_sweep": 1, "fused": 2, "staged": 3, "staged_fma": 4}
 FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3", "r4", "r5", "r6",
           "lam", "mu", "d1", "qp", "qs"]
 
@@ -45,7 +45,7 @@ EXPORTED = [
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
     "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune", "awp_release_cached_memory",
-    "awp_set_field", "awp_checkpoint_write", "awp_checkpoint_read",
+    "awp_set_field", "awp_checkpoint_write", "awp_checkpoint_read", "awp_device_memory",
 ]
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
@@ -353,6 +353,7 @@ def load_library(path: str = LIB_PATH):
         "awp_get_chkj": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
         "awp_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
         "awp_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_device_memory": (C.c_int, [C.c_int, P(C.c_int64), P(C.c_int64)]),
         "awp_checkpoint_write": (C.c_int, [C.c_void_p, C.c_char_p]),
         "awp_checkpoint_read": (C.c_int, [C.c_void_p, C.c_char_p, P(C.c_int)]),
         "awp_get_stats": (C.c_int, [C.c_void_p, P(Stats)]),
@@ -608,6 +609,13 @@ class Solver:
 
     def set_tuning(self, t: Tuning):
         _check(self.lib.awp_set_tuning(self.h, C.byref(t)))
+
+
+def device_memory(device: int = 0):
+    """awp_device_memory: (bytes held by live solvers, bytes idle in the cache)."""
+    live, idle = C.c_int64(0), C.c_int64(0)
+    _check(load_library().awp_device_memory(device, C.byref(live), C.byref(idle)))
+    return live.value, idle.value
 
 
 def release_cached_memory():

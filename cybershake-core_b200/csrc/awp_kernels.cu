@@ -876,14 +876,14 @@ static cudaError_t launch_part_t(const AwpStepArgs &s, int part, cudaStream_t st
     comp_sets<NC>(s, cs, cn);
     const MediaT<TM> md = media_view<TM>(s.md);
     if (part == AWP_PART_VEL) {
-        if (s.staged) return awp_launch_vel_staged(s.staged, s, st);
+        if (s.staged) return s.fma ? awp_launch_vel_staged_fma(s.staged, s, st) : awp_launch_vel_staged(s.staged, s, st);
         const int ty = s.ty == 4 ? 4 : 8;
         return s.unroll == 2 ? launch_vel<NC, TM, 2>(s, md, cs, ty, st) : launch_vel<NC, TM, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FSVEL) {
         dim3 b(32, 8);
         k_fsvel<NC, TM><<<plane_grid(s.g, b, 1), b, 0, st>>>(s.g, md, cs);
     } else if (part == AWP_PART_STR) {
-        if (s.staged) return awp_launch_str_staged(s.staged, s, st);
+        if (s.staged) return s.fma ? awp_launch_str_staged_fma(s.staged, s, st) : awp_launch_str_staged(s.staged, s, st);
         const int ty = s.ty == 4 ? 4 : 8;
         return s.unroll == 2 ? launch_str<NC, TM, TR, 2>(s, md, cs, ty, st) : launch_str<NC, TM, TR, 1>(s, md, cs, ty, st);
     } else if (part == AWP_PART_FUSED) {

@@ -36,6 +36,7 @@ struct AwpStepArgs {
                                     bit 0 stress, bit 1 velocity */
     int *kerr;                   /* device error word (AWP_KERR_*)          */
     int sm_limit;                /* persistent grids sized for this many SMs (0 = all) */
+    int fma;                     /* staged sweeps compiled with multiply-add contraction */
     unsigned long long wait_ns;  /* bound of one barrier wait of the staged sweeps */
     int withhold;                /* test injection, -1 = off: block 0's producer of the
                                     staged stress sweep issues no copies for ring use
@@ -63,6 +64,9 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
 void awp_staged_destroy(AwpStaged *s);
 cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
+/* the same sweeps compiled with multiply-add contraction (AWP_KERNEL_STAGED_FMA) */
+cudaError_t awp_launch_vel_staged_fma(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
+cudaError_t awp_launch_str_staged_fma(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream);
 cudaError_t awp_launch_post(const AwpPostArgs &a, int initial, cudaStream_t st);
 cudaError_t awp_launch_sgt(const AwpSgtArgs &a, cudaStream_t st);
 /* one z-slab of RWG p/s/d volumes ([3][ny][n][nx]) to AWP media order

@@ -25,9 +25,19 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "awp_internal.h"
 #include "awp_kernels.h"
 #include "../../include/awp_sgt.h"
+
+/* NVTX range over a scope: solver phases show up by name on an Nsight
+ * timeline (header-only NVTX 3; without a tool attached a push or pop is a
+ * branch on a null pointer) */
+struct NvtxScope {
+    explicit NvtxScope(const char *name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+};
 
 static thread_local char g_err[512];
 
@@ -90,6 +100,7 @@ struct awp_solver {
     int staged_rpt_vel;              /* staged velocity sweep rows per thread */
     int staged_batch;                /* staged stress: components in one item */
     int sm_limit;                    /* persistent grids for this many SMs (0 = all) */
+    int fma;                         /* staged sweeps with multiply-add contraction */
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -425,6 +436,19 @@ static void dfree(awp_solver *s, void *p)
 
 extern "C" void awp_release_cached_memory(void) { blk_trim(-1); }
 
+extern "C" awp_status awp_device_memory(int device, int64_t *live_bytes, int64_t *idle_bytes)
+{
+    if (!live_bytes || !idle_bytes) return set_err(AWP_ERR_PARAM, "null argument");
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    int64_t live = 0;
+    for (const auto &kv : g_blk_live)
+        if (kv.second.dev == device) live += (int64_t)kv.second.bytes;
+    *live_bytes = live;
+    auto it = g_blk_idle_bytes.find(device);
+    *idle_bytes = it == g_blk_idle_bytes.end() ? 0 : (int64_t)it->second;
+    return AWP_OK;
+}
+
 static awp_status dalloc(awp_solver *s, void **ptr, size_t bytes)
 {
     if (s->fail_alloc > 0 && ++s->nalloc == s->fail_alloc) {
@@ -486,8 +510,9 @@ static awp_status check_params(const awp_params *p)
     if (p->kinematic && p->nst != 2)
         return set_err(AWP_ERR_PARAM, "a kinematic source (IFAULT=5) needs NST = 2 (two rows per subfault)");
     if (p->precision < AWP_PREC_F32 || p->precision > AWP_PREC_BFP) return set_err(AWP_ERR_PARAM, "unknown precision %d", p->precision);
-    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_STAGED) return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
-    if (p->kernel == AWP_KERNEL_STAGED && store_of(p) != AWP_STORE_F32)
+    if (p->kernel < AWP_KERNEL_AUTO || p->kernel > AWP_KERNEL_STAGED_FMA)
+        return set_err(AWP_ERR_PARAM, "unknown kernel %d", p->kernel);
+    if ((p->kernel == AWP_KERNEL_STAGED || p->kernel == AWP_KERNEL_STAGED_FMA) && store_of(p) != AWP_STORE_F32)
         return set_err(AWP_ERR_PARAM, "the staged stepper reads FP32 media (precision f32, mixed or bfp)");
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
     for (int q = 0; q < p->ncomp; q++) {
@@ -518,6 +543,7 @@ static awp_status alloc_media32(awp_solver *s)
 
 extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
 {
+    NvtxScope nvtx_("awp_create");
     *out = NULL;
     awp_status st = check_params(pin);
     if (st != AWP_OK) return st;
@@ -617,7 +643,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
     s->vtst1 = 1.0f / (p->dh * p->dh);
     s->ty = env_int("AWP_TUNE_TY", 8);
     if (s->ty != 4 && s->ty != 16) s->ty = 8;
-    s->staged_on = p->kernel == AWP_KERNEL_STAGED || (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
+    s->staged_on = p->kernel == AWP_KERNEL_STAGED || p->kernel == AWP_KERNEL_STAGED_FMA ||
+                   (p->kernel == AWP_KERNEL_AUTO && s->store == AWP_STORE_F32);
+    s->fma = p->kernel == AWP_KERNEL_STAGED_FMA;
     /* z-loop unroll: 1 or 2 (default 1 for the two-sweep kernels, 2 for the staged ones) */
     s->unroll = env_int("AWP_TUNE_UNROLL", 0);
     if (s->unroll != 1 && s->unroll != 2) s->unroll = s->staged_on ? 2 : 1;
@@ -803,6 +831,7 @@ struct StageLease {
 static awp_status load_media_common(awp_solver *s, slab_reader rd, void *ctx, int rwg_nx = 0, int rwg_ny = 0,
                                     const float *direct = NULL)
 {
+    NvtxScope nvtx_("awp_load_media");
     const awp_params *p = &s->p;
     CU(cudaSetDevice(p->device));
     if (s->started) return set_err(AWP_ERR_STATE, "media must be loaded before the first step (or after awp_reset)");
@@ -1069,6 +1098,7 @@ extern "C" awp_status awp_set_source(awp_solver *s, int comp, int nsrc, const in
 
 extern "C" awp_status awp_set_points(awp_solver *s, int npts, const int *xyz)
 {
+    NvtxScope nvtx_("awp_set_points");
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
     const awp_params *p = &s->p;
     if (npts < 0 || (npts > 0 && !xyz)) return set_err(AWP_ERR_PARAM, "bad point arrays");
@@ -1141,6 +1171,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_rpt_vel = s->staged_rpt_vel;
     a.staged_batch = s->staged_batch;
     a.sm_limit = s->sm_limit;
+    a.fma = s->fma;
     a.kerr = s->flag + 1;
     a.wait_ns = s->wait_ns;
     a.withhold = s->withhold;
@@ -1253,6 +1284,7 @@ static cudaError_t maybe_monitor(awp_solver *s)
 
 extern "C" awp_status awp_run_async(awp_solver *s, int nsteps)
 {
+    NvtxScope nvtx_("awp_run_async");
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
     const awp_params *p = &s->p;
     CU(cudaSetDevice(p->device));
@@ -1298,6 +1330,7 @@ extern "C" int awp_query(awp_solver *s)
 
 extern "C" awp_status awp_sync(awp_solver *s)
 {
+    NvtxScope nvtx_("awp_sync");
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");
     CU(cudaSetDevice(s->p.device));
     if (s->pending) {
@@ -1696,6 +1729,7 @@ static awp_status read_all(FILE *f, void *p, size_t bytes, const char *path)
 
 extern "C" awp_status awp_checkpoint_write(awp_solver *s, const char *dir)
 {
+    NvtxScope nvtx_("awp_checkpoint_write");
     if (!s || !dir) return set_err(AWP_ERR_PARAM, "null argument");
     awp_status st = awp_sync(s);
     if (st != AWP_OK) return st;
@@ -1762,6 +1796,7 @@ extern "C" awp_status awp_checkpoint_write(awp_solver *s, const char *dir)
 
 extern "C" awp_status awp_checkpoint_read(awp_solver *s, const char *dir, int *step_out)
 {
+    NvtxScope nvtx_("awp_checkpoint_read");
     if (!s || !dir) return set_err(AWP_ERR_PARAM, "null argument");
     if (step_out) *step_out = 0;
     const awp_params *p = &s->p;
@@ -2157,7 +2192,8 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
     awp_solver *s = NULL;
     awp_status st = awp_create(&p, &s);
     if (st != AWP_OK) return st;
-    const int stepper = s->staged_on ? AWP_KERNEL_STAGED : (fused_of(&s->p) ? AWP_KERNEL_FUSED : AWP_KERNEL_TWO_SWEEP);
+    const int stepper = s->staged_on ? (s->fma ? AWP_KERNEL_STAGED_FMA : AWP_KERNEL_STAGED)
+                                     : (fused_of(&s->p) ? AWP_KERNEL_FUSED : AWP_KERNEL_TWO_SWEEP);
     char key[320];
     tune_key(&p, stepper, key, sizeof key);
     double rate = 0.0;
@@ -2189,7 +2225,7 @@ extern "C" awp_status awp_autotune(const awp_params *pin, const float *media, in
     /* coordinate descent over the fields the stepper uses */
     enum { F_KSTAGE, F_RPT, F_UNROLL, F_QSLOW, F_RPTV, F_TY, F_KFUSED, F_KSWEEP, F_BATCH };
     int fields[9], nf = 0;
-    if (stepper == AWP_KERNEL_STAGED) {
+    if (stepper == AWP_KERNEL_STAGED || stepper == AWP_KERNEL_STAGED_FMA) {
         if (p.ncomp >= 2) fields[nf++] = F_BATCH;
         fields[nf++] = F_KSTAGE, fields[nf++] = F_RPT, fields[nf++] = F_UNROLL, fields[nf++] = F_QSLOW;
         fields[nf++] = F_RPTV;

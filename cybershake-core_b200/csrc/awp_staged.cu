@@ -71,6 +71,11 @@ struct AwpStaged {
     AwpStagedStrMaps sm;
 };
 
+/* The kernels live in an anonymous namespace: this file is compiled twice,
+ * without (the bit-exact stepper) and with multiply-add contraction
+ * (AWP_STAGED_FMA: AWP_KERNEL_STAGED_FMA), and the two sets must not merge. */
+namespace {
+
 /* ------------------------------------------------------------------ */
 /* mbarrier / TMA primitives (PTX ISA: mbarrier, cp.async.bulk.tensor) */
 /* ------------------------------------------------------------------ */
@@ -1037,10 +1042,19 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
     }
 }
 
+}  // namespace
+
 /* ------------------------------------------------------------------ */
 /* host side                                                           */
 /* ------------------------------------------------------------------ */
 
+#ifdef AWP_STAGED_FMA
+#define AWP_STAGED_ENTRY(name) name##_fma
+#else
+#define AWP_STAGED_ENTRY(name) name
+#endif
+
+#ifndef AWP_STAGED_FMA
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1106,6 +1120,7 @@ cudaError_t awp_staged_create(AwpStaged **out, const AwpGeom &g, int ncomp, cons
 }
 
 void awp_staged_destroy(AwpStaged *s) { free(s); }
+#endif
 
 static AwpWait awp_wait_of(const AwpStepArgs &s)
 {
@@ -1244,7 +1259,7 @@ static cudaError_t launch_vel_bn(const AwpStaged *st, const AwpStepArgs &s, cuda
 
 /* level loops unrolled twice unless asked otherwise: the column queues then
  * rotate by register renaming instead of moves that wait for loads in flight */
-cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+cudaError_t AWP_STAGED_ENTRY(awp_launch_vel_staged)(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
     if ((s.staged_batch & 2) && s.ncomp == 3) return launch_vel_bn<3>(st, s, stream);
@@ -1253,7 +1268,7 @@ cudaError_t awp_launch_vel_staged(const AwpStaged *st, const AwpStepArgs &s, cud
     return s.unroll == 1 ? launch_vel_u<1>(st, s, stream) : launch_vel_u<2>(st, s, stream);
 }
 
-cudaError_t awp_launch_str_staged(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
+cudaError_t AWP_STAGED_ENTRY(awp_launch_str_staged)(const AwpStaged *st, const AwpStepArgs &s, cudaStream_t stream)
 {
     if (!st || s.md.type != AWP_STORE_F32) return cudaErrorInvalidValue;
     if (s.rtype == AWP_STORE_BF16) return launch_str_tr<__nv_bfloat16>(st, s, stream);

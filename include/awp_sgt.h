@@ -75,8 +75,12 @@ typedef enum {
     AWP_KERNEL_TWO_SWEEP = 1, /* velocity sweep, then stress sweep, in place   */
     AWP_KERNEL_FUSED = 2,     /* one z-march per tile: velocity on a 2-cell
                                  halo, then stress; ping-pong wavefields       */
-    AWP_KERNEL_STAGED = 3     /* the two sweeps with TMA-staged xy tiles and a
+    AWP_KERNEL_STAGED = 3,    /* the two sweeps with TMA-staged xy tiles and a
                                  z register queue (FP32 media only)           */
+    AWP_KERNEL_STAGED_FMA = 4 /* the staged sweeps compiled with multiply-add
+                                 contraction: fewer instructions, results
+                                 within FP32 rounding of the others instead
+                                 of bit-identical                              */
 } awp_kernel;
 
 #define AWP_MAX_COMP 3
@@ -471,6 +475,10 @@ typedef struct {
  * awp_destroy.  No reference counterpart (the reference runs one solve per
  * process). */
 void awp_release_cached_memory(void);
+
+/* Device memory of this library on a device: bytes held by live solvers and
+ * bytes idle in the block cache (diagnostic; no reference counterpart). */
+awp_status awp_device_memory(int device, int64_t *live_bytes, int64_t *idle_bytes);
 
 /* hbm_budget <= 0: 90 % of the device's free memory at creation.
  * chunk_steps: fewest steps a resident solve advances per chunk. */

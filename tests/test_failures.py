@@ -11,6 +11,8 @@
   the next solver works.
 Both knobs are read by awp_create; nothing here traps, faults or hangs a GPU.
 """
+import gc
+
 import numpy as np
 import pytest
 
@@ -40,27 +42,22 @@ def test_withheld_tile_copy_times_out_then_next_solve_is_exact(monkeypatch, ncom
         assert_same_state(s, c.oracle(q), q)
 
 
-def free_device_bytes():
-    import torch
-    torch.cuda.synchronize()
-    return torch.cuda.mem_get_info()[0]
-
-
 @pytest.mark.parametrize("nth", [1, 7, 30])
 def test_failed_allocation_is_oom_and_releases_everything(monkeypatch, nth):
     c = Case(nt=20)
-    c.gpu(steps=1).close()               # the library's one-time module and context costs first
-    awpsgt.release_cached_memory()
-    before = free_device_bytes()
+    gc.collect()                                      # solvers of earlier tests released first
+    live0, _ = awpsgt.device_memory(0)
     monkeypatch.setenv("AWP_TEST_FAIL_ALLOC", str(nth))
     p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, igreen=c.igreen, **c.kw())
     with pytest.raises(awpsgt.AwpError) as e:
         awpsgt.Solver(p)
     assert awpsgt.STATUS[e.value.status] == "AWP_ERR_OOM"
     assert "AWP_TEST_FAIL_ALLOC" in str(e.value)
-    awpsgt.release_cached_memory()
-    assert abs(free_device_bytes() - before) <= 16 << 20
+    assert awpsgt.device_memory(0)[0] == live0          # every block of the failed solver released
     monkeypatch.delenv("AWP_TEST_FAIL_ALLOC")
     s = c.gpu()
+    assert awpsgt.device_memory(0)[0] > live0
     assert_same_state(s, c.oracle())
     assert np.abs(s.sgt()).max() > 0
+    s.close()
+    assert awpsgt.device_memory(0)[0] == live0

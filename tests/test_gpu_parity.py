@@ -379,3 +379,24 @@ def test_kinematic_source_matches_oracle(kernel):
     assert rel_l2(gxx, refs["f32"][1]) <= 1e-5
     assert rel_l2(g, refs["f64"][0]) <= 1e-4
 
+
+
+@pytest.mark.parametrize("precision", ["f32", "bfp"])
+def test_staged_fma_within_fp32_rounding_of_oracle(precision):
+    """The staged sweeps compiled with multiply-add contraction: every field
+    and the SGT image within 1e-5 relative L2 of the FP32 oracle (the memory
+    variables within 1e-4: a block-floating-point rounding can land one
+    quantum apart), the SGT point layout unchanged, and the FP64 budget of
+    1e-4 met."""
+    c = Case(nx=44, ny=36, nz=30, nt=60, igreen=(1, 2, 3), srcs=[[(22, 18, 8)], [(20, 16, 12)], [(24, 19, 9)]],
+             stf_seed=11)
+    s = c.gpu(kernel="staged_fma", precision=precision)
+    for q in range(3):
+        o = c.oracle(q, rstore=RSTORE.get(precision, "f32"))
+        for f in ALL_FIELDS[:15]:
+            err = rel_l2(s.field(f, q), o.field(f))
+            assert err <= (1e-4 if f.startswith("r") else 1e-5), (q, f, err)
+        g, ref = s.sgt(q), o.sgt()
+        assert g.shape == ref.shape and np.array_equal(g == 0, ref == 0)
+        assert rel_l2(g, ref) <= 1e-5
+        assert rel_l2(g, c.oracle(q, precision="f64").sgt()) <= 1e-4

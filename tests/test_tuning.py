@@ -177,3 +177,22 @@ def test_single_level_chunk_all_batch_masks(batch):
     s.run(c.nt)
     for q in range(3):
         assert_same_state(s, c.oracle(q), q)
+
+
+@pytest.mark.parametrize("kernel", ["staged", "two_sweep", "fused"])
+def test_sm_limit_is_bit_exact(kernel):
+    """Persistent grids sized for a share of the SMs (as the server sizes
+    solves that share a GPU), switched mid-solve: same results."""
+    c = Case(nx=44, ny=36, nz=30, nt=40, igreen=(1, 2), srcs=[[(22, 18, 8)], [(20, 16, 12)]])
+    s = solver_for(c, kernel)
+    t0 = s.tuning()
+    assert t0.sm_limit == 0
+    s.set_tuning(variant(t0, sm_limit=5))
+    s.run(17)
+    s.set_tuning(variant(t0, sm_limit=37))
+    s.run(c.nt)
+    for q in range(2):
+        assert_same_state(s, c.oracle(q), q)
+    with pytest.raises(awpsgt.AwpError):
+        s.set_tuning(variant(t0, sm_limit=-1))
+    s.close()
