@@ -76,6 +76,7 @@ class Params(C.Structure):
         ("idyna", C.c_int), ("nst", C.c_int), ("ntiskp_sgt", C.c_int), ("write_step", C.c_int),
         ("ncomp", C.c_int), ("igreen", C.c_int * 3), ("precision", C.c_int), ("kernel", C.c_int),
         ("device", C.c_int), ("monitor_every", C.c_int), ("kinematic", C.c_int),
+        ("npc", C.c_int), ("pht", C.c_float),
     ]
 
 
@@ -431,7 +432,7 @@ def _ptr(a: np.ndarray):
 def make_params(nx, ny, nz, dh, dt, nt, *, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5, socalq=0, nve=1,
                 mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10, write_step=None,
                 igreen: Sequence[int] = (1,), precision="f32", kernel="auto", device=0,
-                monitor_every=0, kinematic=0) -> Params:
+                monitor_every=0, kinematic=0, npc=0, pht=0.1) -> Params:
     lib = load_library()
     p = Params()
     lib.awp_params_default(C.byref(p))
@@ -451,6 +452,7 @@ def make_params(nx, ny, nz, dh, dt, nt, *, nd=20, arbc=0.92, fl=0.01, fh=25.0, f
     p.device = device
     p.monitor_every = monitor_every
     p.kinematic = kinematic
+    p.npc, p.pht = npc, pht
     return p
 
 

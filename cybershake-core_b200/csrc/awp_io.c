@@ -256,6 +256,7 @@ void awp_params_from_in3d(const awp_in3d *in, awp_params *p)
     p->kinematic = in->ifault == 5;
     p->nst = in->nst; p->ntiskp_sgt = in->ntiskp_sgt; p->write_step = in->write_step;
     p->ncomp = 1; p->igreen[0] = in->igreen;
+    p->npc = in->npc; p->pht = in->pht;
 }
 
 /* ------------------------------------------------------------------ */

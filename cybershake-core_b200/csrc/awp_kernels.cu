@@ -922,6 +922,10 @@ cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st)
     if (s.fused) return awp_launch_part(s, AWP_PART_FUSED, st);
     for (int part = 0; part < 3; ++part) {
         cudaError_t e = awp_launch_part(s, part, st);
+        /* NPC = 1: the PML zones recomputed after the velocity sweep (before
+         * the free-surface velocity) and after the stress sweep */
+        if (e == cudaSuccess && s.pml && part == AWP_PART_VEL) e = awp_launch_pml(*s.pml, 0, st);
+        if (e == cudaSuccess && s.pml && part == AWP_PART_STR) e = awp_launch_pml(*s.pml, 1, st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

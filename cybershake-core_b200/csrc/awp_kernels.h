@@ -11,6 +11,20 @@ struct AwpStaged;
 /* error word bits the steppers set */
 #define AWP_KERR_TMA_WAIT 1          /* a staged-tile barrier wait ran out */
 
+/* the PML zones of the step (NPC = 1; awp_pml.cu) */
+struct AwpPmlArgs {
+    AwpGeom g;
+    int ncomp, nd;
+    float dt, dth, pht;
+    const float *rf, *rh;         /* damping profiles, index 1..nd            */
+    float *split[3];              /* split arrays of each component           */
+    long long n[5], off[5];       /* cells of each plane S N W E B, offsets   */
+    AwpComp comp[3];              /* wavefields (the two-sweep buffer)        */
+    const float *d1, *lam, *mu;   /* FP32 media                               */
+};
+cudaError_t awp_launch_pml(const AwpPmlArgs &a, int part, cudaStream_t st);
+void awp_pml_profiles(int nd, float arbc, float dh, float vs_min, float vs_max, float *rf, float *rh);
+
 struct AwpStepArgs {
     AwpGeom g;
     AwpMediaT md;                /* typed media                             */
@@ -37,6 +51,7 @@ struct AwpStepArgs {
     int *kerr;                   /* device error word (AWP_KERR_*)          */
     int sm_limit;                /* persistent grids sized for this many SMs (0 = all) */
     int fma;                     /* staged sweeps compiled with multiply-add contraction */
+    const AwpPmlArgs *pml;       /* NPC = 1: the PML zones after each sweep (NULL: Cerjan) */
     unsigned long long wait_ns;  /* bound of one barrier wait of the staged sweeps */
     int withhold;                /* test injection, -1 = off: block 0's producer of the
                                     staged stress sweep issues no copies for ring use
@@ -54,7 +69,8 @@ cudaError_t awp_launch_media_convert(const AwpMedia &src, const AwpMediaT &dst, 
 cudaError_t awp_launch_sg_coeffs(const AwpMediaT &md, int npts, const int *pt_idx, float *sg, cudaStream_t st);
 
 /* the kernels of one step */
-enum { AWP_PART_VEL = 0, AWP_PART_FSVEL = 1, AWP_PART_STR = 2, AWP_PART_FUSED = 3 };
+enum { AWP_PART_VEL = 0, AWP_PART_FSVEL = 1, AWP_PART_STR = 2, AWP_PART_FUSED = 3,
+       AWP_PART_PML_VEL = 4, AWP_PART_PML_STR = 5 };   /* PML parts: awp_launch_pml */
 cudaError_t awp_launch_part(const AwpStepArgs &s, int part, cudaStream_t st);
 /* two-sweep: velocity, free-surface velocity, stress (+ fstr); fused: one kernel */
 cudaError_t awp_launch_step(const AwpStepArgs &s, cudaStream_t st);

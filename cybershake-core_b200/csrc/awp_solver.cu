@@ -101,6 +101,11 @@ struct awp_solver {
     int staged_batch;                /* staged stress: components in one item */
     int sm_limit;                    /* persistent grids for this many SMs (0 = all) */
     int fma;                         /* staged sweeps with multiply-add contraction */
+    /* PML (npc = 1): split arrays per component, damping profiles, kernel arguments */
+    float *pml_split[AWP_MAX_COMP];
+    float *pml_prof;                 /* rf[nd + 1] then rh[nd + 1]         */
+    int64_t pml_floats;              /* floats of one component's splits   */
+    AwpPmlArgs pml_args;
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
     int unroll;                      /* two-sweep z-loop unroll             */
@@ -165,6 +170,7 @@ extern "C" void awp_params_default(awp_params *p)
     p->ncomp = 1; p->igreen[0] = 1; p->igreen[1] = 2; p->igreen[2] = 3;
     p->precision = AWP_PREC_F32; p->kernel = AWP_KERNEL_AUTO; p->device = 0;
     p->monitor_every = 0;
+    p->npc = 0; p->pht = 0.1f;
 }
 
 static AwpGeom make_geom(const awp_params *p)
@@ -265,6 +271,9 @@ extern "C" int64_t awp_footprint_bytes(const awp_params *p, int npts)
     b += file_floats_of(p, npts) * 4 * nc;
     b += (int64_t)p->nt * 12 * nc;
     b += (int64_t)npts * 16;
+    if (p->npc == 1)   /* PML split arrays */
+        b += (int64_t)nc * 18 * 4 *
+             (2 * (int64_t)p->nx * p->nd * p->nz + 2 * (int64_t)p->nd * p->ny * p->nz + (int64_t)p->nx * p->ny * p->nd);
     b += 64ll << 20;   /* media staging slab + small buffers */
     return b;
 }
@@ -318,6 +327,8 @@ static void free_all(awp_solver *s)
     dfree(s, s->tau); dfree(s, s->step); dfree(s, s->ext); dfree(s, s->rng);
     dfree(s, s->pt_idx); dfree(s, s->sg);
     dfree(s, s->en_partial); dfree(s, s->en_out); dfree(s, s->flag);
+    for (int q = 0; q < AWP_MAX_COMP; q++) dfree(s, s->pml_split[q]);
+    dfree(s, s->pml_prof);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -515,6 +526,14 @@ static awp_status check_params(const awp_params *p)
     if ((p->kernel == AWP_KERNEL_STAGED || p->kernel == AWP_KERNEL_STAGED_FMA) && store_of(p) != AWP_STORE_F32)
         return set_err(AWP_ERR_PARAM, "the staged stepper reads FP32 media (precision f32, mixed or bfp)");
     if (p->nve == 1 && !(p->fl > 0 && p->fh > p->fl && p->fp > 0)) return set_err(AWP_ERR_PARAM, "Q band needs 0 < FL < FH and FP > 0");
+    if (p->npc != 0 && p->npc != 1) return set_err(AWP_ERR_PARAM, "NPC must be 0 (Cerjan) or 1 (PML)");
+    if (p->npc == 1) {
+        if (p->kernel == AWP_KERNEL_FUSED)
+            return set_err(AWP_ERR_PARAM, "the PML (NPC = 1) runs with the two-sweep or staged stepper, not the fused one");
+        if (store_of(p) != AWP_STORE_F32) return set_err(AWP_ERR_PARAM, "the PML (NPC = 1) reads FP32 media");
+        if (2 * p->nd >= p->nx || 2 * p->nd >= p->ny || p->nd >= p->nz || p->nd < 2)
+            return set_err(AWP_ERR_PARAM, "PML width ND = %d does not fit the grid (2 ND < NX, NY; ND < NZ; ND >= 2)", p->nd);
+    }
     for (int q = 0; q < p->ncomp; q++) {
         int ig = p->igreen[q];
         if (!(ig == -2 || ig == -1 || (ig >= 1 && ig <= 6))) return set_err(AWP_ERR_PARAM, "IGREEN %d not supported", ig);
@@ -611,9 +630,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
             float *h = (float *)calloc((size_t)n3[a] + 2, sizeof(float));
             for (int i = 1; i <= n3[a]; i++) {
                 float f = 1.0f;
-                if (i <= p->nd) f = f * crj_low(alpha, p->nd, i);
-                if (a < 2 && i >= n3[a] - p->nd + 1) f = f * crj_high(alpha, p->nd, n3[a], i);
-                h[i] = f;
+                if (p->npc == 0 && i <= p->nd) f = f * crj_low(alpha, p->nd, i);
+                if (p->npc == 0 && a < 2 && i >= n3[a] - p->nd + 1) f = f * crj_high(alpha, p->nd, n3[a], i);
+                h[i] = f;   /* with the PML (NPC = 1) no sponge: every factor 1 (pmcl3d.f:928-932) */
             }
             TRY(dalloc(s, (void **)&dst[a], sizeof(float) * ((size_t)n3[a] + 2)));
             cudaError_t e = cudaMemcpy(dst[a], h, sizeof(float) * ((size_t)n3[a] + 2), cudaMemcpyHostToDevice);
@@ -621,6 +640,27 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
             if (a == 0) s->cx = dst[a]; else if (a == 1) s->cy = dst[a]; else s->cz = dst[a];
             TRYCU(e);
         }
+    }
+    if (p->npc == 1) {
+        /* split arrays of the five planes (memory.f:217-300), one buffer per
+         * component: plane after plane S N W E B, each [T/H][field][cells] */
+        AwpPmlArgs &pa = s->pml_args;
+        const long long ns = (long long)p->nx * p->nd * p->nz, nw = (long long)p->nd * p->ny * p->nz,
+                        nb = (long long)p->nx * p->ny * p->nd;
+        const long long n[5] = {ns, ns, nw, nw, nb};
+        long long off = 0;
+        for (int a = 0; a < 5; a++) { pa.n[a] = n[a]; pa.off[a] = off; off += 18 * n[a]; }
+        s->pml_floats = off;
+        for (int q = 0; q < p->ncomp; q++) {
+            TRY(dalloc(s, (void **)&s->pml_split[q], sizeof(float) * (size_t)off));
+            TRYCU(cudaMemsetAsync(s->pml_split[q], 0, sizeof(float) * (size_t)off, s->stream));
+            pa.split[q] = s->pml_split[q];
+            pa.comp[q] = s->comp[0][q];
+        }
+        TRY(dalloc(s, (void **)&s->pml_prof, sizeof(float) * 2 * ((size_t)p->nd + 1)));
+        pa.g = s->g; pa.ncomp = p->ncomp; pa.nd = p->nd;
+        pa.dt = p->dt; pa.dth = p->dt / p->dh; pa.pht = p->pht;
+        pa.rf = s->pml_prof; pa.rh = s->pml_prof + p->nd + 1;
     }
     TRY(dalloc(s, (void **)&s->tau, 16 * sizeof(float)));
     TRY(dalloc(s, (void **)&s->step, sizeof(int)));
@@ -1172,6 +1212,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_batch = s->staged_batch;
     a.sm_limit = s->sm_limit;
     a.fma = s->fma;
+    a.pml = s->p.npc == 1 ? &s->pml_args : NULL;
     a.kerr = s->flag + 1;
     a.wait_ns = s->wait_ns;
     a.withhold = s->withhold;
@@ -1254,6 +1295,16 @@ static awp_status start_if_needed(awp_solver *s)
         /* the arrays are fixed from here on: u v w, the stresses, FP32 media */
         const cudaError_t e = awp_staged_create(&s->staged, s->g, s->p.ncomp, s->comp[0], s->mdt, s->rstore);
         if (e != cudaSuccess) return set_err(AWP_ERR_CUDA, "staged stepper: tensor maps: %s", cudaGetErrorString(e));
+    }
+    if (s->p.npc == 1) {
+        /* inipml (pml.f:4-44) from the media's S velocity range (pmcl3d.f:928-929) */
+        const int nd = s->p.nd;
+        std::vector<float> prof(2 * ((size_t)nd + 1), 0.0f);
+        awp_pml_profiles(nd, s->p.arbc, s->p.dh, s->ext_host[2], s->ext_host[3], &prof[0], &prof[nd + 1]);
+        CU(cudaMemcpy(s->pml_prof, prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
+        s->pml_args.d1 = (const float *)s->mdt.m[AM_D1];
+        s->pml_args.lam = (const float *)s->mdt.m[AM_LAM];
+        s->pml_args.mu = (const float *)s->mdt.m[AM_MU];
     }
     AwpStepArgs a; AwpPostArgs pa; AwpSgtArgs sa;
     fill_args(s, -1, a, pa, sa);       /* addsrc(1) into the buffer step 1 reads */
@@ -1386,6 +1437,15 @@ static double part_bytes(const awp_solver *s, int part)
     case AWP_PART_FSVEL: return (double)p->nx * p->ny * (nc * (8 * 4.0) + 2 * mb);
     case AWP_PART_STR: return cells * (nc * (15 * 4.0 + rcell) + (nmed - 1) * mb);
     case AWP_PART_FUSED: return cells * (nc * (18 * 4.0 + rcell) + nmed * mb);
+    case AWP_PART_PML_VEL:
+    case AWP_PART_PML_STR: {
+        /* per boundary cell: the stresses (velocities) read, two splits of
+         * each updated field read and written, the updated fields written,
+         * the cell's media */
+        const double nb = cells - (double)(p->nx - 2 * p->nd) * (p->ny - 2 * p->nd) * (p->nz - p->nd);
+        return part == AWP_PART_PML_VEL ? nb * (nc * (6 + 12 + 3) * 4.0 + 4.0)
+                                        : nb * (nc * (3 + 24 + 6) * 4.0 + 8.0);
+    }
     }
     return 0.0;
 }
@@ -1401,11 +1461,17 @@ extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_ti
     int todo = nsteps;
     if (todo > p->nt - s->steps_done) todo = p->nt - s->steps_done;
     /* kernel classes: the stepper kernels, then k_post, then k_sgt */
-    int parts[4], np = 0;
+    int parts[6], np = 0;
     if (s->fused) parts[np++] = AWP_PART_FUSED;
-    else { parts[np++] = AWP_PART_VEL; parts[np++] = AWP_PART_FSVEL; parts[np++] = AWP_PART_STR; }
-    static const char *pname[] = {"k_vel", "k_fsvel", "k_str", "k_fused"};
-    static const char *pname_staged[] = {"k_vel_tma", "k_fsvel", "k_str_tma", "k_fused"};
+    else {
+        parts[np++] = AWP_PART_VEL;
+        if (p->npc == 1) parts[np++] = AWP_PART_PML_VEL;
+        parts[np++] = AWP_PART_FSVEL;
+        parts[np++] = AWP_PART_STR;
+        if (p->npc == 1) parts[np++] = AWP_PART_PML_STR;
+    }
+    static const char *pname[] = {"k_vel", "k_fsvel", "k_str", "k_fused", "k_pml_vel", "k_pml_str"};
+    static const char *pname_staged[] = {"k_vel_tma", "k_fsvel", "k_str_tma", "k_fused", "k_pml_vel", "k_pml_str"};
     const int nk = np + 2;
     o->nkernels = nk;
     for (int k = 0; k < np; k++) {
@@ -1429,7 +1495,9 @@ extern "C" awp_status awp_profile_steps(awp_solver *s, int nsteps, awp_kernel_ti
             if (k == np + 1 && !sgt_now) continue;
             cudaError_t e = cudaEventRecord(ev[2 * k], s->stream);
             if (e == cudaSuccess) {
-                if (k < np) e = awp_launch_part(a, parts[k], s->stream);
+                if (k < np && parts[k] == AWP_PART_PML_VEL) e = awp_launch_pml(*a.pml, 0, s->stream);
+                else if (k < np && parts[k] == AWP_PART_PML_STR) e = awp_launch_pml(*a.pml, 1, s->stream);
+                else if (k < np) e = awp_launch_part(a, parts[k], s->stream);
                 else if (k == np) e = awp_launch_post(pa, 0, s->stream);
                 else e = awp_launch_sgt(sa, s->stream);
             }
@@ -1727,6 +1795,45 @@ static awp_status read_all(FILE *f, void *p, size_t bytes, const char *path)
     return AWP_OK;
 }
 
+/* The PML split arrays of one component in the reference's checkpoint files
+ * (pmcl3d.f:1995-2040): ckpew = the east plane then the west, ckpns = north
+ * then south, ckpb = bottom; per plane three records of six arrays, fields u
+ * v w | xx yy zz | xz yz xy, each as its T then its H split, in the plane's
+ * own addressing (the device layout is the same per array). */
+static awp_status pml_ckp_io(awp_solver *s, int q, const char *dir, int step, bool write)
+{
+    static const char *name[3] = {"ckpew", "ckpns", "ckpb"};
+    static const int planes[3][2] = {{3, 2}, {1, 0}, {4, -1}};        /* E W | N S | B */
+    static const int fields[9] = {0, 1, 2, 3, 4, 5, 7, 8, 6};        /* u v w xx yy zz xz yz xy */
+    const AwpPmlArgs &pa = s->pml_args;
+    char path[1200];
+    awp_status st = AWP_OK;
+    for (int fl = 0; fl < 3 && st == AWP_OK; fl++) {
+        snprintf(path, sizeof path, "%s/%s%07d%07d.bin", dir, name[fl], q, step);
+        FILE *f = fopen(path, write ? "wb" : "rb");
+        if (!f) return set_err(AWP_ERR_IO, write ? "cannot create %s" : "checkpoint %s missing", path);
+        for (int pp = 0; pp < 2 && st == AWP_OK; pp++) {
+            const int pl = planes[fl][pp];
+            if (pl < 0) continue;
+            std::vector<float> buf((size_t)pa.n[pl]);
+            for (int fd = 0; fd < 9 && st == AWP_OK; fd++)
+                for (int sp = 0; sp < 2 && st == AWP_OK; sp++) {
+                    float *dev = s->pml_split[q] + pa.off[pl] + (sp * 9 + fields[fd]) * pa.n[pl];
+                    const size_t bytes = sizeof(float) * buf.size();
+                    if (write) {
+                        CU(cudaMemcpy(buf.data(), dev, bytes, cudaMemcpyDeviceToHost));
+                        st = write_all(f, buf.data(), bytes, path);
+                    } else {
+                        st = read_all(f, buf.data(), bytes, path);
+                        if (st == AWP_OK) CU(cudaMemcpy(dev, buf.data(), bytes, cudaMemcpyHostToDevice));
+                    }
+                }
+        }
+        if (fclose(f) != 0 && write && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", path);
+    }
+    return st;
+}
+
 extern "C" awp_status awp_checkpoint_write(awp_solver *s, const char *dir)
 {
     NvtxScope nvtx_("awp_checkpoint_write");
@@ -1764,6 +1871,7 @@ extern "C" awp_status awp_checkpoint_write(awp_solver *s, const char *dir)
         if (st == AWP_OK) st = write_all(f, buf, nvol * sizeof(float), path);
         if (fclose(f) != 0 && st == AWP_OK) st = set_err(AWP_ERR_IO, "cannot write %s", path);
         if (st != AWP_OK) break;
+        if (p->npc == 1 && (st = pml_ckp_io(s, q, dir, step, true)) != AWP_OK) break;
         /* ckpsgt<rank><step>.bin: the SGT file image and CHKJ series so far */
         snprintf(path, sizeof path, "%s/ckpsgt%07d%07d.bin", dir, q, step);
         f = fopen(path, "wb");
@@ -1845,6 +1953,7 @@ extern "C" awp_status awp_checkpoint_read(awp_solver *s, const char *dir, int *s
         }
         fclose(f);
         if (st != AWP_OK) break;
+        if (p->npc == 1 && (st = pml_ckp_io(s, q, dir, t0, false)) != AWP_OK) break;
         CU(cudaSetDevice(p->device));
         snprintf(path, sizeof path, "%s/ckpsgt%07d%07d.bin", dir, q, t0);
         f = fopen(path, "rb");
@@ -1910,6 +2019,8 @@ extern "C" awp_status awp_reset(awp_solver *s)
         CU(cudaMemsetAsync(s->chkj[q], 0, sizeof(float) * 3 * (size_t)p->nt, s->stream));
         if (s->sgt_file[q]) CU(cudaMemsetAsync(s->sgt_file[q], 0, sizeof(float) * (size_t)s->sgt_file_floats, s->stream));
     }
+    for (int q = 0; q < p->ncomp; q++)
+        if (s->pml_split[q]) CU(cudaMemsetAsync(s->pml_split[q], 0, sizeof(float) * (size_t)s->pml_floats, s->stream));
     CU(cudaMemsetAsync(s->step, 0, sizeof(int), s->stream));
     CU(cudaMemsetAsync(s->flag, 0, 2 * sizeof(int), s->stream));
     CU(cudaStreamSynchronize(s->stream));

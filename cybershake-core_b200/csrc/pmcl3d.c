@@ -160,7 +160,6 @@ int main(int argc, char **argv)
     awp_in3d in;
     awp_status st = awp_parse_command_line(argc, argv, &in);
     if (st != AWP_OK) return fail(st, "reading parameters");
-    if (in.npc != 0) { fprintf(stderr, "pmcl3d: NPC=1 (PML) is not supported; use the Cerjan sponge (NPC=0)\n"); return 1; }
     if (in.ifault != 0 && in.ifault != 1 && in.ifault != 5) {
         fprintf(stderr, "pmcl3d: IFAULT=%d is not supported (0, 1 or 5)\n", in.ifault);
         return 1;

@@ -116,6 +116,10 @@ typedef struct {
                                 (AWP-GPU-SGT kernel_kp1_fix_havg_ifault5.cu:
                                 289-376); IGREEN then only selects the SGT
                                 output                                        */
+    int npc;                 /* NPC   0 = Cerjan sponge, 1 = PML absorbing
+                                boundary of width ND (AWP-ODC-SGT/src/pml.f;
+                                the two-sweep and staged steppers, FP32 media) */
+    float pht;               /* PHT   PML damping ratio of the tangential splits */
 } awp_params;
 
 typedef struct {

@@ -81,6 +81,8 @@ typedef struct {
     int igreen;
     int kinematic;   /* 1: IFAULT=5 subfault sources (NST = 2) */
     int rstore;      /* storage of r1..r6 (FP32 build only): ORC_RS_* */
+    int npc;         /* 1: PML absorbing boundary (pml.f), 0: Cerjan sponge */
+    float pht;       /* PHT: PML damping ratio of the splits tangential to a face */
 } orc_params;
 
 /* Storage formats of the memory variables r1..r6 emulated by the FP32 build:
@@ -120,6 +122,10 @@ typedef struct {
     float *chkj;         /* [nt][3] */
     int cur;             /* completed steps */
     int started;
+    /* PML (npc = 1): T and H splits of the nine fields per plane S N W E B */
+    real *pml[5][2][9];
+    real *rf, *rh;       /* damping profiles, index 1..nd */
+    int box[6];          /* x0 x1 y0 y1 z0 z1 of the 4th-order interior zone */
 } orc_t;
 
 #define IDX(h, i, j, k) ((((size_t)((k) + 1)) * (size_t)(h)->sy + (size_t)((j) + 1)) * (size_t)(h)->sx + (size_t)((i) + 1))
@@ -197,6 +203,10 @@ void orc_destroy(orc_t *h)
     free(h->cx); free(h->cy); free(h->cz);
     free(h->src); free(h->stf); free(h->pts); free(h->sg);
     free(h->sgt_buf); free(h->sgt_file); free(h->chkj);
+    for (int a = 0; a < 5; a++)
+        for (int b = 0; b < 2; b++)
+            for (int f = 0; f < 9; f++) free(h->pml[a][b][f]);
+    free(h->rf); free(h->rh);
     free(h);
 }
 
@@ -222,6 +232,23 @@ orc_t *orc_create(const orc_params *p)
     orc_inicrj(h);
     h->chkj = calloc((size_t)p->nt * 3, sizeof(float));
     h->nt_file = orc_nt_file(p);
+    h->box[0] = 1; h->box[1] = p->nx; h->box[2] = 1; h->box[3] = p->ny; h->box[4] = 1; h->box[5] = p->nz;
+    if (p->npc == 1) {
+        /* plane extents (memory.f:217-300): S, N nx x nd x nz; W, E nd x ny x nz; B nx x ny x nd */
+        if (2 * p->nd >= p->nx || 2 * p->nd >= p->ny || p->nd >= p->nz) { orc_destroy(h); return NULL; }
+        const size_t n[5] = {(size_t)p->nx * p->nd * p->nz, (size_t)p->nx * p->nd * p->nz,
+                             (size_t)p->nd * p->ny * p->nz, (size_t)p->nd * p->ny * p->nz,
+                             (size_t)p->nx * p->ny * p->nd};
+        for (int a = 0; a < 5; a++)
+            for (int b = 0; b < 2; b++)
+                for (int f = 0; f < 9; f++)
+                    if (!(h->pml[a][b][f] = calloc(n[a], sizeof(real)))) { orc_destroy(h); return NULL; }
+        h->rf = calloc((size_t)p->nd + 2, sizeof(real));
+        h->rh = calloc((size_t)p->nd + 2, sizeof(real));
+        /* the interior zone 18 (bound.f:890-892) */
+        h->box[0] = p->nd + 1; h->box[1] = p->nx - p->nd; h->box[2] = p->nd + 1; h->box[3] = p->ny - p->nd;
+        h->box[4] = p->nd + 1;
+    }
     return h;
 }
 
@@ -475,9 +502,9 @@ static void orc_dvelc(orc_t *h)
     const real *xy = h->f[F_XY], *xz = h->f[F_XZ], *yz = h->f[F_YZ], *d1 = h->f[F_D1];
     const long sx = 1, sy = h->sx, sz = (long)h->sx * h->sy;
     #pragma omp parallel for schedule(static)
-    for (int k = 1; k <= p->nz; k++)
-        for (int j = 1; j <= p->ny; j++)
-            for (int i = 1; i <= p->nx; i++) {
+    for (int k = h->box[4]; k <= h->box[5]; k++)
+        for (int j = h->box[2]; j <= h->box[3]; j++)
+            for (int i = h->box[0]; i <= h->box[1]; i++) {
                 const long c = (long)IDX(h, i, j, k);
                 real d;
                 d = (real)0.25 * ((d1[c] + d1[c - sy]) + (d1[c - sz] + d1[c - sy - sz]));
@@ -641,11 +668,11 @@ static void orc_dstrqc(orc_t *h)
     const int nz = p->nz;
     const int rs = p->rstore, step = h->cur;
     #pragma omp parallel for schedule(static)
-    for (int k = 1; k <= p->nz; k++) {
+    for (int k = h->box[4]; k <= h->box[5]; k++) {
         const int itz = ((nz + 1) - k) % 2;          /* mod(...,2)+1, 0-based */
-        for (int j = 1; j <= p->ny; j++) {
+        for (int j = h->box[2]; j <= h->box[3]; j++) {
             const int ity = j % 2;
-            for (int i = 1; i <= p->nx; i++) {
+            for (int i = h->box[0]; i <= h->box[1]; i++) {
                 const int itx = i % 2;
                 const real vx1 = h->tau1[itz][ity][itx];
                 const real vx2 = h->tau2[itz][ity][itx];
@@ -741,9 +768,9 @@ static void orc_dstrc(orc_t *h)
     const real *lam = h->f[F_LAM], *mu = h->f[F_MU];
     const long sx = 1, sy = h->sx, sz = (long)h->sx * h->sy;
     #pragma omp parallel for schedule(static)
-    for (int k = 1; k <= p->nz; k++)
-        for (int j = 1; j <= p->ny; j++)
-            for (int i = 1; i <= p->nx; i++) {
+    for (int k = h->box[4]; k <= h->box[5]; k++)
+        for (int j = h->box[2]; j <= h->box[3]; j++)
+            for (int i = h->box[0]; i <= h->box[1]; i++) {
                 const long c = (long)IDX(h, i, j, k);
                 real xl = (real)8. / (lam[c] + lam[c + sx] + lam[c - sy] + lam[c + sx - sy] +
                                       lam[c - sz] + lam[c + sx - sz] + lam[c - sy - sz] + lam[c + sx - sy - sz]);
@@ -963,14 +990,21 @@ static void orc_addkinsrc(orc_t *h, int it)
     }
 }
 
+#include "awp_oracle_pml.h"
+
+/* one step in the order of pmcl3d.f:1234-1388: with NPC = 1 the interior
+ * operators cover zone 18 and the PML routines the other zones, and no
+ * Cerjan sponge is applied */
 static void orc_one_step(orc_t *h, int it)
 {
     const orc_params *p = &h->p;
     orc_dvelc(h);
-    orc_addcrj(h, F_U1, F_W1);
+    if (p->npc == 1) orc_pmlvel(h);
+    else orc_addcrj(h, F_U1, F_W1);
     orc_fvel(h);
     if (p->nve == 1) orc_dstrqc(h); else orc_dstrc(h);
-    orc_addcrj(h, F_XX, F_YZ);
+    if (p->npc == 1) orc_pmlstr(h);
+    else orc_addcrj(h, F_XX, F_YZ);
     if (p->kinematic) {
         orc_fstr(h);
         orc_addkinsrc(h, it);
@@ -997,6 +1031,7 @@ static void orc_one_step(orc_t *h, int it)
 int orc_run(orc_t *h, int nsteps)
 {
     if (!h->started) {
+        if (h->p.npc == 1) orc_inipml(h);   /* pmcl3d.f:928-929, after the media (vse) */
         orc_sgt_coeffs(h);
         if (!h->p.kinematic) orc_addsrc(h, 1);
         h->started = 1;

@@ -35,6 +35,7 @@ class OrcParams(C.Structure):
         ("socalq", C.c_int), ("nve", C.c_int), ("mediastart", C.c_int), ("nvar", C.c_int),
         ("idyna", C.c_int), ("nst", C.c_int), ("nt", C.c_int), ("ntiskp_sgt", C.c_int),
         ("write_step", C.c_int), ("igreen", C.c_int), ("kinematic", C.c_int), ("rstore", C.c_int),
+        ("npc", C.c_int), ("pht", C.c_float),
     ]
 
 
@@ -96,7 +97,8 @@ class Oracle:
 
     def __init__(self, *, nx, ny, nz, dh, dt, nt, nd=20, arbc=0.92, fl=0.01, fh=25.0, fp=0.5,
                  socalq=0, nve=1, mediastart=1, nvar=3, idyna=0, nst=None, ntiskp_sgt=10,
-                 write_step=None, igreen=1, precision="f32", threads=0, kinematic=0, rstore="f32"):
+                 write_step=None, igreen=1, precision="f32", threads=0, kinematic=0, rstore="f32", npc=0,
+                 pht=0.1):
         self.lib = load(precision)
         if threads:
             self.lib.orc_set_num_threads(threads)
@@ -113,6 +115,7 @@ class Oracle:
         if rstore != "f32" and precision != "f32":
             raise ValueError("r storage formats are emulated by the FP32 build only")
         p.rstore = RSTORE[rstore]
+        p.npc, p.pht = npc, pht
         self.p = p
         self.h = self.lib.orc_create(C.byref(p))
         if not self.h:
