@@ -118,12 +118,15 @@ def test_driver_reports_missing_input(tmp_path):
     assert "source" in r.stderr
 
 
-def test_driver_rejects_pml(tmp_path):
+def test_driver_rejects_unknown_boundary(tmp_path):
+    """NPC is 0 (Cerjan) or 1 (PML); anything else is refused before the
+    solver touches a device."""
+    write_inputs(tmp_path)
     w = in3d(tmp_path)
-    w.npc = 1
+    w.npc = 2
     w.write(str(tmp_path / "IN3D"))
     r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
-    assert r.returncode != 0 and "PML" in r.stderr
+    assert r.returncode != 0 and "NPC" in r.stderr, r.stderr
 
 
 @pytest.mark.gpu
