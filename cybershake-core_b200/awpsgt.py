@@ -45,7 +45,7 @@ EXPORTED = [
     "awp_server_destroy", "awp_sgt_floats_for", "awp_field_energy_noalloc", "awp_server_configure",
     "awp_get_sgt_rwg", "awp_sgt_reorder_rwg", "awp_write_sgt_header", "awp_load_media_rwg",
     "awp_reformat_velocity", "awp_get_tuning", "awp_set_tuning", "awp_autotune", "awp_release_cached_memory",
-    "awp_set_field", "awp_checkpoint_write", "awp_checkpoint_read", "awp_device_memory",
+    "awp_set_field", "awp_checkpoint_write", "awp_checkpoint_read", "awp_device_memory", "awp_get_plane",
 ]
 # Every symbol include/awp_synth.h declares.
 EXPORTED_SYNTH = [
@@ -353,6 +353,7 @@ def load_library(path: str = LIB_PATH):
         "awp_get_sgt": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
         "awp_get_chkj": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
         "awp_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+        "awp_get_plane": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "awp_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
         "awp_device_memory": (C.c_int, [C.c_int, P(C.c_int64), P(C.c_int64)]),
         "awp_checkpoint_write": (C.c_int, [C.c_void_p, C.c_char_p]),
@@ -547,6 +548,14 @@ class Solver:
         p = self.p
         out = np.zeros((p.nz + 4, p.ny + 4, p.nx + 4), dtype=np.float32)
         _check(self.lib.awp_get_field(self.h, comp, FIELDS.index(name), _ptr(out)))
+        return out
+
+    def plane(self, name: str, k: int, comp: int = 0) -> np.ndarray:
+        """awp_get_plane: the interior [ny][nx] of level k (1..nz, nz = the
+        free surface) of a wavefield or stress."""
+        p = self.p
+        out = np.zeros((p.ny, p.nx), dtype=np.float32)
+        _check(self.lib.awp_get_plane(self.h, comp, FIELDS.index(name), k, _ptr(out)))
         return out
 
     def set_field(self, name: str, arr, comp: int = 0) -> None:

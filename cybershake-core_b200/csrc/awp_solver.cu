@@ -1663,6 +1663,21 @@ static awp_status bfp_set(awp_solver *s, int q, int field, const float *in)
     return bfp_set_group(s, q, a / 3, v);
 }
 
+extern "C" awp_status awp_get_plane(awp_solver *s, int comp, int field, int k, float *out)
+{
+    if (!s || !out) return set_err(AWP_ERR_PARAM, "null argument");
+    if (comp < 0 || comp >= s->p.ncomp) return set_err(AWP_ERR_PARAM, "bad component");
+    if (field < 0 || field >= AF_R1) return set_err(AWP_ERR_PARAM, "field %d is not a wavefield or stress", field);
+    const AwpGeom &g = s->g;
+    if (k < 1 || k > g.nz) return set_err(AWP_ERR_PARAM, "level %d outside 1..%d", k, g.nz);
+    CU(cudaSetDevice(s->p.device));
+    CU(cudaStreamSynchronize(s->stream));
+    const float *src = s->comp[cur_buf(s, s->steps_done)][comp].f[field];
+    CU(cudaMemcpy2D(out, (size_t)g.nx * sizeof(float), src + g.idx(1, 1, k), (size_t)g.px * sizeof(float),
+                    (size_t)g.nx * sizeof(float), (size_t)g.ny, cudaMemcpyDeviceToHost));
+    return AWP_OK;
+}
+
 extern "C" awp_status awp_get_field(awp_solver *s, int comp, int field, float *out)
 {
     if (!s) return set_err(AWP_ERR_PARAM, "null solver");

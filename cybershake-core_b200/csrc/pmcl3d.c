@@ -60,23 +60,22 @@ static void fmt_e(char *out, size_t cap, double v, int w, int d)
     snprintf(out, cap, "%*s", w, body);
 }
 
-/* Fortran Gw.d for the magnitudes CHKP prints */
+/* Fortran Gw.d: F editing, (d - k) decimals and four trailing blanks, when
+ * the value rounded to d significant digits lies in [0.1, 10^d) with k its
+ * number of integer digits (zero: F with d - 1 decimals); Ew.d otherwise */
 static void fmt_g(char *out, size_t cap, double v, int w, int d)
 {
-    double a = fabs(v);
-    if (a >= 0.1 && a < pow(10.0, d)) {
-        int e = (int)floor(log10(a)) + 1;
-        char f[64];
-        snprintf(f, sizeof f, "%*.*f    ", w - 4, d - e, v);
-        snprintf(out, cap, "%s", f);
-    } else {
-        fmt_e(out, cap, v, w, d);
-    }
+    if (v == 0.0) { snprintf(out, cap, "%*.*f    ", w - 4, d - 1, 0.0); return; }
+    char tmp[64];
+    snprintf(tmp, sizeof tmp, "%.*e", d - 1, fabs(v));
+    const int k = atoi(strchr(tmp, 'e') + 1) + 1;
+    if (k >= 0 && k <= d) snprintf(out, cap, "%*.*f    ", w - 4, d - k, v);
+    else fmt_e(out, cap, v, w, d);
 }
 
 static void mkdir_for(const char *path)
 {
-    char buf[1024];
+    char buf[1200];
     snprintf(buf, sizeof buf, "%s", path);
     for (char *p = buf + 1; *p; p++)
         if (*p == '/') { *p = 0; mkdir(buf, 0755); *p = '/'; }
@@ -88,7 +87,8 @@ static void write_chkp_fortran(const awp_in3d *in, const awp_stats *st)
     FILE *f = fopen(in->chkp, "w");
     if (!f) return;
     char b1[64], b2[64], b3[64];
-    fprintf(f, " igreen = %11d\n", in->igreen);
+    /* list-directed: blank, the string, a blank separator, I11 (gfortran) */
+    fprintf(f, " igreen =  %11d\n", in->igreen);
     fmt_e(b1, sizeof b1, st->vp_max * in->dt / in->dh, 15, 7);
     fprintf(f, "STABILITY CRITERIA .5 > CMAX*DT/DX = %s\n", b1);
     fprintf(f, "# OF X NODES PER PROC%5d\n", in->nx / (in->npx > 0 ? in->npx : 1));
@@ -137,6 +137,111 @@ static void write_chkp_gpu(const awp_in3d *in, const awp_stats *st)
     fprintf(f, "FD SCHEME, VISCO=1 OR ELASTIC=0:\t%d\n", in->nve);
     fprintf(f, "Q, FL,FP,FH:\t%f, %f, %f\n", in->fl, in->fp, in->fh);
     fclose(f);
+}
+
+/* Surface velocity recording of the GPU command line, one rank
+ * (AWP-GPU-SGT/src/pmcl3d.c:300-320, calcRecordingPoints :1336-1395 and the
+ * NTISKP block :962-1031): after every step that is a multiple of NTISKP,
+ * u1 v1 w1 on the NBG*:NSKP*:NED* window (z counted in depth from the free
+ * surface, z = 1 the surface) are stored as sample (step/NTISKP - 1) mod
+ * WRITE_STEP of a buffer [WRITE_STEP][depth][y][x] per component; a full
+ * buffer goes to OUT/SX%07ld, SY, SZ named by the step.  The CHKFILE gets
+ * "step :\tu\tv\tw" at x = y = ND+1, depth ND below the surface, and "END"
+ * when the run is over. */
+typedef struct {
+    int bg[3], skp[3], cnt[3];   /* 0-based first index, stride, count: x, y, depth */
+    int ws;
+    size_t rec;                  /* floats per sample and component */
+    float *buf[3], *plane;
+    FILE *chk;
+} surf_rec;
+
+/* rec_nbg / rec_ned / rec_n* of calcRecordingPoints for the one rank that
+ * holds the whole axis of n points */
+static int rec_axis(int n, int nbg, int ned, int nskp, int lateral, int *bg, int *cnt)
+{
+    if (ned == -1) ned = n;
+    if (nskp < 1 || nbg < 1) return -1;
+    ned = ned - (ned - nbg) % nskp;
+    *bg = nbg - 1;
+    if (nbg > n || (lateral && ned < 1)) { *cnt = 0; return 0; }
+    int ed;
+    if (!lateral) ed = ned - 1;
+    else if (n <= ned) ed = (n + nbg - 1) % nskp - nskp + n;
+    else ed = ned - 1;
+    if (ed > n - 1) return -1;
+    *cnt = ed < *bg ? 0 : (ed - *bg) / nskp + 1;
+    return 0;
+}
+
+static int surf_open(surf_rec *r, const awp_in3d *in, const awp_params *p)
+{
+    memset(r, 0, sizeof *r);
+    const int n[3] = {p->nx, p->ny, p->nz};
+    const int bg[3] = {in->nbgx, in->nbgy, in->nbgz}, ed[3] = {in->nedx, in->nedy, in->nedz};
+    const int sk[3] = {in->nskpx, in->nskpy, in->nskpz};
+    for (int a = 0; a < 3; a++) {
+        r->skp[a] = sk[a];
+        if (rec_axis(n[a], bg[a], ed[a], sk[a], a < 2, &r->bg[a], &r->cnt[a]) != 0) {
+            fprintf(stderr, "pmcl3d: recording window NBG/NED/NSKP outside the grid on axis %c\n", "XYZ"[a]);
+            return -1;
+        }
+    }
+    if (!r->cnt[0] || !r->cnt[1] || !r->cnt[2]) r->cnt[0] = r->cnt[1] = r->cnt[2] = 0;
+    r->ws = p->write_step > 0 ? p->write_step : 1;
+    r->rec = (size_t)r->cnt[0] * r->cnt[1] * r->cnt[2];
+    for (int c = 0; c < 3; c++) r->buf[c] = (float *)calloc(r->rec * r->ws + 1, sizeof(float));
+    r->plane = (float *)malloc(sizeof(float) * (size_t)p->nx * p->ny);
+    r->chk = fopen(in->chkp, "a");
+    if (!r->buf[0] || !r->buf[1] || !r->buf[2] || !r->plane) return -1;
+    return 0;
+}
+
+static int surf_record(surf_rec *r, awp_solver *s, const awp_in3d *in, const awp_params *p, int step)
+{
+    static const char *base[3] = {"SX", "SY", "SZ"};
+    const int sample = (step / in->ntiskp + r->ws - 1) % r->ws;
+    float probe[3] = {0, 0, 0};
+    const int kp = p->nz - in->nd;
+    for (int c = 0; c < 3; c++) {
+        float *dst = r->buf[c] + (size_t)sample * r->rec;
+        for (int dz = 0; dz < r->cnt[2]; dz++) {
+            if (awp_get_plane(s, 0, c, p->nz - (r->bg[2] + dz * r->skp[2]), r->plane) != AWP_OK) return -1;
+            for (int jy = 0; jy < r->cnt[1]; jy++)
+                for (int ix = 0; ix < r->cnt[0]; ix++)
+                    *dst++ = r->plane[(size_t)(r->bg[1] + jy * r->skp[1]) * p->nx + r->bg[0] + ix * r->skp[0]];
+        }
+        if (r->chk && kp >= 1 && in->nd < p->nx && in->nd < p->ny) {
+            if (awp_get_plane(s, 0, c, kp, r->plane) != AWP_OK) return -1;
+            probe[c] = r->plane[(size_t)in->nd * p->nx + in->nd];
+        }
+    }
+    if (r->chk) {
+        fprintf(r->chk, "%ld :\t%e\t%e\t%e\n", (long)step, probe[0], probe[1], probe[2]);
+        fflush(r->chk);
+    }
+    if ((step / in->ntiskp) % r->ws == 0) {
+        for (int c = 0; c < 3; c++) {
+            char name[1100];
+            snprintf(name, sizeof name, "%s/%s%07ld", in->out_dir, base[c], (long)step);
+            mkdir_for(name);
+            FILE *f = fopen(name, "wb");
+            if (!f || fwrite(r->buf[c], sizeof(float), r->rec * r->ws, f) != r->rec * r->ws) {
+                fprintf(stderr, "pmcl3d: cannot write %s\n", name);
+                if (f) fclose(f);
+                return -1;
+            }
+            fclose(f);
+        }
+    }
+    return 0;
+}
+
+static void surf_close(surf_rec *r)
+{
+    if (r->chk) { fprintf(r->chk, "END\n"); fclose(r->chk); }
+    for (int c = 0; c < 3; c++) free(r->buf[c]);
+    free(r->plane);
 }
 
 static int write_chkj(const char *path, const float *chkj, int nt)
@@ -215,27 +320,36 @@ int main(int argc, char **argv)
     if (in.gpu_cli) write_chkp_gpu(&in, &stats);
     else write_chkp_fortran(&in, &stats);
 
+    /* pmcl3d.f:1018-1097: with CHECKPOINT > 0 resume from output_ckp/ when a
+     * checkpoint is there; pmcl3d.f:1967-2045: a checkpoint after every step i
+     * with mod(i, CHECKPOINT) == 0.  The GPU command line records the surface
+     * every NTISKP steps.  The time loop runs in segments between those
+     * steps. */
+    int t0 = 0;
     if (in.checkpoint > 0) {
-        /* pmcl3d.f:1018-1097: resume from output_ckp/ when a checkpoint is
-         * there; pmcl3d.f:1967-2045: a checkpoint after every step i with
-         * mod(i, CHECKPOINT) == 0 */
         mkdir("output_ckp", 0755);
-        int t0 = 0;
         if ((st = awp_checkpoint_read(s, "output_ckp", &t0)) != AWP_OK) return fail(st, "reading the checkpoint");
         if (t0 > 0) printf("Checkpoint found, starting from step %d\n", t0);
-        for (int done = t0; done < p.nt;) {
-            int n = in.checkpoint - done % in.checkpoint;
-            if (n > p.nt - done) n = p.nt - done;
-            if ((st = awp_run(s, n, NULL)) != AWP_OK) return fail(st, "time stepping");
-            done += n;
-            if (done % in.checkpoint == 0) {
-                printf("Writing checkpoint file\n");
-                if ((st = awp_checkpoint_write(s, "output_ckp")) != AWP_OK) return fail(st, "writing the checkpoint");
-            }
-        }
-    } else if ((st = awp_run(s, p.nt, NULL)) != AWP_OK) {
-        return fail(st, "time stepping");
     }
+    surf_rec rec;
+    const int rec_every = in.gpu_cli && in.ntiskp > 0 ? in.ntiskp : 0;
+    if (in.gpu_cli && surf_open(&rec, &in, &p) != 0) return fail(AWP_ERR_PARAM, "setting up the surface recording");
+    if (!in.gpu_cli && in.ntiskp > 0 && in.ntiskp <= p.nt)
+        fprintf(stderr, "pmcl3d: NTISKP %d <= NT: the IN3D form's velocity output files are not written\n", in.ntiskp);
+    for (int done = t0; done < p.nt;) {
+        int n = p.nt - done;
+        if (in.checkpoint > 0 && in.checkpoint - done % in.checkpoint < n) n = in.checkpoint - done % in.checkpoint;
+        if (rec_every && rec_every - done % rec_every < n) n = rec_every - done % rec_every;
+        if ((st = awp_run(s, n, NULL)) != AWP_OK) return fail(st, "time stepping");
+        done += n;
+        if (in.checkpoint > 0 && done % in.checkpoint == 0) {
+            printf("Writing checkpoint file\n");
+            if ((st = awp_checkpoint_write(s, "output_ckp")) != AWP_OK) return fail(st, "writing the checkpoint");
+        }
+        if (rec_every && done % rec_every == 0 && surf_record(&rec, s, &in, &p, done) != 0)
+            return fail(AWP_ERR_IO, "recording the surface");
+    }
+    if (in.gpu_cli) surf_close(&rec);
     awp_get_stats(s, &stats);
     printf("time loop: %d steps in %.3f s, %.3f Gcell-updates/s\n", (int)stats.steps_done, stats.seconds_loop,
            stats.gcell_updates_per_s);

@@ -191,6 +191,15 @@ awp_status awp_get_chkj(awp_solver *s, int comp, float *out);
  * 15..19 = lam mu d1 qp qs (compliances as stored by structure.f:488-519). */
 awp_status awp_get_field(awp_solver *s, int comp, int field, float *out);
 
+/* Copies the interior of one horizontal level of a wavefield or stress
+ * (field 0..8, numbering as awp_get_field) after the steps done so far:
+ * out[(j-1)*nx + (i-1)] = field(i, j, k), i = 1..nx, j = 1..ny, k = 1..nz
+ * (k = nz is the free surface).  Replaces the reference's per-NTISKP device
+ * copies of u1, v1, w1 for the surface velocity files and the CHKP statistics
+ * line (AWP-GPU-SGT/src/pmcl3d.c:962-1031), moving one level instead of the
+ * whole volume. */
+awp_status awp_get_plane(awp_solver *s, int comp, int field, int k, float *out);
+
 /* Sets one state field (0..14, numbering as awp_get_field) of one component
  * from the padded host layout in[(k+1)][(j+1)][(i+1)], extents (nz+4, ny+4,
  * nx+4), float32; memory variables stored in 16 bits are rounded to nearest

@@ -8,6 +8,7 @@ import pytest
 
 import awp_inputs as ai
 import awpsgt
+import fortran_format as ff
 import oracle
 
 NX, NY, NZ, NST = 48, 40, 32, 60
@@ -201,3 +202,134 @@ def test_autotuned_drop_in_run(tmp_path):
         got = np.fromfile(tmp_path / "out" / "sgt" / "awp-strain", dtype=np.float32)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
         assert len(cache.read_text().splitlines()) == 1      # the second run reads it back
+
+
+def test_fortran_format_helper():
+    """The edit-descriptor helper the CHKP / CHKJ comparisons use, on values
+    whose Fortran output follows from the standard's rules by hand."""
+    assert ff.e(0.5, 15, 7) == "  0.5000000E+00"
+    assert ff.e(-1.234e-5, 10, 3) == "-0.123E-04"
+    assert ff.e(0.0, 10, 3) == " 0.000E+00"
+    assert ff.e(9.9996, 10, 3) == " 0.100E+02"        # rounding carries into the exponent
+    assert ff.g(0.92, 13, 4) == "   0.9200    "
+    assert ff.g(0.01, 14, 5) == "   0.10000E-01"
+    assert ff.g(25.0, 14, 5) == "    25.000    "
+    assert ff.g(0.5, 14, 5) == "   0.50000    "
+    assert ff.g(99999.9, 13, 4) == "   0.1000E+06"
+    assert ff.f(200.0, 10, 4) == "  200.0000"
+    assert ff.i(61, 5) == "   61"
+    assert ff.list_directed("igreen = ", 1) == " igreen =            1"
+
+
+def expected_chkp_fortran(w, ext):
+    """io.f:486-531 (wrpm3d) for one rank, every REAL in single precision;
+    ext = the oracle's extremes (vp min/max, vs min/max, rho min/max) of the
+    SoCalQ-corrected media (structure.f:469-530)."""
+    f32 = np.float32
+    vpmin, vpmax, vsmin, vsmax, dmin, dmax = (f32(v) for v in ext)
+    cfl = f32(vpmax * f32(w.dt)) / f32(w.dh)
+    lines = [ff.list_directed("igreen = ", w.igreen),
+             "STABILITY CRITERIA .5 > CMAX*DT/DX = " + ff.e(cfl, 15, 7),
+             "# OF X NODES PER PROC" + ff.i(w.nx // w.npx, 5),
+             "# OF Y NODES PER PROC" + ff.i(w.ny // w.npy, 5),
+             "# OF Z NODES PER PROC" + ff.i(w.nz // w.npz, 5),
+             "# OF TIME STEPS" + ff.i(w.nt, 5),
+             "DISCRETIZATION IN SPACE" + ff.f(f32(w.dh), 10, 4),
+             "DISCRETIZATION IN TIME" + ff.f(f32(w.dt), 10, 4),
+             "PML REFLECTION COEFFICIENT" + ff.g(f32(w.arbc), 13, 4),
+             "HIGHEST P-VELOCITY ENCOUNTERED" + ff.f(vpmax, 10, 2),
+             "LOWEST P-VELOCITY ENCOUNTERED" + ff.f(vpmin, 10, 2),
+             "HIGHEST S-VELOCITY ENCOUNTERED" + ff.f(vsmax, 10, 2),
+             "LOWEST S-VELOCITY ENCOUNTERED" + ff.f(vsmin, 10, 2),
+             "HIGHEST DENSITY ENCOUNTERED" + ff.f(dmax, 15, 2),
+             "LOWEST  DENSITY ENCOUNTERED" + ff.f(dmin, 15, 2),
+             "SKIP OF SEISMOGRAMS IN TIME (LOOP COUNTER)" + ff.i(w.ntiskp, 5),
+             "ABC CONDITION, PML=1 OR CERJAN=0:" + ff.i(w.npc, 5),
+             "FD SCHEME, VISCO=1 OR ELASTIC=0:" + ff.i(w.nve, 5),
+             "Q, FL,FP,FH:" + ff.g(f32(w.fl), 14, 5) + ff.g(f32(w.fp), 14, 5) + ff.g(f32(w.fh), 14, 5)]
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.gpu
+def test_chkp_and_chkj_text_match_the_fortran_writes(tmp_path):
+    """CHKP line for line as wrpm3d writes it (io.f:481-536: the stability
+    number vpe(2)*dt/dh, the media extremes, the parameters, each in its
+    edit descriptor) and CHKJ as (I6,3E10.3) of the oracle's probe values
+    (pmcl3d.f:1478-1479), character for character.  The first CHKP line is
+    list-directed output, whose spacing the standard leaves to the compiler:
+    gfortran's."""
+    media, stf, pts = write_inputs(tmp_path)
+    w = in3d(tmp_path)
+    r = subprocess.run([awpsgt.PMCL3D_PATH, "IN3D"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    o = oracle_sgt(media, stf, pts)
+    got = (tmp_path / "out" / "CHKP").read_text()
+    want = expected_chkp_fortran(w, o.extremes())
+    assert got == want, "\n".join(a + " | " + b for a, b in zip(got.splitlines(), want.splitlines()) if a != b)
+    cj = o.chkj()
+    want_j = "".join(ff.i(n + 1, 6) + "".join(ff.e(v, 10, 3) for v in cj[n]) + "\n" for n in range(len(cj)))
+    assert (tmp_path / "out" / "CHKJ").read_text() == want_j
+    assert np.abs(cj).max() > 0
+
+
+@pytest.mark.gpu
+def test_gpu_command_line_surface_records_and_chkfile(tmp_path):
+    """The GPU command line with NTISKP < NT (AWP-GPU-SGT/src/pmcl3d.c:962-1031,
+    1172-1174): every NTISKP steps u1 v1 w1 on the NBG*:NSKP*:NED* window
+    (z in depth from the surface) fill a WRITE_STEP-sample buffer, written to
+    OUT/SX%07d, SY, SZ when full; the CHKFILE, after the parameter lines of
+    io.c:16-31, gets "step :\tu\tv\tw" at x = y = ND+1, depth ND, and "END"."""
+    media, stf, pts = write_inputs(tmp_path, ifault=1)
+    ntiskp, ws = 4, 3
+    argv = [awpsgt.PMCL3D_PATH, "-T", "0.6", "--IGREEN", "1", "--DH", "200.0", "--DT", "0.01", "--NSRC", "1",
+            "--NST", str(NST), "-X", str(NX), "-Y", str(NY), "-Z", str(NZ), "-x", "1", "-y", "1", "--NPC", "0",
+            "--ARBC", "0.92", "--ND", "8", "--IFAULT", "1", "--MEDIASTART", "1", "--FL", "0.01", "--FH", "25.0",
+            "--FP", "0.5", "--READ_STEP", str(NST), "--WRITE_STEP", str(ws), "-o", "out", "--INSGT", "input/cord",
+            "-c", "out/CHKP", "--INSRC", "input/src", "--INVEL", "input/media", "--NTISKP_SGT", "5",
+            "--NTISKP", str(ntiskp), "--NBGX", "2", "--NEDX", "40", "--NSKPX", "3", "--NBGY", "1", "--NEDY", "-1",
+            "--NSKPY", "2", "--NBGZ", "1", "--NEDZ", "3", "--NSKPZ", "2"]
+    r = subprocess.run(argv, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    nt = int(np.float32(0.6) / np.float32(0.01)) + 1
+    # the window by hand from pmcl3d.c:300-320 and calcRecordingPoints for one
+    # rank: NEDX 40 -> 38 (a record point), x = 2, 5, .., 38; NEDY -1 -> 40 ->
+    # 39, and since NY <= 39 fails, y = 1, 3, .., 39; depth 0 and 2 (z = NZ, NZ-2)
+    xs, ys, ks = np.arange(1, 38, 3), np.arange(0, 39, 2), [NZ, NZ - 2]
+    o = oracle.Oracle(nx=NX, ny=NY, nz=NZ, dh=200.0, dt=0.01, nt=nt, nst=NST, nd=8, fl=0.01, fh=25.0, fp=0.5,
+                      socalq=1, ntiskp_sgt=5, write_step=ws, igreen=1)
+    o.load_media(media)
+    o.set_source([(24, 20, 9)], stf)
+    o.set_points(pts)
+    bufs = {c: np.zeros((ws, len(ks), len(ys), len(xs)), np.float32) for c in ("u1", "v1", "w1")}
+    lines, done, nfiles = [], 0, 0
+    for t in range(ntiskp, nt + 1, ntiskp):
+        o.run(t - done)
+        done = t
+        sample = (t // ntiskp + ws - 1) % ws
+        probe = []
+        for c in ("u1", "v1", "w1"):
+            fld = o.field(c)
+            for dz, k in enumerate(ks):
+                bufs[c][sample, dz] = fld[k + 1, 2:NY + 2, 2:NX + 2][np.ix_(ys, xs)]
+            probe.append(fld[NZ - 8 + 1, 8 + 2, 8 + 2])
+        lines.append("%d :\t%e\t%e\t%e" % (t, *probe))
+        if (t // ntiskp) % ws == 0:
+            nfiles += 1
+            for c, name in (("u1", "SX"), ("v1", "SY"), ("w1", "SZ")):
+                got = np.fromfile(tmp_path / "out" / ("%s%07d" % (name, t)), dtype=np.float32)
+                assert got.size == bufs[c].size
+                assert np.array_equal(got.view(np.uint32), bufs[c].ravel().view(np.uint32)), (name, t)
+    assert nfiles >= 4 and np.abs(bufs["u1"]).max() > 0
+    chk = (tmp_path / "out" / "CHKP").read_text().splitlines()
+    f32 = np.float32
+    ext = o.extremes()
+    head = ["STABILITY CRITERIA .5 > CMAX*DT/DX:\t%f" % (f32(f32(ext[1]) * f32(0.01)) / f32(200.0)),
+            "# OF X,Y,Z NODES PER PROC:\t%d, %d, %d" % (NX, NY, NZ), "# OF TIME STEPS:\t%d" % nt,
+            "DISCRETIZATION IN SPACE:\t%f" % f32(200.0), "DISCRETIZATION IN TIME:\t%f" % f32(0.01),
+            "PML REFLECTION COEFFICIENT:\t%f" % f32(0.92),
+            "HIGHEST P-VELOCITY ENCOUNTERED:\t%f" % ext[1], "LOWEST P-VELOCITY ENCOUNTERED:\t%f" % ext[0],
+            "HIGHEST S-VELOCITY ENCOUNTERED:\t%f" % ext[3], "LOWEST S-VELOCITY ENCOUNTERED:\t%f" % ext[2],
+            "HIGHEST DENSITY ENCOUNTERED:\t%f" % ext[5], "LOWEST  DENSITY ENCOUNTERED:\t%f" % ext[4],
+            "SKIP OF SEISMOGRAMS IN TIME (LOOP COUNTER):\t%d" % ntiskp, "ABC CONDITION, PML=1 OR CERJAN=0:\t0",
+            "FD SCHEME, VISCO=1 OR ELASTIC=0:\t1", "Q, FL,FP,FH:\t%f, %f, %f" % (f32(0.01), f32(0.5), f32(25.0))]
+    assert chk == head + lines + ["END"]
