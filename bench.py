@@ -189,7 +189,14 @@ def workload(args=None):
                                 src_xyz=(nx // 2, ny // 2, min(21, nz)), npts=min(w.npts, nx * ny // 4))
     if args.components:
         w = dataclasses.replace(w, name=w.name + "_c%d" % args.components, igreen=w.igreen[:args.components])
+    if getattr(args, "npc", 0):
+        w = dataclasses.replace(w, name=w.name + "_pml")
     return w
+
+
+def boundary(w):
+    """NPC of a workload: 1 (PML) when its name says so, else 0 (Cerjan)."""
+    return 1 if w.name.endswith("_pml") else 0
 
 
 def solver_params(w, device, precision="f32", kernel="auto"):
@@ -197,7 +204,7 @@ def solver_params(w, device, precision="f32", kernel="auto"):
     return awpsgt.make_params(w.nx, w.ny, w.nz, w.dh, w.dt, w.nt, nst=w.nst, igreen=w.igreen, nd=20,
                               arbc=0.92, fl=w.fl, fh=w.fh, fp=w.fp, socalq=w.socalq, ntiskp_sgt=w.ntiskp_sgt,
                               write_step=w.nst // w.ntiskp_sgt, precision=precision, kernel=kernel,
-                              device=device)
+                              device=device, npc=boundary(w))
 
 
 def make_solver(w, media, pts, stfs, device, precision="f32", kernel="auto", tuning=None):
@@ -587,6 +594,7 @@ def main():
     ap.add_argument("--config", type=int, default=0, help="workload 1..4 (default 2: 400x400x200 fx+fy+fz)")
     ap.add_argument("--grid", default="", help="nx,ny,nz: reduced grid for profiling captures")
     ap.add_argument("--components", type=int, default=0, help="first n of the fx, fy, fz components")
+    ap.add_argument("--npc", type=int, default=0, choices=[0, 1], help="absorbing boundary: 0 Cerjan, 1 PML")
     ap.add_argument("--serve", action="store_true", help="serving stream: p50/p99 latency against serial solves")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-load", type=float, default=1.2, help="offered load / serial service rate")
@@ -714,7 +722,7 @@ def main():
                 "step_frac": (step_bytes * value * 1e9 / (cells * ncomp * world)) / 1e9 / peak,
                 "bytes_per_cell_update": bpcu}
 
-    launches_per_ts = 2 if "k_fused" in prof else 4    # stepper kernel(s) + k_post
+    launches_per_ts = (2 if "k_fused" in prof else 4) + 2 * boundary(w)   # stepper kernel(s) + k_post (+ PML)
     gpu_launches = args.steps * (per_step_ts * launches_per_ts + 1)
 
     line = {
@@ -752,6 +760,13 @@ def main():
                 b["sgt_rel_l2_vs_fp64"] = {k: v.get("bfp") for k, v in study.get("cases", {}).items()}
                 b["error_source"] = study.get("source")
             line["bfp"] = b
+        if args.kernel == "auto" and args.precision == "f32":
+            f = window_rate(w, media, pts, stfs, local, "f32", "staged_fma", None, prefill, warm_ts, timed_ts)
+            f["vs_plain_fp32"] = f["value"] / plain["value"]
+            study = precision_study()
+            if study:
+                f["sgt_rel_l2_vs_fp64"] = {k: v.get("f32/staged_fma") for k, v in study.get("cases", {}).items()}
+            line["staged_fma"] = f
         line["serving"] = serve_stream(16, 0.1, 1.2, 4, "fifo", 0.0)
     if rank == 0:
         line["clocks"] = clk.summary()

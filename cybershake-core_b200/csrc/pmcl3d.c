@@ -73,6 +73,19 @@ static void fmt_g(char *out, size_t cap, double v, int w, int d)
     else fmt_e(out, cap, v, w, d);
 }
 
+/* Fortran Iw: asterisks when the number does not fit */
+static const char *fmt_i(char *out, size_t cap, long v, int w)
+{
+    char tmp[32];
+    const int n = snprintf(tmp, sizeof tmp, "%*ld", w, v);
+    if (n > w) {
+        memset(tmp, '*', (size_t)w);
+        tmp[w] = 0;
+    }
+    snprintf(out, cap, "%s", tmp);
+    return out;
+}
+
 static void mkdir_for(const char *path)
 {
     char buf[1200];
@@ -86,15 +99,15 @@ static void write_chkp_fortran(const awp_in3d *in, const awp_stats *st)
     mkdir_for(in->chkp);
     FILE *f = fopen(in->chkp, "w");
     if (!f) return;
-    char b1[64], b2[64], b3[64];
+    char b1[64], b2[64], b3[64], ib[32];
     /* list-directed: blank, the string, a blank separator, I11 (gfortran) */
     fprintf(f, " igreen =  %11d\n", in->igreen);
     fmt_e(b1, sizeof b1, st->vp_max * in->dt / in->dh, 15, 7);
     fprintf(f, "STABILITY CRITERIA .5 > CMAX*DT/DX = %s\n", b1);
-    fprintf(f, "# OF X NODES PER PROC%5d\n", in->nx / (in->npx > 0 ? in->npx : 1));
-    fprintf(f, "# OF Y NODES PER PROC%5d\n", in->ny / (in->npy > 0 ? in->npy : 1));
-    fprintf(f, "# OF Z NODES PER PROC%5d\n", in->nz / (in->npz > 0 ? in->npz : 1));
-    fprintf(f, "# OF TIME STEPS%5d\n", in->nt);
+    fprintf(f, "# OF X NODES PER PROC%s\n", fmt_i(ib, sizeof ib, in->nx / (in->npx > 0 ? in->npx : 1), 5));
+    fprintf(f, "# OF Y NODES PER PROC%s\n", fmt_i(ib, sizeof ib, in->ny / (in->npy > 0 ? in->npy : 1), 5));
+    fprintf(f, "# OF Z NODES PER PROC%s\n", fmt_i(ib, sizeof ib, in->nz / (in->npz > 0 ? in->npz : 1), 5));
+    fprintf(f, "# OF TIME STEPS%s\n", fmt_i(ib, sizeof ib, in->nt, 5));
     fprintf(f, "DISCRETIZATION IN SPACE%10.4f\n", in->dh);
     fprintf(f, "DISCRETIZATION IN TIME%10.4f\n", in->dt);
     fmt_g(b1, sizeof b1, in->arbc, 13, 4);
@@ -105,9 +118,9 @@ static void write_chkp_fortran(const awp_in3d *in, const awp_stats *st)
     fprintf(f, "LOWEST S-VELOCITY ENCOUNTERED%10.2f\n", st->vs_min);
     fprintf(f, "HIGHEST DENSITY ENCOUNTERED%15.2f\n", st->rho_max);
     fprintf(f, "LOWEST  DENSITY ENCOUNTERED%15.2f\n", st->rho_min);
-    fprintf(f, "SKIP OF SEISMOGRAMS IN TIME (LOOP COUNTER)%5d\n", in->ntiskp);
-    fprintf(f, "ABC CONDITION, PML=1 OR CERJAN=0:%5d\n", in->npc);
-    fprintf(f, "FD SCHEME, VISCO=1 OR ELASTIC=0:%5d\n", in->nve);
+    fprintf(f, "SKIP OF SEISMOGRAMS IN TIME (LOOP COUNTER)%s\n", fmt_i(ib, sizeof ib, in->ntiskp, 5));
+    fprintf(f, "ABC CONDITION, PML=1 OR CERJAN=0:%s\n", fmt_i(ib, sizeof ib, in->npc, 5));
+    fprintf(f, "FD SCHEME, VISCO=1 OR ELASTIC=0:%s\n", fmt_i(ib, sizeof ib, in->nve, 5));
     fmt_g(b1, sizeof b1, in->fl, 14, 5);
     fmt_g(b2, sizeof b2, in->fp, 14, 5);
     fmt_g(b3, sizeof b3, in->fh, 14, 5);
@@ -254,7 +267,8 @@ static int write_chkj(const char *path, const float *chkj, int nt)
         fmt_e(a, sizeof a, chkj[3 * i], 10, 3);
         fmt_e(b, sizeof b, chkj[3 * i + 1], 10, 3);
         fmt_e(c, sizeof c, chkj[3 * i + 2], 10, 3);
-        fprintf(f, "%6d%s%s%s\n", i + 1, a, b, c);
+        char ib[32];
+        fprintf(f, "%s%s%s%s\n", fmt_i(ib, sizeof ib, i + 1, 6), a, b, c);
     }
     fclose(f);
     return 0;

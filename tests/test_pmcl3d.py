@@ -218,6 +218,7 @@ def test_fortran_format_helper():
     assert ff.g(99999.9, 13, 4) == "   0.1000E+06"
     assert ff.f(200.0, 10, 4) == "  200.0000"
     assert ff.i(61, 5) == "   61"
+    assert ff.i(100000, 5) == "*****"                 # CyberShake's NTISKP in an I5 field
     assert ff.list_directed("igreen = ", 1) == " igreen =            1"
 
 

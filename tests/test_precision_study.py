@@ -39,12 +39,13 @@ CASES = {
     "full": [("cfg1_homog160", 160, 160, 80, 200.0, 0.01, 1000, "homogeneous", 11),
              ("layered160", 160, 160, 100, 100.0, 0.005, 2000, "layered", 21)],
 }
-MODES = [("staged", "f32"), ("staged", "mixed"), ("staged", "bfp"), ("two_sweep", "f32"), ("two_sweep", "mixed"),
+MODES = [("staged", "f32"), ("staged", "mixed"), ("staged", "bfp"), ("staged_fma", "f32"), ("staged_fma", "bfp"),
+         ("two_sweep", "f32"), ("two_sweep", "mixed"),
          ("two_sweep", "bfp"), ("fused", "bfp"),
          ("two_sweep", "f16"), ("two_sweep", "bf16"), ("fused", "f32"), ("fused", "mixed"), ("fused", "f16"),
          ("fused", "bf16")]
 # the workload study: every storage mode on its fastest stepper
-CFG_MODES = [("staged", "f32"), ("staged", "mixed"), ("staged", "bfp"), ("two_sweep", "f16"),
+CFG_MODES = [("staged", "f32"), ("staged", "mixed"), ("staged", "bfp"), ("staged_fma", "f32"), ("two_sweep", "f16"),
              ("two_sweep", "bf16")]
 BOUND_1E4 = ("f32", "bfp")
 
