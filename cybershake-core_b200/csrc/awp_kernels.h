@@ -21,7 +21,12 @@ struct AwpPmlArgs {
     long long n[5], off[5];       /* cells of each plane S N W E B, offsets   */
     AwpComp comp[3];              /* wavefields (the two-sweep buffer)        */
     const float *d1, *lam, *mu;   /* FP32 media                               */
+    const int2 *tiles;            /* 32x8 column tiles holding lateral columns */
+    int ntiles;
 };
+/* tiles (bx, by) of 32 x 8 columns that hold a column within nd of a lateral
+ * face; out may be NULL to count them */
+int awp_pml_lateral_tiles(int nx, int ny, int nd, int2 *out);
 cudaError_t awp_launch_pml(const AwpPmlArgs &a, int part, cudaStream_t st);
 void awp_pml_profiles(int nd, float arbc, float dh, float vs_min, float vs_max, float *rf, float *rh);
 

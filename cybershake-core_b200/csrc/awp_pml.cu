@@ -8,14 +8,18 @@
  * usual sweeps step every cell without a sponge, and two kernels then
  * recompute the boundary zones from the same inputs: k_pml<0> after the
  * velocity sweep (before the free-surface velocity), k_pml<1> after the
- * stress sweep, followed by the free-surface stress image of the columns it
- * rewrote (fstr, operator.f:594-606).  The sweeps' values in the boundary
- * zones are overwritten; their memory variables there are never read (the
- * PML is elastic and r is a point quantity).
+ * stress sweep, followed by k_pml_fstr, the free-surface stress image of the
+ * lateral columns it rewrote (fstr, operator.f:594-606).  The sweeps' values
+ * in the boundary zones are overwritten; their memory variables there are
+ * never read (the PML is elastic and r is a point quantity).
  *
- * One thread per (i, j) column walks the column upward: the lateral zones
- * (x or y within ND of a face) span the whole depth, under the interior
- * columns only the bottom ND levels are PML.  The split arrays of a
+ * The lateral zones (x or y within ND of a face) span the whole depth, under
+ * the interior columns only the bottom ND levels are PML.  One thread takes
+ * up to eight levels of one (i, j) column: one launch covers the bottom ND
+ * levels of every column, a second the levels above of the columns in the
+ * tiles that touch a lateral band (a tile list made once per solver), so the
+ * thread count follows the PML volume rather than the columns.  The split
+ * arrays of a
  * component sit in one device buffer, plane after plane (S N W E B), each
  * plane [split T/H][field][cells of the plane] with the plane's own
  * addressing (memory.f:217-300): S, N nx x ND x nz (N counted from the north
@@ -126,17 +130,39 @@ __device__ __forceinline__ void pml_str_cell(int zone, const PmlCell &x)
     }
 }
 
-/* PART 0: velocities of the boundary zones; PART 1: their stresses, then
- * the free-surface image of each lateral column (blockIdx.z = component) */
-template <int PART>
+constexpr int PML_KC = 8;   /* z levels per thread */
+
+/* PART 0: velocities of the boundary zones; PART 1: their stresses.  The
+ * bottom launch (LATERAL 0) covers levels 1..nd of every column, the lateral
+ * one levels nd+1..nz of the columns within nd of a lateral face, its blocks
+ * taken from the tile list; blockIdx.z = chunk of PML_KC levels x component.
+ * Cells are independent within a part (a velocity update reads stresses and
+ * its own splits, a stress update velocities and its own splits). */
+template <int PART, int LATERAL>
 __global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
 {
-    const int i = blockIdx.x * 32 + threadIdx.x + 1, j = blockIdx.y * 8 + threadIdx.y + 1, q = blockIdx.z;
     const AwpGeom &g = a.g;
-    if (i > g.nx || j > g.ny || q >= a.ncomp) return;
+    int tx, ty;
+    if (LATERAL) {
+        const int2 t = a.tiles[blockIdx.x];
+        tx = t.x; ty = t.y;
+    } else {
+        tx = blockIdx.x; ty = blockIdx.y;
+    }
+    const int i = tx * 32 + threadIdx.x + 1, j = ty * 8 + threadIdx.y + 1;
+    const int q = blockIdx.z % a.ncomp, kc = blockIdx.z / a.ncomp;
+    if (i > g.nx || j > g.ny) return;
     const int nd = a.nd;
     const int xs = i <= nd ? 1 : (i > g.nx - nd ? 2 : 0), ys = j <= nd ? 1 : (j > g.ny - nd ? 2 : 0);
-    const int kmax = (xs || ys) ? g.nz : nd;
+    int k0, k1;
+    if (LATERAL) {
+        if (!xs && !ys) return;
+        k0 = nd + 1 + kc * PML_KC;
+        k1 = min(g.nz, k0 + PML_KC - 1);
+    } else {
+        k0 = 1 + kc * PML_KC;
+        k1 = min(nd, k0 + PML_KC - 1);
+    }
     const AwpComp &cp = a.comp[q];
     PmlCell x;
     x.u1 = cp.f[AF_U]; x.v1 = cp.f[AF_V]; x.w1 = cp.f[AF_W];
@@ -147,7 +173,7 @@ __global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
     x.SY = g.px; x.SZ = g.plane;
     x.i = i; x.j = j; x.nx = g.nx; x.ny = g.ny;
     x.dt = a.dt; x.dth = a.dth; x.pht = a.pht;
-    for (int k = 1; k <= kmax; ++k) {
+    for (int k = k0; k <= k1; ++k) {
         x.k = k;
         x.c = g.idx(i, j, k);
         x.pidx[PS] = ((long long)(k - 1) * nd + (j - 1)) * g.nx + (i - 1);
@@ -159,27 +185,63 @@ __global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
         if (PART == 0) pml_vel_cell(zone, x);
         else pml_str_cell(zone, x);
     }
-    if (PART == 1 && (xs || ys)) {
-        const long sz = g.plane, ct = g.idx(i, j, g.nz);
-        float *ZZ = x.zz, *XZ = x.xz, *YZ = x.yz;
-        ZZ[ct + sz] = -ZZ[ct];
-        ZZ[ct + 2 * sz] = -ZZ[ct - sz];
-        XZ[ct + sz] = -XZ[ct - sz];
-        XZ[ct + 2 * sz] = -XZ[ct - 2 * sz];
-        YZ[ct + sz] = -YZ[ct - sz];
-        YZ[ct + 2 * sz] = -YZ[ct - 2 * sz];
-        XZ[ct] = 0.0f;
-        YZ[ct] = 0.0f;
-    }
+}
+
+/* after the stress part: the free-surface image of each lateral column
+ * (fstr, operator.f:594-606), which the stress sweep wrote from the values
+ * the PML has since replaced */
+__global__ void __launch_bounds__(256) k_pml_fstr(AwpPmlArgs a)
+{
+    const AwpGeom &g = a.g;
+    const int2 t = a.tiles[blockIdx.x];
+    const int i = t.x * 32 + threadIdx.x + 1, j = t.y * 8 + threadIdx.y + 1, q = blockIdx.z;
+    if (i > g.nx || j > g.ny || q >= a.ncomp) return;
+    const int nd = a.nd;
+    if (i > nd && i <= g.nx - nd && j > nd && j <= g.ny - nd) return;
+    const AwpComp &cp = a.comp[q];
+    const long sz = g.plane, ct = g.idx(i, j, g.nz);
+    float *ZZ = cp.f[AF_ZZ], *XZ = cp.f[AF_XZ], *YZ = cp.f[AF_YZ];
+    ZZ[ct + sz] = -ZZ[ct];
+    ZZ[ct + 2 * sz] = -ZZ[ct - sz];
+    XZ[ct + sz] = -XZ[ct - sz];
+    XZ[ct + 2 * sz] = -XZ[ct - 2 * sz];
+    YZ[ct + sz] = -YZ[ct - sz];
+    YZ[ct + 2 * sz] = -YZ[ct - 2 * sz];
+    XZ[ct] = 0.0f;
+    YZ[ct] = 0.0f;
 }
 
 }  // namespace
 
+int awp_pml_lateral_tiles(int nx, int ny, int nd, int2 *out)
+{
+    int n = 0;
+    for (int by = 0; by < (ny + 7) / 8; by++)
+        for (int bx = 0; bx < (nx + 31) / 32; bx++) {
+            const int i0 = bx * 32 + 1, i1 = bx * 32 + 32 < nx ? bx * 32 + 32 : nx;
+            const int j0 = by * 8 + 1, j1 = by * 8 + 8 < ny ? by * 8 + 8 : ny;
+            if (i0 <= nd || i1 > nx - nd || j0 <= nd || j1 > ny - nd) {
+                if (out) out[n] = make_int2(bx, by);
+                n++;
+            }
+        }
+    return n;
+}
+
 cudaError_t awp_launch_pml(const AwpPmlArgs &a, int part, cudaStream_t st)
 {
-    const dim3 b(32, 8), grid((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, a.ncomp);
-    if (part == 0) k_pml<0><<<grid, b, 0, st>>>(a);
-    else k_pml<1><<<grid, b, 0, st>>>(a);
+    const dim3 b(32, 8);
+    const int nbot = (a.nd + PML_KC - 1) / PML_KC, nlat = (a.g.nz - a.nd + PML_KC - 1) / PML_KC;
+    const dim3 gbot((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, nbot * a.ncomp);
+    const dim3 glat(a.ntiles, 1, nlat * a.ncomp);
+    if (part == 0) {
+        k_pml<0, 0><<<gbot, b, 0, st>>>(a);
+        if (a.ntiles > 0 && nlat > 0) k_pml<0, 1><<<glat, b, 0, st>>>(a);
+    } else {
+        k_pml<1, 0><<<gbot, b, 0, st>>>(a);
+        if (a.ntiles > 0 && nlat > 0) k_pml<1, 1><<<glat, b, 0, st>>>(a);
+        if (a.ntiles > 0) k_pml_fstr<<<dim3(a.ntiles, 1, a.ncomp), b, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
