@@ -600,7 +600,8 @@ def main():
     ap.add_argument("--serve-load", type=float, default=1.2, help="offered load / serial service rate")
     ap.add_argument("--serve-active", type=int, default=4, help="requests on the GPU at once")
     ap.add_argument("--serve-nst-scale", type=float, default=1.0, help="scales every request's NST")
-    ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="admission order")
+    ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf", "fifo_srpt"],
+                    help="admission order (fifo_srpt: arrival order, double SM share for the least remaining work)")
     ap.add_argument("--serve-fill", type=float, default=0.0, help="resident cells x components that fill the GPU")
     ap.add_argument("--synth", action="store_true", help="reciprocity synthesis: rupture variations per second")
     ap.add_argument("--autotune", action="store_true", help="time launch shapes on this grid first (untimed)")

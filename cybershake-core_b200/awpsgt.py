@@ -707,9 +707,11 @@ class Server:
         return rid.value
 
     def configure(self, policy: str = "fifo", fill_cells: float = 0.0, chunk_cells: float = 0.0):
-        """Admission order ("fifo" or "sjf"), GPU-fill threshold and chunk size
-        in cell-updates (<= 0 keeps the current value)."""
-        _check(self.lib.awp_server_configure(self.h, {"fifo": 0, "sjf": 1}[policy], fill_cells, chunk_cells))
+        """Admission order ("fifo", "sjf" or "fifo_srpt": arrival order with a
+        double SM share for the resident solve with the least remaining work),
+        GPU-fill threshold and chunk size in cell-updates (<= 0 keeps the
+        current value)."""
+        _check(self.lib.awp_server_configure(self.h, {"fifo": 0, "sjf": 1, "fifo_srpt": 2}[policy], fill_cells, chunk_cells))
 
     def poll(self, rid: int) -> dict:
         info = RequestInfo()

@@ -84,7 +84,7 @@ struct awp_server {
     void sched_loop();
     void admit_loop();
     void reap_loop();
-    awp_status share_sms(Req *r, int resident);
+    awp_status share_sms(Req *r, int resident, bool first);
     void end(Req *r, int state, awp_status st);
     awp_status build(Req *r);
     double resident_cells() const
@@ -134,12 +134,14 @@ awp_status awp_server::build(Req *r)
 
 /* Each resident solve's persistent grids span its share of the SMs (all of
  * them when it is alone), so that solves sharing the GPU run side by side
- * instead of taking turns with grids that each fill the device.  The share is
- * set between chunks, when nothing of the solve is in flight; launch shapes
- * do not change results. */
-awp_status awp_server::share_sms(Req *r, int resident)
+ * instead of taking turns with grids that each fill the device: equal shares,
+ * or under AWP_SERVE_FIFO_SRPT a double share for the solve with the least
+ * remaining work (`first`).  The share is set between chunks, when nothing of
+ * the solve is in flight; launch shapes do not change results. */
+awp_status awp_server::share_sms(Req *r, int resident, bool first)
 {
-    const int want = resident <= 1 ? 0 : (nsm + resident - 1) / resident;
+    int want = resident <= 1 ? 0 : (nsm + resident - 1) / resident;
+    if (resident > 1 && policy == AWP_SERVE_FIFO_SRPT) want = (nsm * (first ? 2 : 1) + resident) / (resident + 1);
     if (want == r->sm_share) return AWP_OK;
     awp_tuning t;
     awp_status st = awp_get_tuning(r->s, &t);
@@ -223,7 +225,15 @@ void awp_server::sched_loop()
             }
             if (q < 0 && st == AWP_OK) st = AWP_ERR_CUDA;
             if (st == AWP_OK && !r->cancel && steps < r->rq.params.nt) {
-                st = share_sms(r, (int)snap.size());
+                /* least remaining work among the resident solves (ties: lower id) */
+                bool first = true;
+                const double left = r->cells * (double)(r->rq.params.nt - steps);
+                for (Req *o : snap) {
+                    if (o == r) continue;
+                    const double ol = o->cells * (double)(o->rq.params.nt - o->info.steps_done);
+                    if (ol < left || (ol == left && o->id < r->id)) first = false;
+                }
+                st = share_sms(r, (int)snap.size(), first);
                 if (st == AWP_OK) st = awp_run_async(r->s, chunk_steps_for(this, r));
                 r->in_flight = st == AWP_OK;
             }
@@ -305,7 +315,8 @@ extern "C" awp_status awp_server_create(int device, int64_t hbm_budget, int max_
 extern "C" awp_status awp_server_configure(awp_server *sv, int policy, double fill_cells, double chunk_cells)
 {
     if (!sv) return fail(AWP_ERR_PARAM, "null server");
-    if (policy != AWP_SERVE_FIFO && policy != AWP_SERVE_SJF) return fail(AWP_ERR_PARAM, "unknown admission policy");
+    if (policy != AWP_SERVE_FIFO && policy != AWP_SERVE_SJF && policy != AWP_SERVE_FIFO_SRPT)
+        return fail(AWP_ERR_PARAM, "unknown admission policy");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->policy = policy;
     if (fill_cells > 0) sv->fill_cells = fill_cells;

@@ -497,9 +497,13 @@ awp_status awp_device_memory(int device, int64_t *live_bytes, int64_t *idle_byte
  * chunk_steps: fewest steps a resident solve advances per chunk. */
 awp_status awp_server_create(int device, int64_t hbm_budget, int max_active, int chunk_steps, awp_server **out);
 
-enum { AWP_SERVE_FIFO = 0, AWP_SERVE_SJF = 1 };
+enum { AWP_SERVE_FIFO = 0, AWP_SERVE_SJF = 1, AWP_SERVE_FIFO_SRPT = 2 };
 /* Admission order (AWP_SERVE_FIFO: arrival; AWP_SERVE_SJF: least total work,
- * cells x components x steps, first); fill_cells: resident cells x components
+ * cells x components x steps, first; AWP_SERVE_FIFO_SRPT: arrival, and of the
+ * n >= 2 resident solves the one with the least remaining work has its grids
+ * sized for 2/(n+1) of the SMs, the others for 1/(n+1) each, instead of equal
+ * shares -- short solves leave sooner, long ones are still admitted in
+ * order); fill_cells: resident cells x components
  * at which the GPU counts as full, so that a request is admitted next to
  * others only while their sum stays below it (default 32e6); chunk_cells:
  * cell-updates per chunk (default 4e8; at least chunk_steps steps).  Values

@@ -38,7 +38,7 @@ REQS = [(1, (64, 48, 40), (1,), 120), (2, (96, 80, 48), (1, 2), 90), (3, (40, 40
         (4, (128, 96, 64), (2,), 60), (5, (50, 60, 36), (3, 1), 100), (6, (72, 72, 40), (1,), 80)]
 
 
-@pytest.mark.parametrize("policy,fill", [("fifo", 0.0), ("sjf", 1.0e6)])
+@pytest.mark.parametrize("policy,fill", [("fifo", 0.0), ("sjf", 1.0e6), ("fifo_srpt", 0.0)])
 def test_mix_equals_alone(policy, fill):
     reqs = [make_request(*r) for r in REQS]
     alone = [run_alone(*r) for r in reqs]
