@@ -5,8 +5,9 @@ pinned by properties the discrete equations must have:
   * FP32 and FP64 builds agree to rounding level;
   * exact linearity in the source amplitude (scaling by 2 commutes with IEEE
     rounding, so the FP32 SGT scales bit for bit) and superposition;
-  * P waves travel at Vp: the delay between two receivers on the force axis
-    matches the analytic travel-time difference;
+  * P waves travel at Vp and S waves at Vs: the delay between two receivers
+    on the force axis (P) or across it (S) matches the analytic travel-time
+    difference;
   * reciprocity: the SGT recorded at R from a force at S equals the particle
     velocity at S from a moment-rate source at R (the relation strain Green
     tensors are used for), which pins the SGT coefficients and the source
@@ -186,6 +187,37 @@ def test_chkj_series_recorded():
     c = o.chkj()
     assert c.shape == (30, 3)
     assert np.isfinite(c).all()
+
+
+def test_s_wave_travel_time():
+    """Force along x, receivers on the y axis through the source, where a
+    force radiates no P wave: the shear strain pulse is delayed by
+    (r2 - r1)/Vs between the two receivers."""
+    nx, ny, nz, nt = 48, 140, 72, 450
+    dh, dt, f0 = 200.0, 0.01, 2.0
+    vp, vs = 6000.0, 3464.0
+    media = ai.homogeneous_media(nx, ny, nz, vp=vp, vs=vs, rho=2700.0)
+    stf = ai.gaussian_derivative_stf(nt, dt, f0=f0)
+    o = oracle.Oracle(nx=nx, ny=ny, nz=nz, dh=dh, dt=dt, nt=nt, nd=12, socalq=0, ntiskp_sgt=1, write_step=nt,
+                      igreen=1, precision="f64", fl=0.01, fh=25.0, fp=0.5)
+    o.load_media(media)
+    src = (24, 30, 36)
+    o.set_source([src], stf)
+    r1, r2 = 20, 60
+    o.set_points([(24, src[1] + r1, 36), (24, src[1] + r2, 36)])
+    o.run(nt)
+    s = o.sgt().reshape(2, 6, -1).astype(np.float64)
+    exy1, exy2 = s[0, 3], s[1, 3]
+    assert np.abs(exy1).max() > 10 * np.abs(s[0, 1]).max()     # shear dominates: no P on this axis
+    up = 8
+    t = np.arange(exy1.size)
+    tf = np.linspace(0, exy1.size - 1, (exy1.size - 1) * up + 1)
+    a = np.interp(tf, t, exy1)
+    b = np.interp(tf, t, exy2)
+    xc = np.correlate(b, a, mode="full")
+    lag = (np.argmax(xc) - (a.size - 1)) / up * dt
+    expect = (r2 - r1) * dh / vs
+    assert abs(lag - expect) < 0.03 * expect, (lag, expect)
 
 
 def _reciprocity_pair(nve, cols):
