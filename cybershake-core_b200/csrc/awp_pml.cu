@@ -37,28 +37,24 @@ enum { PS = 0, PN = 1, PW = 2, PE = 3, PB = 4 };
 enum { T_ = 0, H_ = 1 };
 enum { PU, PV, PW_, PXX, PYY, PZZ, PXY, PXZ, PYZ };
 
-/* one cell of one component, as the zone routines see it; pb[plane] is the
- * plane's split array at the cell, its 18 fields n[plane] apart */
+/* one cell of one component, as the zone routines see it */
 struct PmlCell {
     float *u1, *v1, *w1, *xx, *yy, *zz, *xy, *xz, *yz;
     const float *d1, *lam, *mu, *rf, *rh;
-    float *pb[5];
-    int n[5];
+    float *split;
+    const long long *n, *off;
+    long long pidx[5];
     long c, SY, SZ;
     int i, j, k, nx, ny;
     float dt, dth, pht;
 };
 
 #define R(v) ((float)(v))
-#define PML(pl, sp, fd) x.pb[pl][(size_t)((sp) * 9 + (fd)) * x.n[pl]]
-/* the arrays are distinct: restrict lets the compiler keep a loaded
- * neighbour or profile value across the split-array stores */
+#define PML(pl, sp, fd) x.split[x.off[pl] + ((sp) * 9 + (fd)) * x.n[pl] + x.pidx[pl]]
 #define PML_CELL_LOCALS                                                                             \
-    float *__restrict__ u1 = x.u1, *__restrict__ v1 = x.v1, *__restrict__ w1 = x.w1;               \
-    float *__restrict__ xx = x.xx, *__restrict__ yy = x.yy, *__restrict__ zz = x.zz;               \
-    float *__restrict__ xy = x.xy, *__restrict__ xz = x.xz, *__restrict__ yz = x.yz;               \
-    const float *__restrict__ d1 = x.d1, *__restrict__ lam = x.lam, *__restrict__ mu = x.mu;       \
-    const float *__restrict__ rf = x.rf, *__restrict__ rh = x.rh;                                  \
+    float *u1 = x.u1, *v1 = x.v1, *w1 = x.w1, *xx = x.xx, *yy = x.yy, *zz = x.zz;                  \
+    float *xy = x.xy, *xz = x.xz, *yz = x.yz;                                                       \
+    const float *d1 = x.d1, *lam = x.lam, *mu = x.mu, *rf = x.rf, *rh = x.rh;                       \
     const long c = x.c, SX = 1, SY = x.SY, SZ = x.SZ;                                               \
     const int i = x.i, j = x.j, k = x.k, nx = x.nx, ny = x.ny;                                      \
     const float dt = x.dt, dth = x.dth, pht = x.pht;                                                \
@@ -135,9 +131,6 @@ __device__ __forceinline__ void pml_str_cell(int zone, const PmlCell &x)
 }
 
 constexpr int PML_KC = 8;   /* z levels per thread */
-#ifndef AWP_PML_MINB
-#define AWP_PML_MINB 1      /* resident blocks per SM the register budget is set for */
-#endif
 
 /* PART 0: velocities of the boundary zones; PART 1: their stresses.  The
  * bottom launch (LATERAL 0) covers levels 1..nd of every column, the lateral
@@ -146,7 +139,7 @@ constexpr int PML_KC = 8;   /* z levels per thread */
  * Cells are independent within a part (a velocity update reads stresses and
  * its own splits, a stress update velocities and its own splits). */
 template <int PART, int LATERAL>
-__global__ void __launch_bounds__(256, AWP_PML_MINB) k_pml(AwpPmlArgs a)
+__global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
 {
     const AwpGeom &g = a.g;
     int tx, ty;
@@ -176,20 +169,18 @@ __global__ void __launch_bounds__(256, AWP_PML_MINB) k_pml(AwpPmlArgs a)
     x.xx = cp.f[AF_XX]; x.yy = cp.f[AF_YY]; x.zz = cp.f[AF_ZZ];
     x.xy = cp.f[AF_XY]; x.xz = cp.f[AF_XZ]; x.yz = cp.f[AF_YZ];
     x.d1 = a.d1; x.lam = a.lam; x.mu = a.mu; x.rf = a.rf; x.rh = a.rh;
-    float *const split = a.split[q];
-#pragma unroll
-    for (int pl = 0; pl < 5; ++pl) x.n[pl] = (int)a.n[pl];
+    x.split = a.split[q]; x.n = a.n; x.off = a.off;
     x.SY = g.px; x.SZ = g.plane;
     x.i = i; x.j = j; x.nx = g.nx; x.ny = g.ny;
     x.dt = a.dt; x.dth = a.dth; x.pht = a.pht;
     for (int k = k0; k <= k1; ++k) {
         x.k = k;
         x.c = g.idx(i, j, k);
-        x.pb[PS] = split + a.off[PS] + ((long long)(k - 1) * nd + (j - 1)) * g.nx + (i - 1);
-        x.pb[PN] = split + a.off[PN] + ((long long)(k - 1) * nd + (g.ny - j)) * g.nx + (i - 1);
-        x.pb[PW] = split + a.off[PW] + ((long long)(k - 1) * g.ny + (j - 1)) * nd + (i - 1);
-        x.pb[PE] = split + a.off[PE] + ((long long)(k - 1) * g.ny + (j - 1)) * nd + (g.nx - i);
-        x.pb[PB] = split + a.off[PB] + ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
+        x.pidx[PS] = ((long long)(k - 1) * nd + (j - 1)) * g.nx + (i - 1);
+        x.pidx[PN] = ((long long)(k - 1) * nd + (g.ny - j)) * g.nx + (i - 1);
+        x.pidx[PW] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (i - 1);
+        x.pidx[PE] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (g.nx - i);
+        x.pidx[PB] = ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
         const int zone = pml_zone(xs, ys, k <= nd);
         if (PART == 0) pml_vel_cell(zone, x);
         else pml_str_cell(zone, x);
