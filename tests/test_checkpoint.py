@@ -178,3 +178,25 @@ def test_set_field_block_floating_point():
             s.set_field(f, a)
         for f, a in zip(("r1", "r2", "r3", "r4", "r5", "r6"), got):
             assert np.array_equal(s.field(f).view(np.uint32), a.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["staged", "fused"])
+def test_get_plane_equals_the_field_level(kernel):
+    """awp_get_plane returns level k of a wavefield or stress as it stands
+    after the steps done so far: the fused stepper alternates between two
+    buffers, so the level must come from the current one (odd and even step
+    counts); memory variables and out-of-range levels are refused."""
+    with make_solver(kernel, "f32", 2) as s:
+        for steps in (7, 6):
+            s.run(steps)
+            for q in range(2):
+                for f in ("u1", "w1", "zz", "xy"):
+                    full = s.field(f, q)
+                    for k in (1, NZ // 2, NZ):
+                        assert np.array_equal(s.plane(f, k, q).view(np.uint32),
+                                              full[k + 1, 2:NY + 2, 2:NX + 2].view(np.uint32))
+            assert np.abs(s.plane("u1", NZ - 9, 0)).max() > 0
+        for bad in (("r1", 1), ("u1", 0), ("u1", NZ + 1)):
+            with pytest.raises(awpsgt.AwpError):
+                s.plane(*bad)
