@@ -747,8 +747,9 @@ def main():
         "kernels": prof,
     }
     if world == 1 and not args.no_extras and not args.grid:
-        # the plain FP32 two-sweep stepper (the comparison point of the north-star
-        # ratio) and block floating point memory variables on the same window
+        # the plain FP32 two-sweep stepper (the comparison point of the batched
+        # stepper's speed-up), block floating point memory variables and the
+        # contracted stepper on the same window
         warm_ts, timed_ts = args.warmup * per_step_ts, min(args.steps, 10) * per_step_ts
         plain = window_rate(w, media, pts, stfs, local, "f32", "two_sweep", None, prefill, warm_ts, timed_ts)
         line["plain_fp32"] = plain

@@ -246,7 +246,7 @@ awp_status awp_destroy(awp_solver *s);
 /* Asynchronous stepping: enqueues up to `nsteps` steps on the solver's CUDA
  * stream and returns at once.  awp_query returns 1 when all enqueued work has
  * finished (0 otherwise, negative on error); awp_sync waits for it and
- * reports the stability monitor's verdict.  No reference counterpart (the
+ * reports the stability monitor's result.  No reference counterpart (the
  * reference loop is synchronous, AWP-GPU-SGT/src/pmcl3d.c:841-960). */
 awp_status awp_run_async(awp_solver *s, int nsteps);
 int awp_query(awp_solver *s);
