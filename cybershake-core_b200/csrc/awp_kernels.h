@@ -21,12 +21,14 @@ struct AwpPmlArgs {
     long long n[5], off[5];       /* cells of each plane S N W E B, offsets   */
     AwpComp comp[3];              /* wavefields (the two-sweep buffer)        */
     const float *d1, *lam, *mu;   /* FP32 media                               */
-    const int2 *tiles;            /* 32x8 column tiles holding lateral columns */
-    int ntiles;
+    /* the 17 zone boxes (zone, first cell and extent per axis) with their
+     * first block and block count, then the 8 lateral boxes' columns for
+     * the free-surface image (awp_pml_boxes) */
+    struct Box { int zone, i0, ni, j0, nj, k0, nk, b0, nb; } box[17], col[8];
+    int nblk, ncolblk;
 };
-/* tiles (bx, by) of 32 x 8 columns that hold a column within nd of a lateral
- * face; out may be NULL to count them */
-int awp_pml_lateral_tiles(int nx, int ny, int nd, int2 *out);
+/* fills a.box / a.col and the block counts from a.g and a.nd */
+void awp_pml_boxes(AwpPmlArgs &a);
 cudaError_t awp_launch_pml(const AwpPmlArgs &a, int part, cudaStream_t st);
 void awp_pml_profiles(int nd, float arbc, float dh, float vs_min, float vs_max, float *rf, float *rh);
 

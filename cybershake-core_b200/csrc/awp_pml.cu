@@ -14,14 +14,12 @@
  * never read (the PML is elastic and r is a point quantity).
  *
  * The lateral zones (x or y within ND of a face) span the whole depth, under
- * the interior columns only the bottom ND levels are PML.  One thread takes
- * up to eight levels of one (i, j) column: one launch covers the bottom ND
- * levels of every column, a second the levels above of the columns in the
- * tiles that touch a lateral band (a tile list made once per solver), so the
- * thread count follows the PML volume rather than the columns.  The split
- * arrays of a
- * component sit in one device buffer, plane after plane (S N W E B), each
- * plane [split T/H][field][cells of the plane] with the plane's own
+ * the interior columns only the bottom ND levels are PML.  The 17 zones are
+ * boxes of cells; each box gets its own run of thread blocks, one thread per
+ * cell with x fastest, so every warp runs one zone's routine on consecutive
+ * cells and a launch covers the PML volume and nothing else.  The split
+ * arrays of a component sit in one device buffer, plane after plane (S N W E
+ * B), each plane [split T/H][field][cells of the plane] with the plane's own
  * addressing (memory.f:217-300): S, N nx x ND x nz (N counted from the north
  * face), W, E ND x ny x nz (E from the east face), B nx x ny x ND.
  * Compiled without multiply-add contraction: bit-identical to the oracle.
@@ -67,7 +65,7 @@ struct PmlCell {
 
 /* zone of a cell (bound.f:837-893): xs / ys 1 = within ND of the west /
  * south face, 2 = of the east / north face; zs 1 = within ND of the bottom */
-__device__ __forceinline__ int pml_zone(int xs, int ys, int zs)
+__host__ __device__ __forceinline__ int pml_zone(int xs, int ys, int zs)
 {
     if (!zs) {
         if (!xs) return ys == 1 ? 1 : (ys == 2 ? 3 : 18);
@@ -130,39 +128,35 @@ __device__ __forceinline__ void pml_str_cell(int zone, const PmlCell &x)
     }
 }
 
-constexpr int PML_KC = 8;   /* z levels per thread */
+constexpr int PML_BLOCK = 256;
 
-/* PART 0: velocities of the boundary zones; PART 1: their stresses.  The
- * bottom launch (LATERAL 0) covers levels 1..nd of every column, the lateral
- * one levels nd+1..nz of the columns within nd of a lateral face, its blocks
- * taken from the tile list; blockIdx.z = chunk of PML_KC levels x component.
- * Cells are independent within a part (a velocity update reads stresses and
- * its own splits, a stress update velocities and its own splits). */
-template <int PART, int LATERAL>
-__global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
+/* the box a block belongs to: every thread of a block works in one zone, so
+ * the zone dispatch below never diverges within a warp */
+template <int N>
+__device__ __forceinline__ const AwpPmlArgs::Box &pml_box_of(const AwpPmlArgs::Box (&box)[N], int b)
+{
+    int n = 0;
+#pragma unroll
+    for (int z = 1; z < N; ++z)
+        if (b >= box[z].b0) n = z;
+    return box[n];
+}
+
+/* PART 0: velocities of the boundary zones; PART 1: their stresses.  One
+ * thread per cell of a zone box, x fastest, so a warp reads consecutive
+ * cells of each array; blockIdx.y = component.  Cells are independent within
+ * a part (a velocity update reads stresses and its own splits, a stress
+ * update velocities and its own splits). */
+template <int PART>
+__global__ void __launch_bounds__(PML_BLOCK) k_pml(AwpPmlArgs a)
 {
     const AwpGeom &g = a.g;
-    int tx, ty;
-    if (LATERAL) {
-        const int2 t = a.tiles[blockIdx.x];
-        tx = t.x; ty = t.y;
-    } else {
-        tx = blockIdx.x; ty = blockIdx.y;
-    }
-    const int i = tx * 32 + threadIdx.x + 1, j = ty * 8 + threadIdx.y + 1;
-    const int q = blockIdx.z % a.ncomp, kc = blockIdx.z / a.ncomp;
-    if (i > g.nx || j > g.ny) return;
-    const int nd = a.nd;
-    const int xs = i <= nd ? 1 : (i > g.nx - nd ? 2 : 0), ys = j <= nd ? 1 : (j > g.ny - nd ? 2 : 0);
-    int k0, k1;
-    if (LATERAL) {
-        if (!xs && !ys) return;
-        k0 = nd + 1 + kc * PML_KC;
-        k1 = min(g.nz, k0 + PML_KC - 1);
-    } else {
-        k0 = 1 + kc * PML_KC;
-        k1 = min(nd, k0 + PML_KC - 1);
-    }
+    const AwpPmlArgs::Box &bx = pml_box_of(a.box, (int)blockIdx.x);
+    const long long t = (long long)(blockIdx.x - bx.b0) * PML_BLOCK + threadIdx.x;
+    const long long row = t / bx.ni;
+    const int i = bx.i0 + (int)(t - row * bx.ni), j = bx.j0 + (int)(row % bx.nj), k = bx.k0 + (int)(row / bx.nj);
+    if (k >= bx.k0 + bx.nk) return;
+    const int q = blockIdx.y, nd = a.nd;
     const AwpComp &cp = a.comp[q];
     PmlCell x;
     x.u1 = cp.f[AF_U]; x.v1 = cp.f[AF_V]; x.w1 = cp.f[AF_W];
@@ -173,32 +167,28 @@ __global__ void __launch_bounds__(256) k_pml(AwpPmlArgs a)
     x.SY = g.px; x.SZ = g.plane;
     x.i = i; x.j = j; x.nx = g.nx; x.ny = g.ny;
     x.dt = a.dt; x.dth = a.dth; x.pht = a.pht;
-    for (int k = k0; k <= k1; ++k) {
-        x.k = k;
-        x.c = g.idx(i, j, k);
-        x.pidx[PS] = ((long long)(k - 1) * nd + (j - 1)) * g.nx + (i - 1);
-        x.pidx[PN] = ((long long)(k - 1) * nd + (g.ny - j)) * g.nx + (i - 1);
-        x.pidx[PW] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (i - 1);
-        x.pidx[PE] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (g.nx - i);
-        x.pidx[PB] = ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
-        const int zone = pml_zone(xs, ys, k <= nd);
-        if (PART == 0) pml_vel_cell(zone, x);
-        else pml_str_cell(zone, x);
-    }
+    x.k = k;
+    x.c = g.idx(i, j, k);
+    x.pidx[PS] = ((long long)(k - 1) * nd + (j - 1)) * g.nx + (i - 1);
+    x.pidx[PN] = ((long long)(k - 1) * nd + (g.ny - j)) * g.nx + (i - 1);
+    x.pidx[PW] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (i - 1);
+    x.pidx[PE] = ((long long)(k - 1) * g.ny + (j - 1)) * nd + (g.nx - i);
+    x.pidx[PB] = ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
+    if (PART == 0) pml_vel_cell(bx.zone, x);
+    else pml_str_cell(bx.zone, x);
 }
 
 /* after the stress part: the free-surface image of each lateral column
  * (fstr, operator.f:594-606), which the stress sweep wrote from the values
- * the PML has since replaced */
-__global__ void __launch_bounds__(256) k_pml_fstr(AwpPmlArgs a)
+ * the PML has since replaced; one thread per column of the lateral boxes */
+__global__ void __launch_bounds__(PML_BLOCK) k_pml_fstr(AwpPmlArgs a)
 {
     const AwpGeom &g = a.g;
-    const int2 t = a.tiles[blockIdx.x];
-    const int i = t.x * 32 + threadIdx.x + 1, j = t.y * 8 + threadIdx.y + 1, q = blockIdx.z;
-    if (i > g.nx || j > g.ny || q >= a.ncomp) return;
-    const int nd = a.nd;
-    if (i > nd && i <= g.nx - nd && j > nd && j <= g.ny - nd) return;
-    const AwpComp &cp = a.comp[q];
+    const AwpPmlArgs::Box &bx = pml_box_of(a.col, (int)blockIdx.x);
+    const int t = (int)(blockIdx.x - bx.b0) * PML_BLOCK + (int)threadIdx.x;
+    const int i = bx.i0 + t % bx.ni, j = bx.j0 + t / bx.ni;
+    if (j >= bx.j0 + bx.nj) return;
+    const AwpComp &cp = a.comp[blockIdx.y];
     const long sz = g.plane, ct = g.idx(i, j, g.nz);
     float *ZZ = cp.f[AF_ZZ], *XZ = cp.f[AF_XZ], *YZ = cp.f[AF_YZ];
     ZZ[ct + sz] = -ZZ[ct];
@@ -213,34 +203,56 @@ __global__ void __launch_bounds__(256) k_pml_fstr(AwpPmlArgs a)
 
 }  // namespace
 
-int awp_pml_lateral_tiles(int nx, int ny, int nd, int2 *out)
+/* The 17 zones as boxes: x (and y) within nd of the low face, of the high
+ * face, or between; z within nd of the bottom or above.  Each box gets a
+ * contiguous run of blocks, in increasing order (pml_box_of relies on it). */
+void awp_pml_boxes(AwpPmlArgs &a)
 {
-    int n = 0;
-    for (int by = 0; by < (ny + 7) / 8; by++)
-        for (int bx = 0; bx < (nx + 31) / 32; bx++) {
-            const int i0 = bx * 32 + 1, i1 = bx * 32 + 32 < nx ? bx * 32 + 32 : nx;
-            const int j0 = by * 8 + 1, j1 = by * 8 + 8 < ny ? by * 8 + 8 : ny;
-            if (i0 <= nd || i1 > nx - nd || j0 <= nd || j1 > ny - nd) {
-                if (out) out[n] = make_int2(bx, by);
-                n++;
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz, nd = a.nd;
+    const int n3[3] = {nx, ny, nz};
+    auto range = [&](int axis, int side, int &s0, int &n) {   /* side 1 low band, 2 high band, 0 between */
+        const int N = n3[axis];
+        if (axis == 2) { s0 = side ? 1 : nd + 1; n = side ? nd : N - nd; return; }
+        if (side == 1) { s0 = 1; n = nd; }
+        else if (side == 2) { s0 = N - nd + 1; n = nd; }
+        else { s0 = nd + 1; n = N - 2 * nd; }
+    };
+    int nb = 0, nbox = 0, ncol = 0, ncb = 0;
+    for (int zs = 1; zs >= 0; --zs)
+        for (int ys = 0; ys < 3; ++ys)
+            for (int xs = 0; xs < 3; ++xs) {
+                if (!xs && !ys && !zs) continue;
+                AwpPmlArgs::Box b;
+                b.zone = pml_zone(xs, ys, zs);
+                range(0, xs, b.i0, b.ni);
+                range(1, ys, b.j0, b.nj);
+                range(2, zs, b.k0, b.nk);
+                const long long cells = (long long)b.ni * b.nj * b.nk;
+                b.b0 = nb;
+                b.nb = (int)((cells + PML_BLOCK - 1) / PML_BLOCK);
+                nb += b.nb;
+                a.box[nbox++] = b;
+                if (!zs) {                                   /* a lateral box: its columns */
+                    AwpPmlArgs::Box c = b;
+                    c.b0 = ncb;
+                    c.nb = (b.ni * b.nj + PML_BLOCK - 1) / PML_BLOCK;
+                    ncb += c.nb;
+                    a.col[ncol++] = c;
+                }
             }
-        }
-    return n;
+    a.nblk = nb;
+    a.ncolblk = ncb;
 }
 
 cudaError_t awp_launch_pml(const AwpPmlArgs &a, int part, cudaStream_t st)
 {
-    const dim3 b(32, 8);
-    const int nbot = (a.nd + PML_KC - 1) / PML_KC, nlat = (a.g.nz - a.nd + PML_KC - 1) / PML_KC;
-    const dim3 gbot((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, nbot * a.ncomp);
-    const dim3 glat(a.ntiles, 1, nlat * a.ncomp);
+    const dim3 grid(a.nblk, a.ncomp), gcol(a.ncolblk, a.ncomp);
+    if (a.nblk <= 0 || a.ncomp <= 0) return cudaErrorInvalidValue;
     if (part == 0) {
-        k_pml<0, 0><<<gbot, b, 0, st>>>(a);
-        if (a.ntiles > 0 && nlat > 0) k_pml<0, 1><<<glat, b, 0, st>>>(a);
+        k_pml<0><<<grid, PML_BLOCK, 0, st>>>(a);
     } else {
-        k_pml<1, 0><<<gbot, b, 0, st>>>(a);
-        if (a.ntiles > 0 && nlat > 0) k_pml<1, 1><<<glat, b, 0, st>>>(a);
-        if (a.ntiles > 0) k_pml_fstr<<<dim3(a.ntiles, 1, a.ncomp), b, 0, st>>>(a);
+        k_pml<1><<<grid, PML_BLOCK, 0, st>>>(a);
+        if (a.ncolblk > 0) k_pml_fstr<<<gcol, PML_BLOCK, 0, st>>>(a);
     }
     return cudaGetLastError();
 }

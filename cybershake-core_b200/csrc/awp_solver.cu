@@ -105,7 +105,6 @@ struct awp_solver {
     float *pml_split[AWP_MAX_COMP];
     float *pml_prof;                 /* rf[nd + 1] then rh[nd + 1]         */
     int64_t pml_floats;              /* floats of one component's splits   */
-    int2 *pml_tiles;                 /* lateral column tiles (device)      */
     AwpPmlArgs pml_args;
     AwpStaged *staged;               /* their tensor maps (first step)      */
     int ty;                          /* thread-block rows of the steppers   */
@@ -330,7 +329,6 @@ static void free_all(awp_solver *s)
     dfree(s, s->en_partial); dfree(s, s->en_out); dfree(s, s->flag);
     for (int q = 0; q < AWP_MAX_COMP; q++) dfree(s, s->pml_split[q]);
     dfree(s, s->pml_prof);
-    dfree(s, s->pml_tiles);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -660,15 +658,10 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
             pa.comp[q] = s->comp[0][q];
         }
         TRY(dalloc(s, (void **)&s->pml_prof, sizeof(float) * 2 * ((size_t)p->nd + 1)));
-        pa.ntiles = awp_pml_lateral_tiles(p->nx, p->ny, p->nd, NULL);
-        std::vector<int2> tiles((size_t)pa.ntiles + 1);
-        awp_pml_lateral_tiles(p->nx, p->ny, p->nd, tiles.data());
-        TRY(dalloc(s, (void **)&s->pml_tiles, sizeof(int2) * tiles.size()));
-        TRYCU(cudaMemcpy(s->pml_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
-        pa.tiles = s->pml_tiles;
         pa.g = s->g; pa.ncomp = p->ncomp; pa.nd = p->nd;
         pa.dt = p->dt; pa.dth = p->dt / p->dh; pa.pht = p->pht;
         pa.rf = s->pml_prof; pa.rh = s->pml_prof + p->nd + 1;
+        awp_pml_boxes(pa);                             /* from g and nd */
     }
     TRY(dalloc(s, (void **)&s->tau, 16 * sizeof(float)));
     TRY(dalloc(s, (void **)&s->step, sizeof(int)));
