@@ -129,6 +129,12 @@ __device__ __forceinline__ void pml_str_cell(int zone, const PmlCell &x)
 }
 
 constexpr int PML_BLOCK = 256;
+/* Register budgets: the zone kernels wait on global loads, so resident warps
+ * count for more than spills to L1.  Measured per step on 400x400x200 with
+ * three components (velocity + stress part): 1.23 + 2.17 ms at 54 registers
+ * (4 blocks per SM), 1.04 + 1.94 at 48 (5), 0.93 + 1.72 at 40 (6), 0.95 +
+ * 1.68 at 32 (8, more spills). */
+constexpr int PML_MINB_VEL = 6, PML_MINB_STR = 8;
 
 /* the box a block belongs to: every thread of a block works in one zone, so
  * the zone dispatch below never diverges within a warp */
@@ -148,7 +154,7 @@ __device__ __forceinline__ const AwpPmlArgs::Box &pml_box_of(const AwpPmlArgs::B
  * a part (a velocity update reads stresses and its own splits, a stress
  * update velocities and its own splits). */
 template <int PART>
-__global__ void __launch_bounds__(PML_BLOCK) k_pml(AwpPmlArgs a)
+__global__ void __launch_bounds__(PML_BLOCK, PART == 0 ? PML_MINB_VEL : PML_MINB_STR) k_pml(AwpPmlArgs a)
 {
     const AwpGeom &g = a.g;
     const AwpPmlArgs::Box &bx = pml_box_of(a.box, (int)blockIdx.x);
