@@ -269,9 +269,9 @@ def test_reciprocity_elastic_exact():
 
 
 def test_reciprocity_viscoelastic_close():
-    """With attenuation the coarse-grained memory variables (relaxation times
-    alternating with the cell parity) break exact reciprocity: measured 3 %
-    (amplitude, no time shift), the same at half the frequency, so it is the
-    scheme and not discretisation error."""
+    """With attenuation the scheme is not exactly reciprocal: measured 3 %
+    (amplitude, no time shift), the same at half the frequency, so the
+    difference comes from the memory-variable update, not from grid
+    dispersion."""
     for v, g in _reciprocity_pair(1, [(5, 3), (1, 1)]):
         assert rel_l2(v, g) <= 6e-2, rel_l2(v, g)
