@@ -191,9 +191,14 @@ __device__ __forceinline__ bool mb_wait_or_abort(uint64_t *b, uint32_t parity, c
     return false;
 }
 
+/* the ring starts at the first 128-byte boundary of the dynamic shared
+ * memory; the pad is added to the shared pointer itself (no round trip
+ * through an integer), so the compiler keeps knowing the ring is shared
+ * memory and reads its tiles with shared-memory loads, not generic ones */
 __device__ __forceinline__ float *ring_base(unsigned char *raw)
 {
-    return (float *)(((uintptr_t)raw + 127) & ~(uintptr_t)127);
+    const unsigned pad = (unsigned)(-(uintptr_t)raw) & 127u;
+    return (float *)(raw + pad);
 }
 
 template <int S>
