@@ -577,6 +577,14 @@ k_vel_tmab(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<
 #define STR_SLOT (STR_ST + 12 * ST_PT)           /* r tiles fit in 6 x 256   */
 
 /* media of planes k and k-1 at the cell */
+/* the six stresses of a cell, times the sponge factor, to global memory
+ * (the array pointers come from a shared-memory table) */
+__device__ __forceinline__ void gst6(const AwpComp &o, int c, const Stress6 &s, float crj)
+{
+    __stwb(o.f[AF_XX] + c, s.xx * crj); __stwb(o.f[AF_YY] + c, s.yy * crj); __stwb(o.f[AF_ZZ] + c, s.zz * crj);
+    __stwb(o.f[AF_XY] + c, s.xy * crj); __stwb(o.f[AF_XZ] + c, s.xz * crj); __stwb(o.f[AF_YZ] + c, s.yz * crj);
+}
+
 struct TMed {
     const float *p0, *pm; /* media tiles (lam first) of planes k and k-1, at the cell */
     __device__ __forceinline__ float m(int a, int dx, int dy, int dz) const
@@ -730,9 +738,9 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             itxy[r] = ((j & 1) << 1) | (i & 1);
             up1[r] = up2[r] = vp1[r] = vp2[r] = wm2[r] = wp1[r] = cxy[r] = 0.f;
             if (live[r]) {
-                up1[r] = U[c + sz]; up2[r] = U[c + 2 * sz];
-                vp1[r] = V[c + sz]; vp2[r] = V[c + 2 * sz];
-                wm2[r] = W[c - 2 * sz]; wp1[r] = W[c + sz];
+                up1[r] = __ldg(&U[c + sz]); up2[r] = __ldg(&U[c + 2 * sz]);
+                vp1[r] = __ldg(&V[c + sz]); vp2[r] = __ldg(&V[c + 2 * sz]);
+                wm2[r] = __ldg(&W[c - 2 * sz]); wp1[r] = __ldg(&W[c + sz]);
                 cxy[r] = cx[i] * cy[j];
             }
         }
@@ -746,7 +754,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             for (int r = 0; r < RPT; ++r) {
                 const int c = cc + r * CW * sy;
                 up3[r] = vp3[r] = wp2[r] = 0.f;
-                if (live[r] && k < k1) { up3[r] = U[c + 3 * sz]; vp3[r] = V[c + 3 * sz]; wp2[r] = W[c + 2 * sz]; }
+                if (live[r] && k < k1) { up3[r] = __ldg(&U[c + 3 * sz]); vp3[r] = __ldg(&V[c + 3 * sz]); wp2[r] = __ldg(&W[c + 2 * sz]); }
             }
             bool ok = true;
             if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s, wt.ns);
@@ -781,8 +789,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                         o = str_elastic(kc, Vq, s0, dth);
                     }
                     const float crj = cxy[r] * czk;
-                    tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj; tab[q].f[AF_ZZ][c] = o.zz * crj;
-                    tab[q].f[AF_XY][c] = o.xy * crj; tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
+                    gst6(tab[q], c, o, crj);
                 }
                 up1[r] = up2[r]; up2[r] = up3[r];
                 vp1[r] = vp2[r]; vp2[r] = vp3[r];
@@ -934,11 +941,11 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                 wm2[r][q] = wm1[r][q] = um1[r][q] = vm1[r][q] = 0.f;
                 if (live[r]) {
                     const float *U = tab[q].f[AF_U], *V = tab[q].f[AF_V], *W = tab[q].f[AF_W];
-                    up2[r][q] = U[c + sz]; pu[r][q] = U[c + 2 * sz];
-                    vp2[r][q] = V[c + sz]; pv[r][q] = V[c + 2 * sz];
-                    pw[r][q] = W[c + sz];
-                    wm2[r][q] = W[c - 2 * sz]; wm1[r][q] = W[c - sz];
-                    um1[r][q] = U[c - sz]; vm1[r][q] = V[c - sz];
+                    up2[r][q] = __ldg(&U[c + sz]); pu[r][q] = __ldg(&U[c + 2 * sz]);
+                    vp2[r][q] = __ldg(&V[c + sz]); pv[r][q] = __ldg(&V[c + 2 * sz]);
+                    pw[r][q] = __ldg(&W[c + sz]);
+                    wm2[r][q] = __ldg(&W[c - 2 * sz]); wm1[r][q] = __ldg(&W[c - sz]);
+                    um1[r][q] = __ldg(&U[c - sz]); vm1[r][q] = __ldg(&V[c - sz]);
                 }
             }
         }
@@ -977,9 +984,9 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                     wp1[r][q] = pw[r][q];
                     pu[r][q] = pv[r][q] = pw[r][q] = 0.f;
                     if (live[r] && k < k1) {
-                        pu[r][q] = tab[q].f[AF_U][c + 3 * sz];
-                        pv[r][q] = tab[q].f[AF_V][c + 3 * sz];
-                        pw[r][q] = tab[q].f[AF_W][c + 2 * sz];
+                        pu[r][q] = __ldg(&tab[q].f[AF_U][c + 3 * sz]);
+                        pv[r][q] = __ldg(&tab[q].f[AF_V][c + 3 * sz]);
+                        pw[r][q] = __ldg(&tab[q].f[AF_W][c + 2 * sz]);
                     }
                 }
                 ok = mb_wait_or_abort(&cfull[uc % STB_CS], (uc / STB_CS) & 1, &abort_s, wt.ns);
@@ -1010,9 +1017,7 @@ k_str_tmab(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<
                             o = str_elastic(kc[r], Vq, s0, dth);
                         }
                         const float crj = cxy[r] * czk;
-                        tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj;
-                        tab[q].f[AF_ZZ][c] = o.zz * crj; tab[q].f[AF_XY][c] = o.xy * crj;
-                        tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
+                        gst6(tab[q], c, o, crj);
                     }
                     wm2[r][q] = wm1[r][q];
                     um1[r][q] = nu; vm1[r][q] = nv; wm1[r][q] = nw;

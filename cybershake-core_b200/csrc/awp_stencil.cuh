@@ -38,19 +38,23 @@ __device__ __forceinline__ void work_item(const AwpGeom &g, const AwpWork &w, in
 #define C1 (9.0f / 8.0f)
 #define C2 (-(1.0f / 24.0f))
 
+/* Stores go to global memory through __stwb (a global store with the
+ * default write-back policy): some kernels keep their array pointers in a
+ * shared-memory table, and a store through such a pointer would otherwise be
+ * a generic one. */
 template <class T> struct Store;
 template <> struct Store<float> {
     static __device__ __forceinline__ float ld(const float *p, int c, float) { return p[c]; }
-    static __device__ __forceinline__ void st(float *p, int c, float v, float) { p[c] = v; }
+    static __device__ __forceinline__ void st(float *p, int c, float v, float) { __stwb(p + c, v); }
 };
 template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16 *p, int c, float) { return __bfloat162float(p[c]); }
-    static __device__ __forceinline__ void st(__nv_bfloat16 *p, int c, float v, float) { p[c] = __float2bfloat16_rn(v); }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, int c, float v, float) { __stwb(p + c, __float2bfloat16_rn(v)); }
 };
 /* binary16 arrays hold value * 2^e; ld multiplies by inv = 2^-e (exact) */
 template <> struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half *p, int c, float inv) { return __half2float(p[c]) * inv; }
-    static __device__ __forceinline__ void st(__half *p, int c, float v, float scale) { p[c] = __float2half_rn(v * scale); }
+    static __device__ __forceinline__ void st(__half *p, int c, float v, float scale) { __stwb(p + c, __float2half_rn(v * scale)); }
 };
 
 /* 16-bit block floating point of r1..r6 (AWP_STORE_BFP; the rule is stated
@@ -120,8 +124,8 @@ struct RVars<RBfp> {
         const uint32_t e0 = bfp_enc3(r[0], r[1], r[2], m[0], m[1], m[2]);
         const uint32_t e1 = bfp_enc3(r[3], r[4], r[5], m[3], m[4], m[5]);
 #pragma unroll
-        for (int a = 0; a < 6; ++a) ((short *)o.f[AF_R1 + a])[c] = m[a];
-        ((unsigned short *)o.f[AF_RX])[c] = (unsigned short)(e0 | (e1 << 8));
+        for (int a = 0; a < 6; ++a) __stwb((short *)o.f[AF_R1 + a] + c, m[a]);
+        __stwb((unsigned short *)o.f[AF_RX] + c, (unsigned short)(e0 | (e1 << 8)));
     }
 };
 
