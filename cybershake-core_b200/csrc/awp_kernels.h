@@ -58,6 +58,7 @@ struct AwpStepArgs {
     int *kerr;                   /* device error word (AWP_KERR_*)          */
     int sm_limit;                /* persistent grids sized for this many SMs (0 = all) */
     int fma;                     /* staged sweeps compiled with multiply-add contraction */
+    int staged_generic;          /* one-component staged sweeps read their rings with generic loads */
     const AwpPmlArgs *pml;       /* NPC = 1: the PML zones after each sweep (NULL: Cerjan) */
     unsigned long long wait_ns;  /* bound of one barrier wait of the staged sweeps */
     int withhold;                /* test injection, -1 = off: block 0's producer of the

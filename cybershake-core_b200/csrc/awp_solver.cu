@@ -99,6 +99,7 @@ struct awp_solver {
     int staged_rpt;                  /* staged stress sweep rows per thread */
     int staged_rpt_vel;              /* staged velocity sweep rows per thread */
     int staged_batch;                /* staged stress: components in one item */
+    int staged_generic;              /* staged one-component sweeps: generic ring loads */
     int sm_limit;                    /* persistent grids for this many SMs (0 = all) */
     int fma;                         /* staged sweeps with multiply-add contraction */
     /* PML (npc = 1): split arrays per component, damping profiles, kernel arguments */
@@ -715,6 +716,9 @@ extern "C" awp_status awp_create(const awp_params *pin, awp_solver **out)
          * so by default up to 32 GiB of solver state */
         const int batch_default = (double)awp_footprint_bytes(p, 0) <= 32.0 * (double)(1ull << 30) ? 1 : 0;
         s->staged_batch = env_int("AWP_TUNE_BATCH", batch_default) & 3;
+        /* the one-component sweeps read their rings with generic loads above
+         * 32 GiB of state, where that measured faster (awp_staged.cu) */
+        s->staged_generic = env_int("AWP_TUNE_GENERIC", batch_default ? 0 : 1) != 0;
     }
     s->nt_file = nt_file_of(p);
     s->nsamp_written = ((p->nt / p->ntiskp_sgt) / p->write_step) * p->write_step;
@@ -1211,6 +1215,7 @@ static void fill_args(awp_solver *s, int steps, AwpStepArgs &a, AwpPostArgs &pa,
     a.staged_rpt = s->staged_rpt;
     a.staged_rpt_vel = s->staged_rpt_vel;
     a.staged_batch = s->staged_batch;
+    a.staged_generic = s->staged_generic;
     a.sm_limit = s->sm_limit;
     a.fma = s->fma;
     a.pml = s->p.npc == 1 ? &s->pml_args : NULL;

@@ -201,6 +201,20 @@ __device__ __forceinline__ float *ring_base(unsigned char *raw)
     return (float *)(raw + pad);
 }
 
+/* GL: the same address through an integer, so that the compiler reads the
+ * ring with generic loads.  On the 1400 x 1000 x 400 workload (78 GB of
+ * state, one component per work item) the sweeps ran faster that way:
+ * 28.7 against 24.4 Gcell-updates/s on one box, velocity sweep 12.3 against
+ * 14.3 ms and stress sweep 26.1 against 31.6 ms per launch, while on the 6.4
+ * and 14.7 GB workloads shared-memory loads are 5-8 % faster.  The cause is
+ * not known; the solver picks GL above 32 GiB of state (AWP_TUNE_GENERIC). */
+template <bool GL>
+__device__ __forceinline__ float *ring_base_t(unsigned char *raw)
+{
+    if (GL) return (float *)(((uintptr_t)raw + 127) & ~(uintptr_t)127);
+    return ring_base(raw);
+}
+
 template <int S>
 __device__ __forceinline__ void ring_init(uint64_t *full, uint64_t *empty, volatile int *abort, int consumers = ST_CW)
 {
@@ -282,7 +296,7 @@ __device__ __forceinline__ void vel_issue(const CUtensorMap *ms, const CUtensorM
 }
 
 /* work items: (x tile, y tile, z chunk, component); see split_item for the order */
-template <int D, int UNR, int RPT>
+template <int D, int UNR, int RPT, bool GL = false>
 __global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ d1, const float *__restrict__ cx, const float *__restrict__ cy,
@@ -291,7 +305,7 @@ k_vel_tma(const __grid_constant__ AwpStagedVelMaps maps, AwpGeom g, AwpCompSet<A
     constexpr int S = 1 + D;          /* level k in use, D in flight */
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
-    float *ring = ring_base(st_smem);
+    float *ring = ring_base_t<GL>(st_smem);
     uint64_t *full = (uint64_t *)(ring + S * VEL_SLOT), *empty = full + S;
     __shared__ volatile int abort_s;
     ring_init<S>(full, empty, &abort_s, CW);
@@ -672,7 +686,7 @@ __device__ __forceinline__ void str_issue(const AwpStagedStrMaps &maps, int q, i
 /* work items: (x tile, y tile, z chunk, component); see split_item for the order.
  * RPT rows of the tile per consumer thread (ST_Y / RPT consumer warps): with
  * RPT = 2 a thread carries two independent cells per level. */
-template <class TR, int UNR, int RPT>
+template <class TR, int UNR, int RPT, bool GL = false>
 __global__ void __launch_bounds__(32 * (ST_Y / RPT + 1), 3)
 k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<AWP_MAX_COMP> cs, int ncomp, int qslow,
           const float *__restrict__ cx, const float *__restrict__ cy, const float *__restrict__ cz,
@@ -681,7 +695,7 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
     constexpr int S = 2 + STR_D;      /* levels k-1 and k in use, STR_D in flight */
     constexpr int CW = ST_Y / RPT;    /* consumer warps */
     extern __shared__ unsigned char st_smem[];
-    float *ring = ring_base(st_smem);
+    float *ring = ring_base_t<GL>(st_smem);
     uint64_t *full = (uint64_t *)(ring + S * STR_SLOT), *empty = full + S;
     __shared__ volatile int abort_s;
     __shared__ AwpComp tab[AWP_MAX_COMP];
@@ -754,7 +768,10 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
             for (int r = 0; r < RPT; ++r) {
                 const int c = cc + r * CW * sy;
                 up3[r] = vp3[r] = wp2[r] = 0.f;
-                if (live[r] && k < k1) { up3[r] = __ldg(&U[c + 3 * sz]); vp3[r] = __ldg(&V[c + 3 * sz]); wp2[r] = __ldg(&W[c + 2 * sz]); }
+                if (live[r] && k < k1) {
+                    if (GL) { up3[r] = U[c + 3 * sz]; vp3[r] = V[c + 3 * sz]; wp2[r] = W[c + 2 * sz]; }
+                    else { up3[r] = __ldg(&U[c + 3 * sz]); vp3[r] = __ldg(&V[c + 3 * sz]); wp2[r] = __ldg(&W[c + 2 * sz]); }
+                }
             }
             bool ok = true;
             if (k == k0) ok = mb_wait_or_abort(&full[usem % S], (usem / S) & 1, &abort_s, wt.ns);
@@ -789,7 +806,12 @@ k_str_tma(const __grid_constant__ AwpStagedStrMaps maps, AwpGeom g, AwpCompSet<A
                         o = str_elastic(kc, Vq, s0, dth);
                     }
                     const float crj = cxy[r] * czk;
-                    gst6(tab[q], c, o, crj);
+                    if (GL) {
+                        tab[q].f[AF_XX][c] = o.xx * crj; tab[q].f[AF_YY][c] = o.yy * crj; tab[q].f[AF_ZZ][c] = o.zz * crj;
+                        tab[q].f[AF_XY][c] = o.xy * crj; tab[q].f[AF_XZ][c] = o.xz * crj; tab[q].f[AF_YZ][c] = o.yz * crj;
+                    } else {
+                        gst6(tab[q], c, o, crj);
+                    }
                 }
                 up1[r] = up2[r]; up2[r] = up3[r];
                 vp1[r] = vp2[r]; vp2[r] = vp3[r];
@@ -1186,6 +1208,14 @@ static cudaError_t launch_vel_u(const AwpStaged *st, const AwpStepArgs &s, cudaS
     const size_t smem = ring_bytes(1 + ST_VEL_D, VEL_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
+    if (s.staged_generic && UNR == 2) {                 /* generic ring loads (ring_base_t) */
+        cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, 2, 1, true>, smem, w.nitems, &grid, s.sm_limit, 32 * (ST_Y + 1));
+        if (e != cudaSuccess) return e;
+        k_vel_tma<ST_VEL_D, 2, 1, true><<<grid, dim3(32, ST_Y + 1), smem, stream>>>(
+            st->vm, s.g, comp_set3(s), s.ncomp, s.staged_qslow, (const float *)s.md.m[AM_D1], s.cx, s.cy, s.cz, s.dth,
+            w, s.kerr, awp_wait_of(s));
+        return cudaGetLastError();
+    }
     cudaError_t e = staged_grid(k_vel_tma<ST_VEL_D, U, RPT>, smem, w.nitems, &grid, s.sm_limit, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_vel_tma<ST_VEL_D, U, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(
@@ -1201,6 +1231,15 @@ static cudaError_t launch_str_rpt(const AwpStaged *st, const AwpStepArgs &s, cud
     const size_t smem = ring_bytes(2 + STR_D, STR_SLOT);
     const AwpWork w = staged_work(s.g, s.kchunk_staged, s.ncomp);
     int grid = 0;
+    if (s.staged_generic && UNR == 2 && RPT == 1) {     /* generic ring loads (ring_base_t) */
+        cudaError_t e = staged_grid(k_str_tma<TR, 2, 1, true>, smem, w.nitems, &grid, s.sm_limit, 32 * (ST_Y + 1));
+        if (e != cudaSuccess) return e;
+        k_str_tma<TR, 2, 1, true><<<grid, dim3(32, ST_Y + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,
+                                                                            s.staged_qslow, s.cx, s.cy, s.cz, s.tau,
+                                                                            s.dth, s.dt, s.dh1, w, s.nve, s.kerr,
+                                                                            awp_wait_of(s));
+        return cudaGetLastError();
+    }
     cudaError_t e = staged_grid(k_str_tma<TR, UNR, RPT>, smem, w.nitems, &grid, s.sm_limit, 32 * (CW + 1));
     if (e != cudaSuccess) return e;
     k_str_tma<TR, UNR, RPT><<<grid, dim3(32, CW + 1), smem, stream>>>(st->sm, s.g, comp_set3(s), s.ncomp,

@@ -196,3 +196,34 @@ def test_sm_limit_is_bit_exact(kernel):
     with pytest.raises(awpsgt.AwpError):
         s.set_tuning(variant(t0, sm_limit=-1))
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["f32", "mixed"])
+def test_generic_ring_loads_are_bit_exact(monkeypatch, precision):
+    """AWP_TUNE_GENERIC=1 (the default above 32 GiB of state) makes the
+    one-component staged sweeps read their rings with generic loads: same
+    arithmetic, so the same bits as the default sweeps and, in FP32, as the
+    oracle."""
+    c = Case(nx=45, ny=37, nz=29, nt=30, igreen=(1, 2), srcs=[[(20, 18, 6)], [(22, 16, 9)]])
+    runs = []
+    for gen in ("0", "1"):
+        monkeypatch.setenv("AWP_TUNE_GENERIC", gen)
+        p = awpsgt.make_params(c.nx, c.ny, c.nz, c.dh, c.dt, c.nt, igreen=c.igreen, kernel="staged",
+                               precision=precision, **c.kw())
+        s = awpsgt.Solver(p)
+        s.set_tuning(variant(s.tuning(), staged_batch=0, kchunk_staged=11))
+        s.load_media(c.media)
+        for q in range(2):
+            s.set_source(q, c.srcs[q], c.stfs[q])
+        s.set_points(c.pts)
+        s.run(c.nt)
+        runs.append(s)
+    a, b = runs
+    for q in range(2):
+        for f in STATE:
+            assert bits_equal(a.field(f, q), b.field(f, q)), (q, f)
+        assert bits_equal(a.sgt(q), b.sgt(q))
+    if precision == "f32":
+        assert_same_state(b, c.oracle(0), 0)
+    for s in runs:
+        s.close()
