@@ -7,7 +7,7 @@ wavefield does not depend on the points, so these records equal those of the
 full solve), rounded to float32.  The output is too large to commit; pass its
 directory to the study through AWP_PRECISION_REF.
 
-    python tests/golden/make_precision_ref.py --config 3 --points 1000 --out REF [--steps N]
+    python tests/golden/make_precision_ref.py --config 3 --points 1000 --out REF [--steps N] [--components 2]
 """
 import argparse
 import json
@@ -29,6 +29,7 @@ def main():
     ap.add_argument("--points", type=int, default=1000)
     ap.add_argument("--steps", type=int, default=0, help="time steps - 1 (default: the workload's NST)")
     ap.add_argument("--out", required=True)
+    ap.add_argument("--components", default="", help="IGREEN values to make, e.g. 2 (default: all of the workload's)")
     args = ap.parse_args()
     w = ai.config(args.config)
     nst = args.steps or w.nst
@@ -38,7 +39,10 @@ def main():
     media = w.media()
     pts = w.points()[:args.points]
     t0 = time.time()
+    want = [int(c) for c in args.components.split(",")] if args.components else list(w.igreen)
     for q, g in enumerate(w.igreen):
+        if g not in want:
+            continue
         o = oracle.Oracle(nx=w.nx, ny=w.ny, nz=w.nz, dh=w.dh, dt=w.dt, nt=nt, nst=w.nst, nd=20, arbc=0.92, fl=w.fl,
                           fh=w.fh, fp=w.fp, socalq=w.socalq, ntiskp_sgt=w.ntiskp_sgt, write_step=write_step,
                           igreen=g, precision="f64")
